@@ -1,0 +1,357 @@
+"""Benchmark: nonlinear magnetostatic solves per second to a 1e-8 relative Newton residual.
+
+Workload (seeded, synthetic; no dataset): window-frame iron yoke (outer 0.6 x 0.6 m, aperture
+0.3 x 0.2 m, 0.5 m long) in a 1.0 x 1.0 x 1.2 m air box, two racetrack filament coils around
+the vertical legs at J = 3 A/mm^2, iron reluctivity from the atan B(H) law (mu_r 3000,
+Js 1.9 T) as a 40-knot PCHIP, first-order Nedelec tetrahedra (~1.2M tets), 4-point rule,
+n x A = 0 on the box, reduced vector potential formulation.  One step = one full Newton
+solve from A = 0 until ||F_free|| <= 1e-8 ||F_free(0)|| (F = K(A) A - rhs(A)).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): every rank solves its own copy (independent replicas, weak scaling);
+the only communication is the timing barrier and a max over ranks.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Nonlinear solves/s to 1e-8 residual @1.2M tets: plain FP64 vs mixed+warm-start"
+UNIT = "solves/s"
+RTOL = 1e-8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--tets", type=int, default=1_200_000)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(tets):
+    from snoopy_b200 import materials as MAT
+    from snoopy_b200 import mesh as M
+
+    msh = M.window_frame_mesh(tets, jitter=0.15, seed=7)
+    return msh, msh.geometry.coils(), MAT.atan_reluctance()
+
+
+# ---------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) of SM clock, power and throttle reasons."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = np.array([float(r[1]) for r in rows])
+        mx = float(rows[0][2])
+        power = np.array([float(r[3]) for r in rows if r[3] not in ("[N/A]", "")] or [0.0])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        load = sm[sm > 0.5 * mx] if (sm > 0.5 * mx).any() else sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows),
+                "power_w_max": float(power.max())}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------- our arm
+
+def bytes_pcg_iteration(nnz, n):
+    """Algorithmic bytes of one Jacobi-PCG iteration on a CSR (float64 values, int32 indices):
+    SpMV nnz*(8+4) + (n+1)*4 + 2n*8 (p read, q write) plus 9n*8 of fused vector streams."""
+    return nnz * 12 + (n + 1) * 4 + 2 * n * 8 + 9 * n * 8
+
+
+def bytes_spmv(nnz, n):
+    return nnz * 12 + (n + 1) * 4 + 2 * n * 8
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    import snoopy_b200 as S
+    from snoopy_b200 import _lib
+    from snoopy_b200 import mesh as M
+    from snoopy_b200.device import upload, zeros
+
+    t_setup = time.perf_counter()
+    msh, coils, rel = workload(args.tets)
+    solver = S.RedMVPSolver(msh, coils, [M.TAG_IRON], [M.TAG_AIR], [rel], max_newton_iterations=60, quad_order=2)
+    solver.verbose = False
+    eng = solver.newton_engine()
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t_setup
+    prec = {"fp64": 0, "mixed": 1}[args.precision]
+    n = msh.num_dofs
+    nnz = eng.pattern.nnz
+    x = zeros(n)[:n]
+
+    def one_solve():
+        return eng.solve(None, mode=1, tol=RTOL, max_newton=60, precision=prec, x_out=x)[1]
+
+    for _ in range(args.warmup):
+        one_solve()
+    clocks = ClockSampler(local)
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0.record(stream)
+    stats = [one_solve() for _ in range(args.steps)]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # dominant kernel: the PCG iteration (k_spmv with p.q, k_update, k_pupdate), timed by
+    # the solver's CUDA events around every Krylov solve of the timed region
+    cg_its = sum(s["cg_iterations"] for s in stats)
+    t_kry = sum(s["t_krylov_ms"] for s in stats)
+    t_asm = sum(s["t_assemble_ms"] for s in stats)
+    newton = sum(s["newton_iterations"] for s in stats)
+    peak, peak_kind = measured_peaks()
+    it_ms = t_kry / max(cg_its, 1)
+    b_it = bytes_pcg_iteration(nnz, n)
+    achieved = b_it / (it_ms / 1e3) / 1e9
+    # SpMV alone on the final Jacobian, CUDA events over 50 back-to-back launches
+    J = eng.assemble(x, J=True, F=False)["J"]
+    pat = eng.pattern
+    fm = eng.free_mask
+    y = zeros(n)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        _lib.call("snp_spmv", n, _lib.ptr(pat.row_ptr), _lib.ptr(pat.col_idx), _lib.ptr(J), _lib.ptr(fm), _lib.ptr(x),
+                  _lib.ptr(y), _lib.stream_ptr())
+    e0.record(stream)
+    for _ in range(50):
+        _lib.call("snp_spmv", n, _lib.ptr(pat.row_ptr), _lib.ptr(pat.col_idx), _lib.ptr(J), _lib.ptr(fm), _lib.ptr(x),
+                  _lib.ptr(y), _lib.stream_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = e0.elapsed_time(e1) / 50
+    spmv_gbs = bytes_spmv(nnz, n) / (spmv_ms / 1e3) / 1e9
+
+    # end to end through the public API: host x0 (pinned) in, host solution out
+    x0_host = torch.zeros(n, dtype=torch.float64).pin_memory()
+    e2e_times = []
+    for _ in range(max(args.e2e_steps, 1)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xs, _st = solver.solve_to_residual(RTOL, x_0=x0_host, precision=args.precision, max_newton=60)
+        t1 = time.perf_counter()
+        e2e_times.append(t1 - t0)
+    e2e_s = float(np.median(e2e_times))
+    tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = world / float(tt.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(msh, coils, rel, newton / args.steps, cg_its / args.steps, solver)
+
+    launches = int(sum(s.get("kernel_launches", 0) for s in stats)) or None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded window-frame yoke mesh and coils, no dataset)",
+        "config": {"workload": f"reduced-MVP Newton solve to rel. residual 1e-8, window-frame yoke, "
+                               f"{msh.num_elements} tets / {n} edge DoFs, Q=4, {args.precision}",
+                   "tets": msh.num_elements, "dofs": n, "nnz": nnz, "precision": args.precision,
+                   "newton_per_solve": newton / args.steps, "cg_per_solve": cg_its / args.steps,
+                   "assembly_ms_per_solve": t_asm / args.steps, "krylov_ms_per_solve": t_kry / args.steps,
+                   "setup_s": t_setup, "l2": "matrix values+indices > 126 MB L2 (no flush needed)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"kernel": "pcg_iteration (k_spmv+dot, k_update, k_pupdate)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "bytes_per_launch": b_it, "launch_ms": it_ms, "traffic": None,
+                     "spmv_alone": {"achieved": spmv_gbs, "frac": spmv_gbs / peak, "ms": spmv_ms,
+                                    "bytes": bytes_spmv(nnz, n)}},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------- CPU reference
+
+def reference_sample(msh, coils, rel, newton_per_solve, cg_per_solve, n_cg_sample=10, quad_order=2):
+    """Time the reference's CPU path on the full workload and project one solve.
+
+    Times one Newton-step assembly through the reference's own C kernels (oracle/_ref,
+    compute_K_dK_Hcurl[_red] via the Cython layer's marshalling) with scipy's COO->CSR, the
+    per-material ``K +=`` adds, ``dK + K``, the Dirichlet fancy-indexing and the Jacobi
+    preconditioner, then ``n_cg_sample`` iterations of scipy's cg on that system.  A solve is
+    (Newton steps + 1) assemblies plus the solve's CG iterations.
+    """
+    import oracle as O
+    from scipy.sparse import diags
+    from scipy.sparse.linalg import cg
+
+    import snoopy_b200 as S
+    from snoopy_b200 import finite_element as FE
+    from snoopy_b200 import mesh as M
+
+    backend = "ref" if O.ref_available() else "oracle"
+    w, q = FE.quadrature_rule(quad_order)
+    dphi = FE.evaluate_basis_derivative(q)
+    phi = FE.evaluate_basis(q)
+    curls, _ = FE.curl_edge_basis_functions(q)
+    iron = msh.domain_elements(M.TAG_IRON)
+    air = msh.domain_elements(M.TAG_AIR)
+    mats = [dict(cells=msh.cells[iron], glob_ids=msh.elem_edges[iron], orientations=msh.orientations[iron],
+                 reluctance=rel),
+            dict(cells=msh.cells[air], glob_ids=msh.elem_edges[air], orientations=msh.orientations[air],
+                 reluctance=S.ConstantReluctance(0.25 / np.pi * 1e7))]
+    t0 = time.perf_counter()
+    P = np.einsum("qi,eid->eqd", phi, msh.nodes[msh.cells[iron]]).reshape(-1, 3)
+    Bs = sum(O.compute_B_line_segs_cpp(c.get_segments(), P, c.current, c.rad, backend=backend) for c in coils)
+    t_src = time.perf_counter() - t0
+    A = O.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, w, q, dphi, curls, backend=backend)
+    mask = np.ones(msh.num_dofs, bool)
+    mask[msh.get_edge_boundary_dofs() - 1] = False
+    x = np.random.default_rng(0).normal(0.0, 1e-3, msh.num_dofs)
+    x[~mask] = 0.0
+    t0 = time.perf_counter()
+    K, J, rhs = A.compute_stiffness_and_jacobi_matrix_c(x, [Bs, np.zeros((0, 3))])
+    F = K @ x - rhs
+    J_c = J[mask, :][:, mask]
+    M_ = diags(1.0 / J_c.diagonal(), shape=J_c.shape)
+    t_asm = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cg(J_c, -F[mask], rtol=1e-30, atol=0.0, M=M_, maxiter=n_cg_sample)
+    t_it = (time.perf_counter() - t0) / n_cg_sample
+    t_solve = t_src + (newton_per_solve + 1) * t_asm + cg_per_solve * t_it
+    return {"value": 1.0 / t_solve, "unit": UNIT, "cores": 1, "kind": "reference" if backend == "ref" else "port",
+            "sample": (f"1 full Newton assembly ({t_asm:.2f} s: reference C kernels + scipy COO->CSR, sparse adds, "
+                       f"masking) and {n_cg_sample} scipy Jacobi-CG iterations ({t_it * 1e3:.1f} ms each) on the "
+                       f"{msh.num_elements}-tet system; solve projected as source field + "
+                       f"{newton_per_solve:.1f}+1 assemblies + {cg_per_solve:.0f} CG iterations"),
+            "t_assembly_s": t_asm, "t_cg_iteration_s": t_it, "t_source_s": t_src, "t_solve_projected_s": t_solve}
+
+
+def cpu_baseline_sample(msh, coils, rel, newton_per_solve, cg_per_solve, solver):
+    try:
+        return reference_sample(msh, coils, rel, newton_per_solve, cg_per_solve)
+    except Exception as exc:  # the baseline must not take the GPU line down
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {exc}"}
+
+
+# Newton steps and CG iterations per solve of this workload, measured with the CPU oracle
+# (oracle.newton_residual with forcing="ew", the device solver's algorithm) on the 1.16M-tet
+# mesh; the reference arm projects its per-iteration times with these counts.
+REFERENCE_COUNTS = {"newton": 26.0, "cg": 3500.0}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    msh, coils, rel = workload(args.tets)
+    vals = []
+    sample = None
+    for _ in range(args.warmup + args.steps):
+        sample = reference_sample(msh, coils, rel, REFERENCE_COUNTS["newton"], REFERENCE_COUNTS["cg"])
+        vals.append(sample["value"])
+    timed = vals[args.warmup:]
+    value = float(np.median(timed))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"reduced-MVP Newton solve to rel. residual 1e-8, window-frame yoke, "
+                                   f"{msh.num_elements} tets / {msh.num_dofs} edge DoFs, Q=4, fp64",
+                       "counts_per_solve": REFERENCE_COUNTS},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": sample["cores"], "kind": sample["kind"],
+                             "sample": sample["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

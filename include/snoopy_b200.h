@@ -1,0 +1,244 @@
+/*
+ * snoopy_b200: sm_100a kernels for snoo.py's nonlinear magnetostatic path, behind a
+ * plain C ABI (load with ctypes / cffi / dlopen).
+ *
+ * Conventions
+ *   - Every pointer argument is a DEVICE pointer unless its comment says "host".
+ *   - Indices are 0-based int32 (the reference subtracts gmsh's 1 before calling C,
+ *     snoopy/curl_curl_assembler.py:916-917).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  Calls
+ *     are asynchronous on it unless their comment says they synchronise.
+ *   - Every function returns an snp_status; snp_last_error() gives the message of the
+ *     calling thread's last failure.  The reference's C returns void and prints
+ *     (fem_c/ctools.c:428, fem_c/interface_c.pyx:71,234,952-959).
+ *   - Assembly entry points ACCUMULATE (+=) into their outputs, like the reference's
+ *     `K += this_K` per material (snoopy/curl_curl_assembler.py:928-930): zero first.
+ *
+ * Table layouts are the reference C kernels' (fem_c/ctools.c):
+ *   nodes[N][3]; cells[E][4]; glob_ids[E][6]; orientations[E];
+ *   d_phi[Q][4][3]; curls[n_orient][Q][6][3]; w[Q]; phi[Q][4].
+ * Materials:
+ *   reluctance  (fem_c/ctools.h:56-63, interface_c.pyx:226-234):
+ *       n_int == -1 -> constant nu = rel_c[0]; else PCHIP in PP form,
+ *       rel_c[4][n_int] row-major, rel_x[n_int+1].
+ *   permeability (fem_c/ctools.h:44-54, interface_c.pyx:56-68):
+ *       type 0 -> mu = mu_H_min; type 1 -> cubic (degree k) B-spline in log10|H| with
+ *       knots t[n_ctrl+k+1], coefficients c[n_ctrl], constant mu_H_min below H_min.
+ */
+#ifndef SNOOPY_B200_H
+#define SNOOPY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SNP_OK = 0,
+    SNP_BAD_ARG = 1,
+    SNP_CUDA_ERROR = 2,
+    SNP_NOT_CONVERGED = 3,
+    SNP_NAN_DETECTED = 4,
+    SNP_ZERO_PIVOT = 5,
+    SNP_NO_MEMORY = 6
+} snp_status;
+
+/* Message of the calling thread's last failure ("" if none). */
+const char *snp_last_error(void);
+
+/* ABI version of this library. */
+int snp_version(void);
+
+/* ------------------------------------------------------------------ CSR pattern
+ * Replaces the COO->CSR conversion of fem_c/interface_c.pyx:154-155,367-368
+ * (csr_array((vals,(i,j))): duplicates summed, sorted column indices).  The pattern of
+ * an element -> DoF connectivity holds row_ptr/col_idx and the slot map
+ * slot[e][a][b] = position of (elem_dofs[e][a], elem_dofs[e][b]) in the CSR arrays, so
+ * assembly scatters element values straight into CSR values. */
+typedef struct snp_pattern snp_pattern;
+
+/* elem_dofs[n_elems][dofs_per_elem] (device).  dofs_per_elem is 6 (edge elements) or 4
+ * (nodal P1).  Synchronises `stream` (the nnz is read back). */
+int snp_pattern_create(const int32_t *elem_dofs, int64_t n_elems, int32_t dofs_per_elem, int32_t n_rows,
+                       void *stream, snp_pattern **out);
+/* Host outputs: rows, nnz, elements, dofs per element. */
+int snp_pattern_info(const snp_pattern *pat, int32_t *n_rows, int64_t *nnz, int64_t *n_elems, int32_t *dofs_per_elem);
+/* Device arrays owned by the pattern: row_ptr[n_rows+1], col_idx[nnz], slots[n_elems*dpe*dpe]. */
+int snp_pattern_arrays(const snp_pattern *pat, const int32_t **row_ptr, const int32_t **col_idx, const int32_t **slots);
+/* Position of each row's diagonal entry, diag_pos[n_rows] (-1 if absent). */
+int snp_pattern_diag(const snp_pattern *pat, const int32_t **diag_pos);
+int snp_pattern_destroy(snp_pattern *pat);
+
+/* ------------------------------------------------------------------ curl-curl assembly
+ * Replaces fem_c.compute_stiffness_and_jacobi_matrix_curl_curl (fem_c/interface_c.pyx:162-374)
+ * -> compute_K_dK_Hcurl (fem_c/ctools.c:960-1193) when B_s == NULL and
+ * compute_K_dK_Hcurl_red (fem_c/ctools.c:1195-1388) otherwise.
+ *
+ * One material's elements, which are elements [elem_offset, elem_offset + n_elems) of
+ * `pat`.  First-order tetrahedra with quadrature-independent tables (affine elements).
+ * Outputs (each may be NULL), accumulated:
+ *   K_vals[nnz]   stiffness values K(x)             (reference K)
+ *   dK_vals[nnz]  Newton correction dK(x)           (reference dK)
+ *   J_vals[nnz]   Jacobian K + dK                   (reference dK + K)
+ *   rhs[n]        reduced rhs sum (nu0 - nu) curl w.B_s w (reduced kernel only)
+ *   F[n]          residual K(x) x - rhs(x)
+ * B_s[n_elems][Q][3] or NULL.  x[n] the DoF vector. */
+int snp_curlcurl_assemble(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems,
+                          const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                          const int32_t *orientations, const double *curls, int32_t n_orient,
+                          const double *d_phi, const double *w, int32_t n_quad,
+                          const double *x, const double *B_s,
+                          int32_t n_int, const double *rel_c, const double *rel_x,
+                          double *K_vals, double *dK_vals, double *J_vals, double *rhs, double *F,
+                          void *stream);
+
+/* Same element arithmetic (float64) accumulating float32 Jacobian values K + dK
+ * (mixed-precision Newton: the Krylov solve runs on these, the residual F stays float64
+ * through snp_curlcurl_assemble with only F requested).  Same source as
+ * snp_curlcurl_assemble (fem_c/ctools.c:960-1388). */
+int snp_curlcurl_assemble_f32(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems,
+                              const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                              const int32_t *orientations, const double *curls, int32_t n_orient,
+                              const double *d_phi, const double *w, int32_t n_quad,
+                              const double *x, const double *B_s,
+                              int32_t n_int, const double *rel_c, const double *rel_x,
+                              float *J_vals, void *stream);
+
+/* Reduced rhs only.  Replaces fem_c.compute_rhs_Hcurl_red_c (fem_c/interface_c.pyx:377-552)
+ * -> compute_rhs_Hcurl_red (fem_c/ctools.c:1390-1497).  Accumulates into rhs[n]. */
+int snp_curlcurl_rhs_red(int64_t n_elems, const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                         const int32_t *orientations, const double *curls, int32_t n_orient,
+                         const double *d_phi, const double *w, int32_t n_quad, const double *x,
+                         const double *B_s, int32_t n_int, const double *rel_c, const double *rel_x,
+                         double *rhs, void *stream);
+
+/* ------------------------------------------------------------------ grad-grad assembly
+ * Replaces fem_c.compute_stiffness_and_jacobi_matrix (fem_c/interface_c.pyx:11-160)
+ * -> compute_K_dK (fem_c/ctools.c:730-919).  P1 nodal elements [elem_offset, +n_elems)
+ * of a pattern built with dofs_per_elem = 4 over `cells`.  Outputs may be NULL, accumulated:
+ * K_vals, dK_vals, J_vals = K + dK (all [nnz]). */
+int snp_gradgrad_assemble(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems,
+                          const double *nodes, const int32_t *cells, const double *d_phi,
+                          const double *w, int32_t n_quad, const double *x,
+                          int32_t perm_type, int32_t degree, int32_t n_ctrl, const double *knots,
+                          const double *ctrl, double H_min, double mu_H_min,
+                          double *K_vals, double *dK_vals, double *J_vals, void *stream);
+
+/* ------------------------------------------------------------------ fields
+ * B at quadrature points.  Replaces fem_c.compute_B_Hcurl (fem_c/interface_c.pyx:555-696)
+ * -> compute_B_Hcurl (fem_c/ctools.c:1500-1563).  points[E][Q][3], B[E][Q][3]. */
+int snp_b_hcurl(int64_t n_elems, const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                const int32_t *orientations, const double *curls, int32_t n_orient, const double *phi,
+                const double *d_phi, int32_t n_quad, const double *x, double *points, double *B,
+                void *stream);
+
+/* Physical quadrature points only, points[E][Q][3] (snoopy/curl_curl_assembler.py:1521-1593). */
+int snp_quad_points(int64_t n_elems, const double *nodes, const int32_t *cells, const double *phi,
+                    int32_t n_quad, double *points, void *stream);
+
+/* B of one element-constant curl at arbitrary points: B[i] = curl of x in element elem[i]
+ * (first-order elements; elem[i] < 0 gives 0).  Probe evaluation
+ * (snoopy/evaluators.py:155-295 locates points with gmsh; here the caller passes elem). */
+int snp_b_at_elements(int64_t n_points, const int32_t *elem, const double *nodes, const int32_t *cells,
+                      const int32_t *glob_ids, const int32_t *orientations, const double *curls,
+                      int32_t n_orient, const double *d_phi, int32_t n_quad, const double *x, double *B,
+                      void *stream);
+
+/* Source rhs of the total-potential formulation from a nodal electric potential x_p[N]:
+ * rhs[g_k] += sum_q (J^-T w_hat_k) . (J^-T grad_hat phi) w_q det, with the edge basis
+ * functions basis[n_orient][Q][6][3] (not their curls).  Replaces the pure-Python
+ * CurlCurlAssembler.compute_rhs_electric_potential (snoopy/curl_curl_assembler.py:1154-1284).
+ * Accumulates into rhs[n]. */
+int snp_rhs_grad_potential(int64_t n_elems, const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                           const int32_t *orientations, const double *basis, int32_t n_orient, const double *d_phi,
+                           const double *w, int32_t n_quad, const double *x_p, double *rhs, void *stream);
+
+/* Biot-Savart of straight filament segments.  Replaces fem_c.compute_B_line_segs_cpp
+ * (fem_c/interface_c.pyx:928-991) -> compute_B_line_segs (fem_c/ctools.c:1761-1923).
+ * src[S][6], tar[T][3], B[T][3] (overwritten). */
+int snp_biot_savart(const double *src, int64_t n_src, const double *tar, int64_t n_tar, double current,
+                    double radius, double *B, void *stream);
+
+/* ------------------------------------------------------------------ sparse linear algebra
+ * y = A x on the rows/cols with free[i] != 0 (free == NULL: all).  Rows with free[i] == 0
+ * give y[i] = 0, and their columns are skipped.  (scipy `J @ x`, `J[mask,:][:,mask]`,
+ * snoopy/red_mvp_solver.py:186,195-196.) */
+int snp_spmv(int32_t n_rows, const int32_t *row_ptr, const int32_t *col_idx, const double *vals,
+             const uint8_t *free_mask, const double *x, double *y, void *stream);
+
+/* Jacobi-preconditioned CG on A restricted to the free DoFs, with scipy.sparse.linalg.cg's
+ * stopping rule ||r|| < max(atol, rtol ||b_free||) (snoopy/red_mvp_solver.py:199-203).
+ * x: in = initial guess (free entries), out = solution (non-free entries set to 0).
+ * maxiter < 0: 10 * n_free like scipy.  Host outputs: iterations, final ||r||.
+ * Synchronises `stream`.  Returns SNP_NOT_CONVERGED when maxiter is reached (x is the
+ * last iterate) and SNP_NAN_DETECTED on a non-finite residual. */
+int snp_pcg(int32_t n_rows, const int32_t *row_ptr, const int32_t *col_idx, const double *vals,
+            const uint8_t *free_mask, const double *b, double *x, double rtol, double atol,
+            int64_t maxiter, int64_t *iterations, double *res_norm, void *stream);
+
+/* ------------------------------------------------------------------ Newton solver
+ * Persistent device problem for the Newton loops of RedMVPSolver.solve
+ * (snoopy/red_mvp_solver.py:121-224) and MVPSolver.solve_nonlin (snoopy/mvp_solver.py:222-334):
+ * owns the concatenated element lists, the CSR pattern and slot map, the Dirichlet mask,
+ * the source fields and all work vectors. */
+typedef struct snp_solver snp_solver;
+
+/* Tables are shared by all materials; free_mask[n_dofs] (device) marks non-Dirichlet DoFs.
+ * Everything is copied into the solver. */
+int snp_solver_create(int32_t n_dofs, const double *nodes, int64_t n_nodes, const double *curls,
+                      int32_t n_orient, const double *d_phi, const double *w, int32_t n_quad,
+                      const uint8_t *free_mask, void *stream, snp_solver **out);
+
+/* Append one material (the reference's per-volume-tag loop).  B_s[n_elems][Q][3] or NULL. */
+int snp_solver_add_material(snp_solver *s, const int32_t *cells, const int32_t *glob_ids,
+                            const int32_t *orientations, int64_t n_elems, int32_t n_int,
+                            const double *rel_c, const double *rel_x, const double *B_s);
+
+/* Extra constant rhs added to every residual (MVPSolver's coil source rhs_mvp), or NULL. */
+int snp_solver_set_rhs(snp_solver *s, const double *rhs);
+
+/* Build the CSR pattern over all materials.  Synchronises. */
+int snp_solver_finalize(snp_solver *s);
+
+/* Solve options (host struct). */
+typedef struct {
+    int32_t mode;            /* 0: the reference's increment test and CG(atol=tol, rtol=1e-5);
+                                1: relative Newton residual ||F_free|| <= tol ||F_free(x0)|| */
+    double tol;              /* mode 0: increment tolerance (reference default 1e-4); mode 1: residual rtol */
+    int64_t cg_maxiter;      /* < 0: 10 * n_free (scipy default) */
+    int32_t max_newton;      /* reference default 25 */
+    double cg_rtol;          /* mode 0: scipy default 1e-5; mode 1: cap of the adaptive forcing term */
+    int32_t precision;       /* 0: float64 throughout; 1: float32 Jacobian + Krylov inside float64 Newton */
+    int32_t verbose;         /* print one line per Newton step to stdout */
+} snp_solve_opts;
+
+/* Solve statistics (host struct). */
+typedef struct {
+    int32_t newton_iterations;
+    int64_t cg_iterations;       /* total */
+    double res0;                 /* ||F_free(x0)|| */
+    double res;                  /* ||F_free(x_final)|| (mode 1; mode 0: at the last assembly) */
+    double t_assemble_ms, t_krylov_ms, t_total_ms;
+    int32_t status;
+    int64_t kernel_launches;     /* this library's kernels launched by the solve (graph nodes counted per execution) */
+} snp_solve_stats;
+
+/* x[n_dofs] (device): in = initial guess, out = solution.  Synchronises. */
+int snp_solver_solve(snp_solver *s, double *x, const snp_solve_opts *opts, snp_solve_stats *stats);
+
+/* Assemble at x into the solver's pattern and copy out (each may be NULL):
+ * K_vals/J_vals [nnz], rhs/F [n].  Uses the solver's materials and source fields. */
+int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *J_vals, double *rhs,
+                        double *F, void *stream);
+
+/* The solver's CSR pattern (owned by the solver). */
+int snp_solver_pattern(const snp_solver *s, const snp_pattern **pat);
+
+int snp_solver_destroy(snp_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SNOOPY_B200_H */

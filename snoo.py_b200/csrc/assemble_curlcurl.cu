@@ -1,0 +1,466 @@
+// Newton assembly of the curl-curl operator on first-order Nedelec tetrahedra.
+//
+// Element arithmetic of the reference kernels compute_K_dK_Hcurl (fem_c/ctools.c:960-1193)
+// and compute_K_dK_Hcurl_red (fem_c/ctools.c:1195-1388), one thread per element, fused
+// with the scatter into a fixed CSR pattern and with the residual F = K(x) x - rhs(x):
+//
+//   Jm        = sum_i X_i (x) dphi_i                     (ctools.c:373-413)
+//   c_j       = Jm curl_hat_j(orientation)               (physical curl = c_j / det)
+//   B_q       = B_s,q + sum_j c_j x_j / det              (ctools.c:922-958)
+//   nu_q, nu'_q = PCHIP(|B_q|)                           (ctools.c:130-204)
+//   K_jk      = sum_q nu_q w_q (c_j . c_k) / det
+//   dK_jk     = sum_q [|B_q| >= 1e-14] nu'_q w_q (c_j . B_q)(c_k . B_q) / (det |B_q|)
+//   rhs_j     = sum_q (nu0 - nu_q) (c_j . B_s,q) w_q     (reduced kernel, ctools.c:1332-1335)
+//
+// For first-order tetrahedra d_phi and the curls do not depend on the quadrature point,
+// so Jm, det and c_j are computed once per element and the sums over q factor:
+// K_jk = (c_j . c_k) * sum_q nu_q w_q / det.  Without a source field B is constant over
+// the element and nu, nu' are evaluated once.  Values agree with the reference's
+// per-point sums to rounding.
+//
+// Data per element: cells 16 B, glob_ids 24 B, orientation 4 B, slot map 144 B, plus
+// gathered coordinates and x (mostly cache hits for a locality-ordered mesh).
+#include "snp_common.cuh"
+#include "snp_internal.cuh"
+
+namespace snp {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+struct SmemLayout {
+    int off_ctab, off_dphi, off_w, off_relc, off_relx, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int n_orient, int nq, int n_int) {
+    SmemLayout L;
+    int o = 0;
+    L.off_ctab = o;
+    o += n_orient * 18;
+    L.off_dphi = o;
+    o += 12;
+    L.off_w = o;
+    o += nq;
+    int nc = n_int < 0 ? 1 : 4 * n_int;
+    int nx = n_int < 0 ? 1 : n_int + 1;
+    L.off_relc = o;
+    o += nc;
+    L.off_relx = o;
+    o += nx;
+    L.total = o;
+    return L;
+}
+
+template <typename T>
+__device__ __forceinline__ void red_add(T *p, T v) {
+    atomicAdd(p, v);
+}
+
+// HAS_BS: reduced formulation with a source field at each quadrature point.
+// NQ: compile-time number of quadrature points (0 = runtime count).
+template <bool HAS_BS, int NQ, typename VT>
+__global__ void __launch_bounds__(kBlock)
+    k_curlcurl(CurlArgs a, int quad_stride_ctab) {
+    extern __shared__ double sm[];
+    const SmemLayout L = smem_layout(a.n_orient, a.nq, a.n_int);
+    double *s_ctab = sm + L.off_ctab;
+    double *s_dphi = sm + L.off_dphi;
+    double *s_w = sm + L.off_w;
+    double *s_relc = sm + L.off_relc;
+    double *s_relx = sm + L.off_relx;
+    // stage tables: curls at q = 0 for every orientation, d_phi at q = 0, weights, PCHIP
+    for (int t = threadIdx.x; t < a.n_orient * 18; t += blockDim.x) {
+        int o = t / 18, r = t - o * 18;
+        s_ctab[t] = a.ctab[(int64_t)o * quad_stride_ctab + r];
+    }
+    for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = a.dphi0[t];
+    for (int t = threadIdx.x; t < a.nq; t += blockDim.x) s_w[t] = a.w[t];
+    const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
+    const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
+    for (int t = threadIdx.x; t < nx; t += blockDim.x) s_relx[t] = (a.n_int < 0) ? 0.0 : a.rel_x[t];
+    __syncthreads();
+
+    const int nq = NQ > 0 ? NQ : a.nq;
+    double wsum = 0.0;
+    for (int q = 0; q < nq; ++q) wsum += s_w[q];
+
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x) {
+        const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
+        const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
+        // Jacobian J[k][l] = sum_i X[i][k] dphi[i][l]
+        double Jm[9];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) Jm[r] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const double X0 = __ldg(a.nodes + 3 * (int64_t)cidx[i]);
+            const double X1 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 1);
+            const double X2 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 2);
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                const double d = s_dphi[3 * i + l];
+                Jm[0 + l] += X0 * d;
+                Jm[3 + l] += X1 * d;
+                Jm[6 + l] += X2 * d;
+            }
+        }
+        const double det = Jm[0] * (Jm[4] * Jm[8] - Jm[7] * Jm[5]) - Jm[1] * (Jm[3] * Jm[8] - Jm[5] * Jm[6]) +
+                           Jm[2] * (Jm[3] * Jm[7] - Jm[4] * Jm[6]);
+        const double idet = 1.0 / det;
+        const int o = __ldg(a.orient + e);
+        const double *ct = s_ctab + o * 18;
+        int g[6];
+        {
+            const int2 *gp = reinterpret_cast<const int2 *>(a.gids + 6 * e);
+            int2 g01 = __ldg(gp), g23 = __ldg(gp + 1), g45 = __ldg(gp + 2);
+            g[0] = g01.x; g[1] = g01.y; g[2] = g23.x; g[3] = g23.y; g[4] = g45.x; g[5] = g45.y;
+        }
+        double c[6][3], xv[6];
+        double Bc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const double h0 = ct[3 * j], h1 = ct[3 * j + 1], h2 = ct[3 * j + 2];
+            c[j][0] = Jm[0] * h0 + Jm[1] * h1 + Jm[2] * h2;
+            c[j][1] = Jm[3] * h0 + Jm[4] * h1 + Jm[5] * h2;
+            c[j][2] = Jm[6] * h0 + Jm[7] * h1 + Jm[8] * h2;
+            xv[j] = __ldg(a.x + g[j]);
+            Bc[0] += c[j][0] * xv[j];
+            Bc[1] += c[j][1] * xv[j];
+            Bc[2] += c[j][2] * xv[j];
+        }
+        Bc[0] *= idet;
+        Bc[1] *= idet;
+        Bc[2] *= idet;
+
+        double kfac;                 // sum_q nu_q w_q / det
+        double Fj[6];
+        const bool want_mat = (a.K != nullptr) | (a.dK != nullptr) | (a.J != nullptr) | (a.J32 != nullptr);
+        const int32_t *sl = want_mat ? a.slots + 36 * e : nullptr;
+        if constexpr (!HAS_BS) {
+            const double bm = sqrt(Bc[0] * Bc[0] + Bc[1] * Bc[1] + Bc[2] * Bc[2]);
+            double dnu;
+            const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, bm, dnu);
+            kfac = nu * wsum * idet;
+            const double af = (bm >= 1e-14) ? dnu * wsum * idet / bm : 0.0;
+            double p[6];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) p[j] = c[j][0] * Bc[0] + c[j][1] * Bc[1] + c[j][2] * Bc[2];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) Fj[j] = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+#pragma unroll
+                for (int k = j; k < 6; ++k) {
+                    const double kv = kfac * (c[j][0] * c[k][0] + c[j][1] * c[k][1] + c[j][2] * c[k][2]);
+                    const double dv = af * p[j] * p[k];
+                    const int s1 = want_mat ? __ldg(sl + j * 6 + k) : 0;
+                    if (a.K) red_add(a.K + s1, kv);
+                    if (a.dK) red_add(a.dK + s1, dv);
+                    if (a.J) red_add(a.J + s1, kv + dv);
+                    if (a.J32) red_add(a.J32 + s1, (float)(kv + dv));
+                    Fj[j] += kv * xv[k];
+                    if (k != j) {
+                        const int s2 = want_mat ? __ldg(sl + k * 6 + j) : 0;
+                        if (a.K) red_add(a.K + s2, kv);
+                        if (a.dK) red_add(a.dK + s2, dv);
+                        if (a.J) red_add(a.J + s2, kv + dv);
+                        if (a.J32) red_add(a.J32 + s2, (float)(kv + dv));
+                        Fj[k] += kv * xv[j];
+                    }
+                }
+            }
+            if (a.F) {
+#pragma unroll
+                for (int j = 0; j < 6; ++j) red_add(a.F + g[j], Fj[j]);
+            }
+        } else {
+            // one pass over the quadrature points: accumulate sum_q nu w, the reduced rhs
+            // and the 21 dK pair sums (any number of points, fixed register footprint)
+            double dk[21], r[6];
+#pragma unroll
+            for (int t = 0; t < 21; ++t) dk[t] = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) r[j] = 0.0;
+            kfac = 0.0;
+            const double *bs = a.Bs + (int64_t)e * nq * 3;
+#pragma unroll(NQ > 0 ? NQ : 1)
+            for (int q = 0; q < nq; ++q) {
+                const double s0 = __ldg(bs + 3 * q), s1 = __ldg(bs + 3 * q + 1), s2 = __ldg(bs + 3 * q + 2);
+                const double B0 = s0 + Bc[0], B1 = s1 + Bc[1], B2 = s2 + Bc[2];
+                const double bm = sqrt(B0 * B0 + B1 * B1 + B2 * B2);
+                double dnu;
+                const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, bm, dnu);
+                const double wq = s_w[q];
+                kfac += nu * wq;
+                const double aq = (bm >= 1e-14) ? dnu * wq * idet / bm : 0.0;
+                const double rq = (kNu0 - nu) * wq;
+                double p[6];
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    p[j] = c[j][0] * B0 + c[j][1] * B1 + c[j][2] * B2;
+                    r[j] += rq * (c[j][0] * s0 + c[j][1] * s1 + c[j][2] * s2);
+                }
+                int t = 0;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    const double apj = aq * p[j];
+#pragma unroll
+                    for (int k = j; k < 6; ++k) dk[t++] += apj * p[k];
+                }
+            }
+            kfac *= idet;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                if (a.rhs) red_add(a.rhs + g[j], r[j]);
+                Fj[j] = -r[j];
+            }
+            int t = 0;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+#pragma unroll
+                for (int k = j; k < 6; ++k) {
+                    const double kv = kfac * (c[j][0] * c[k][0] + c[j][1] * c[k][1] + c[j][2] * c[k][2]);
+                    const double dv = dk[t++];
+                    const int s1 = want_mat ? __ldg(sl + j * 6 + k) : 0;
+                    if (a.K) red_add(a.K + s1, kv);
+                    if (a.dK) red_add(a.dK + s1, dv);
+                    if (a.J) red_add(a.J + s1, kv + dv);
+                    if (a.J32) red_add(a.J32 + s1, (float)(kv + dv));
+                    Fj[j] += kv * xv[k];
+                    if (k != j) {
+                        const int s2 = want_mat ? __ldg(sl + k * 6 + j) : 0;
+                        if (a.K) red_add(a.K + s2, kv);
+                        if (a.dK) red_add(a.dK + s2, dv);
+                        if (a.J) red_add(a.J + s2, kv + dv);
+                        if (a.J32) red_add(a.J32 + s2, (float)(kv + dv));
+                        Fj[k] += kv * xv[j];
+                    }
+                }
+            }
+            if (a.F) {
+#pragma unroll
+                for (int j = 0; j < 6; ++j) red_add(a.F + g[j], Fj[j]);
+            }
+        }
+    }
+}
+
+// Reduced rhs only (compute_rhs_Hcurl_red, fem_c/ctools.c:1390-1497).
+__global__ void __launch_bounds__(kBlock)
+    k_rhs_red(CurlArgs a, int quad_stride_ctab) {
+    extern __shared__ double sm[];
+    const SmemLayout L = smem_layout(a.n_orient, a.nq, a.n_int);
+    double *s_ctab = sm + L.off_ctab;
+    double *s_dphi = sm + L.off_dphi;
+    double *s_w = sm + L.off_w;
+    double *s_relc = sm + L.off_relc;
+    double *s_relx = sm + L.off_relx;
+    for (int t = threadIdx.x; t < a.n_orient * 18; t += blockDim.x) {
+        int o = t / 18, r = t - o * 18;
+        s_ctab[t] = a.ctab[(int64_t)o * quad_stride_ctab + r];
+    }
+    for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = a.dphi0[t];
+    for (int t = threadIdx.x; t < a.nq; t += blockDim.x) s_w[t] = a.w[t];
+    const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
+    const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
+    for (int t = threadIdx.x; t < nx; t += blockDim.x) s_relx[t] = (a.n_int < 0) ? 0.0 : a.rel_x[t];
+    __syncthreads();
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x) {
+        const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
+        const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
+        double Jm[9];
+        for (int r = 0; r < 9; ++r) Jm[r] = 0.0;
+        for (int i = 0; i < 4; ++i)
+            for (int k = 0; k < 3; ++k) {
+                const double X = __ldg(a.nodes + 3 * (int64_t)cidx[i] + k);
+                for (int l = 0; l < 3; ++l) Jm[3 * k + l] += X * s_dphi[3 * i + l];
+            }
+        const double det = Jm[0] * (Jm[4] * Jm[8] - Jm[7] * Jm[5]) - Jm[1] * (Jm[3] * Jm[8] - Jm[5] * Jm[6]) +
+                           Jm[2] * (Jm[3] * Jm[7] - Jm[4] * Jm[6]);
+        const double idet = 1.0 / det;
+        const double *ct = s_ctab + __ldg(a.orient + e) * 18;
+        const int32_t *gp = a.gids + 6 * e;
+        double c[6][3];
+        double Bc[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < 6; ++j) {
+            for (int k = 0; k < 3; ++k) c[j][k] = Jm[3 * k] * ct[3 * j] + Jm[3 * k + 1] * ct[3 * j + 1] + Jm[3 * k + 2] * ct[3 * j + 2];
+            const double xj = __ldg(a.x + __ldg(gp + j));
+            for (int k = 0; k < 3; ++k) Bc[k] += c[j][k] * xj;
+        }
+        for (int k = 0; k < 3; ++k) Bc[k] *= idet;
+        double r[6] = {0, 0, 0, 0, 0, 0};
+        const double *bs = a.Bs + (int64_t)e * a.nq * 3;
+        for (int q = 0; q < a.nq; ++q) {
+            const double s0 = __ldg(bs + 3 * q), s1 = __ldg(bs + 3 * q + 1), s2 = __ldg(bs + 3 * q + 2);
+            const double B0 = s0 + Bc[0], B1 = s1 + Bc[1], B2 = s2 + Bc[2];
+            double dnu;
+            const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, sqrt(B0 * B0 + B1 * B1 + B2 * B2), dnu);
+            const double f = (kNu0 - nu) * s_w[q];
+            for (int j = 0; j < 6; ++j) r[j] += f * (c[j][0] * s0 + c[j][1] * s1 + c[j][2] * s2);
+        }
+        for (int j = 0; j < 6; ++j) atomicAdd(a.rhs + __ldg(gp + j), r[j]);
+    }
+}
+
+__global__ void k_check_affine(const double *curls, int n_orient, const double *dphi, int nq, int *bad) {
+    const int64_t per_o = (int64_t)nq * 18;
+    const int64_t total = (int64_t)n_orient * per_o + (int64_t)nq * 12;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        if (t < (int64_t)n_orient * per_o) {
+            int64_t o = t / per_o, r = t - o * per_o;
+            if (curls[o * per_o + r] != curls[o * per_o + (r % 18)]) atomicExch(bad, 1);
+        } else {
+            int64_t r = t - (int64_t)n_orient * per_o;
+            if (dphi[r] != dphi[r % 12]) atomicExch(bad, 1);
+        }
+    }
+}
+
+template <bool HAS_BS, int NQ>
+int launch_t(const CurlArgs &a, cudaStream_t st, size_t smem, int qstride) {
+    if (a.n_elems == 0) return SNP_OK;
+    if (smem > 48 * 1024) {
+        SNP_CUDA_TRY(cudaFuncSetAttribute(k_curlcurl<HAS_BS, NQ, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    }
+    const int grid = stride_grid(a.n_elems, kBlock, 16);
+    k_curlcurl<HAS_BS, NQ, double><<<grid, kBlock, smem, st>>>(a, qstride);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+}  // namespace
+
+int check_affine_tables(const double *curls, int32_t n_orient, const double *d_phi, int32_t nq, cudaStream_t st,
+                        bool *affine) {
+    DevBuf<int> bad;
+    SNP_TRY(bad.alloc(1));
+    SNP_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+    k_check_affine<<<64, 256, 0, st>>>(curls, n_orient, d_phi, nq, bad.p);
+    SNP_LAUNCH_CHECK();
+    int h = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&h, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SNP_CUDA_TRY(cudaStreamSynchronize(st));
+    *affine = (h == 0);
+    return SNP_OK;
+}
+
+int launch_curlcurl(const CurlArgs &a, cudaStream_t st) {
+    const SmemLayout L = smem_layout(a.n_orient, a.nq, a.n_int);
+    const size_t smem = sizeof(double) * (size_t)L.total;
+    SNP_REQUIRE(smem <= 200 * 1024, "curl-curl assembly: tables need %zu bytes of shared memory (max 200 KiB)", smem);
+    const int qstride = a.nq * 18;
+    if (a.Bs == nullptr) {
+        if (a.nq == 1) return launch_t<false, 1>(a, st, smem, qstride);
+        if (a.nq == 4) return launch_t<false, 4>(a, st, smem, qstride);
+        return launch_t<false, 0>(a, st, smem, qstride);
+    }
+    if (a.nq == 1) return launch_t<true, 1>(a, st, smem, qstride);
+    if (a.nq == 4) return launch_t<true, 4>(a, st, smem, qstride);
+    if (a.nq == 5) return launch_t<true, 5>(a, st, smem, qstride);
+    return launch_t<true, 0>(a, st, smem, qstride);
+}
+
+static int fill_args(CurlArgs &a, const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,
+                     const int32_t *cells, const int32_t *glob_ids, const int32_t *orientations, const double *curls,
+                     int32_t n_orient, const double *d_phi, const double *w, int32_t n_quad, const double *x,
+                     const double *B_s, int32_t n_int, const double *rel_c, const double *rel_x) {
+    SNP_REQUIRE(n_elems >= 0, "negative element count");
+    SNP_REQUIRE(n_quad >= 1, "n_quad must be >= 1");
+    SNP_REQUIRE(n_orient >= 1, "n_orient must be >= 1");
+    SNP_REQUIRE(n_int == -1 || n_int >= 1, "n_int must be -1 (constant) or >= 1");
+    SNP_REQUIRE(rel_c != nullptr && (n_int < 0 || rel_x != nullptr), "reluctance tables are NULL");
+    SNP_REQUIRE(n_elems == 0 || (nodes && cells && glob_ids && orientations && curls && d_phi && w && x),
+                "a required input pointer is NULL");
+    SNP_REQUIRE(((uintptr_t)cells & 15) == 0, "cells must be 16-byte aligned");
+    SNP_REQUIRE(((uintptr_t)glob_ids & 7) == 0, "glob_ids must be 8-byte aligned");
+    if (pat) {
+        SNP_REQUIRE(pat->dpe == 6, "pattern was not built for 6 DoFs per element");
+        SNP_REQUIRE(elem_offset >= 0 && elem_offset + n_elems <= pat->n_elems,
+                    "element range [%lld, %lld) outside the pattern's %lld elements", (long long)elem_offset,
+                    (long long)(elem_offset + n_elems), (long long)pat->n_elems);
+    }
+    a = CurlArgs{};
+    a.n_elems = n_elems;
+    a.nodes = nodes;
+    a.cells = cells;
+    a.gids = glob_ids;
+    a.orient = orientations;
+    a.ctab = curls;
+    a.n_orient = n_orient;
+    a.dphi0 = d_phi;
+    a.w = w;
+    a.nq = n_quad;
+    a.x = x;
+    a.Bs = B_s;
+    a.n_int = n_int;
+    a.rel_c = rel_c;
+    a.rel_x = rel_x;
+    a.slots = pat ? pat->slots.p + 36 * elem_offset : nullptr;
+    return SNP_OK;
+}
+
+}  // namespace snp
+
+extern "C" {
+
+int snp_curlcurl_assemble(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,
+                          const int32_t *cells, const int32_t *glob_ids, const int32_t *orientations,
+                          const double *curls, int32_t n_orient, const double *d_phi, const double *w,
+                          int32_t n_quad, const double *x, const double *B_s, int32_t n_int, const double *rel_c,
+                          const double *rel_x, double *K_vals, double *dK_vals, double *J_vals, double *rhs,
+                          double *F, void *stream) {
+    snp::clear_error();
+    const bool want_mat = K_vals || dK_vals || J_vals;
+    SNP_REQUIRE(!want_mat || pat != nullptr, "snp_curlcurl_assemble: matrix outputs need a pattern");
+    snp::CurlArgs a;
+    SNP_TRY(snp::fill_args(a, pat, elem_offset, n_elems, nodes, cells, glob_ids, orientations, curls, n_orient, d_phi,
+                           w, n_quad, x, B_s, n_int, rel_c, rel_x));
+    a.K = K_vals;
+    a.dK = dK_vals;
+    a.J = J_vals;
+    a.rhs = rhs;
+    a.F = F;
+    return snp::launch_curlcurl(a, snp::as_stream(stream));
+}
+
+int snp_curlcurl_assemble_f32(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,
+                              const int32_t *cells, const int32_t *glob_ids, const int32_t *orientations,
+                              const double *curls, int32_t n_orient, const double *d_phi, const double *w,
+                              int32_t n_quad, const double *x, const double *B_s, int32_t n_int, const double *rel_c,
+                              const double *rel_x, float *J_vals, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(pat != nullptr, "snp_curlcurl_assemble_f32: pattern is NULL");
+    snp::CurlArgs a;
+    SNP_TRY(snp::fill_args(a, pat, elem_offset, n_elems, nodes, cells, glob_ids, orientations, curls, n_orient, d_phi,
+                           w, n_quad, x, B_s, n_int, rel_c, rel_x));
+    a.J32 = J_vals;
+    return snp::launch_curlcurl(a, snp::as_stream(stream));
+}
+
+int snp_curlcurl_rhs_red(int64_t n_elems, const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                         const int32_t *orientations, const double *curls, int32_t n_orient, const double *d_phi,
+                         const double *w, int32_t n_quad, const double *x, const double *B_s, int32_t n_int,
+                         const double *rel_c, const double *rel_x, double *rhs, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(rhs != nullptr && (n_elems == 0 || B_s != nullptr), "snp_curlcurl_rhs_red: rhs and B_s are required");
+    snp::CurlArgs a;
+    SNP_TRY(snp::fill_args(a, nullptr, 0, n_elems, nodes, cells, glob_ids, orientations, curls, n_orient, d_phi, w,
+                           n_quad, x, B_s, n_int, rel_c, rel_x));
+    a.rhs = rhs;
+    if (n_elems == 0) return SNP_OK;
+    const snp::SmemLayout L = snp::smem_layout(a.n_orient, a.nq, a.n_int);
+    const size_t smem = sizeof(double) * (size_t)L.total;
+    SNP_REQUIRE(smem <= 200 * 1024, "tables too large for shared memory");
+    if (smem > 48 * 1024)
+        SNP_CUDA_TRY(cudaFuncSetAttribute(snp::k_rhs_red, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    snp::k_rhs_red<<<snp::stride_grid(n_elems, snp::kBlock, 16), snp::kBlock, smem, snp::as_stream(stream)>>>(
+        a, a.nq * 18);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,531 @@
+// Sparse linear algebra on the device: masked CSR SpMV and Jacobi-preconditioned CG.
+//
+// The reference extracts J_c = J[mask,:][:,mask], builds M = diags(1/diag(J_c)) and calls
+// scipy.sparse.linalg.cg (snoopy/red_mvp_solver.py:195-203).  Here the Dirichlet mask is
+// applied inside the kernels (rows and columns with free[i] == 0 are skipped), so J is
+// never copied, and the CG iteration runs entirely on the device:
+//
+//   per iteration  k_spmv_dot : q = A p, last block reduces p.q  -> alpha
+//                  k_update   : x += alpha p, r -= alpha q, z = dinv r, last block
+//                               reduces r.z and r.r -> beta, convergence flag
+//                  k_pupdate  : p = z + beta p
+//
+// Block partial sums are reduced by whichever block finishes last (one atomicInc ticket
+// per launch, no waiting), in a fixed order, so results are deterministic.  The loop is a
+// CUDA-graph conditional WHILE node whose body clears its condition once the flag is set;
+// the flag is set at convergence, at `maxiter` and on a non-finite residual, so the loop
+// always ends.  Stopping rule of scipy's cg: ||r|| < max(atol, rtol * ||b||).
+#include <cstdio>
+#include <cstdlib>
+
+#include "snp_common.cuh"
+#include "snp_internal.cuh"
+#include "snp_krylov.cuh"
+
+namespace snp {
+
+namespace {
+
+constexpr int kVecBlock = 256;
+constexpr int kSpmvBlock = 256;
+
+__device__ __forceinline__ bool is_free(const uint8_t *free_mask, int64_t i) { return free_mask == nullptr || free_mask[i]; }
+
+// The block that takes the last ticket reduces `part[0 .. nparts)` (stride `width`).
+__device__ __forceinline__ bool last_block(unsigned int *counter) {
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int t = atomicInc(counter, gridDim.x - 1);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return s_last;
+}
+
+template <typename T>
+__device__ double reduce_parts(const T *part, int nparts, int width, int comp, double *sh) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) v += (double)__ldcg(part + (int64_t)i * width + comp);
+    v = block_sum(v, sh);
+    return v;  // valid in thread 0
+}
+
+// y = A x restricted to free rows/cols; TPR threads per row.  DOT: also p.y partial sums.
+template <typename VT, typename XT, int TPR, bool MASKCOL, bool DOT>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmv(int32_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci, const VT *__restrict__ v,
+           const uint8_t *__restrict__ free_mask, const XT *__restrict__ x, XT *__restrict__ y, PcgState *st,
+           double *part) {
+    __shared__ double sh[32];
+    if (DOT && st->done) return;
+    const int lane = threadIdx.x % TPR;
+    const int group = threadIdx.x / TPR;
+    const int groups_per_block = kSpmvBlock / TPR;
+    double dot = 0.0;
+    // the loop bound is uniform across the block, so every lane reaches the shuffles
+    for (int64_t base = (int64_t)blockIdx.x * groups_per_block; base < n; base += (int64_t)gridDim.x * groups_per_block) {
+        const int64_t row = base + group;
+        const bool valid = row < n;
+        double s = 0.0;
+        const bool fr = valid && is_free(free_mask, row);
+        if (fr) {
+            const int b = __ldg(rp + row), e = __ldg(rp + row + 1);
+            for (int k = b + lane; k < e; k += TPR) {
+                const int c = __ldg(ci + k);
+                if (!MASKCOL || is_free(free_mask, c)) s += (double)__ldg(v + k) * (double)__ldg(x + c);
+            }
+        }
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+        if (lane == 0 && valid) {
+            y[row] = fr ? (XT)s : (XT)0;
+            if (DOT && fr) dot += (double)x[row] * s;
+        }
+    }
+    if (DOT) {
+        dot = block_sum(dot, sh);
+        if (threadIdx.x == 0) part[blockIdx.x] = dot;
+        if (last_block(&st->counter)) {
+            const double pq = reduce_parts(part, gridDim.x, 1, 0, sh);
+            if (threadIdx.x == 0) {
+                st->pq = pq;
+                st->alpha = st->rz / pq;
+            }
+        }
+    }
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kVecBlock)
+    k_update(int32_t n, const uint8_t *__restrict__ free_mask, XT *__restrict__ x, XT *__restrict__ r,
+             XT *__restrict__ z, const XT *__restrict__ p, const XT *__restrict__ q, const XT *__restrict__ dinv,
+             PcgState *st, double *part, int use_cond, cudaGraphConditionalHandle cond) {
+    __shared__ double sh[32];
+    if (st->done) {
+        if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
+        return;
+    }
+    const XT alpha = (XT)st->alpha;
+    double rz = 0.0, rr = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (is_free(free_mask, i)) {
+            x[i] += alpha * p[i];
+            const XT ri = r[i] - alpha * q[i];
+            const XT zi = dinv[i] * ri;
+            r[i] = ri;
+            z[i] = zi;
+            rz += (double)ri * (double)zi;
+            rr += (double)ri * (double)ri;
+        }
+    }
+    const double brz = block_sum(rz, sh);
+    if (threadIdx.x == 0) part[2 * blockIdx.x] = brz;
+    const double brr = block_sum(rr, sh);
+    if (threadIdx.x == 0) part[2 * blockIdx.x + 1] = brr;
+    if (last_block(&st->counter)) {
+        const double rz_new = reduce_parts(part, gridDim.x, 2, 0, sh);
+        const double rr_new = reduce_parts(part, gridDim.x, 2, 1, sh);
+        if (threadIdx.x == 0) {
+            st->beta = rz_new / st->rz;
+            st->rz = rz_new;
+            st->rr = rr_new;
+            st->iter += 1;
+            int done = 0;
+            if (!(rr_new == rr_new) || isinf(rr_new)) done = 3;
+            else if (sqrt(rr_new) < st->atol_eff) done = 1;
+            else if (st->iter >= st->maxit) done = 2;
+            st->done = done;
+            if (use_cond && done) cudaGraphSetConditional(cond, 0);
+        }
+    }
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kVecBlock)
+    k_pupdate(int32_t n, const uint8_t *__restrict__ free_mask, XT *__restrict__ p, const XT *__restrict__ z,
+              const PcgState *st) {
+    if (st->done) return;
+    const XT beta = (XT)st->beta;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (is_free(free_mask, i)) p[i] = z[i] + beta * p[i];
+}
+
+// r = b - q (free rows), z = dinv r, p = z; x = 0 on non-free rows; partials of r.z, r.r, b.b
+template <typename XT>
+__global__ void __launch_bounds__(kVecBlock)
+    k_init(int32_t n, const uint8_t *__restrict__ free_mask, const XT *__restrict__ b, XT *__restrict__ x,
+           XT *__restrict__ r, XT *__restrict__ z, XT *__restrict__ p, const XT *__restrict__ q,
+           const XT *__restrict__ dinv, PcgState *st, double *part, double rtol, double atol, long long maxit,
+           int zero_x) {
+    __shared__ double sh[32];
+    double rz = 0.0, rr = 0.0, bb = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (is_free(free_mask, i)) {
+            const XT bi = b[i];
+            const XT ri = zero_x ? bi : (XT)(bi - q[i]);
+            const XT zi = dinv[i] * ri;
+            if (zero_x) x[i] = (XT)0;
+            r[i] = ri;
+            z[i] = zi;
+            p[i] = zi;
+            rz += (double)ri * (double)zi;
+            rr += (double)ri * (double)ri;
+            bb += (double)bi * (double)bi;
+        } else {
+            x[i] = (XT)0;
+            r[i] = (XT)0;
+            z[i] = (XT)0;
+            p[i] = (XT)0;
+        }
+    }
+    const double a0 = block_sum(rz, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x] = a0;
+    const double a1 = block_sum(rr, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x + 1] = a1;
+    const double a2 = block_sum(bb, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x + 2] = a2;
+    if (last_block(&st->counter)) {
+        const double s_rz = reduce_parts(part, gridDim.x, 3, 0, sh);
+        const double s_rr = reduce_parts(part, gridDim.x, 3, 1, sh);
+        const double s_bb = reduce_parts(part, gridDim.x, 3, 2, sh);
+        if (threadIdx.x == 0) {
+            st->rz = s_rz;
+            st->rr = s_rr;
+            st->bnorm = sqrt(s_bb);
+            st->atol_eff = fmax(atol, rtol * st->bnorm);
+            st->iter = 0;
+            st->maxit = maxit;
+            st->alpha = 0.0;
+            st->beta = 0.0;
+            int done = 0;
+            if (s_bb == 0.0) done = 4;
+            else if (!(s_rr == s_rr) || isinf(s_rr)) done = 3;
+            else if (sqrt(s_rr) < st->atol_eff) done = 1;
+            else if (maxit <= 0) done = 2;
+            st->done = done;
+        }
+    }
+}
+
+template <typename VT, typename XT>
+__global__ void k_dinv(int32_t n, const int32_t *__restrict__ diag_pos, const VT *__restrict__ vals,
+                       const uint8_t *__restrict__ free_mask, XT *__restrict__ dinv, int *bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (is_free(free_mask, i)) {
+            const int d = diag_pos[i];
+            const double v = d >= 0 ? (double)vals[d] : 0.0;
+            if (v == 0.0 || !(v == v)) {
+                atomicExch(bad, 1);
+                dinv[i] = (XT)0;
+            } else {
+                dinv[i] = (XT)(1.0 / v);
+            }
+        } else {
+            dinv[i] = (XT)0;
+        }
+    }
+}
+
+__global__ void k_find_diag(int32_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                            int32_t *__restrict__ diag) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        int lo = rp[r], hi = rp[r + 1] - 1, pos = -1;
+        while (lo <= hi) {
+            const int mid = (lo + hi) >> 1;
+            const int c = ci[mid];
+            if (c == r) {
+                pos = mid;
+                break;
+            }
+            if (c < r) lo = mid + 1; else hi = mid - 1;
+        }
+        diag[r] = pos;
+    }
+}
+
+}  // namespace
+
+int find_diag(int32_t n, const int32_t *rp, const int32_t *ci, int32_t *diag, cudaStream_t s) {
+    k_find_diag<<<stride_grid(n, kVecBlock, 8), kVecBlock, 0, s>>>(n, rp, ci, diag);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int choose_tpr(int64_t nnz, int32_t n) {
+    const double avg = n > 0 ? (double)nnz / n : 0.0;
+    if (avg > 48) return 32;
+    if (avg > 24) return 16;
+    if (avg > 10) return 8;
+    return 4;
+}
+
+template <typename VT, typename XT, bool MASKCOL, bool DOT>
+static int spmv_dispatch(int tpr, int32_t n, const int32_t *rp, const int32_t *ci, const VT *v, const uint8_t *fm,
+                         const XT *x, XT *y, PcgState *st, double *part, int grid, cudaStream_t s) {
+    switch (tpr) {
+        case 4: k_spmv<VT, XT, 4, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
+        case 8: k_spmv<VT, XT, 8, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
+        case 16: k_spmv<VT, XT, 16, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
+        default: k_spmv<VT, XT, 32, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
+    }
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int spmv_grid(int32_t n, int tpr) {
+    const int64_t groups = kSpmvBlock / tpr;
+    return stride_grid((n + groups - 1) / groups * kSpmvBlock, kSpmvBlock, 8);
+}
+
+int spmv_f64(const CsrView<double> &A, const uint8_t *free_mask, const double *x, double *y, cudaStream_t s) {
+    const int tpr = choose_tpr(A.nnz, A.n);
+    const int grid = spmv_grid(A.n, tpr);
+    if (free_mask)
+        return spmv_dispatch<double, double, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, y, nullptr, nullptr,
+                                                          grid, s);
+    return spmv_dispatch<double, double, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, y, nullptr, nullptr, grid, s);
+}
+
+int spmv_f32(const CsrView<float> &A, const uint8_t *free_mask, const float *x, float *y, cudaStream_t s) {
+    const int tpr = choose_tpr(A.nnz, A.n);
+    const int grid = spmv_grid(A.n, tpr);
+    if (free_mask)
+        return spmv_dispatch<float, float, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, y, nullptr, nullptr,
+                                                        grid, s);
+    return spmv_dispatch<float, float, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, y, nullptr, nullptr, grid, s);
+}
+
+// float32 matrix applied to a float64 vector with float64 accumulation (refinement residuals)
+int spmv_f32_f64(const CsrView<float> &A, const uint8_t *free_mask, const double *x, double *y, cudaStream_t s) {
+    const int tpr = choose_tpr(A.nnz, A.n);
+    const int grid = spmv_grid(A.n, tpr);
+    if (free_mask)
+        return spmv_dispatch<float, double, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, y, nullptr, nullptr,
+                                                         grid, s);
+    return spmv_dispatch<float, double, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, y, nullptr, nullptr, grid, s);
+}
+
+// ------------------------------------------------------------------ PCG engine
+
+template <typename VT, typename XT>
+Pcg<VT, XT>::~Pcg() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+}
+
+template <typename VT, typename XT>
+int Pcg<VT, XT>::reserve(int32_t n_) {
+    if (n_ <= cap) {
+        n = n_;
+        return SNP_OK;
+    }
+    drop_graph();
+    n = cap = n_;
+    SNP_TRY(r.alloc(n));
+    SNP_TRY(z.alloc(n));
+    SNP_TRY(p.alloc(n));
+    SNP_TRY(q.alloc(n));
+    SNP_TRY(dinv.alloc(n));
+    const int gmax = sm_count() * 8 + 1;
+    SNP_TRY(part.alloc(3 * (size_t)gmax));
+    SNP_TRY(st.alloc(1));
+    SNP_TRY(hst.alloc(1));
+    SNP_TRY(bad.alloc(1));
+    SNP_CUDA_TRY(cudaMemset(st.p, 0, sizeof(PcgState)));
+    return SNP_OK;
+}
+
+template <typename VT, typename XT>
+void Pcg<VT, XT>::drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+}
+
+template <typename VT, typename XT>
+int Pcg<VT, XT>::set_jacobi(const CsrView<VT> &A, const int32_t *diag_pos, const uint8_t *free_mask, cudaStream_t s,
+                            bool *zero_pivot) {
+    SNP_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    k_dinv<VT, XT><<<stride_grid(A.n, kVecBlock, 8), kVecBlock, 0, s>>>(A.n, diag_pos, A.v, free_mask, dinv.p, bad.p);
+    SNP_LAUNCH_CHECK();
+    launches += 1;
+    int h = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&h, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    *zero_pivot = h != 0;
+    return SNP_OK;
+}
+
+template <typename VT, typename XT>
+int Pcg<VT, XT>::launch_iteration(const CsrView<VT> &A, const uint8_t *free_mask, XT *x, cudaStream_t s, int use_cond,
+                                  cudaGraphConditionalHandle cond) {
+    const int tpr = choose_tpr(A.nnz, A.n);
+    const int g_spmv = spmv_grid(A.n, tpr);
+    if (free_mask) SNP_TRY((spmv_dispatch<VT, XT, false, true>(tpr, A.n, A.rp, A.ci, A.v, free_mask, p.p, q.p, st.p, part.p, g_spmv, s)));
+    else SNP_TRY((spmv_dispatch<VT, XT, false, true>(tpr, A.n, A.rp, A.ci, A.v, nullptr, p.p, q.p, st.p, part.p, g_spmv, s)));
+    const int g = stride_grid(A.n, kVecBlock, 8);
+    k_update<XT><<<g, kVecBlock, 0, s>>>(A.n, free_mask, x, r.p, z.p, p.p, q.p, dinv.p, st.p, part.p, use_cond, cond);
+    SNP_LAUNCH_CHECK();
+    k_pupdate<XT><<<g, kVecBlock, 0, s>>>(A.n, free_mask, p.p, z.p, st.p);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+template <typename VT, typename XT>
+int Pcg<VT, XT>::build_graph(const CsrView<VT> &A, const uint8_t *free_mask, XT *x, cudaStream_t s) {
+    drop_graph();
+    const char *env = getenv("SNP_PCG_GRAPH");
+    if (env && env[0] == '0') return SNP_OK;
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return SNP_OK;
+    }
+    cudaGraphConditionalHandle h;
+    cudaGraphNode_t node;
+    cudaGraphNodeParams cp = {};
+    bool ok = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, g, nullptr, 0, &cp) == cudaSuccess;
+    }
+    cudaStream_t cs = nullptr;
+    if (ok) ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            int rc = launch_iteration(A, free_mask, x, cs, 1, h);
+            cudaGraph_t out = nullptr;
+            cudaError_t e = cudaStreamEndCapture(cs, &out);
+            ok = (rc == SNP_OK) && e == cudaSuccess;
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+    if (cs) cudaStreamDestroy(cs);
+    if (!ok) {
+        cudaGetLastError();
+        clear_error();
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        cudaGraphDestroy(g);
+        return SNP_OK;
+    }
+    graph = g;
+    key_rp = A.rp;
+    key_v = A.v;
+    key_fm = free_mask;
+    key_x = x;
+    key_n = A.n;
+    (void)s;
+    return SNP_OK;
+}
+
+template <typename VT, typename XT>
+int Pcg<VT, XT>::solve(const CsrView<VT> &A, const uint8_t *free_mask, const XT *b, XT *x, double rtol, double atol,
+                       int64_t maxit, bool zero_x, cudaStream_t s, int64_t *its, double *res, int *status) {
+    SNP_TRY(reserve(A.n));
+    if (maxit < 0) maxit = 10 * (int64_t)A.n;  // scipy's default uses n_free; A.n bounds it
+    // initial residual
+    const int g = stride_grid(A.n, kVecBlock, 8);
+    if (!zero_x) {
+        const int tpr = choose_tpr(A.nnz, A.n);
+        if (free_mask)
+            SNP_TRY((spmv_dispatch<VT, XT, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, q.p, nullptr, nullptr,
+                                                         spmv_grid(A.n, tpr), s)));
+        else
+            SNP_TRY((spmv_dispatch<VT, XT, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, q.p, nullptr, nullptr,
+                                                          spmv_grid(A.n, tpr), s)));
+        launches += 1;
+    }
+    k_init<XT><<<g, kVecBlock, 0, s>>>(A.n, free_mask, b, x, r.p, z.p, p.p, q.p, dinv.p, st.p, part.p, rtol, atol,
+                                       (long long)maxit, zero_x ? 1 : 0);
+    SNP_LAUNCH_CHECK();
+    launches += 1;
+    int64_t chunk_launches = -1;
+    // iterate
+    const bool same = exec && key_rp == A.rp && key_v == A.v && key_fm == free_mask && key_x == x && key_n == A.n;
+    if (!same) SNP_TRY(build_graph(A, free_mask, x, s));
+    if (exec) {
+        SNP_CUDA_TRY(cudaGraphLaunch(exec, s));
+    } else {
+        // chunked host loop: launch a batch, then check the flag
+        const int chunk = 32;
+        int64_t launched = 0;
+        while (true) {
+            for (int k = 0; k < chunk; ++k) SNP_TRY(launch_iteration(A, free_mask, x, s, 0, 0));
+            launched += chunk;
+            SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+            SNP_CUDA_TRY(cudaStreamSynchronize(s));
+            if (hst.p->done || launched > maxit + chunk) break;
+        }
+        chunk_launches = 3 * launched;
+    }
+    SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+    SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    const PcgState &H = *hst.p;
+    // the WHILE body runs once per iteration (once if the initial residual already passes)
+    launches += chunk_launches >= 0 ? chunk_launches : 3 * (H.iter > 0 ? H.iter : 1);
+    if (its) *its = H.iter;
+    if (res) *res = sqrt(H.rr);
+    int stt = SNP_OK;
+    if (H.done == 2) stt = SNP_NOT_CONVERGED;
+    else if (H.done == 3) stt = SNP_NAN_DETECTED;
+    if (status) *status = stt;
+    last_bnorm = H.bnorm;
+    return SNP_OK;
+}
+
+template struct Pcg<double, double>;
+template struct Pcg<float, float>;
+
+}  // namespace snp
+
+extern "C" {
+
+int snp_spmv(int32_t n_rows, const int32_t *row_ptr, const int32_t *col_idx, const double *vals,
+             const uint8_t *free_mask, const double *x, double *y, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(n_rows >= 0, "snp_spmv: negative size");
+    if (n_rows == 0) return SNP_OK;
+    SNP_REQUIRE(row_ptr && col_idx && vals && x && y, "snp_spmv: NULL argument");
+    snp::CsrView<double> A{n_rows, -1, row_ptr, col_idx, vals};
+    A.nnz = (int64_t)n_rows * 16;  // thread-per-row choice only
+    return snp::spmv_f64(A, free_mask, x, y, snp::as_stream(stream));
+}
+
+int snp_pcg(int32_t n_rows, const int32_t *row_ptr, const int32_t *col_idx, const double *vals,
+            const uint8_t *free_mask, const double *b, double *x, double rtol, double atol, int64_t maxiter,
+            int64_t *iterations, double *res_norm, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(n_rows > 0, "snp_pcg: n_rows must be positive");
+    SNP_REQUIRE(row_ptr && col_idx && vals && b && x, "snp_pcg: NULL argument");
+    SNP_REQUIRE(rtol >= 0 && atol >= 0, "snp_pcg: tolerances must be non-negative");
+    cudaStream_t s = snp::as_stream(stream);
+    // diagonal positions (rows are sorted; found by a search kernel)
+    snp::DevBuf<int32_t> diag;
+    SNP_TRY(diag.alloc(n_rows));
+    SNP_TRY(snp::find_diag(n_rows, row_ptr, col_idx, diag.p, s));
+    int32_t nnz_last = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&nnz_last, row_ptr + n_rows, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    snp::CsrView<double> A{n_rows, nnz_last, row_ptr, col_idx, vals};
+    snp::Pcg<double, double> pcg;
+    SNP_TRY(pcg.reserve(n_rows));
+    bool zp = false;
+    SNP_TRY(pcg.set_jacobi(A, diag.p, free_mask, s, &zp));
+    if (zp) return snp::fail(SNP_ZERO_PIVOT, "snp_pcg: zero or missing diagonal entry on a free row");
+    int status = SNP_OK;
+    SNP_TRY(pcg.solve(A, free_mask, b, x, rtol, atol, maxiter, false, s, iterations, res_norm, &status));
+    if (status == SNP_NOT_CONVERGED) return snp::fail(status, "snp_pcg: maxiter reached");
+    if (status == SNP_NAN_DETECTED) return snp::fail(status, "snp_pcg: non-finite residual");
+    return SNP_OK;
+}
+
+}  // extern "C"

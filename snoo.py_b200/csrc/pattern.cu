@@ -1,0 +1,197 @@
+// CSR pattern and element slot map (one-time setup per mesh).
+//
+// The reference converts every assembly's triplets with scipy (fem_c/interface_c.pyx:367-368:
+// csr_array((v,(i,j))) -> sort, sum duplicates).  Here the sort happens once: the
+// (row, col) keys of all element couplings are radix-sorted on the device, duplicates
+// collapse to one CSR position, and the slot map records for every element coupling
+// where its value goes.  Assembly then adds element values straight into CSR values.
+#include <cub/cub.cuh>
+
+#include <cstdio>
+
+#include "snp_common.cuh"
+#include "snp_internal.cuh"
+
+namespace snp {
+
+namespace {
+
+__global__ void k_make_keys(const int32_t *__restrict__ dofs, int64_t n_elems, int dpe,
+                            unsigned long long *__restrict__ keys, uint32_t *__restrict__ ids) {
+    const int64_t per = (int64_t)dpe * dpe;
+    const int64_t total = n_elems * per;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t e = t / per;
+        int ab = (int)(t - e * per);
+        int a = ab / dpe, b = ab - a * dpe;
+        uint32_t r = (uint32_t)dofs[e * dpe + a];
+        uint32_t c = (uint32_t)dofs[e * dpe + b];
+        keys[t] = ((unsigned long long)r << 32) | c;
+        ids[t] = (uint32_t)t;
+    }
+}
+
+__global__ void k_check_dofs(const int32_t *__restrict__ dofs, int64_t n, int32_t n_rows, int *bad) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        int32_t d = dofs[t];
+        if (d < 0 || d >= n_rows) atomicExch(bad, 1);
+    }
+}
+
+__global__ void k_heads(const unsigned long long *__restrict__ keys, int64_t n, uint32_t *__restrict__ head) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        head[t] = (t == 0 || keys[t] != keys[t - 1]) ? 1u : 0u;
+}
+
+// pos = inclusive scan of heads (1-based position of each sorted key's unique entry)
+__global__ void k_scatter(const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ ids,
+                          const uint32_t *__restrict__ head, const uint32_t *__restrict__ pos, int64_t n,
+                          int32_t *__restrict__ slots, int32_t *__restrict__ col_idx, int32_t *__restrict__ row_cnt,
+                          int32_t *__restrict__ diag_pos) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        int32_t p = (int32_t)pos[t] - 1;
+        slots[ids[t]] = p;
+        if (head[t]) {
+            unsigned long long k = keys[t];
+            int32_t r = (int32_t)(k >> 32), c = (int32_t)(k & 0xffffffffu);
+            col_idx[p] = c;
+            atomicAdd(row_cnt + r, 1);
+            if (r == c) diag_pos[r] = p;
+        }
+    }
+}
+
+__global__ void k_fill_i32(int32_t *p, int64_t n, int32_t v) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) p[t] = v;
+}
+
+int bits_for(uint32_t v) {
+    int b = 0;
+    while (b < 32 && (1ull << b) <= v) ++b;
+    return b;
+}
+
+}  // namespace
+
+int pattern_create(const int32_t *elem_dofs, int64_t n_elems, int32_t dpe, int32_t n_rows, cudaStream_t st,
+                   snp_pattern **out) {
+    SNP_REQUIRE(out != nullptr, "snp_pattern_create: out is NULL");
+    *out = nullptr;
+    SNP_REQUIRE(dpe == 4 || dpe == 6, "snp_pattern_create: dofs_per_elem must be 4 or 6 (got %d)", dpe);
+    SNP_REQUIRE(n_rows > 0, "snp_pattern_create: n_rows must be positive");
+    SNP_REQUIRE(n_elems >= 0, "snp_pattern_create: negative element count");
+    const int64_t n = n_elems * dpe * dpe;
+    SNP_REQUIRE(n < (int64_t)0xffffffffll, "snp_pattern_create: %lld couplings exceed the 32-bit slot range", (long long)n);
+    SNP_REQUIRE(n_elems == 0 || elem_dofs != nullptr, "snp_pattern_create: elem_dofs is NULL");
+
+    snp_pattern *P = new snp_pattern();
+    P->n_rows = n_rows;
+    P->n_elems = n_elems;
+    P->dpe = dpe;
+    DevBuf<unsigned long long> keys, keys2;
+    DevBuf<uint32_t> ids, ids2, head, pos;
+    DevBuf<int> bad;
+    DevBuf<unsigned char> temp;
+    auto cleanup_fail = [&](int code) {
+        delete P;
+        return code;
+    };
+    int rc;
+    if ((rc = P->row_ptr.alloc(n_rows + 1)) || (rc = P->diag_pos.alloc(n_rows)) || (rc = P->slots.alloc(n > 0 ? n : 1)) ||
+        (rc = bad.alloc(1)))
+        return cleanup_fail(rc);
+    if (cudaMemsetAsync(bad.p, 0, sizeof(int), st) != cudaSuccess) return cleanup_fail(fail(SNP_CUDA_ERROR, "memset"));
+    if (n > 0) {
+        k_check_dofs<<<stride_grid(n_elems * dpe, 256, 8), 256, 0, st>>>(elem_dofs, n_elems * dpe, n_rows, bad.p);
+        int hbad = 0;
+        if (cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: %s", cudaGetErrorString(cudaGetLastError())));
+        if (hbad) return cleanup_fail(fail(SNP_BAD_ARG, "snp_pattern_create: a DoF index lies outside [0, %d)", n_rows));
+        if ((rc = keys.alloc(n)) || (rc = keys2.alloc(n)) || (rc = ids.alloc(n)) || (rc = ids2.alloc(n)) ||
+            (rc = head.alloc(n)) || (rc = pos.alloc(n)))
+            return cleanup_fail(rc);
+        k_make_keys<<<stride_grid(n, 256, 16), 256, 0, st>>>(elem_dofs, n_elems, dpe, keys.p, ids.p);
+        int end_bit = 32 + bits_for((uint32_t)n_rows);
+        if (end_bit > 64) end_bit = 64;
+        size_t tb_sort = 0, tb_scan = 0;
+        cub::DoubleBuffer<unsigned long long> dk(keys.p, keys2.p);
+        cub::DoubleBuffer<uint32_t> dv(ids.p, ids2.p);
+        cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, dk, dv, n, 0, end_bit, st);
+        cub::DeviceScan::InclusiveSum(nullptr, tb_scan, head.p, pos.p, n, st);
+        size_t tb_scan2 = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb_scan2, P->row_ptr.p, P->row_ptr.p, n_rows + 1, st);
+        size_t tb = tb_sort > tb_scan ? tb_sort : tb_scan;
+        if (tb_scan2 > tb) tb = tb_scan2;
+        if ((rc = temp.alloc(tb > 0 ? tb : 1))) return cleanup_fail(rc);
+        if (cub::DeviceRadixSort::SortPairs(temp.p, tb, dk, dv, n, 0, end_bit, st) != cudaSuccess)
+            return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: radix sort failed"));
+        k_heads<<<stride_grid(n, 256, 16), 256, 0, st>>>(dk.Current(), n, head.p);
+        if (cub::DeviceScan::InclusiveSum(temp.p, tb, head.p, pos.p, n, st) != cudaSuccess)
+            return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: scan failed"));
+        uint32_t h_nnz = 0;
+        if (cudaMemcpyAsync(&h_nnz, pos.p + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: nnz readback failed"));
+        P->nnz = h_nnz;
+        if ((rc = P->col_idx.alloc(P->nnz))) return cleanup_fail(rc);
+        if (cudaMemsetAsync(P->row_ptr.p, 0, sizeof(int32_t) * (n_rows + 1), st) != cudaSuccess)
+            return cleanup_fail(fail(SNP_CUDA_ERROR, "memset"));
+        k_fill_i32<<<stride_grid(n_rows, 256, 8), 256, 0, st>>>(P->diag_pos.p, n_rows, -1);
+        k_scatter<<<stride_grid(n, 256, 16), 256, 0, st>>>(dk.Current(), dv.Current(), head.p, pos.p, n, P->slots.p,
+                                                           P->col_idx.p, P->row_ptr.p, P->diag_pos.p);
+        if (cub::DeviceScan::ExclusiveSum(temp.p, tb, P->row_ptr.p, P->row_ptr.p, n_rows + 1, st) != cudaSuccess)
+            return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: row scan failed"));
+    } else {
+        P->nnz = 0;
+        if ((rc = P->col_idx.alloc(1))) return cleanup_fail(rc);
+        if (cudaMemsetAsync(P->row_ptr.p, 0, sizeof(int32_t) * (n_rows + 1), st) != cudaSuccess)
+            return cleanup_fail(fail(SNP_CUDA_ERROR, "memset"));
+        k_fill_i32<<<stride_grid(n_rows, 256, 8), 256, 0, st>>>(P->diag_pos.p, n_rows, -1);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: %s", cudaGetErrorString(e)));
+    *out = P;
+    return SNP_OK;
+}
+
+}  // namespace snp
+
+extern "C" {
+
+int snp_pattern_create(const int32_t *elem_dofs, int64_t n_elems, int32_t dofs_per_elem, int32_t n_rows,
+                       void *stream, snp_pattern **out) {
+    snp::clear_error();
+    return snp::pattern_create(elem_dofs, n_elems, dofs_per_elem, n_rows, snp::as_stream(stream), out);
+}
+
+int snp_pattern_info(const snp_pattern *pat, int32_t *n_rows, int64_t *nnz, int64_t *n_elems, int32_t *dpe) {
+    SNP_REQUIRE(pat != nullptr, "snp_pattern_info: pattern is NULL");
+    if (n_rows) *n_rows = pat->n_rows;
+    if (nnz) *nnz = pat->nnz;
+    if (n_elems) *n_elems = pat->n_elems;
+    if (dpe) *dpe = pat->dpe;
+    return SNP_OK;
+}
+
+int snp_pattern_arrays(const snp_pattern *pat, const int32_t **row_ptr, const int32_t **col_idx, const int32_t **slots) {
+    SNP_REQUIRE(pat != nullptr, "snp_pattern_arrays: pattern is NULL");
+    if (row_ptr) *row_ptr = pat->row_ptr.p;
+    if (col_idx) *col_idx = pat->col_idx.p;
+    if (slots) *slots = pat->slots.p;
+    return SNP_OK;
+}
+
+int snp_pattern_diag(const snp_pattern *pat, const int32_t **diag_pos) {
+    SNP_REQUIRE(pat != nullptr, "snp_pattern_diag: pattern is NULL");
+    if (diag_pos) *diag_pos = pat->diag_pos.p;
+    return SNP_OK;
+}
+
+int snp_pattern_destroy(snp_pattern *pat) {
+    delete pat;
+    return SNP_OK;
+}
+
+}  // extern "C"

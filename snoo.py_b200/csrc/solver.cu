@@ -1,0 +1,526 @@
+// Persistent Newton solver for the (reduced) magnetic vector potential formulation.
+//
+// Mirrors the Newton loops of RedMVPSolver.solve (snoopy/red_mvp_solver.py:121-224) and
+// MVPSolver.solve_nonlin (snoopy/mvp_solver.py:222-334) with every step on the device:
+// assembly into the cached CSR pattern (the reference re-runs scipy's COO->CSR, the sparse
+// adds and the Dirichlet fancy-indexing every step), the masked Jacobi-PCG, and the vector
+// updates.  The host only reads a few scalars per Newton step.
+//
+// Mode 0 keeps the reference's semantics: b = J x - K x + rhs, zero-excitation exit when
+// max|b| < 1e-14, x_{n+1} = CG(J_free, b_free, x0 = x_n, atol = tol, rtol = cg_rtol),
+// stop when max|x_{n+1} - x_n| < tol * max|x_{n+1}|.
+// Mode 1 is Newton on F(x) = K(x) x - rhs(x) until ||F_free|| <= tol * ||F_free(x0)||, each
+// step J h = -F solved by CG to an Eisenstat-Walker forcing tolerance; with precision 1 the
+// Jacobian values and the CG run in float32 while F, the update and the norms stay float64
+// (the Newton loop is the iterative refinement of the float32 solves).
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "snp_common.cuh"
+#include "snp_internal.cuh"
+#include "snp_krylov.cuh"
+
+namespace snp {
+namespace {
+
+constexpr int kVB = 256;
+
+struct Material {
+    int64_t offset = 0, count = 0;
+    int32_t n_int = -1;
+    DevBuf<int32_t> cells, gids, orient;
+    DevBuf<double> relc, relx, Bs;
+    bool has_bs = false;
+};
+
+// res[0] += sum over free i of v[i]^2 (deterministic last-block reduction)
+// res[1]  = max over all i of |v[i]|; res[2] = max |v - w| and res[3] = max |v| (when w != null)
+__global__ void k_vstats(int32_t n, const uint8_t *__restrict__ fm, const double *__restrict__ v,
+                         const double *__restrict__ w, double *part, unsigned int *counter, double *res) {
+    __shared__ double sh[32];
+    double ss = 0.0, mx = 0.0, md = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double a = v[i];
+        if (fm == nullptr || fm[i]) ss += a * a;
+        mx = fmax(mx, fabs(a));
+        if (w) md = fmax(md, fabs(a - w[i]));
+    }
+    // sum
+    ss = block_sum(ss, sh);
+    __syncthreads();
+    // max via warp shuffles
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    }
+    __shared__ double smx[32], smd[32];
+    if ((threadIdx.x & 31) == 0) {
+        smx[threadIdx.x >> 5] = mx;
+        smd[threadIdx.x >> 5] = md;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            mx = fmax(mx, smx[k]);
+            md = fmax(md, smd[k]);
+        }
+        part[3 * blockIdx.x] = ss;
+        part[3 * blockIdx.x + 1] = mx;
+        part[3 * blockIdx.x + 2] = md;
+        __threadfence();
+    }
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicInc(counter, gridDim.x - 1) == gridDim.x - 1;
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        double s = 0.0, m = 0.0, d = 0.0;
+        for (unsigned int b = 0; b < gridDim.x; ++b) {
+            s += __ldcg(part + 3 * b);
+            m = fmax(m, __ldcg(part + 3 * b + 1));
+            d = fmax(d, __ldcg(part + 3 * b + 2));
+        }
+        res[0] = s;
+        res[1] = m;
+        res[2] = d;
+    }
+}
+
+__global__ void k_sub(int32_t n, double *__restrict__ b, const double *__restrict__ F) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] -= F[i];
+}
+
+__global__ void k_neg_free(int32_t n, const uint8_t *__restrict__ fm, const double *__restrict__ F, double *__restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = fm[i] ? -F[i] : 0.0;
+}
+
+__global__ void k_neg_free_f32(int32_t n, const uint8_t *__restrict__ fm, const double *__restrict__ F, float *__restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = fm[i] ? (float)(-F[i]) : 0.0f;
+}
+
+__global__ void k_add_free(int32_t n, const uint8_t *__restrict__ fm, double *__restrict__ x, const double *__restrict__ h) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (fm[i]) x[i] += h[i];
+}
+
+__global__ void k_add_free_f32(int32_t n, const uint8_t *__restrict__ fm, double *__restrict__ x, const float *__restrict__ h) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (fm[i]) x[i] += (double)h[i];
+}
+
+__global__ void k_zero_nonfree(int32_t n, const uint8_t *__restrict__ fm, double *__restrict__ x) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (!fm[i]) x[i] = 0.0;
+}
+
+__global__ void k_count_free(int32_t n, const uint8_t *__restrict__ fm, unsigned long long *cnt) {
+    unsigned long long c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) c += fm[i] ? 1 : 0;
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, c);
+}
+
+}  // namespace
+}  // namespace snp
+
+struct snp_solver {
+    int32_t n = 0;
+    int64_t n_nodes = 0;
+    int32_t nq = 0, n_orient = 0;
+    int64_t n_free = 0;
+    cudaStream_t stream = nullptr;
+    snp::DevBuf<double> nodes, curls, dphi, w, rhs_extra;
+    snp::DevBuf<uint8_t> free_mask;
+    bool has_extra = false;
+    std::vector<std::unique_ptr<snp::Material>> mats;
+    snp_pattern *pat = nullptr;
+    bool finalized = false;
+    snp::DevBuf<double> J, F, b, xw, h, part, res;
+    snp::DevBuf<float> J32, b32, h32;
+    snp::DevBuf<unsigned int> counter;
+    snp::HostBuf<double> hres;
+    snp::Pcg<double, double> pcg64;
+    snp::Pcg<float, float> pcg32;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int64_t launches = 0;  // kernels of this library launched by the current solve
+
+    ~snp_solver() {
+        if (pat) snp_pattern_destroy(pat);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+
+    int64_t n_elems_total() const {
+        int64_t t = 0;
+        for (auto &m : mats) t += m->count;
+        return t;
+    }
+
+    int vstats(const double *v, const double *w2, bool free_only, double out[3]) {
+        const int grid = snp::stride_grid(n, snp::kVB, 4);
+        snp::k_vstats<<<grid, snp::kVB, 0, stream>>>(n, free_only ? free_mask.p : nullptr, v, w2, part.p, counter.p, res.p);
+        SNP_LAUNCH_CHECK();
+        ++launches;
+        SNP_CUDA_TRY(cudaMemcpyAsync(hres.p, res.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        SNP_CUDA_TRY(cudaStreamSynchronize(stream));
+        for (int k = 0; k < 3; ++k) out[k] = hres.p[k];
+        return SNP_OK;
+    }
+
+    // J (f64 or f32), F = K x - rhs - rhs_extra; optional K and rhs.
+    int assemble(const double *x, double *Kv, double *Jv, float *J32v, double *rhsv, double *Fv) {
+        const int64_t nnz = pat->nnz;
+        if (Kv) SNP_CUDA_TRY(cudaMemsetAsync(Kv, 0, sizeof(double) * nnz, stream));
+        if (Jv) SNP_CUDA_TRY(cudaMemsetAsync(Jv, 0, sizeof(double) * nnz, stream));
+        if (J32v) SNP_CUDA_TRY(cudaMemsetAsync(J32v, 0, sizeof(float) * nnz, stream));
+        if (rhsv) SNP_CUDA_TRY(cudaMemsetAsync(rhsv, 0, sizeof(double) * n, stream));
+        if (Fv) SNP_CUDA_TRY(cudaMemsetAsync(Fv, 0, sizeof(double) * n, stream));
+        for (auto &m : mats) {
+            snp::CurlArgs a{};
+            a.n_elems = m->count;
+            a.nodes = nodes.p;
+            a.cells = m->cells.p;
+            a.gids = m->gids.p;
+            a.orient = m->orient.p;
+            a.ctab = curls.p;
+            a.n_orient = n_orient;
+            a.dphi0 = dphi.p;
+            a.w = w.p;
+            a.nq = nq;
+            a.x = x;
+            a.Bs = m->has_bs ? m->Bs.p : nullptr;
+            a.n_int = m->n_int;
+            a.rel_c = m->relc.p;
+            a.rel_x = m->relx.p;
+            a.slots = pat->slots.p + 36 * m->offset;
+            a.K = Kv;
+            a.J = Jv;
+            a.J32 = J32v;
+            a.rhs = rhsv;
+            a.F = Fv;
+            SNP_TRY(snp::launch_curlcurl(a, stream));
+            if (m->count) ++launches;
+        }
+        if (Fv && has_extra) {
+            snp::k_sub<<<snp::stride_grid(n, snp::kVB, 4), snp::kVB, 0, stream>>>(n, Fv, rhs_extra.p);
+            SNP_LAUNCH_CHECK();
+            ++launches;
+        }
+        return SNP_OK;
+    }
+
+    float elapsed(int a, int b2) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[a], ev[b2]);
+        return ms;
+    }
+
+    int solve(double *x, const snp_solve_opts &o, snp_solve_stats &S) {
+        std::memset(&S, 0, sizeof(S));
+        launches = 0;
+        pcg64.launches = 0;
+        pcg32.launches = 0;
+        const int grid = snp::stride_grid(n, snp::kVB, 4);
+        SNP_CUDA_TRY(cudaEventRecord(ev[2], stream));
+        snp::CsrView<double> A{n, pat->nnz, pat->row_ptr.p, pat->col_idx.p, J.p};
+        snp::CsrView<float> A32{n, pat->nnz, pat->row_ptr.p, pat->col_idx.p, J32.p};
+        const int64_t cg_maxit = o.cg_maxiter < 0 ? 10 * n_free : o.cg_maxiter;
+        double st3[3];
+        int status = SNP_OK;
+        if (o.mode == 0) {
+            SNP_REQUIRE(o.precision == 0, "mode 0 (reference semantics) runs in float64 only");
+            for (int it = 0; it < o.max_newton; ++it) {
+                SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+                SNP_TRY(assemble(x, nullptr, J.p, nullptr, nullptr, F.p));
+                SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                // b = J x - (K x - rhs)
+                SNP_TRY(snp::spmv_f64(A, nullptr, x, b.p, stream));
+                snp::k_sub<<<grid, snp::kVB, 0, stream>>>(n, b.p, F.p);
+                SNP_LAUNCH_CHECK();
+                launches += 2;  // with the SpMV above
+                SNP_TRY(vstats(F.p, nullptr, true, st3));
+                S.res = std::sqrt(st3[0]);
+                if (it == 0) S.res0 = S.res;
+                SNP_TRY(vstats(b.p, nullptr, false, st3));
+                S.t_assemble_ms += elapsed(0, 1);
+                S.newton_iterations = it + 1;
+                if (st3[1] < 1e-14) {
+                    SNP_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
+                    if (o.verbose) printf("  zero excitation!\n");
+                    break;
+                }
+                bool zp = false;
+                SNP_TRY(pcg64.set_jacobi(A, pat->diag_pos.p, free_mask.p, stream, &zp));
+                if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
+                SNP_CUDA_TRY(cudaMemcpyAsync(xw.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+                SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+                int64_t its = 0;
+                double rn = 0.0;
+                int st = SNP_OK;
+                SNP_TRY(pcg64.solve(A, free_mask.p, b.p, xw.p, o.cg_rtol, o.tol, cg_maxit, false, stream, &its, &rn, &st));
+                SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                if (st == SNP_NAN_DETECTED) return snp::fail(st, "Newton step %d: non-finite CG residual", it);
+                S.cg_iterations += its;
+                SNP_TRY(vstats(xw.p, x, false, st3));  // st3[1] = max|x_new|, st3[2] = max|x_new - x|
+                S.t_krylov_ms += elapsed(0, 1);
+                SNP_CUDA_TRY(cudaMemcpyAsync(x, xw.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+                if (o.verbose)
+                    printf("  step %d: max relative increment %.3e, cg its %lld\n", it,
+                           st3[1] > 0 ? st3[2] / st3[1] : 0.0, (long long)its);
+                if (st3[2] < o.tol * st3[1]) break;
+            }
+        } else if (o.mode == 1) {
+            double F0 = 0.0, fprev = 0.0, eta_prev = 0.0;
+            double eta_max = o.cg_rtol > 0 ? o.cg_rtol : 0.1;
+            if (eta_max > 0.5) eta_max = 0.5;
+            snp::k_zero_nonfree<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x);
+            SNP_LAUNCH_CHECK();
+            ++launches;
+            for (int it = 0; it <= o.max_newton; ++it) {
+                SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+                if (o.precision == 1) {
+                    SNP_TRY(assemble(x, nullptr, nullptr, J32.p, nullptr, F.p));
+                } else {
+                    SNP_TRY(assemble(x, nullptr, J.p, nullptr, nullptr, F.p));
+                }
+                SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                SNP_TRY(vstats(F.p, nullptr, true, st3));
+                S.t_assemble_ms += elapsed(0, 1);
+                const double fn = std::sqrt(st3[0]);
+                if (!(fn == fn)) return snp::fail(SNP_NAN_DETECTED, "Newton step %d: non-finite residual", it);
+                if (it == 0) {
+                    F0 = fn;
+                    S.res0 = fn;
+                }
+                S.res = fn;
+                if (o.verbose) printf("  newton %d: |F| = %.6e (rel %.3e)\n", it, fn, F0 > 0 ? fn / F0 : 0.0);
+                if (F0 == 0.0 || fn <= o.tol * F0) break;
+                if (it == o.max_newton) {
+                    status = SNP_NOT_CONVERGED;
+                    break;
+                }
+                // Eisenstat-Walker forcing term (choice 2) with safeguards
+                double eta = eta_max;
+                if (it > 0) {
+                    const double ratio = fn / fprev;
+                    eta = 0.9 * ratio * ratio;
+                    const double sg = 0.9 * eta_prev * eta_prev;
+                    if (sg > 0.1 && sg > eta) eta = sg;
+                    if (eta > eta_max) eta = eta_max;
+                }
+                const double floor_eta = 0.5 * o.tol * F0 / fn;
+                if (eta < floor_eta) eta = floor_eta;
+                if (o.precision == 1 && eta < 1e-6) eta = 1e-6;
+                if (eta > 0.5) eta = 0.5;
+                fprev = fn;
+                eta_prev = eta;
+                int64_t its = 0;
+                double rn = 0.0;
+                int st = SNP_OK;
+                bool zp = false;
+                SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+                if (o.precision == 1) {
+                    SNP_TRY(pcg32.set_jacobi(A32, pat->diag_pos.p, free_mask.p, stream, &zp));
+                    if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
+                    snp::k_neg_free_f32<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, F.p, b32.p);
+                    SNP_LAUNCH_CHECK();
+                    SNP_TRY(pcg32.solve(A32, free_mask.p, b32.p, h32.p, eta, 0.0, cg_maxit, true, stream, &its, &rn, &st));
+                    snp::k_add_free_f32<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x, h32.p);
+                } else {
+                    SNP_TRY(pcg64.set_jacobi(A, pat->diag_pos.p, free_mask.p, stream, &zp));
+                    if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
+                    snp::k_neg_free<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, F.p, b.p);
+                    SNP_LAUNCH_CHECK();
+                    SNP_TRY(pcg64.solve(A, free_mask.p, b.p, h.p, eta, 0.0, cg_maxit, true, stream, &its, &rn, &st));
+                    snp::k_add_free<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x, h.p);
+                }
+                SNP_LAUNCH_CHECK();
+                launches += 2;  // -F and the update
+                SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
+                S.t_krylov_ms += elapsed(0, 1);
+                if (st == SNP_NAN_DETECTED) return snp::fail(st, "Newton step %d: non-finite CG residual", it);
+                S.cg_iterations += its;
+                S.newton_iterations = it + 1;
+                if (o.verbose) printf("    cg: eta %.2e, %lld its\n", eta, (long long)its);
+            }
+        } else {
+            return snp::fail(SNP_BAD_ARG, "unknown solve mode %d", o.mode);
+        }
+        SNP_CUDA_TRY(cudaEventRecord(ev[3], stream));
+        SNP_CUDA_TRY(cudaEventSynchronize(ev[3]));
+        S.t_total_ms = elapsed(2, 3);
+        S.status = status;
+        S.kernel_launches = launches + pcg64.launches + pcg32.launches;
+        return status == SNP_OK ? SNP_OK : snp::fail(status, "Newton did not reach the tolerance in %d steps", o.max_newton);
+    }
+};
+
+extern "C" {
+
+int snp_solver_create(int32_t n_dofs, const double *nodes, int64_t n_nodes, const double *curls, int32_t n_orient,
+                      const double *d_phi, const double *w, int32_t n_quad, const uint8_t *free_mask, void *stream,
+                      snp_solver **out) {
+    snp::clear_error();
+    SNP_REQUIRE(out != nullptr, "snp_solver_create: out is NULL");
+    *out = nullptr;
+    SNP_REQUIRE(n_dofs > 0 && n_nodes > 0 && n_orient > 0 && n_quad > 0, "snp_solver_create: sizes must be positive");
+    SNP_REQUIRE(nodes && curls && d_phi && w && free_mask, "snp_solver_create: NULL argument");
+    cudaStream_t st = snp::as_stream(stream);
+    bool affine = false;
+    SNP_TRY(snp::check_affine_tables(curls, n_orient, d_phi, n_quad, st, &affine));
+    SNP_REQUIRE(affine, "snp_solver_create: d_phi/curls vary across quadrature points; only affine first-order tetrahedra are supported");
+    auto S = std::make_unique<snp_solver>();
+    S->n = n_dofs;
+    S->n_nodes = n_nodes;
+    S->nq = n_quad;
+    S->n_orient = n_orient;
+    S->stream = st;
+    SNP_TRY(S->nodes.alloc(3 * n_nodes));
+    SNP_TRY(S->curls.alloc((size_t)n_orient * n_quad * 18));
+    SNP_TRY(S->dphi.alloc((size_t)n_quad * 12));
+    SNP_TRY(S->w.alloc(n_quad));
+    SNP_TRY(S->free_mask.alloc(n_dofs));
+    SNP_CUDA_TRY(cudaMemcpyAsync(S->nodes.p, nodes, sizeof(double) * 3 * n_nodes, cudaMemcpyDeviceToDevice, st));
+    SNP_CUDA_TRY(cudaMemcpyAsync(S->curls.p, curls, sizeof(double) * n_orient * n_quad * 18, cudaMemcpyDeviceToDevice, st));
+    SNP_CUDA_TRY(cudaMemcpyAsync(S->dphi.p, d_phi, sizeof(double) * n_quad * 12, cudaMemcpyDeviceToDevice, st));
+    SNP_CUDA_TRY(cudaMemcpyAsync(S->w.p, w, sizeof(double) * n_quad, cudaMemcpyDeviceToDevice, st));
+    SNP_CUDA_TRY(cudaMemcpyAsync(S->free_mask.p, free_mask, n_dofs, cudaMemcpyDeviceToDevice, st));
+    for (auto &e : S->ev) SNP_CUDA_TRY(cudaEventCreate(&e));
+    *out = S.release();
+    return SNP_OK;
+}
+
+int snp_solver_add_material(snp_solver *s, const int32_t *cells, const int32_t *glob_ids, const int32_t *orientations,
+                            int64_t n_elems, int32_t n_int, const double *rel_c, const double *rel_x, const double *B_s) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr, "snp_solver_add_material: solver is NULL");
+    SNP_REQUIRE(!s->finalized, "snp_solver_add_material: solver already finalized");
+    SNP_REQUIRE(n_elems >= 0, "snp_solver_add_material: negative element count");
+    SNP_REQUIRE(n_int == -1 || n_int >= 1, "snp_solver_add_material: n_int must be -1 or >= 1");
+    SNP_REQUIRE(rel_c && (n_int < 0 || rel_x), "snp_solver_add_material: reluctance tables missing");
+    SNP_REQUIRE(n_elems == 0 || (cells && glob_ids && orientations), "snp_solver_add_material: NULL mesh arrays");
+    auto m = std::make_unique<snp::Material>();
+    m->offset = s->n_elems_total();
+    m->count = n_elems;
+    m->n_int = n_int;
+    cudaStream_t st = s->stream;
+    SNP_TRY(m->cells.alloc(4 * n_elems));
+    SNP_TRY(m->gids.alloc(6 * n_elems));
+    SNP_TRY(m->orient.alloc(n_elems));
+    if (n_elems) {
+        SNP_CUDA_TRY(cudaMemcpyAsync(m->cells.p, cells, sizeof(int32_t) * 4 * n_elems, cudaMemcpyDeviceToDevice, st));
+        SNP_CUDA_TRY(cudaMemcpyAsync(m->gids.p, glob_ids, sizeof(int32_t) * 6 * n_elems, cudaMemcpyDeviceToDevice, st));
+        SNP_CUDA_TRY(cudaMemcpyAsync(m->orient.p, orientations, sizeof(int32_t) * n_elems, cudaMemcpyDeviceToDevice, st));
+    }
+    const int nc = n_int < 0 ? 1 : 4 * n_int, nx = n_int < 0 ? 1 : n_int + 1;
+    SNP_TRY(m->relc.alloc(nc));
+    SNP_TRY(m->relx.alloc(nx));
+    SNP_CUDA_TRY(cudaMemcpyAsync(m->relc.p, rel_c, sizeof(double) * nc, cudaMemcpyDeviceToDevice, st));
+    if (n_int >= 0) SNP_CUDA_TRY(cudaMemcpyAsync(m->relx.p, rel_x, sizeof(double) * nx, cudaMemcpyDeviceToDevice, st));
+    else SNP_CUDA_TRY(cudaMemsetAsync(m->relx.p, 0, sizeof(double), st));
+    if (B_s && n_elems) {
+        m->has_bs = true;
+        SNP_TRY(m->Bs.alloc((size_t)n_elems * s->nq * 3));
+        SNP_CUDA_TRY(cudaMemcpyAsync(m->Bs.p, B_s, sizeof(double) * n_elems * s->nq * 3, cudaMemcpyDeviceToDevice, st));
+    }
+    s->mats.push_back(std::move(m));
+    return SNP_OK;
+}
+
+int snp_solver_set_rhs(snp_solver *s, const double *rhs) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr, "snp_solver_set_rhs: solver is NULL");
+    if (!rhs) {
+        s->has_extra = false;
+        return SNP_OK;
+    }
+    if (!s->rhs_extra.p) SNP_TRY(s->rhs_extra.alloc(s->n));
+    SNP_CUDA_TRY(cudaMemcpyAsync(s->rhs_extra.p, rhs, sizeof(double) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+    s->has_extra = true;
+    return SNP_OK;
+}
+
+int snp_solver_finalize(snp_solver *s) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr, "snp_solver_finalize: solver is NULL");
+    SNP_REQUIRE(!s->finalized, "snp_solver_finalize: already finalized");
+    SNP_REQUIRE(!s->mats.empty(), "snp_solver_finalize: no materials");
+    const int64_t E = s->n_elems_total();
+    cudaStream_t st = s->stream;
+    snp::DevBuf<int32_t> all;
+    SNP_TRY(all.alloc(6 * E));
+    for (auto &m : s->mats)
+        if (m->count)
+            SNP_CUDA_TRY(cudaMemcpyAsync(all.p + 6 * m->offset, m->gids.p, sizeof(int32_t) * 6 * m->count,
+                                         cudaMemcpyDeviceToDevice, st));
+    SNP_TRY(snp::pattern_create(all.p, E, 6, s->n, st, &s->pat));
+    const int64_t nnz = s->pat->nnz;
+    SNP_TRY(s->J.alloc(nnz));
+    SNP_TRY(s->J32.alloc(nnz));
+    SNP_TRY(s->F.alloc(s->n));
+    SNP_TRY(s->b.alloc(s->n));
+    SNP_TRY(s->xw.alloc(s->n));
+    SNP_TRY(s->h.alloc(s->n));
+    SNP_TRY(s->b32.alloc(s->n));
+    SNP_TRY(s->h32.alloc(s->n));
+    SNP_TRY(s->part.alloc(3 * (size_t)(snp::sm_count() * 4 + 1)));
+    SNP_TRY(s->res.alloc(3));
+    SNP_TRY(s->counter.alloc(1));
+    SNP_TRY(s->hres.alloc(3));
+    SNP_CUDA_TRY(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned int), st));
+    snp::DevBuf<unsigned long long> cnt;
+    SNP_TRY(cnt.alloc(1));
+    SNP_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), st));
+    snp::k_count_free<<<snp::stride_grid(s->n, snp::kVB, 4), snp::kVB, 0, st>>>(s->n, s->free_mask.p, cnt.p);
+    SNP_LAUNCH_CHECK();
+    unsigned long long hc = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&hc, cnt.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    SNP_CUDA_TRY(cudaStreamSynchronize(st));
+    s->n_free = (int64_t)hc;
+    SNP_TRY(s->pcg64.reserve(s->n));
+    SNP_TRY(s->pcg32.reserve(s->n));
+    s->finalized = true;
+    return SNP_OK;
+}
+
+int snp_solver_solve(snp_solver *s, double *x, const snp_solve_opts *opts, snp_solve_stats *stats) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_solve: solver missing or not finalized");
+    SNP_REQUIRE(x && opts, "snp_solver_solve: NULL argument");
+    SNP_REQUIRE(opts->max_newton >= 1, "snp_solver_solve: max_newton must be >= 1");
+    SNP_REQUIRE(opts->tol > 0, "snp_solver_solve: tol must be positive");
+    SNP_REQUIRE(opts->precision == 0 || opts->precision == 1, "snp_solver_solve: precision must be 0 or 1");
+    snp_solve_stats tmp;
+    snp_solve_stats &S = stats ? *stats : tmp;
+    return s->solve(x, *opts, S);
+}
+
+int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *J_vals, double *rhs, double *F,
+                        void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_assemble: solver missing or not finalized");
+    SNP_REQUIRE(x != nullptr, "snp_solver_assemble: x is NULL");
+    cudaStream_t keep = s->stream;
+    if (stream) s->stream = snp::as_stream(stream);
+    int rc = s->assemble(x, K_vals, J_vals, nullptr, rhs, F);
+    s->stream = keep;
+    return rc;
+}
+
+int snp_solver_pattern(const snp_solver *s, const snp_pattern **pat) {
+    SNP_REQUIRE(s != nullptr && pat != nullptr && s->finalized, "snp_solver_pattern: solver missing or not finalized");
+    *pat = s->pat;
+    return SNP_OK;
+}
+
+int snp_solver_destroy(snp_solver *s) {
+    delete s;
+    return SNP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+"""``MVPSolver``: total magnetic vector potential with coil currents from Laplace subdomain
+solves (``snoopy/mvp_solver.py``).  ``solve_nonlin`` keeps the reference's Newton loop
+(``mvp_solver.py:222-334``) with every step on the device; the coil source rhs comes from
+``CurlCurlAssembler.compute_rhs_electric_potential`` on the device.
+"""
+
+import numpy as np
+
+from .curl_curl_assembler import CurlCurlAssembler
+from .laplace_subdomain_solver import LaplaceSubdomainSolver
+from .materials import ConstantReluctance
+from .newton import MODE_REFERENCE, MODE_RESIDUAL, DeviceNewton
+
+
+class MVPSolver:
+    """:param gmsh_model: ``TetMesh``; :param coil_terminals: per coil, two terminal node-index arrays."""
+
+    def __init__(self, gmsh_model, coil_tags, iron_tags, air_tags, coil_terminals, reluctances,
+                 max_newton_iterations=25, element_order=1, quad_order=-1):
+        self.coil_sd_solvers = [LaplaceSubdomainSolver(gmsh_model.mesh, ct, coil_terminals[i])
+                                for i, ct in enumerate(coil_tags)]
+        domain_tags = list(coil_tags) + list(iron_tags) + list(air_tags)
+        nu0 = ConstantReluctance(0.25 / np.pi * 1e7)
+        material_properties = [nu0] * len(coil_tags) + list(reluctances) + [nu0] * len(air_tags)
+        self.max_newton_iterations = max_newton_iterations
+        self.element_order = element_order
+        if element_order > 3:
+            print("Error! Element order {} not implemented! Choosing 1.")
+            element_order = 1
+        self.quad_order = element_order + 2 if quad_order < 0 else quad_order
+        self.dirichlet_dofs = gmsh_model.get_edge_boundary_dofs(["Dirichlet Boundary"], element_order)
+        self.curl_curl_factory = CurlCurlAssembler(gmsh_model.mesh, domain_tags, material_properties, element_order)
+        self.num_dofs_mvp = self.curl_curl_factory.num_dofs
+        self.verbose = True
+        self._newton = None
+        self._rhs_key = None
+
+    def get_global_ids(self):
+        return self.curl_curl_factory.global_ids
+
+    def make_boundary_mask(self):
+        mask = np.ones((self.num_dofs_mvp,), dtype=bool)
+        mask[np.asarray(self.dirichlet_dofs, dtype=np.int64) - 1] = False
+        return mask
+
+    def compute_source_rhs(self, phi_list):
+        """rhs_mvp: sum over coils of the rhs from each coil's Laplace potential (``mvp_solver.py:256-271``)."""
+        rhs = np.zeros((self.num_dofs_mvp,))
+        self.sol_sp = []
+        for i, sol in enumerate(self.coil_sd_solvers):
+            self.sol_sp.append(sol.solve(phi_list[i]))
+            rhs += self.curl_curl_factory.compute_rhs_electric_potential(self.sol_sp[-1], quad_order=self.quad_order,
+                                                                         select_mat=[i])
+        return rhs
+
+    def _engine(self, phi_list):
+        key = tuple(float(p) for p in phi_list)
+        if self._newton is None or self._rhs_key != key:
+            rhs_mvp = self.compute_source_rhs(phi_list)
+            self._newton = DeviceNewton(self.curl_curl_factory, self.make_boundary_mask(), (), self.quad_order,
+                                        rhs_extra=rhs_mvp)
+            self._rhs_key = key
+        return self._newton
+
+    def solve_nonlin(self, phi_list, tolerance=1e-4, x_0=np.zeros((0,)), maxiter=-1, apply_gauge=False,
+                     plot_current_density=False):
+        """Newton with the reference's increment test; returns float64[num_dofs] (numpy)."""
+        if apply_gauge:
+            raise NotImplementedError("the tree-cotree gauge (apply_gauge=True) is not implemented")
+        eng = self._engine(phi_list)
+        x0 = None if len(x_0) == 0 else np.asarray(x_0, dtype=np.float64)
+        if self.verbose:
+            print("***********************")
+            print("start Newton iterations")
+        x, stats = eng.solve(x0, mode=MODE_REFERENCE, tol=tolerance, cg_maxiter=maxiter,
+                             max_newton=self.max_newton_iterations, cg_rtol=1e-5, verbose=self.verbose)
+        self.last_stats = stats
+        return x.cpu().numpy()
+
+    def solve_to_residual(self, phi_list, rtol=1e-8, x_0=None, precision="fp64", max_newton=None):
+        eng = self._engine(phi_list)
+        x, stats = eng.solve(x_0, mode=MODE_RESIDUAL, tol=rtol, max_newton=max_newton or self.max_newton_iterations,
+                             precision={"fp64": 0, "mixed": 1}[precision])
+        self.last_stats = stats
+        return x.cpu().numpy(), stats

@@ -1,0 +1,91 @@
+"""Device Newton solver: Python owner of the native ``snp_solver`` handle."""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .device import torch, upload, zeros
+
+MODE_REFERENCE = 0  # increment test + scipy-style CG (red_mvp_solver.py:121-224)
+MODE_RESIDUAL = 1   # ||F_free|| <= tol * ||F_free(x0)||
+
+
+class DeviceNewton:
+    """Newton solver over a ``CurlCurlAssembler``'s materials, Dirichlet mask and source fields.
+
+    Everything (mesh arrays, CSR pattern, Jacobian, work vectors) lives on the device; a
+    solve returns a float64 CUDA tensor.
+    """
+
+    def __init__(self, assembler, free_mask, source_fields=(), quad_order=2, rhs_extra=None, stream=None):
+        _lib.require_cuda()
+        self.assembler = assembler
+        self.n = assembler.num_dofs
+        d = assembler._device_state()
+        tb = assembler.tables(quad_order)
+        self.tables = tb
+        self.free_mask = free_mask if hasattr(free_mask, "data_ptr") else upload(np.asarray(free_mask, dtype=np.uint8), np.uint8)
+        self._stream = stream
+        h = ctypes.c_void_p()
+        _lib.call("snp_solver_create", self.n, _lib.ptr(d["nodes"]), assembler.nodes.shape[0], _lib.ptr(tb.curls_d),
+                  tb.n_orient, _lib.ptr(tb.d_phi_d), _lib.ptr(tb.w_d), tb.nq, _lib.ptr(self.free_mask),
+                  _lib.stream_ptr(stream), ctypes.byref(h))
+        self.handle = h
+        bs = assembler.upload_source_fields(source_fields)
+        for n, m in enumerate(d["mats"]):
+            n_int, rc, rx = d["rel"][n]
+            _lib.call("snp_solver_add_material", self.handle, _lib.ptr(m["cells"]), _lib.ptr(m["gids"]),
+                      _lib.ptr(m["orient"]), m["count"], n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(bs[n]))
+        if rhs_extra is not None:
+            r = rhs_extra if hasattr(rhs_extra, "data_ptr") else upload(rhs_extra, np.float64)
+            _lib.call("snp_solver_set_rhs", self.handle, _lib.ptr(r))
+        _lib.call("snp_solver_finalize", self.handle)
+        p = ctypes.c_void_p()
+        _lib.call("snp_solver_pattern", self.handle, ctypes.byref(p))
+        from .device import Pattern
+
+        self.pattern = Pattern(None, 0, 6, self.n, handle=p, owned=False)
+
+    def solve(self, x0=None, mode=MODE_RESIDUAL, tol=1e-8, cg_maxiter=-1, max_newton=25, cg_rtol=None, precision=0,
+              verbose=False, x_out=None, raise_on_failure=True):
+        """Run Newton from ``x0`` (zeros if None).  Returns (x CUDA tensor, stats dict)."""
+        t = torch()
+        if x_out is None:
+            x = zeros(self.n)[: self.n]
+        else:
+            x = x_out
+        if x0 is not None:
+            src = x0 if hasattr(x0, "data_ptr") else t.from_numpy(np.ascontiguousarray(x0, dtype=np.float64))
+            x.copy_(src.to(x.device, non_blocking=True))
+        else:
+            x.zero_()
+        if cg_rtol is None:
+            cg_rtol = 1e-5 if mode == MODE_REFERENCE else 0.1
+        opts = _lib.SolveOpts(int(mode), float(tol), int(cg_maxiter), int(max_newton), float(cg_rtol), int(precision),
+                              1 if verbose else 0)
+        st = _lib.SolveStats()
+        rc = _lib.load().snp_solver_solve(self.handle, _lib.ptr(x), ctypes.byref(opts), ctypes.byref(st))
+        stats = st.as_dict()
+        stats["rel_res"] = stats["res"] / stats["res0"] if stats["res0"] > 0 else 0.0
+        if rc != 0 and (raise_on_failure or rc not in (3,)):
+            _lib.check(rc)
+        stats["converged"] = rc == 0
+        return x, stats
+
+    def assemble(self, x, K=False, J=True, rhs=False, F=True):
+        x_d = x if hasattr(x, "data_ptr") else upload(x, np.float64)
+        nnz = self.pattern.nnz
+        out = {"K": zeros(nnz) if K else None, "J": zeros(nnz) if J else None, "rhs": zeros(self.n) if rhs else None,
+               "F": zeros(self.n) if F else None}
+        _lib.call("snp_solver_assemble", self.handle, _lib.ptr(x_d), _lib.ptr(out["K"]), _lib.ptr(out["J"]),
+                  _lib.ptr(out["rhs"]), _lib.ptr(out["F"]), _lib.stream_ptr(self._stream))
+        return out
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) is not None and _lib._lib is not None:
+                _lib.load().snp_solver_destroy(self.handle)
+        except Exception:
+            pass
+        self.handle = None

@@ -1,0 +1,147 @@
+"""The CPU oracle (oracle/restated.c + oracle/oracle.py) against the reference.
+
+Pins the restatement to golden vectors produced by the reference's own C kernels
+(tests/golden/make_golden.py), and, where the reference library was compiled here
+(oracle/_ref), to live calls on fresh inputs.
+"""
+
+import numpy as np
+import pytest
+
+import snoopy_b200 as S
+from helpers import golden_materials, abs_contrib, assert_csr_close, assert_same_pattern, csr_from, rel_max
+from snoopy_b200 import finite_element as FE
+from snoopy_b200 import materials as MAT
+from snoopy_b200 import mesh as M
+
+
+@pytest.fixture(scope="module")
+def rel(golden):
+    return golden_materials(golden)[0]
+
+
+@pytest.fixture(scope="module")
+def perm(golden):
+    return golden_materials(golden)[1]
+
+
+def test_golden_inputs_regenerate(golden):
+    from golden.make_golden import golden_inputs
+
+    msh, w, q, dphi, phi, curls, x, iron, air, Bs, xn = golden_inputs()
+    assert np.array_equal(msh.cells, golden["cells"])
+    assert np.array_equal(msh.elem_edges, golden["glob_ids"])
+    assert np.allclose(msh.nodes, golden["nodes"], rtol=0, atol=1e-15)
+    assert np.array_equal(msh.orientations, golden["orientations"])
+
+
+def test_pchip_matches_reference(golden, oracle_mod, rel):
+    nu, dnu = oracle_mod.pchip_eval(rel, golden["pchip_B"], backend="oracle")
+    assert rel_max(nu, golden["pchip_nu"]) < 1e-14
+    assert rel_max(dnu, golden["pchip_dnu"]) < 1e-13
+    # below the first knot (and NaN-free negative input) the law gives 0, as the reference
+    assert nu[-2] == 0.0 and dnu[-2] == 0.0
+
+
+def test_bspline_mu_matches_reference(golden, oracle_mod, perm):
+    mu, dmu = oracle_mod.mu_eval(perm, golden["mu_H"], backend="oracle")
+    np.testing.assert_array_equal(mu, golden["mu_mu"])
+    np.testing.assert_allclose(dmu, golden["mu_dmu"], rtol=1e-14, atol=0)
+
+
+def test_bspline_mu_agrees_with_scipy(oracle_mod):
+    from scipy.interpolate import splev
+
+    perm = MAT.atan_permeability()
+    H = np.logspace(0, 6, 200)
+    H = H[H > perm.H_min]
+    mu, dmu = oracle_mod.mu_eval(perm, H)
+    np.testing.assert_allclose(mu, splev(np.log10(H), perm.spl), rtol=1e-12)
+    np.testing.assert_allclose(dmu, splev(np.log10(H), perm.spl, der=1) / H / np.log(10), rtol=1e-10, atol=1e-30)
+
+
+@pytest.mark.parametrize("name", ["air", "iron_red", "iron_plain"])
+def test_curlcurl_matches_reference(golden, oracle_mod, rel, name):
+    g = golden
+    n = int(g["num_dofs"])
+    el = g["air"] if name == "air" else g["iron"]
+    mat = S.ConstantReluctance(0.25 / np.pi * 1e7) if name == "air" else rel
+    bs = g["B_s"] if name == "iron_red" else np.zeros((0, 3))
+    ti, tj, vK, vdK, rhs = oracle_mod.curl_curl_triplets(g["nodes"], g["cells"][el], g["glob_ids"][el], g["curls"],
+                                                         g["d_phi"], g["orientations"][el], g["x"], bs, mat, g["q"],
+                                                         g["w"], n, 6)
+    from scipy.sparse import csr_array
+
+    K = csr_array((vK, (ti, tj)), shape=(n, n))
+    dK = csr_array((vdK, (ti, tj)), shape=(n, n))
+    assert_csr_close(K, csr_from(g, f"cc_{name}_K", n), 1e-13, abs_contrib(ti, tj, vK, n))
+    assert_csr_close(dK, csr_from(g, f"cc_{name}_dK", n), 1e-13, abs_contrib(ti, tj, vdK, n))
+    ref_rhs = g[f"cc_{name}_rhs"]
+    if name == "iron_red":
+        assert rel_max(rhs, ref_rhs) < 1e-13
+    else:
+        assert not ref_rhs.any() and not rhs.any()
+
+
+def test_rhs_red_matches_reference(golden, oracle_mod, rel):
+    g = golden
+    el = g["iron"]
+    rhs = oracle_mod.compute_rhs_Hcurl_red_c(g["nodes"], g["cells"][el], g["glob_ids"][el], g["curls"], g["d_phi"],
+                                             g["orientations"][el], g["B_s"], rel, g["x"], g["q"], g["w"],
+                                             int(g["num_dofs"]), 6)
+    assert rel_max(rhs, g["rhs_red"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["bspline", "const"])
+def test_gradgrad_matches_reference(golden, oracle_mod, perm, name):
+    g = golden
+    pm = perm if name == "bspline" else S.ConstantPermeability(1.0)
+    n = g["nodes"].shape[0]
+    ti, tj, vK, vdK = oracle_mod.grad_grad_triplets(g["nodes"], g["cells"], g["d_phi"], g["x_nodal"], pm, g["q"], g["w"])
+    from scipy.sparse import csr_array
+
+    assert_csr_close(csr_array((vK, (ti, tj)), shape=(n, n)), csr_from(g, f"gg_{name}_K", n), 1e-13,
+                     abs_contrib(ti, tj, vK, n))
+    assert_csr_close(csr_array((vdK, (ti, tj)), shape=(n, n)), csr_from(g, f"gg_{name}_dK", n), 1e-12,
+                     abs_contrib(ti, tj, vdK, n))
+
+
+def test_b_hcurl_matches_reference(golden, oracle_mod):
+    g = golden
+    pts, B = oracle_mod.compute_B_Hcurl(g["nodes"], g["cells"], g["glob_ids"], g["curls"], g["phi"], g["d_phi"],
+                                        g["orientations"], g["x"], g["q"], g["w"], int(g["num_dofs"]), 6)
+    assert rel_max(pts, g["bq_points"]) < 1e-15
+    assert rel_max(B, g["bq_B"]) < 1e-13
+
+
+def test_biot_savart_matches_reference(golden, oracle_mod):
+    g = golden
+    B = oracle_mod.compute_B_line_segs_cpp(g["bs_src"], g["bs_tar"], float(g["bs_current"]), float(g["bs_rad"]))
+    ref = g["bs_B"]
+    # a target exactly on a filament gives 0/0 in the reference's inner-conductor branch
+    nan = np.isnan(ref)
+    assert nan.any() and np.array_equal(np.isnan(B), nan)
+    assert rel_max(B[~nan], ref[~nan]) < 1e-14
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference C not compiled here")
+def test_restatement_vs_live_reference(oracle_mod, rel):
+    """Fresh seeded inputs through both backends (reduced kernel, 5-point rule with a negative weight)."""
+    msh = M.window_frame_mesh(3000, jitter=0.2, seed=99)
+    w, q = FE.quadrature_rule(3)
+    dphi = FE.evaluate_basis_derivative(q)
+    curls, _ = FE.curl_edge_basis_functions(q)
+    rng = np.random.default_rng(5)
+    x = rng.normal(0, 5e-3, msh.num_dofs)
+    el = msh.domain_elements(M.TAG_IRON)
+    Bs = rng.normal(0, 1.0, (len(el) * len(w), 3))
+    n = msh.num_dofs
+    a = oracle_mod.compute_stiffness_and_jacobi_matrix_curl_curl(msh.nodes, msh.cells[el], msh.elem_edges[el], curls,
+                                                                 dphi, msh.orientations[el], x, Bs, rel, q, w, n, 6)
+    b = oracle_mod.compute_stiffness_and_jacobi_matrix_curl_curl(msh.nodes, msh.cells[el], msh.elem_edges[el], curls,
+                                                                 dphi, msh.orientations[el], x, Bs, rel, q, w, n, 6,
+                                                                 backend="ref")
+    assert_same_pattern(a[0], b[0])
+    assert_csr_close(a[0], b[0], 1e-12, atol_rel=1e-15)
+    assert_csr_close(a[1], b[1], 1e-12, atol_rel=1e-15)
+    assert rel_max(a[2], b[2]) < 1e-13
