@@ -211,6 +211,7 @@ typedef struct {
     double cg_rtol;          /* mode 0: scipy default 1e-5; mode 1: cap of the adaptive forcing term */
     int32_t precision;       /* 0: float64 throughout; 1: float32 Jacobian + Krylov inside float64 Newton */
     int32_t verbose;         /* print one line per Newton step to stdout */
+    int32_t line_search;     /* mode 1: Armijo backtracking on ||F_free|| (quadratic interpolation, factor in [0.1, 0.5]) */
 } snp_solve_opts;
 
 /* Solve statistics (host struct). */
@@ -222,6 +223,7 @@ typedef struct {
     double t_assemble_ms, t_krylov_ms, t_total_ms;
     int32_t status;
     int64_t kernel_launches;     /* this library's kernels launched by the solve (graph nodes counted per execution) */
+    int32_t residual_evals;      /* extra residual-only assemblies of the line search */
 } snp_solve_stats;
 
 /* x[n_dofs] (device): in = initial guess, out = solution.  Synchronises. */

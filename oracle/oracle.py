@@ -118,7 +118,7 @@ def lib(backend="oracle"):
                             ctypes.c_double, ctypes.c_double, _dp]
         L.or_curlcurl.restype = _i64
         L.or_curlcurl.argtypes = [_i64, ctypes.c_int, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp,
-                                  ctypes.c_int, _dp, _dp, _ip, _ip, _dp, _dp, _dp]
+                                  ctypes.c_int, _dp, _dp, _ip, _ip, _dp, _dp, _dp, _dp, _dp]
         L.or_rhs_red.restype = ctypes.c_int
         L.or_rhs_red.argtypes = [_i64, ctypes.c_int, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp,
                                  ctypes.c_int, _dp, _dp, _dp]
@@ -126,7 +126,8 @@ def lib(backend="oracle"):
         L.or_B_hcurl.argtypes = [_i64, ctypes.c_int, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp]
         L.or_gradgrad.restype = _i64
         L.or_gradgrad.argtypes = [_i64, ctypes.c_int, _dp, _ip, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
-                                  ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double, _ip, _ip, _dp, _dp]
+                                  ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double, _ip, _ip, _dp, _dp, _dp,
+                                  _dp]
         L.or_biot_savart.restype = None
         L.or_biot_savart.argtypes = [_dp, _i64, _dp, _i64, ctypes.c_double, ctypes.c_double, _dp]
     elif backend == "ref":
@@ -230,8 +231,11 @@ def mu_eval(permeability, H, backend="oracle"):
 # ------------------------------------------------------------------ fem_c_mod restatement
 
 def curl_curl_triplets(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_s, reluctance, q, w,
-                       num_dofs, num_el_dofs, backend="oracle"):
-    """Triplets (i, j, vK, vdK) and rhs of one material, as the C kernels emit them."""
+                       num_dofs, num_el_dofs, backend="oracle", scales=None):
+    """Triplets (i, j, vK, vdK) and rhs of one material, as the C kernels emit them.
+
+    ``scales``: an optional dict that receives "K" and "dK", the per-triplet sums of term
+    magnitudes (restatement only), the scale of any evaluation order's rounding error."""
     if num_el_dofs != 6:
         raise ValueError("only first-order edge elements (6 DoFs) are supported")
     nodes_c, cells_c, gid_c = _f64(nodes), _i32(cells), _i32(glob_ids)
@@ -250,9 +254,14 @@ def curl_curl_triplets(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_
     L = lib(backend)
     if backend == "oracle":
         bs_ptr = _d(Bs_c) if len(Bs_c) > 0 else None
+        sK = np.empty(nt) if scales is not None else None
+        sdK = np.empty(nt) if scales is not None else None
         got = L.or_curlcurl(E, Q, _d(nodes_c), _i(cells_c), _i(gid_c), _i(or_c), _d(curls_c), _d(dphi_c),
-                            _d(w_c), _d(x_c), bs_ptr, n_int, _d(rc), _d(rx), _i(ti), _i(tj), _d(vK), _d(vdK), _d(rhs))
+                            _d(w_c), _d(x_c), bs_ptr, n_int, _d(rc), _d(rx), _i(ti), _i(tj), _d(vK), _d(vdK), _d(rhs),
+                            _d(sK) if sK is not None else None, _d(sdK) if sdK is not None else None)
         assert got == nt, got
+        if scales is not None:
+            scales["K"], scales["dK"] = sK, sdK
     else:
         tK = _Triplets(0, _i(ti), _i(tj), _d(vK), nt)
         ti2 = np.empty(nt, dtype=np.int32)
@@ -325,7 +334,7 @@ def compute_B_Hcurl(nodes, cells, glob_ids, curls, phi, d_phi, orientations, x, 
     return pts.reshape(-1, 3), B.reshape(-1, 3)
 
 
-def grad_grad_triplets(nodes, cells, d_phi, x, permeability, q, w, backend="oracle"):
+def grad_grad_triplets(nodes, cells, d_phi, x, permeability, q, w, backend="oracle", scales=None):
     nodes_c, cells_c, dphi_c, x_c, q_c, w_c = _f64(nodes), _i32(cells), _f64(d_phi), _f64(x), _f64(q), _f64(w)
     E, Q = len(cells_c) // 4, len(w_c)
     nt = E * 16
@@ -336,9 +345,14 @@ def grad_grad_triplets(nodes, cells, d_phi, x, permeability, q, w, backend="orac
     typ, k, n, t, c, hmin, muhmin = permeability_arrays(permeability)
     L = lib(backend)
     if backend == "oracle":
+        sK = np.empty(nt) if scales is not None else None
+        sdK = np.empty(nt) if scales is not None else None
         got = L.or_gradgrad(E, Q, _d(nodes_c), _i(cells_c), _d(dphi_c), _d(w_c), _d(x_c), typ, k, n, _d(t), _d(c),
-                            hmin, muhmin, _i(ti), _i(tj), _d(vK), _d(vdK))
+                            hmin, muhmin, _i(ti), _i(tj), _d(vK), _d(vdK), _d(sK) if sK is not None else None,
+                            _d(sdK) if sdK is not None else None)
         assert got == nt
+        if scales is not None:
+            scales["K"], scales["dK"] = sK, sdK
     else:
         tK = _Triplets(0, _i(ti), _i(tj), _d(vK), nt)
         ti2 = np.empty(nt, dtype=np.int32)
@@ -422,6 +436,22 @@ class OracleCurlCurlAssembler:
         self.timings["csr"] += time.perf_counter() - t1
         return K, J, rhs
 
+    def scales(self, x, source_fields=()):
+        """Per-entry sums of term magnitudes of K and of J = K + dK (comparison scales)."""
+        n = self.num_dofs
+        sK = csr_array((n, n))
+        sJ = csr_array((n, n))
+        use_sf = len(source_fields) == len(self.materials)
+        for m, mat in enumerate(self.materials):
+            B_s = source_fields[m] if use_sf and len(source_fields[m]) > 0 else np.zeros((0, 3))
+            sc = {}
+            ti, tj, _, _, _ = curl_curl_triplets(self.nodes, mat["cells"], mat["glob_ids"], self.curls, self.d_phi,
+                                                 mat["orientations"], x, B_s, mat["reluctance"], self.q, self.w, n, 6,
+                                                 "oracle", scales=sc)
+            sK = sK + csr_array((sc["K"], (ti, tj)), shape=(n, n))
+            sJ = sJ + csr_array((sc["K"] + sc["dK"], (ti, tj)), shape=(n, n))
+        return sK, sJ
+
 
 class OracleGradGradAssembler:
     """``GradGradAssembler.compute_stiffness_and_jacobi_matrix_c`` (``matrix_assembly.py:1059-1135``)."""
@@ -443,6 +473,20 @@ class OracleGradGradAssembler:
             dK += my_dK
             dK += K
         return K, dK
+
+    def scales(self, x, mu_list):
+        """Comparison scales of K and of the returned J (with the reference's per-material
+        ``dK += K``, J sums the running K after every material)."""
+        n = self.nodes.shape[0]
+        sK = csr_array((n, n))
+        sJ = csr_array((n, n))
+        for m, perm in enumerate(mu_list):
+            sc = {}
+            ti, tj, _, _ = grad_grad_triplets(self.nodes, self.cells_list[m], self.d_phi, x, perm, self.q, self.w,
+                                              "oracle", scales=sc)
+            sK = sK + csr_array((sc["K"], (ti, tj)), shape=(n, n))
+            sJ = sJ + csr_array((sc["dK"], (ti, tj)), shape=(n, n)) + sK
+        return sK, sJ
 
 
 # ------------------------------------------------------------------ Newton loops
@@ -505,25 +549,35 @@ def ew_forcing(it, fn, fprev, eta_prev, F0, tol, eta_max=0.1, fp32=False):
 
 
 def newton_residual(assembler, mask, source_fields=(), rtol=1e-8, x_0=None, cg_rtol=1e-12, cg_maxiter=None,
-                    max_newton_iterations=50, verbose=False, forcing="fixed"):
+                    max_newton_iterations=50, verbose=False, forcing="fixed", line_search=False):
     """Newton on F(x) = K(x) x - rhs(x) until ||F_free|| <= rtol ||F_free(x_0)||.
 
     Each step solves J_free h = -F_free with Jacobi-preconditioned scipy CG to the
     relative tolerance ``cg_rtol``, but never below the absolute level 0.1 * rtol * ||F_free(x_0)||:
     the curl-curl Jacobian is singular (gradients), and rounding in F leaves a small
     inconsistent component that a CG asked for more drives along that null space.
-    Returns x and stats (residual history, CG counts).
+    With ``line_search`` the step is damped by Armijo backtracking on ||F_free||: from alpha = 1,
+    each rejected alpha is replaced by the minimiser of the quadratic model of ||F||^2 along h,
+    kept within [0.1, 0.5] alpha, until ||F(x + alpha h)|| <= (1 - 1e-4 alpha) ||F(x)|| (at most
+    30 reductions).  ``forcing="ew"`` uses the device solver's inner tolerances (``ew_forcing``).
+    Returns x and stats (residual history, CG counts, step lengths).
     """
     n = assembler.num_dofs
     x = np.zeros(n) if x_0 is None or len(x_0) == 0 else np.array(x_0, dtype=np.float64)
     x[~mask] = 0.0
-    stats = {"newton": 0, "cg": [], "res": [], "eta": []}
+    stats = {"newton": 0, "cg": [], "res": [], "eta": [], "alpha": [], "assemblies": 0}
     F0 = None
     fprev = eta_prev = 0.0
+    cached = None
     for i in range(max_newton_iterations + 1):
-        K, J, rhs = assembler.compute_stiffness_and_jacobi_matrix_c(x, source_fields)
-        F = K @ x - rhs
-        fn = np.linalg.norm(F[mask])
+        if cached is None:
+            K, J, rhs = assembler.compute_stiffness_and_jacobi_matrix_c(x, source_fields)
+            stats["assemblies"] += 1
+            F = K @ x - rhs
+            fn = np.linalg.norm(F[mask])
+        else:
+            K, J, rhs, F, fn = cached
+            cached = None
         if F0 is None:
             F0 = fn
         stats["res"].append(fn)
@@ -546,7 +600,54 @@ def newton_residual(assembler, mask, source_fields=(), rtol=1e-8, x_0=None, cg_r
         else:
             h, _ = cg(J_c, -F[mask], rtol=cg_rtol, atol=0.1 * rtol * F0, M=M, callback=cb, maxiter=cg_maxiter)
         stats["cg"].append(its[0])
-        x[mask] += h
+        if line_search == "energy":
+            # F is the gradient of the magnetic energy W (convex for a monotone B-H law), so
+            # phi'(a) = F(x + a h) . h increases along h: accept the full step when
+            # phi'(1) <= 0.5 |phi'(0)|, else find phi'(a) ~ 0 by a safeguarded secant
+            g0 = float(F[mask] @ h)
+            a_lo, g_lo, a_hi, g_hi = 0.0, g0, None, None
+            alpha = 1.0
+            for ls in range(12):
+                xt = x.copy()
+                xt[mask] += alpha * h
+                Kt, Jt, rt = assembler.compute_stiffness_and_jacobi_matrix_c(xt, source_fields)
+                stats["assemblies"] += 1
+                Ft = Kt @ xt - rt
+                g = float(Ft[mask] @ h)
+                if g <= 0.5 * abs(g0) or ls == 11:
+                    break
+                a_hi, g_hi = alpha, g
+                a_new = a_lo - g_lo * (a_hi - a_lo) / (g_hi - g_lo)
+                width = a_hi - a_lo
+                alpha = min(max(a_new, a_lo + 0.01 * width), a_hi - 0.01 * width)
+            ft = np.linalg.norm(Ft[mask])
+            x = xt
+            cached = (Kt, Jt, rt, Ft, ft)
+            stats["alpha"].append(alpha)
+        elif line_search:
+            alpha = 1.0
+            for ls in range(31):
+                xt = x.copy()
+                xt[mask] += alpha * h
+                Kt, Jt, rt = assembler.compute_stiffness_and_jacobi_matrix_c(xt, source_fields)
+                stats["assemblies"] += 1
+                Ft = Kt @ xt - rt
+                ft = np.linalg.norm(Ft[mask])
+                if (ft == ft and ft <= (1.0 - 1e-4 * alpha) * fn) or ls >= 30:
+                    break
+                # minimiser of the quadratic through phi(0) = fn^2, phi'(0) = -2 fn^2, phi(alpha) = ft^2,
+                # kept within [0.1, 0.5] alpha (the device solver's rule)
+                a_new = 0.5 * alpha
+                if ft == ft:
+                    den = ft * ft - fn * fn + 2.0 * fn * fn * alpha
+                    if den > 0:
+                        a_new = fn * fn * alpha * alpha / den
+                alpha = min(max(a_new, 0.1 * alpha), 0.5 * alpha)
+            x = xt
+            cached = (Kt, Jt, rt, Ft, ft)
+            stats["alpha"].append(alpha)
+        else:
+            x[mask] += h
         stats["newton"] = i + 1
     stats["rel_res"] = stats["res"][-1] / F0 if F0 else 0.0
     return x, stats

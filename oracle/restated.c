@@ -166,11 +166,15 @@ static double or_dot(const double *a, const double *b) { return a[0] * b[0] + a[
  * (j <= k, mirrored when j != k) into ti/tj/vK/vdK in the reference's order.
  * B_s == NULL: plain kernel (ctools.c:960-1193); otherwise reduced kernel with the
  * source field B_s[E][Q][3] and rhs accumulation (ctools.c:1195-1388).
+ * sK/sdK (optional) receive, per triplet, the sum of the magnitudes of the terms that make
+ * it up (|nu| |cu| |cv| |w| / |det| and |nu'| |cu| |cv| |B| |w| / |det|): the scale of the
+ * rounding error any evaluation order makes, used as the comparison scale in the tests.
  * Returns the number of triplets written, or -1 on a bad argument. */
 int64_t or_curlcurl(int64_t E, int Q, const double *nodes, const int *cells, const int *glob_ids,
                     const int *orient, const double *curls, const double *dphi, const double *w,
                     const double *x, const double *B_s, int n_int, const double *rel_c,
-                    const double *rel_x, int *ti, int *tj, double *vK, double *vdK, double *rhs)
+                    const double *rel_x, int *ti, int *tj, double *vK, double *vdK, double *rhs,
+                    double *sK, double *sdK)
 {
     if (Q <= 0 || Q > OR_MAXQ) return -1;
     const double nu0 = 1.0 / 4.0 / M_PI * 1e7;
@@ -196,21 +200,28 @@ int64_t or_curlcurl(int64_t E, int Q, const double *nodes, const int *cells, con
         }
         for (int j = 0; j < 6; ++j) {
             for (int k = j; k < 6; ++k) {
-                double sK = 0.0, sdK = 0.0;
+                double aK = 0.0, adK = 0.0, mK = 0.0, mdK = 0.0;
                 for (int q = 0; q < Q; ++q) {
                     double cu[3], cv[3];
                     or_mv(J[q], ct + 3 * (q * 6 + j), cu);
                     or_mv(J[q], ct + 3 * (q * 6 + k), cv);
-                    sK += nu[q] * or_dot(cu, cv) * w[q] / det[q];
+                    aK += nu[q] * or_dot(cu, cv) * w[q] / det[q];
+                    double nn = sqrt(or_dot(cu, cu) * or_dot(cv, cv)) * fabs(w[q] / det[q]);
+                    mK += fabs(nu[q]) * nn;
                     if (Bm[q] >= 1e-14) {
                         double pu = or_dot(cu, B[q]), pv = or_dot(cv, B[q]);
-                        sdK += dnu[q] * pu * pv * w[q] / det[q] / Bm[q];
+                        adK += dnu[q] * pu * pv * w[q] / det[q] / Bm[q];
+                        mdK += fabs(dnu[q]) * nn * Bm[q];
                     }
                     if (B_s && j == k) rhs[g[j]] += (nu0 - nu[q]) * or_dot(cu, B_s + (e * Q + q) * 3) * w[q];
                 }
-                ti[cnt] = g[j]; tj[cnt] = g[k]; vK[cnt] = sK; vdK[cnt] = sdK; ++cnt;
+                ti[cnt] = g[j]; tj[cnt] = g[k]; vK[cnt] = aK; vdK[cnt] = adK;
+                if (sK) { sK[cnt] = mK; sdK[cnt] = mdK; }
+                ++cnt;
                 if (j != k) {
-                    ti[cnt] = g[k]; tj[cnt] = g[j]; vK[cnt] = sK; vdK[cnt] = sdK; ++cnt;
+                    ti[cnt] = g[k]; tj[cnt] = g[j]; vK[cnt] = aK; vdK[cnt] = adK;
+                    if (sK) { sK[cnt] = mK; sdK[cnt] = mdK; }
+                    ++cnt;
                 }
             }
         }
@@ -292,7 +303,7 @@ int or_B_hcurl(int64_t E, int Q, const double *nodes, const int *cells, const in
 int64_t or_gradgrad(int64_t E, int Q, const double *nodes, const int *cells, const double *dphi,
                     const double *w, const double *x, int type, int k_deg, int n_ctrl,
                     const double *t, const double *c, double H_min, double mu_H_min, int *ti,
-                    int *tj, double *vK, double *vdK)
+                    int *tj, double *vK, double *vdK, double *sK, double *sdK)
 {
     if (Q <= 0 || Q > OR_MAXQ) return -1;
     double J[9], Ji[OR_MAXQ][9], det[OR_MAXQ], H[OR_MAXQ][3], Hm[OR_MAXQ], mu[OR_MAXQ], dmu[OR_MAXQ];
@@ -311,17 +322,26 @@ int64_t or_gradgrad(int64_t E, int Q, const double *nodes, const int *cells, con
         }
         for (int a = 0; a < 4; ++a) {
             for (int b = a; b < 4; ++b) {
-                double sK = 0.0, sdK = 0.0;
+                double aK = 0.0, adK = 0.0, mK = 0.0, mdK = 0.0;
                 for (int q = 0; q < Q; ++q) {
                     double gu[3], gv[3];
                     or_mtv(Ji[q], dphi + 12 * q + 3 * a, gu);
                     or_mtv(Ji[q], dphi + 12 * q + 3 * b, gv);
-                    sK += mu[q] * det[q] * w[q] * or_dot(gu, gv);
-                    if (Hm[q] >= 1e-14) sdK += dmu[q] * det[q] * w[q] * or_dot(gu, H[q]) * or_dot(gv, H[q]) / Hm[q];
+                    aK += mu[q] * det[q] * w[q] * or_dot(gu, gv);
+                    double nn = sqrt(or_dot(gu, gu) * or_dot(gv, gv)) * fabs(det[q] * w[q]);
+                    mK += fabs(mu[q]) * nn;
+                    if (Hm[q] >= 1e-14) {
+                        adK += dmu[q] * det[q] * w[q] * or_dot(gu, H[q]) * or_dot(gv, H[q]) / Hm[q];
+                        mdK += fabs(dmu[q]) * nn * Hm[q];
+                    }
                 }
-                ti[cnt] = cell[a]; tj[cnt] = cell[b]; vK[cnt] = sK; vdK[cnt] = sdK; ++cnt;
+                ti[cnt] = cell[a]; tj[cnt] = cell[b]; vK[cnt] = aK; vdK[cnt] = adK;
+                if (sK) { sK[cnt] = mK; sdK[cnt] = mdK; }
+                ++cnt;
                 if (a != b) {
-                    ti[cnt] = cell[b]; tj[cnt] = cell[a]; vK[cnt] = sK; vdK[cnt] = sdK; ++cnt;
+                    ti[cnt] = cell[b]; tj[cnt] = cell[a]; vK[cnt] = aK; vdK[cnt] = adK;
+                    if (sK) { sK[cnt] = mK; sdK[cnt] = mdK; }
+                    ++cnt;
                 }
             }
         }

@@ -31,13 +31,13 @@ STATUS = {0: "SNP_OK", 1: "SNP_BAD_ARG", 2: "SNP_CUDA_ERROR", 3: "SNP_NOT_CONVER
 
 class SolveOpts(ctypes.Structure):
     _fields_ = [("mode", _c_i32), ("tol", _c_f64), ("cg_maxiter", _c_i64), ("max_newton", _c_i32),
-                ("cg_rtol", _c_f64), ("precision", _c_i32), ("verbose", _c_i32)]
+                ("cg_rtol", _c_f64), ("precision", _c_i32), ("verbose", _c_i32), ("line_search", _c_i32)]
 
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("newton_iterations", _c_i32), ("cg_iterations", _c_i64), ("res0", _c_f64), ("res", _c_f64),
                 ("t_assemble_ms", _c_f64), ("t_krylov_ms", _c_f64), ("t_total_ms", _c_f64), ("status", _c_i32),
-                ("kernel_launches", _c_i64)]
+                ("kernel_launches", _c_i64), ("residual_evals", _c_i32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -88,6 +88,27 @@ __global__ void k_vstats(int32_t n, const uint8_t *__restrict__ fm, const double
     }
 }
 
+__global__ void k_vdot(int32_t n, const uint8_t *__restrict__ fm, const double *__restrict__ a,
+                       const double *__restrict__ b, double *part, unsigned int *counter, double *res) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (fm[i]) s += a[i] * b[i];
+    s = block_sum(s, sh);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s;
+        __threadfence();
+        last = atomicInc(counter, gridDim.x - 1) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        double t = 0.0;
+        for (unsigned int k = 0; k < gridDim.x; ++k) t += __ldcg(part + k);
+        res[0] = t;
+    }
+}
+
 __global__ void k_sub(int32_t n, double *__restrict__ b, const double *__restrict__ F) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] -= F[i];
 }
@@ -110,6 +131,18 @@ __global__ void k_add_free(int32_t n, const uint8_t *__restrict__ fm, double *__
 __global__ void k_add_free_f32(int32_t n, const uint8_t *__restrict__ fm, double *__restrict__ x, const float *__restrict__ h) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         if (fm[i]) x[i] += (double)h[i];
+}
+
+// y = x + alpha h on free rows, y = x elsewhere
+__global__ void k_axpy_free(int32_t n, const uint8_t *__restrict__ fm, const double *__restrict__ x,
+                            const double *__restrict__ h, double alpha, double *__restrict__ y) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = fm[i] ? x[i] + alpha * h[i] : x[i];
+}
+
+__global__ void k_f32_to_f64(int32_t n, const float *__restrict__ a, double *__restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
 }
 
 __global__ void k_zero_nonfree(int32_t n, const uint8_t *__restrict__ fm, double *__restrict__ x) {
@@ -168,6 +201,18 @@ struct snp_solver {
         SNP_CUDA_TRY(cudaMemcpyAsync(hres.p, res.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
         SNP_CUDA_TRY(cudaStreamSynchronize(stream));
         for (int k = 0; k < 3; ++k) out[k] = hres.p[k];
+        return SNP_OK;
+    }
+
+    // sum over free i of a[i] * b[i] (deterministic, read back)
+    int vdot(const double *a, const double *bb, double *out) {
+        const int grid = snp::stride_grid(n, snp::kVB, 4);
+        snp::k_vdot<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, a, bb, part.p, counter.p, res.p);
+        SNP_LAUNCH_CHECK();
+        ++launches;
+        SNP_CUDA_TRY(cudaMemcpyAsync(hres.p, res.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        SNP_CUDA_TRY(cudaStreamSynchronize(stream));
+        *out = hres.p[0];
         return SNP_OK;
     }
 
@@ -274,28 +319,26 @@ struct snp_solver {
                 if (st3[2] < o.tol * st3[1]) break;
             }
         } else if (o.mode == 1) {
+            // Newton on F(x) = K(x) x - rhs(x).  Every assembly produces the Jacobian and F at
+            // once, so an accepted (trial) point already carries the next step's system.
             double F0 = 0.0, fprev = 0.0, eta_prev = 0.0;
             double eta_max = o.cg_rtol > 0 ? o.cg_rtol : 0.1;
             if (eta_max > 0.5) eta_max = 0.5;
+            const bool f32 = o.precision == 1;
             snp::k_zero_nonfree<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x);
             SNP_LAUNCH_CHECK();
             ++launches;
-            for (int it = 0; it <= o.max_newton; ++it) {
-                SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
-                if (o.precision == 1) {
-                    SNP_TRY(assemble(x, nullptr, nullptr, J32.p, nullptr, F.p));
-                } else {
-                    SNP_TRY(assemble(x, nullptr, J.p, nullptr, nullptr, F.p));
-                }
-                SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
-                SNP_TRY(vstats(F.p, nullptr, true, st3));
-                S.t_assemble_ms += elapsed(0, 1);
-                const double fn = std::sqrt(st3[0]);
+            SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+            SNP_TRY(assemble(x, nullptr, f32 ? nullptr : J.p, f32 ? J32.p : nullptr, nullptr, F.p));
+            SNP_TRY(vstats(F.p, nullptr, true, st3));
+            SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+            SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
+            S.t_assemble_ms += elapsed(0, 1);
+            double fn = std::sqrt(st3[0]);
+            F0 = fn;
+            S.res0 = fn;
+            for (int it = 0;; ++it) {
                 if (!(fn == fn)) return snp::fail(SNP_NAN_DETECTED, "Newton step %d: non-finite residual", it);
-                if (it == 0) {
-                    F0 = fn;
-                    S.res0 = fn;
-                }
                 S.res = fn;
                 if (o.verbose) printf("  newton %d: |F| = %.6e (rel %.3e)\n", it, fn, F0 > 0 ? fn / F0 : 0.0);
                 if (F0 == 0.0 || fn <= o.tol * F0) break;
@@ -314,7 +357,7 @@ struct snp_solver {
                 }
                 const double floor_eta = 0.5 * o.tol * F0 / fn;
                 if (eta < floor_eta) eta = floor_eta;
-                if (o.precision == 1 && eta < 1e-6) eta = 1e-6;
+                if (f32 && eta < 1e-6) eta = 1e-6;
                 if (eta > 0.5) eta = 0.5;
                 fprev = fn;
                 eta_prev = eta;
@@ -323,30 +366,61 @@ struct snp_solver {
                 int st = SNP_OK;
                 bool zp = false;
                 SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
-                if (o.precision == 1) {
+                if (f32) {
                     SNP_TRY(pcg32.set_jacobi(A32, pat->diag_pos.p, free_mask.p, stream, &zp));
                     if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
                     snp::k_neg_free_f32<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, F.p, b32.p);
                     SNP_LAUNCH_CHECK();
                     SNP_TRY(pcg32.solve(A32, free_mask.p, b32.p, h32.p, eta, 0.0, cg_maxit, true, stream, &its, &rn, &st));
-                    snp::k_add_free_f32<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x, h32.p);
+                    snp::k_f32_to_f64<<<grid, snp::kVB, 0, stream>>>(n, h32.p, h.p);
+                    SNP_LAUNCH_CHECK();
+                    launches += 2;
                 } else {
                     SNP_TRY(pcg64.set_jacobi(A, pat->diag_pos.p, free_mask.p, stream, &zp));
                     if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
                     snp::k_neg_free<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, F.p, b.p);
                     SNP_LAUNCH_CHECK();
                     SNP_TRY(pcg64.solve(A, free_mask.p, b.p, h.p, eta, 0.0, cg_maxit, true, stream, &its, &rn, &st));
-                    snp::k_add_free<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x, h.p);
+                    launches += 1;
                 }
-                SNP_LAUNCH_CHECK();
-                launches += 2;  // -F and the update
                 SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
                 SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
                 S.t_krylov_ms += elapsed(0, 1);
                 if (st == SNP_NAN_DETECTED) return snp::fail(st, "Newton step %d: non-finite CG residual", it);
                 S.cg_iterations += its;
                 S.newton_iterations = it + 1;
-                if (o.verbose) printf("    cg: eta %.2e, %lld its\n", eta, (long long)its);
+                // step length: the full step, or (line search) the point along h where the
+                // energy's slope phi'(a) = F(x + a h) . h has fallen to 0.5 |phi'(0)|; F is
+                // the gradient of the magnetic energy, convex for a monotone B-H law, so
+                // phi' increases along h and a safeguarded secant brackets the step
+                double alpha = 1.0, g0 = 0.0, a_lo = 0.0, g_lo = 0.0;
+                SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+                if (o.line_search) {
+                    SNP_TRY(vdot(F.p, h.p, &g0));
+                    g_lo = g0;
+                }
+                for (int ls = 0;; ++ls) {
+                    snp::k_axpy_free<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x, h.p, alpha, xw.p);
+                    SNP_LAUNCH_CHECK();
+                    ++launches;
+                    SNP_TRY(assemble(xw.p, nullptr, f32 ? nullptr : J.p, f32 ? J32.p : nullptr, nullptr, F.p));
+                    if (ls > 0) S.residual_evals += 1;
+                    if (!o.line_search) break;
+                    double g = 0.0;
+                    SNP_TRY(vdot(F.p, h.p, &g));
+                    if (!(g > 0.5 * std::fabs(g0)) || ls >= 11) break;
+                    const double a_hi = alpha, g_hi = g;
+                    const double a_new = a_lo - g_lo * (a_hi - a_lo) / (g_hi - g_lo);
+                    const double width = a_hi - a_lo;
+                    alpha = std::fmin(std::fmax(a_new, a_lo + 0.01 * width), a_hi - 0.01 * width);
+                }
+                SNP_CUDA_TRY(cudaMemcpyAsync(x, xw.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+                SNP_TRY(vstats(F.p, nullptr, true, st3));
+                SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
+                S.t_assemble_ms += elapsed(0, 1);
+                fn = std::sqrt(st3[0]);
+                if (o.verbose) printf("    cg: eta %.2e, %lld its, step %.3e\n", eta, (long long)its, alpha);
             }
         } else {
             return snp::fail(SNP_BAD_ARG, "unknown solve mode %d", o.mode);

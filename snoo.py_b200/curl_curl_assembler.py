@@ -213,8 +213,12 @@ class CurlCurlAssembler:
         elements = np.asarray(elements, dtype=np.int64)
         x_d = x if hasattr(x, "data_ptr") else upload(x, np.float64)
         B = zeros(3 * len(elements))
-        _lib.call("snp_b_at_elements", len(elements), _lib.ptr(upload(elements, np.int32)), _lib.ptr(d["nodes"]),
-                  _lib.ptr(upload(self.mesh.cells, np.int32)), _lib.ptr(upload(self.mesh.elem_edges, np.int32)),
-                  _lib.ptr(upload(self.mesh.orientations, np.int32)), _lib.ptr(tb.curls_d), tb.n_orient,
-                  _lib.ptr(tb.d_phi_d), tb.nq, _lib.ptr(x_d), _lib.ptr(B), _lib.stream_ptr())
+        if "all" not in d:
+            d["all"] = (upload(self.mesh.cells, np.int32), upload(self.mesh.elem_edges, np.int32),
+                        upload(self.mesh.orientations, np.int32))
+        cells_d, gids_d, or_d = d["all"]
+        el_d = upload(elements, np.int32)
+        _lib.call("snp_b_at_elements", len(elements), _lib.ptr(el_d), _lib.ptr(d["nodes"]), _lib.ptr(cells_d),
+                  _lib.ptr(gids_d), _lib.ptr(or_d), _lib.ptr(tb.curls_d), tb.n_orient, _lib.ptr(tb.d_phi_d), tb.nq,
+                  _lib.ptr(x_d), _lib.ptr(B), _lib.stream_ptr())
         return B[: 3 * len(elements)].cpu().numpy().reshape(-1, 3)

@@ -22,6 +22,23 @@ def _n_quad(w):
     return int(np.asarray(w).reshape(-1).shape[0])
 
 
+def _check_range(name, a, hi):
+    """Indices that the kernels gather with must lie in [0, hi); checked on the host."""
+    a = np.asarray(a)
+    if a.size and (a.min() < 0 or a.max() >= hi):
+        raise ValueError(f"{name} holds indices outside [0, {hi})")
+
+
+def _check_mesh(nodes, cells, glob_ids=None, num_dofs=None, orientations=None, n_orient=None):
+    _check_range("cells", cells, np.asarray(nodes).reshape(-1, 3).shape[0])
+    if glob_ids is not None:
+        _check_range("glob_ids", glob_ids, int(num_dofs))
+    if orientations is not None:
+        _check_range("orientations", orientations, int(n_orient))
+        if np.asarray(orientations).size * 6 != np.asarray(glob_ids).size:
+            raise ValueError("one orientation and six glob_ids per element are required")
+
+
 def compute_stiffness_and_jacobi_matrix(nodes, cells, d_phi, x, permeability, q, w):
     """Grad-grad stiffness matrix and Jacobian of the scalar potential (``interface_c.pyx:11-160``).
 
@@ -35,15 +52,18 @@ def compute_stiffness_and_jacobi_matrix(nodes, cells, d_phi, x, permeability, q,
         raise ValueError("only 4-node tetrahedra are supported")
     nq = _n_quad(w)
     check_affine(np.zeros((1, nq, 6, 3)), d_phi, nq)
+    _check_mesh(nodes, cells)
     cells_d = upload(cells, np.int32)
     num_el = cells_d.numel() // el_nodes
     pat = Pattern(cells_d, num_el, 4, num_nodes)
     typ, k, n, t, c, hmin, muh = permeability_tables(permeability)
     K = zeros(pat.nnz)
     dK = zeros(pat.nnz)
-    _lib.call("snp_gradgrad_assemble", pat.handle, 0, num_el, _lib.ptr(upload(nodes, np.float64)), _lib.ptr(cells_d),
-              _lib.ptr(upload(d_phi, np.float64)), _lib.ptr(upload(w, np.float64)), nq,
-              _lib.ptr(upload(x, np.float64)), typ, k, n, _lib.ptr(t), _lib.ptr(c), hmin, muh, _lib.ptr(K),
+    # every device buffer stays referenced until after the launch (freed blocks are reused)
+    nodes_d, dphi_d, w_d, x_d = (upload(nodes, np.float64), upload(d_phi, np.float64), upload(w, np.float64),
+                                 upload(x, np.float64))
+    _lib.call("snp_gradgrad_assemble", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d), _lib.ptr(dphi_d),
+              _lib.ptr(w_d), nq, _lib.ptr(x_d), typ, k, n, _lib.ptr(t), _lib.ptr(c), hmin, muh, _lib.ptr(K),
               _lib.ptr(dK), None, _lib.stream_ptr())
     return pat.to_scipy(K), pat.to_scipy(dK)
 
@@ -62,6 +82,8 @@ def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls,
         raise ValueError("only 4-node tetrahedra are supported")
     nq = _n_quad(w)
     check_affine(curls, d_phi, nq)
+    n_orient = int(np.asarray(curls).size // (nq * 18))
+    _check_mesh(nodes, cells, glob_ids, num_dofs, orientations, n_orient)
     cells_d = upload(cells, np.int32)
     num_el = cells_d.numel() // 4
     gids_d = upload(glob_ids, np.int32)
@@ -73,11 +95,12 @@ def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls,
     K = zeros(pat.nnz)
     dK = zeros(pat.nnz)
     rhs = zeros(int(num_dofs))
-    _lib.call("snp_curlcurl_assemble", pat.handle, 0, num_el, _lib.ptr(upload(nodes, np.float64)), _lib.ptr(cells_d),
-              _lib.ptr(gids_d), _lib.ptr(upload(orientations, np.int32)), _lib.ptr(upload(curls, np.float64)),
-              n_orient, _lib.ptr(upload(d_phi, np.float64)), _lib.ptr(upload(w, np.float64)), nq,
-              _lib.ptr(upload(x, np.float64)), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(K),
-              _lib.ptr(dK), None, _lib.ptr(rhs), None, _lib.stream_ptr())
+    nodes_d, or_d, curls_d = upload(nodes, np.float64), upload(orientations, np.int32), upload(curls, np.float64)
+    dphi_d, w_d, x_d = upload(d_phi, np.float64), upload(w, np.float64), upload(x, np.float64)
+    _lib.call("snp_curlcurl_assemble", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d), _lib.ptr(gids_d),
+              _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(dphi_d), _lib.ptr(w_d), nq, _lib.ptr(x_d),
+              _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(K), _lib.ptr(dK), None, _lib.ptr(rhs), None,
+              _lib.stream_ptr())
     return pat.to_scipy(K), pat.to_scipy(dK), rhs[: int(num_dofs)].cpu().numpy()
 
 
@@ -89,16 +112,18 @@ def compute_rhs_Hcurl_red_c(nodes, cells, glob_ids, curls, d_phi, orientations, 
         raise ValueError("only first-order edge elements (6 DoFs per element) are supported")
     nq = _n_quad(w)
     check_affine(curls, d_phi, nq)
+    _check_mesh(nodes, cells, glob_ids, num_dofs, orientations, int(np.asarray(curls).size // (nq * 18)))
     cells_d = upload(cells, np.int32)
     num_el = cells_d.numel() // 4
     n_int, rc, rx = reluctance_tables(reluctance)
     n_orient = int(np.asarray(curls).size // (nq * 18))
     rhs = zeros(int(num_dofs))
-    _lib.call("snp_curlcurl_rhs_red", num_el, _lib.ptr(upload(nodes, np.float64)), _lib.ptr(cells_d),
-              _lib.ptr(upload(glob_ids, np.int32)), _lib.ptr(upload(orientations, np.int32)),
-              _lib.ptr(upload(curls, np.float64)), n_orient, _lib.ptr(upload(d_phi, np.float64)),
-              _lib.ptr(upload(w, np.float64)), nq, _lib.ptr(upload(x, np.float64)), _lib.ptr(upload(B_s, np.float64)),
-              n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(rhs), _lib.stream_ptr())
+    nodes_d, gids_d, or_d = upload(nodes, np.float64), upload(glob_ids, np.int32), upload(orientations, np.int32)
+    curls_d, dphi_d, w_d = upload(curls, np.float64), upload(d_phi, np.float64), upload(w, np.float64)
+    x_d, bs_d = upload(x, np.float64), upload(B_s, np.float64)
+    _lib.call("snp_curlcurl_rhs_red", num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d), _lib.ptr(gids_d), _lib.ptr(or_d),
+              _lib.ptr(curls_d), n_orient, _lib.ptr(dphi_d), _lib.ptr(w_d), nq, _lib.ptr(x_d), _lib.ptr(bs_d), n_int,
+              _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(rhs), _lib.stream_ptr())
     return rhs[: int(num_dofs)].cpu().numpy()
 
 
@@ -108,16 +133,18 @@ def compute_B_Hcurl(nodes, cells, glob_ids, curls, phi, d_phi, orientations, x, 
     if num_el_dofs != 6:
         raise ValueError("only first-order edge elements (6 DoFs per element) are supported")
     nq = _n_quad(w)
+    n_orient = int(np.asarray(curls).size // (nq * 18))
+    _check_mesh(nodes, cells, glob_ids, num_dofs, orientations, n_orient)
     cells_d = upload(cells, np.int32)
     num_el = cells_d.numel() // 4
-    n_orient = int(np.asarray(curls).size // (nq * 18))
     pts = zeros(3 * num_el * nq)
     B = zeros(3 * num_el * nq)
-    _lib.call("snp_b_hcurl", num_el, _lib.ptr(upload(nodes, np.float64)), _lib.ptr(cells_d),
-              _lib.ptr(upload(glob_ids, np.int32)), _lib.ptr(upload(orientations, np.int32)),
-              _lib.ptr(upload(curls, np.float64)), n_orient, _lib.ptr(upload(phi, np.float64)),
-              _lib.ptr(upload(d_phi, np.float64)), nq, _lib.ptr(upload(x, np.float64)), _lib.ptr(pts), _lib.ptr(B),
-              _lib.stream_ptr())
+    nodes_d, gids_d, or_d = upload(nodes, np.float64), upload(glob_ids, np.int32), upload(orientations, np.int32)
+    curls_d, phi_d, dphi_d, x_d = (upload(curls, np.float64), upload(phi, np.float64), upload(d_phi, np.float64),
+                                   upload(x, np.float64))
+    _lib.call("snp_b_hcurl", num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d), _lib.ptr(gids_d), _lib.ptr(or_d),
+              _lib.ptr(curls_d), n_orient, _lib.ptr(phi_d), _lib.ptr(dphi_d), nq, _lib.ptr(x_d), _lib.ptr(pts),
+              _lib.ptr(B), _lib.stream_ptr())
     n = 3 * num_el * nq
     return pts[:n].cpu().numpy().reshape(-1, 3), B[:n].cpu().numpy().reshape(-1, 3)
 
@@ -137,8 +164,9 @@ def compute_B_line_segs_cpp(src, tar, current, radius):
         return -1
     _lib.require_cuda()
     B = zeros(3 * tar.shape[0])
-    _lib.call("snp_biot_savart", _lib.ptr(upload(src, np.float64)), src.shape[0], _lib.ptr(upload(tar, np.float64)),
-              tar.shape[0], float(current), float(radius), _lib.ptr(B), _lib.stream_ptr())
+    src_d, tar_d = upload(src, np.float64), upload(tar, np.float64)
+    _lib.call("snp_biot_savart", _lib.ptr(src_d), src.shape[0], _lib.ptr(tar_d), tar.shape[0], float(current),
+              float(radius), _lib.ptr(B), _lib.stream_ptr())
     return B[: 3 * tar.shape[0]].cpu().numpy().reshape(-1, 3).copy()
 
 

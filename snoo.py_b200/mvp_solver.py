@@ -77,9 +77,10 @@ class MVPSolver:
         self.last_stats = stats
         return x.cpu().numpy()
 
-    def solve_to_residual(self, phi_list, rtol=1e-8, x_0=None, precision="fp64", max_newton=None):
+    def solve_to_residual(self, phi_list, rtol=1e-8, x_0=None, precision="fp64", max_newton=None, cg_maxiter=50000):
+        """Newton until ||F_free(x)|| <= rtol ||F_free(x_0)|| (see ``RedMVPSolver.solve_to_residual``)."""
         eng = self._engine(phi_list)
         x, stats = eng.solve(x_0, mode=MODE_RESIDUAL, tol=rtol, max_newton=max_newton or self.max_newton_iterations,
-                             precision={"fp64": 0, "mixed": 1}[precision])
+                             precision={"fp64": 0, "mixed": 1}[precision], cg_maxiter=cg_maxiter)
         self.last_stats = stats
         return x.cpu().numpy(), stats

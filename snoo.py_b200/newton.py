@@ -48,8 +48,13 @@ class DeviceNewton:
         self.pattern = Pattern(None, 0, 6, self.n, handle=p, owned=False)
 
     def solve(self, x0=None, mode=MODE_RESIDUAL, tol=1e-8, cg_maxiter=-1, max_newton=25, cg_rtol=None, precision=0,
-              verbose=False, x_out=None, raise_on_failure=True):
-        """Run Newton from ``x0`` (zeros if None).  Returns (x CUDA tensor, stats dict)."""
+              verbose=False, x_out=None, raise_on_failure=True, line_search=None):
+        """Run Newton from ``x0`` (zeros if None).  Returns (x CUDA tensor, stats dict).
+
+        ``line_search`` (default: on in residual mode, off in reference mode) damps each step by
+        Armijo backtracking on ||F_free||."""
+        if line_search is None:
+            line_search = mode == MODE_RESIDUAL
         t = torch()
         if x_out is None:
             x = zeros(self.n)[: self.n]
@@ -63,7 +68,7 @@ class DeviceNewton:
         if cg_rtol is None:
             cg_rtol = 1e-5 if mode == MODE_REFERENCE else 0.1
         opts = _lib.SolveOpts(int(mode), float(tol), int(cg_maxiter), int(max_newton), float(cg_rtol), int(precision),
-                              1 if verbose else 0)
+                              1 if verbose else 0, 1 if line_search else 0)
         st = _lib.SolveStats()
         rc = _lib.load().snp_solver_solve(self.handle, _lib.ptr(x), ctypes.byref(opts), ctypes.byref(st))
         stats = st.as_dict()

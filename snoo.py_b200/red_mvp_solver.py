@@ -96,12 +96,13 @@ class RedMVPSolver:
         self.last_stats = stats
         return x.cpu().numpy()
 
-    def solve_to_residual(self, rtol=1e-8, x_0=None, precision="fp64", max_newton=None, cg_maxiter=-1,
+    def solve_to_residual(self, rtol=1e-8, x_0=None, precision="fp64", max_newton=None, cg_maxiter=50000,
                           return_device=False, verbose=False):
         """Newton until ||F_free(x)|| <= rtol ||F_free(x_0)||.
 
         :param precision: "fp64", or "mixed" for float32 Jacobian values and CG inside the
             float64 Newton residual and update.
+        :param cg_maxiter: cap on CG iterations per Newton step (-1: 10 x free DoFs, as scipy).
         :return: (x, stats); x is numpy unless ``return_device``.
         """
         eng = self.newton_engine()

@@ -55,29 +55,53 @@ def assert_same_pattern(A, B):
     assert np.array_equal(A.indices, B.indices), "column indices differ"
 
 
-def assert_csr_close(A, B, rtol=1e-12, scale=None, atol_rel=0.0):
-    """Same pattern and |A - B| <= rtol * (|B| + scale) entrywise.
+def scale_csr(ti, tj, s, n):
+    """CSR of the per-entry sums of term magnitudes (``scales`` output of the oracle)."""
+    return csr_array((s, (ti, tj)), shape=(n, n))
 
-    ``scale`` (CSR with B's pattern) is the sum of absolute element contributions of each
-    entry; for entries whose contributions cancel it bounds the rounding error that any
-    summation order makes, so the tolerance stays relative to the data.
+
+def _at(M, rows, cols):
+    if len(rows) == 0:
+        return np.zeros(0)
+    return np.asarray(M[rows, cols]).reshape(-1)
+
+
+def assert_csr_close(A, B, rtol=1e-12, scale=None, atol_rel=0.0, zero_pattern_diff=False):
+    """CSR parity: same structure and |A - B| <= rtol * max(|B|, scale) entrywise.
+
+    ``scale`` (CSR, any superset of the pattern) holds, per entry, the sum of the magnitudes
+    of the terms that make it up; rounding error of any evaluation order is bounded by a
+    small multiple of it, so the bound stays relative to the data even where terms cancel.
+    ``zero_pattern_diff``: for matrices with exact zeros dropped (scipy's ``K += this_K``),
+    an entry stored on one side only is accepted when it is zero up to that scale (one
+    side's arithmetic gave an exact 0, the other a rounding residue); their number is
+    returned.
     """
-    assert_same_pattern(A, B)
     a = csr_array(A)
     b = csr_array(B)
     a.sort_indices()
     b.sort_indices()
-    ref = np.abs(b.data)
+    n_diff = 0
+    if not zero_pattern_diff:
+        assert_same_pattern(a, b)
+    else:
+        pa = csr_array((np.ones(a.nnz), a.indices, a.indptr), shape=a.shape)
+        pb = csr_array((np.ones(b.nnz), b.indices, b.indptr), shape=b.shape)
+        n_diff = int((pa - pb).count_nonzero())
+    d = csr_array(a - b)
+    d.eliminate_zeros()
+    if d.nnz == 0:
+        return n_diff
+    rows, cols = d.nonzero()
+    err = np.abs(_at(d, rows, cols))
+    ref = np.abs(_at(b, rows, cols))
     if scale is not None:
-        s = csr_array(scale)
-        s.sort_indices()
-        assert np.array_equal(s.indices, b.indices)
-        ref = np.maximum(ref, s.data)
+        ref = np.maximum(ref, np.abs(_at(csr_array(scale), rows, cols)))
     bound = rtol * ref + atol_rel * (np.abs(b.data).max() if b.nnz else 0.0)
-    err = np.abs(a.data - b.data)
     bad = err > bound
     assert not bad.any(), (f"{bad.sum()} of {b.nnz} entries off: max err {err.max():.3e}, "
                            f"worst rel {(err / np.maximum(ref, 1e-300)).max():.3e}")
+    return n_diff
 
 
 def rel_max(a, b):

@@ -10,7 +10,7 @@ import pytest
 from scipy.sparse import csr_array
 
 import snoopy_b200 as S
-from helpers import golden_materials, abs_contrib, assert_csr_close, assert_same_pattern, csr_from, rel_max
+from helpers import assert_csr_close, csr_from, golden_materials, rel_max, scale_csr
 from snoopy_b200 import finite_element as FE
 from snoopy_b200 import materials as MAT
 from snoopy_b200 import mesh as M
@@ -47,9 +47,10 @@ def test_curlcurl_golden(golden, fem_c, oracle_mod, rel, name):
     args = (g["nodes"], g["cells"][el], g["glob_ids"][el], g["curls"], g["d_phi"], g["orientations"][el], g["x"], bs, mat,
             g["q"], g["w"], n, 6)
     K, dK, rhs = fem_c.compute_stiffness_and_jacobi_matrix_curl_curl(*args)
-    ti, tj, vK, vdK, _ = oracle_mod.curl_curl_triplets(*args)
-    assert_csr_close(K, csr_from(g, f"cc_{name}_K", n), 1e-12, abs_contrib(ti, tj, vK, n))
-    assert_csr_close(dK, csr_from(g, f"cc_{name}_dK", n), 1e-12, abs_contrib(ti, tj, vdK, n))
+    sc = {}
+    ti, tj, vK, vdK, _ = oracle_mod.curl_curl_triplets(*args, scales=sc)
+    assert_csr_close(K, csr_from(g, f"cc_{name}_K", n), 1e-12, scale_csr(ti, tj, sc["K"], n))
+    assert_csr_close(dK, csr_from(g, f"cc_{name}_dK", n), 1e-12, scale_csr(ti, tj, sc["dK"], n))
     if name == "iron_red":
         assert rel_max(rhs, g[f"cc_{name}_rhs"]) < 1e-12
     else:
@@ -62,9 +63,11 @@ def test_gradgrad_golden(golden, fem_c, oracle_mod, perm, name):
     pm = perm if name == "bspline" else S.ConstantPermeability(1.0)
     nn = g["nodes"].shape[0]
     K, dK = fem_c.compute_stiffness_and_jacobi_matrix(g["nodes"], g["cells"], g["d_phi"], g["x_nodal"], pm, g["q"], g["w"])
-    ti, tj, vK, vdK = oracle_mod.grad_grad_triplets(g["nodes"], g["cells"], g["d_phi"], g["x_nodal"], pm, g["q"], g["w"])
-    assert_csr_close(K, csr_from(g, f"gg_{name}_K", nn), 1e-12, abs_contrib(ti, tj, vK, nn))
-    assert_csr_close(dK, csr_from(g, f"gg_{name}_dK", nn), 1e-12, abs_contrib(ti, tj, vdK, nn))
+    sc = {}
+    ti, tj, vK, vdK = oracle_mod.grad_grad_triplets(g["nodes"], g["cells"], g["d_phi"], g["x_nodal"], pm, g["q"], g["w"],
+                                                    scales=sc)
+    assert_csr_close(K, csr_from(g, f"gg_{name}_K", nn), 1e-12, scale_csr(ti, tj, sc["K"], nn))
+    assert_csr_close(dK, csr_from(g, f"gg_{name}_dK", nn), 1e-12, scale_csr(ti, tj, sc["dK"], nn))
 
 
 def test_rhs_red_golden(golden, fem_c, rel):
@@ -108,9 +111,10 @@ def test_curlcurl_orders_and_sizes(fem_c, oracle_mod, rel, order):
         mat = rel if tag == M.TAG_IRON else S.ConstantReluctance(NU0)
         args = (msh.nodes, msh.cells[el], msh.elem_edges[el], curls, dphi, msh.orientations[el], x, bs, mat, q, w, n, 6)
         K, dK, rhs = fem_c.compute_stiffness_and_jacobi_matrix_curl_curl(*args)
-        ti, tj, vK, vdK, rr = oracle_mod.curl_curl_triplets(*args)
-        assert_csr_close(K, csr_array((vK, (ti, tj)), shape=(n, n)), 1e-12, abs_contrib(ti, tj, vK, n))
-        assert_csr_close(dK, csr_array((vdK, (ti, tj)), shape=(n, n)), 1e-12, abs_contrib(ti, tj, vdK, n))
+        sc = {}
+        ti, tj, vK, vdK, rr = oracle_mod.curl_curl_triplets(*args, scales=sc)
+        assert_csr_close(K, csr_array((vK, (ti, tj)), shape=(n, n)), 1e-12, scale_csr(ti, tj, sc["K"], n))
+        assert_csr_close(dK, csr_array((vdK, (ti, tj)), shape=(n, n)), 1e-12, scale_csr(ti, tj, sc["dK"], n))
         if bs_on:
             assert rel_max(rhs, rr) < 1e-12
 
@@ -154,8 +158,12 @@ def test_assembler_vs_oracle_assembler(oracle_mod):
     O = oracle_mod.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, tb.w, tb.q, tb.d_phi, tb.curls)
     Kr, Jr, rr = O.compute_stiffness_and_jacobi_matrix_c(x, [Bs, np.zeros((0, 3))])
     K, J, r = A.compute_stiffness_and_jacobi_matrix_c(x, quad_order=2, source_fields=[Bs, np.zeros((0, 3))])
-    assert_csr_close(K, Kr, 1e-12, atol_rel=1e-15)
-    assert_csr_close(J, Jr, 1e-12, atol_rel=1e-15)
+    sK, sJ = O.scales(x, [Bs, np.zeros((0, 3))])
+    # exact zeros are dropped on both sides: entries that one side computes as an exact 0 and
+    # the other as a rounding residue may differ in presence (jittered nodes keep this rare)
+    nd = assert_csr_close(K, Kr, 1e-12, sK, zero_pattern_diff=True)
+    nd += assert_csr_close(J, Jr, 1e-12, sJ, zero_pattern_diff=True)
+    assert nd <= 1e-4 * Kr.nnz
     assert rel_max(r, rr) < 1e-12
     assert np.array_equal(A.global_ids[0], msh.elem_edges[iron] + 1)
 
@@ -188,12 +196,15 @@ def test_spmv_and_pcg_match_scipy(oracle_mod):
     ref = np.zeros(msh.num_dofs)
     ref[mask] = Jc @ x[mask]
     assert rel_max(y.cpu().numpy()[: msh.num_dofs], ref) < 1e-13
-    b = rng.normal(0, 1.0, msh.num_dofs)
+    # a consistent right-hand side (J is singular: gradients lie in its kernel)
+    b = np.zeros(msh.num_dofs)
+    b[mask] = Jc @ rng.normal(0, 1.0, int(mask.sum()))
     its = ctypes.c_int64()
     res = ctypes.c_double()
     xs = zeros(msh.num_dofs)
+    b_d = upload(b, np.float64)
     _lib.call("snp_pcg", msh.num_dofs, _lib.ptr(pat.row_ptr), _lib.ptr(pat.col_idx), _lib.ptr(out["J"]), _lib.ptr(fm),
-              _lib.ptr(upload(b, np.float64)), _lib.ptr(xs), 1e-8, 0.0, -1, ctypes.byref(its), ctypes.byref(res),
+              _lib.ptr(b_d), _lib.ptr(xs), 1e-8, 0.0, -1, ctypes.byref(its), ctypes.byref(res),
               _lib.stream_ptr())
     count = [0]
 
@@ -302,8 +313,12 @@ def test_gradgrad_assembler_and_laplace(oracle_mod):
     O = oracle_mod.OracleGradGradAssembler(msh.nodes, [msh.cells[msh.domain_elements(t)] for t in tags], w, q,
                                            FE.evaluate_basis_derivative(q))
     Kr, Jr = O.compute_stiffness_and_jacobi_matrix_c(xn, [S.ConstantPermeability(1.0), perm])
-    assert_csr_close(K, Kr, 1e-12, atol_rel=1e-15)
-    assert_csr_close(J, Jr, 1e-12, atol_rel=1e-15)
+    sK, sJ = O.scales(xn, [S.ConstantPermeability(1.0), perm])
+    # axis-aligned tets on the unjittered material planes give gradients that are exactly
+    # orthogonal: exact zeros on one side may be rounding residues on the other
+    nd = assert_csr_close(K, Kr, 1e-12, sK, zero_pattern_diff=True)
+    nd += assert_csr_close(J, Jr, 1e-12, sJ, zero_pattern_diff=True)
+    assert nd <= 0.01 * Kr.nnz
     t1, t2 = msh.coil_terminals[M.TAG_COIL_1]
     L = S.LaplaceSubdomainSolver(msh, M.TAG_COIL_1, (t1, t2), quad_order=2)
     phi = L.solve(1.0)
@@ -315,14 +330,20 @@ def test_gradgrad_assembler_and_laplace(oracle_mod):
 
 
 def test_mvp_solver_total_potential(oracle_mod):
-    """MVPSolver: Laplace coil potentials -> source rhs -> Newton, against the oracle chain."""
+    """MVPSolver: Laplace coil potentials -> source rhs -> Newton with the reference's increment
+    test, against the oracle restatement of the same chain.
+
+    The coil's terminal faces make the source current open, so the rhs has a component in the
+    curl-curl null space and ||F|| cannot go to zero: this path keeps the reference's stopping
+    rule (solve_nonlin), driven to a tight increment tolerance on both sides.
+    """
     msh = M.window_frame_mesh(8000, jitter=0.1, seed=5, coils=True)
     rel = MAT.atan_reluctance()
     terms = [msh.coil_terminals[M.TAG_COIL_1], msh.coil_terminals[M.TAG_COIL_2]]
-    solver = S.MVPSolver(msh, [M.TAG_COIL_1, M.TAG_COIL_2], [M.TAG_IRON], [M.TAG_AIR], terms, [rel], quad_order=2)
+    solver = S.MVPSolver(msh, [M.TAG_COIL_1, M.TAG_COIL_2], [M.TAG_IRON], [M.TAG_AIR], terms, [rel], quad_order=2,
+                         max_newton_iterations=60)
     solver.verbose = False
-    x, stats = solver.solve_to_residual([5e-3, -5e-3], rtol=1e-9)
-    assert stats["rel_res"] <= 1e-9
+    x = solver.solve_nonlin([5e-3, -5e-3], tolerance=1e-10)
     # oracle chain: Laplace solves, rhs by a numpy statement of compute_rhs_electric_potential, Newton
     w, q = FE.quadrature_rule(2)
     dphi = FE.evaluate_basis_derivative(q)
@@ -356,9 +377,10 @@ def test_mvp_solver_total_potential(oracle_mod):
             return K, J, r + rhs
 
     O = WithRhs(msh.nodes, mats, msh.num_dofs, w, q, dphi, curls)
-    xr, st = oracle_mod.newton_residual(O, solver.make_boundary_mask(), (), rtol=1e-9, cg_rtol=1e-10)
+    xr, st = oracle_mod.newton_reference(O, solver.make_boundary_mask(), (), tolerance=1e-10,
+                                         max_newton_iterations=60)
     cen = msh.element_centroids()
-    el = np.flatnonzero(np.linalg.norm(cen - [0, 0, 0], axis=1) < 0.12)[:200]
+    el = np.flatnonzero(msh.elem_domain == M.TAG_IRON)[::7]
     Bg = solver.curl_curl_factory.compute_B_at_points(x, cen[el], el)
     Bo = solver.curl_curl_factory.compute_B_at_points(xr, cen[el], el)
     assert rel_max(Bg, Bo) < 1e-6
@@ -378,7 +400,7 @@ def test_error_statuses():
     msh, g, coils, rel, solver = _red_setup(3000)
     eng = solver.newton_engine()
     x0 = np.zeros(msh.num_dofs)
-    x0[5] = np.nan
+    x0[int(np.flatnonzero(solver.make_boundary_mask())[0])] = np.nan
     with pytest.raises(_lib.SnpError) as e:
         eng.solve(x0, mode=1, tol=1e-8)
     assert e.value.status in (4, 5)
@@ -389,14 +411,16 @@ def test_error_statuses():
     fm = upload(solver.make_boundary_mask().astype(np.uint8), np.uint8)
     its = ctypes.c_int64()
     res = ctypes.c_double()
+    x1 = zeros(msh.num_dofs)
     rc = _lib.load().snp_pcg(msh.num_dofs, _lib.ptr(pat.row_ptr), _lib.ptr(pat.col_idx), _lib.ptr(out["J"]),
-                             _lib.ptr(fm), _lib.ptr(out["rhs"]), _lib.ptr(zeros(msh.num_dofs)), 1e-12, 0.0, 1,
+                             _lib.ptr(fm), _lib.ptr(out["rhs"]), _lib.ptr(x1), 1e-12, 0.0, 1,
                              ctypes.byref(its), ctypes.byref(res), _lib.stream_ptr())
     assert rc == 3 and its.value == 1
     # a zero Jacobian diagonal on a free row
     Jz = out["J"].clone()
     Jz[pat.diag_pos[int(np.flatnonzero(solver.make_boundary_mask())[0])].long()] = 0.0
+    x2 = zeros(msh.num_dofs)
     rc = _lib.load().snp_pcg(msh.num_dofs, _lib.ptr(pat.row_ptr), _lib.ptr(pat.col_idx), _lib.ptr(Jz), _lib.ptr(fm),
-                             _lib.ptr(out["rhs"]), _lib.ptr(zeros(msh.num_dofs)), 1e-8, 0.0, 10, ctypes.byref(its),
+                             _lib.ptr(out["rhs"]), _lib.ptr(x2), 1e-8, 0.0, 10, ctypes.byref(its),
                              ctypes.byref(res), _lib.stream_ptr())
     assert rc == 5

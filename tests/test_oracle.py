@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import snoopy_b200 as S
-from helpers import golden_materials, abs_contrib, assert_csr_close, assert_same_pattern, csr_from, rel_max
+from helpers import abs_contrib, assert_csr_close, assert_same_pattern, csr_from, golden_materials, rel_max
 from snoopy_b200 import finite_element as FE
 from snoopy_b200 import materials as MAT
 from snoopy_b200 import mesh as M
