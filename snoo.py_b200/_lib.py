@@ -69,6 +69,8 @@ _SIGS = {
     "snp_spmv": [_c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snp_pcg": [_c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _c_f64, _c_f64, _c_i64, ctypes.POINTER(_c_i64),
                 ctypes.POINTER(_c_f64), _vp],
+    "snp_pcg_noalloc": [_c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _c_f64, _c_f64, _c_i64, ctypes.POINTER(_c_i64),
+                        ctypes.POINTER(_c_f64), _vp],
     "snp_solver_create": [_c_i32, _vp, _c_i64, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp, _pp],
     "snp_solver_add_material": [_vp, _vp, _vp, _vp, _c_i64, _c_i32, _vp, _vp, _vp],
     "snp_solver_set_rhs": [_vp, _vp],

@@ -485,6 +485,66 @@ int Pcg<VT, XT>::solve(const CsrView<VT> &A, const uint8_t *free_mask, const XT 
 template struct Pcg<double, double>;
 template struct Pcg<float, float>;
 
+int pcg_on_buffers(const CsrView<double> &A, const uint8_t *free_mask, const double *b, double *x, double rtol,
+                   double atol, int64_t maxit, const PcgBuffers &B, cudaStream_t s, int64_t *its, double *res,
+                   int *status) {
+    if (maxit < 0) maxit = 10 * (int64_t)A.n;
+    // the state (with its reduction ticket) and the pivot flag must start at zero
+    SNP_CUDA_TRY(cudaMemsetAsync(B.st, 0, sizeof(PcgState), s));
+    SNP_CUDA_TRY(cudaMemsetAsync(B.bad, 0, sizeof(int), s));
+    SNP_TRY(find_diag(A.n, A.rp, A.ci, B.diag, s));
+    const int gv = stride_grid(A.n, kVecBlock, 8);
+    SNP_REQUIRE(gv <= B.max_blocks, "pcg: %d blocks exceed the %d partial-sum slots", gv, B.max_blocks);
+    k_dinv<double, double><<<gv, kVecBlock, 0, s>>>(A.n, B.diag, A.v, free_mask, B.dinv, B.bad);
+    SNP_LAUNCH_CHECK();
+    int hbad = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&hbad, B.bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hbad) return fail(SNP_ZERO_PIVOT, "pcg: zero or missing diagonal entry on a free row");
+    const int tpr = choose_tpr(A.nnz, A.n);
+    const int gs = spmv_grid(A.n, tpr);
+    SNP_REQUIRE(gs <= B.max_blocks, "pcg: %d blocks exceed the %d partial-sum slots", gs, B.max_blocks);
+    if (free_mask)
+        SNP_TRY((spmv_dispatch<double, double, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, B.q, nullptr,
+                                                             nullptr, gs, s)));
+    else
+        SNP_TRY((spmv_dispatch<double, double, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, B.q, nullptr,
+                                                              nullptr, gs, s)));
+    k_init<double><<<gv, kVecBlock, 0, s>>>(A.n, free_mask, b, x, B.r, B.z, B.p, B.q, B.dinv, B.st, B.part, rtol, atol,
+                                            (long long)maxit, 0);
+    SNP_LAUNCH_CHECK();
+    // iterations in chunks; every kernel returns at once after the flag is set, so the
+    // overshoot of the last chunk does no work
+    PcgState H;
+    const int chunk = 32;
+    int64_t launched = 0;
+    while (true) {
+        SNP_CUDA_TRY(cudaMemcpyAsync(&H, B.st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+        SNP_CUDA_TRY(cudaStreamSynchronize(s));
+        if (H.done || launched > maxit + chunk) break;
+        for (int k = 0; k < chunk; ++k) {
+            if (free_mask)
+                SNP_TRY((spmv_dispatch<double, double, false, true>(tpr, A.n, A.rp, A.ci, A.v, free_mask, B.p, B.q, B.st,
+                                                                     B.part, gs, s)));
+            else
+                SNP_TRY((spmv_dispatch<double, double, false, true>(tpr, A.n, A.rp, A.ci, A.v, nullptr, B.p, B.q, B.st,
+                                                                     B.part, gs, s)));
+            k_update<double><<<gv, kVecBlock, 0, s>>>(A.n, free_mask, x, B.r, B.z, B.p, B.q, B.dinv, B.st, B.part, 0, 0);
+            SNP_LAUNCH_CHECK();
+            k_pupdate<double><<<gv, kVecBlock, 0, s>>>(A.n, free_mask, B.p, B.z, B.st);
+            SNP_LAUNCH_CHECK();
+        }
+        launched += chunk;
+    }
+    if (its) *its = H.iter;
+    if (res) *res = sqrt(H.rr);
+    int stt = SNP_OK;
+    if (H.done == 2) stt = SNP_NOT_CONVERGED;
+    else if (H.done == 3) stt = SNP_NAN_DETECTED;
+    if (status) *status = stt;
+    return SNP_OK;
+}
+
 }  // namespace snp
 
 extern "C" {

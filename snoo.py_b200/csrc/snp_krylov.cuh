@@ -25,6 +25,21 @@ struct PcgState {
     unsigned int counter;
 };
 
+// Work space of one CG solve on caller-owned device memory (nothing is allocated).
+struct PcgBuffers {
+    double *r, *z, *p, *q, *dinv, *part;  // part: 3 * max_blocks doubles
+    int32_t *diag;
+    PcgState *st;
+    int *bad;
+    int max_blocks;
+};
+
+// Jacobi-PCG (float64) with scipy cg's stopping rule on the given buffers; launches only
+// kernels, async copies of scalars and stream synchronisations.
+int pcg_on_buffers(const CsrView<double> &A, const uint8_t *free_mask, const double *b, double *x, double rtol,
+                   double atol, int64_t maxit, const PcgBuffers &B, cudaStream_t s, int64_t *its, double *res,
+                   int *status);
+
 int choose_tpr(int64_t nnz, int32_t n);
 int find_diag(int32_t n, const int32_t *rp, const int32_t *ci, int32_t *diag, cudaStream_t s);
 int spmv_f64(const CsrView<double> &A, const uint8_t *free_mask, const double *x, double *y, cudaStream_t s);
