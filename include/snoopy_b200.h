@@ -249,6 +249,26 @@ int snp_solver_solve(snp_solver *s, double *x, const snp_solve_opts *opts, snp_s
 int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *J_vals, double *rhs,
                         double *F, void *stream);
 
+/* Storage of the Jacobian inside the residual-mode Newton loop, chosen at finalize from the
+ * environment variable SNP_JACOBIAN ("elem" default, "csr", "sell"):
+ *   SNP_LAYOUT_ELEM  matrix-free: per element the 3x3 symmetric tensor S_e with
+ *                    J_e,jk = s_j s_k chat_j . S_e chat_k (first-order Nedelec, affine tets);
+ *                    falls back to CSR when the orientation tables are not sign flips
+ *   SNP_LAYOUT_CSR   assembled CSR on the solver's pattern
+ *   SNP_LAYOUT_SELL  assembled SELL-C-sigma (C = 32, sigma = 256) copy of that pattern
+ * Reference-semantics solves (mode 0) and snp_solver_assemble always use the CSR. */
+#define SNP_LAYOUT_CSR 0
+#define SNP_LAYOUT_SELL 1
+#define SNP_LAYOUT_ELEM 2
+int snp_solver_jacobian_layout(const snp_solver *s, int *layout);
+
+/* y = J x on the free rows and columns (y = 0 on constrained rows) with the Newton Jacobian
+ * the solver holds from its last solve, in the layout the solver's Krylov loop uses.
+ * precision 0: the float64 Jacobian, x/y double[n]; precision 1: the float32 Jacobian of a
+ * mixed-precision solve, x/y float[n].  SNP_BAD_ARGUMENT when no solve of that precision ran.
+ * No counterpart in the reference (Jacobian-vector product of the Newton step). */
+int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void *y, void *stream);
+
 /* The solver's CSR pattern (owned by the solver). */
 int snp_solver_pattern(const snp_solver *s, const snp_pattern **pat);
 

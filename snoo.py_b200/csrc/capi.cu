@@ -1,7 +1,9 @@
 // Error reporting and device queries of the C ABI.
 #include <cstdarg>
 #include <cstdio>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 #include "snp_common.cuh"
 
@@ -37,6 +39,28 @@ int sm_count() {
         cached[dev] = v;
     }
     return cached[dev];
+}
+
+int resident_blocks(const void *kernel, int block, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void *, int, size_t, int>, int> cached;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        dev = -1;
+    }
+    const auto key = std::make_tuple(kernel, block, smem, dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cached.find(key);
+    if (it != cached.end()) return it->second;
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, block, smem) != cudaSuccess || v <= 0) {
+        cudaGetLastError();
+        v = 1;
+    }
+    if (v > 8) v = 8;
+    cached[key] = v;
+    return v;
 }
 
 }  // namespace snp

@@ -1,0 +1,714 @@
+// Matrix-free Newton Jacobian and its Jacobi-PCG.
+//
+// The assembled Jacobian of the reference (a CSR built by scipy from element triplets,
+// snoopy/red_mvp_solver.py:160-203) costs 12 bytes per stored entry and ~16 entries per row
+// on a tetrahedral mesh.  For first-order Nedelec elements on affine tetrahedra each element
+// block is J_e,jk = s_j s_k chat_j . S_e chat_k with a 3x3 symmetric S_e, so the operator is
+// kept as six numbers per element plus the fixed topology, and a product is two passes:
+//
+//   element pass  p_j formed on the fly, u_e = sum_j s_j p_j chat_j, v_e = S_e u_e, p.q
+//                 partial sums (p.J p = sum_e u_e . v_e); stores v_e
+//   DoF pass      q_i = sum_(e,k) s_k chat_k . v_e over the DoF's incident elements, then the
+//                 CG update of the DoF: p = z + beta p, x += alpha p, r -= alpha q,
+//                 z = dinv r, r.z and r.r partial sums
+//
+// Neither pass uses atomics; every sum runs in a fixed order, so the iteration is
+// deterministic.  The per-DoF CG state is split so the element pass gathers only {z, p}
+// (16 bytes per DoF in float64).  The direction p_k = z_k + beta p_(k-1) is formed in both
+// passes by the same rounded expression, so both see the same p.
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "snp_common.cuh"
+#include "snp_internal.cuh"
+#include "snp_krylov.cuh"
+#include "snp_reduce.cuh"
+
+namespace snp {
+
+namespace {
+
+constexpr int kEBlock = 256;
+#ifndef SNP_INC_UNROLL
+#define SNP_INC_UNROLL 4
+#endif
+#ifndef SNP_PASS1_PREFETCH
+#define SNP_PASS1_PREFETCH 1
+#endif
+constexpr int kIncUnroll = SNP_INC_UNROLL;    // incidence gathers in flight per lane in the DoF pass
+constexpr int kWarpSlab = 256;                // incidence terms staged per warp (shared memory)
+constexpr bool kPass1Prefetch = SNP_PASS1_PREFETCH;  // element pass loads element e+stride before e's gathers
+constexpr uint32_t kSignBit = 0x80000000u;
+
+// p = z + beta p_old, rounded the same way wherever it is formed
+__device__ __forceinline__ double pnext(double beta, double p_old, double z) { return __fma_rn(beta, p_old, z); }
+__device__ __forceinline__ float pnext(float beta, float p_old, float z) { return __fmaf_rn(beta, p_old, z); }
+
+// ---------------------------------------------------------------- topology build
+
+__global__ void k_edof(int64_t count, int64_t offset, int64_t ne, const int32_t *__restrict__ gids,
+                       const int32_t *__restrict__ orient, const int8_t *__restrict__ sgn, int32_t n_orient,
+                       int32_t n, int32_t *__restrict__ edof, int *bad) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
+        const int o = orient[e];
+        if (o < 0 || o >= n_orient) {
+            atomicExch(bad, 1);
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int32_t g = gids[6 * e + k];
+            if (g < 0 || g >= n) {
+                atomicExch(bad, 1);
+                continue;
+            }
+            edof[(int64_t)k * ne + offset + e] = (int32_t)((uint32_t)g | (sgn[6 * o + k] < 0 ? kSignBit : 0u));
+        }
+    }
+}
+
+// sort keys (DoF) and values (e << 3 | k | sign) of every element edge; counts per DoF
+__global__ void k_inc_keys(int64_t ne, const int32_t *__restrict__ edof, int32_t *__restrict__ key,
+                           int32_t *__restrict__ val, int32_t *__restrict__ count) {
+    const int64_t total = 6 * ne;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t / 6;
+        const int k = (int)(t - 6 * e);
+        const uint32_t d = (uint32_t)edof[(int64_t)k * ne + e];
+        const int32_t g = (int32_t)(d & ~kSignBit);
+        key[t] = g;
+        val[t] = (int32_t)(((uint32_t)e << 3) | (uint32_t)k | (d & kSignBit));
+        atomicAdd(count + g, 1);
+    }
+}
+
+// per-DoF sums of element-edge terms, in incidence order
+__global__ void k_sum_to_dofs(int32_t n, int64_t ne, const int32_t *__restrict__ inc_ptr,
+                              const int32_t *__restrict__ inc, const double *__restrict__ Fe,
+                              const double *__restrict__ De, const double *__restrict__ rhs_extra,
+                              double *__restrict__ F, double *__restrict__ diag) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double f = 0.0, d = 0.0;
+        for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
+            const uint32_t u = (uint32_t)inc[t] & ~kSignBit;
+            const int64_t idx = (int64_t)(u & 7u) * ne + (u >> 3);
+            f += Fe[idx];
+            d += De[idx];
+        }
+        F[i] = rhs_extra ? f - rhs_extra[i] : f;
+        diag[i] = d;
+    }
+}
+
+// ---------------------------------------------------------------- PCG kernels
+
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_einit(int32_t n, const uint8_t *__restrict__ free_mask, const double *__restrict__ b, double b_scale,
+            const double *__restrict__ diag, DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R,
+            TT *__restrict__ D, PcgState *st, double *part, double rtol, double atol, long long maxit, int *bad) {
+    __shared__ double sh[32];
+    double rz = 0.0, rr = 0.0, bb = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        TT r = TT(0), d = TT(0), z = TT(0);
+        if (is_free(free_mask, i)) {
+            const double dg = diag[i];
+            if (dg == 0.0 || !isfinite(dg)) {
+                atomicExch(bad, 1);
+            } else {
+                d = (TT)(1.0 / dg);
+            }
+            r = (TT)(b_scale * b[i]);
+            z = d * r;
+            rz += (double)r * (double)z;
+            rr += (double)r * (double)r;
+            bb += (double)r * (double)r;
+        }
+        G[i] = DofPair<TT>{z, TT(0)};
+        R[i] = DofPair<TT>{r, TT(0)};
+        D[i] = d;
+    }
+    const double a0 = block_sum(rz, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x] = a0;
+    const double a1 = block_sum(rr, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x + 1] = a1;
+    const double a2 = block_sum(bb, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x + 2] = a2;
+    if (last_block(&st->counter)) {
+        const double s_rz = reduce_parts(part, gridDim.x, 3, 0, sh);
+        const double s_rr = reduce_parts(part, gridDim.x, 3, 1, sh);
+        const double s_bb = reduce_parts(part, gridDim.x, 3, 2, sh);
+        if (threadIdx.x == 0) {
+            st->rz = s_rz;
+            st->rr = s_rr;
+            st->bnorm = sqrt(s_bb);
+            st->atol_eff = fmax(atol, rtol * st->bnorm);
+            st->iter = 0;
+            st->maxit = maxit;
+            st->alpha = 0.0;
+            st->beta = 0.0;
+            int done = 0;
+            if (s_bb == 0.0) done = 4;
+            else if (!(s_rr == s_rr) || isinf(s_rr)) done = 3;
+            else if (sqrt(s_rr) < st->atol_eff) done = 1;
+            else if (maxit <= 0) done = 2;
+            st->done = done;
+        }
+    }
+}
+
+template <typename TT>
+__device__ __forceinline__ void load_chat(TT *sc, const TT *chat) {
+    if (threadIdx.x < 18) sc[threadIdx.x] = chat[threadIdx.x];
+    __syncthreads();
+}
+
+// element pass of a CG iteration: p from the DoF states, v_e = S_e u_e, p.J p -> alpha.
+// The next element's DoF words and tensor are loaded before this element's gathers.
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_epass1(int64_t ne, const int32_t *__restrict__ edof, const TT *__restrict__ T, const TT *__restrict__ chat,
+             const DofPair<TT> *__restrict__ G, ElemVec<TT> *__restrict__ V, PcgState *st, double *part) {
+    __shared__ TT sc[18];
+    __shared__ double sh[32];
+    if (st->done) return;
+    load_chat(sc, chat);
+    const TT beta = (TT)st->beta;
+    double dot = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t nd[6];
+    TT nt[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        nd[k] = e < ne ? __ldcs(edof + (int64_t)k * ne + e) : 0;
+        nt[k] = e < ne ? __ldcs(T + (int64_t)k * ne + e) : TT(0);
+    }
+    for (; e < ne; e += stride) {
+        int32_t d[6];
+        TT t[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            d[k] = nd[k];
+            t[k] = nt[k];
+        }
+        DofPair<TT> w[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) w[k] = G[(uint32_t)d[k] & ~kSignBit];
+        if (kPass1Prefetch) {
+            const int64_t en = e + stride;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                nd[k] = en < ne ? __ldcs(edof + (int64_t)k * ne + en) : 0;
+                nt[k] = en < ne ? __ldcs(T + (int64_t)k * ne + en) : TT(0);
+            }
+        }
+        TT u0 = TT(0), u1 = TT(0), u2 = TT(0);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            TT pk = pnext(beta, w[k].b, w[k].a);
+            if (d[k] < 0) pk = -pk;
+            u0 += pk * sc[3 * k];
+            u1 += pk * sc[3 * k + 1];
+            u2 += pk * sc[3 * k + 2];
+        }
+        const TT v0 = t[0] * u0 + t[1] * u1 + t[2] * u2;
+        const TT v1 = t[1] * u0 + t[3] * u1 + t[4] * u2;
+        const TT v2 = t[2] * u0 + t[4] * u1 + t[5] * u2;
+        dot += (double)u0 * (double)v0 + (double)u1 * (double)v1 + (double)u2 * (double)v2;
+        V[e] = ElemVec<TT>{v0, v1, v2, TT(0)};
+        if (!kPass1Prefetch) {
+            const int64_t en = e + stride;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                nd[k] = en < ne ? __ldcs(edof + (int64_t)k * ne + en) : 0;
+                nt[k] = en < ne ? __ldcs(T + (int64_t)k * ne + en) : TT(0);
+            }
+        }
+    }
+    dot = block_sum(dot, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = dot;
+    if (last_block(&st->counter)) {
+        const double pq = reduce_parts(part, gridDim.x, 1, 0, sh);
+        if (threadIdx.x == 0) {
+            st->pq = pq;
+            st->alpha = st->rz / pq;
+        }
+    }
+}
+
+// Signed contribution s_k chat_k . v_e of one incidence entry, rounded the same way on
+// every path that forms it.
+template <typename TT>
+__device__ __forceinline__ double inc_term(const TT *sc, int32_t ent, const ElemVec<TT> &v) {
+    const int k = (int)((uint32_t)ent & 7u);
+    TT c;
+    if constexpr (sizeof(TT) == 8)
+        c = __fma_rn(sc[3 * k + 2], v.c, __fma_rn(sc[3 * k + 1], v.b, __dmul_rn(sc[3 * k], v.a)));
+    else
+        c = __fmaf_rn(sc[3 * k + 2], v.c, __fmaf_rn(sc[3 * k + 1], v.b, __fmul_rn(sc[3 * k], v.a)));
+    return ent < 0 ? -(double)c : (double)c;
+}
+
+// q_i = sum over the incidence entries of DoF i, in entry order.  A warp takes 32 consecutive
+// DoFs; when their entries fit in the warp's shared-memory slab, the lanes stride over the
+// flattened entry range (coalesced entry loads, kIncUnroll gathers in flight per lane, no
+// divergence from uneven list lengths) and each lane then sums its own DoF's terms from
+// shared memory.  Otherwise each lane walks its own list.  Both give the same bits.
+template <typename TT>
+__device__ __forceinline__ double warp_gather_q(bool valid, int b0, int b1, const int32_t *__restrict__ inc,
+                                                const TT *sc, const ElemVec<TT> *__restrict__ V, double *slab) {
+    const int lane = threadIdx.x & 31;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    const int last = 31 - __clz(vmask);
+    const int rb = __shfl_sync(0xffffffffu, b0, 0);
+    const int re = __shfl_sync(0xffffffffu, b1, last);
+    const int cnt = re - rb;
+    double q = 0.0;
+    if (cnt <= kWarpSlab) {
+        for (int t0 = lane; t0 < cnt; t0 += 32 * kIncUnroll) {
+            int32_t ent[kIncUnroll];
+            ElemVec<TT> v[kIncUnroll];
+#pragma unroll
+            for (int u = 0; u < kIncUnroll; ++u) {
+                const int t = t0 + 32 * u;
+                ent[u] = t < cnt ? __ldcs(inc + rb + t) : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < kIncUnroll; ++u) v[u] = V[((uint32_t)ent[u] & ~kSignBit) >> 3];
+#pragma unroll
+            for (int u = 0; u < kIncUnroll; ++u) {
+                const int t = t0 + 32 * u;
+                if (t < cnt) slab[t] = inc_term(sc, ent[u], v[u]);
+            }
+        }
+        __syncwarp();
+        if (valid)
+            for (int t = b0 - rb; t < b1 - rb; ++t) q += slab[t];
+        __syncwarp();
+    } else if (valid) {
+        for (int t = b0; t < b1; ++t) {
+            const int32_t ent = inc[t];
+            q += inc_term(sc, ent, V[((uint32_t)ent & ~kSignBit) >> 3]);
+        }
+    }
+    return q;
+}
+
+// DoF pass of a CG iteration: q_i gathered from v_e, then the update of DoF i
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_epass2(int32_t n, const uint8_t *__restrict__ free_mask, const int32_t *__restrict__ inc_ptr,
+             const int32_t *__restrict__ inc, const TT *__restrict__ chat, const ElemVec<TT> *__restrict__ V,
+             DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R, const TT *__restrict__ D, PcgState *st,
+             double *part, int use_cond, cudaGraphConditionalHandle cond) {
+    __shared__ TT sc[18];
+    __shared__ double sh2[2][32];
+    __shared__ double s_slab[kEBlock / 32][kWarpSlab];
+    if (st->done) {
+        if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
+        return;
+    }
+    load_chat(sc, chat);
+    const TT alpha = (TT)st->alpha, beta = (TT)st->beta;
+    double *slab = s_slab[threadIdx.x >> 5];
+    double rz = 0.0, rr = 0.0;
+    // the loop bound is uniform across each warp (32 consecutive DoFs per warp and pass); the
+    // next pass's list bounds and this pass's own-row state are loaded ahead of the gathers
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    int nb0 = 0, nb1 = 0;
+    if (base + (threadIdx.x & 31) < n) {
+        nb0 = __ldcs(inc_ptr + base + (threadIdx.x & 31));
+        nb1 = __ldcs(inc_ptr + base + (threadIdx.x & 31) + 1);
+    }
+    for (; base < n; base += stride) {
+        const int64_t i = base + (threadIdx.x & 31);
+        const bool valid = i < n;
+        const int b0 = nb0, b1 = nb1;
+        const bool upd = valid && is_free(free_mask, i);
+        DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
+        TT dv = TT(0);
+        if (upd) {
+            g = G[i];
+            rx = R[i];
+            dv = D[i];
+        }
+        // lanes past the end carry an empty list, so their slab range is empty too
+        nb0 = nb1 = 0;
+        if (i + stride < n) {
+            nb0 = __ldcs(inc_ptr + i + stride);
+            nb1 = __ldcs(inc_ptr + i + stride + 1);
+        }
+        const double q = warp_gather_q(valid, b0, b1, inc, sc, V, slab);
+        if (!upd) continue;
+        const TT p = pnext(beta, g.b, g.a);
+        const TT r = rx.a - alpha * (TT)q;
+        const TT z = dv * r;
+        G[i] = DofPair<TT>{z, p};
+        R[i] = DofPair<TT>{r, rx.b + alpha * p};
+        rz += (double)r * (double)z;
+        rr += (double)r * (double)r;
+    }
+    block_sum2(rz, rr, sh2);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = rz;
+        part[2 * blockIdx.x + 1] = rr;
+    }
+    if (last_block(&st->counter)) {
+        double a = 0.0, b = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+            a += __ldcg(part + 2 * i);
+            b += __ldcg(part + 2 * i + 1);
+        }
+        __syncthreads();
+        block_sum2(a, b, sh2);
+        if (threadIdx.x == 0) {
+            const double rz_new = a, rr_new = b;
+            st->beta = rz_new / st->rz;
+            st->rz = rz_new;
+            st->rr = rr_new;
+            st->iter += 1;
+            int done = 0;
+            if (!(rr_new == rr_new) || isinf(rr_new)) done = 3;
+            else if (sqrt(rr_new) < st->atol_eff) done = 1;
+            else if (st->iter >= st->maxit) done = 2;
+            st->done = done;
+            if (use_cond && done) cudaGraphSetConditional(cond, 0);
+        }
+    }
+}
+
+template <typename TT>
+__global__ void k_eextract(int32_t n, const DofPair<TT> *__restrict__ R, double *__restrict__ h) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        h[i] = (double)R[i].b;
+}
+
+// ---------------------------------------------------------------- plain product y = J x
+
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_eapply1(int64_t ne, const int32_t *__restrict__ edof, const TT *__restrict__ T, const TT *__restrict__ chat,
+              const uint8_t *__restrict__ free_mask, const TT *__restrict__ x, ElemVec<TT> *__restrict__ V) {
+    __shared__ TT sc[18];
+    load_chat(sc, chat);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
+        TT u0 = TT(0), u1 = TT(0), u2 = TT(0);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int32_t d = edof[(int64_t)k * ne + e];
+            const uint32_t g = (uint32_t)d & ~kSignBit;
+            TT xk = is_free(free_mask, g) ? x[g] : TT(0);
+            if (d < 0) xk = -xk;
+            u0 += xk * sc[3 * k];
+            u1 += xk * sc[3 * k + 1];
+            u2 += xk * sc[3 * k + 2];
+        }
+        TT t[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) t[k] = T[(int64_t)k * ne + e];
+        V[e] = ElemVec<TT>{t[0] * u0 + t[1] * u1 + t[2] * u2, t[1] * u0 + t[3] * u1 + t[4] * u2,
+                           t[2] * u0 + t[4] * u1 + t[5] * u2, TT(0)};
+    }
+}
+
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_eapply2(int32_t n, const uint8_t *__restrict__ free_mask, const int32_t *__restrict__ inc_ptr,
+              const int32_t *__restrict__ inc, const TT *__restrict__ chat, const ElemVec<TT> *__restrict__ V,
+              TT *__restrict__ y) {
+    __shared__ TT sc[18];
+    load_chat(sc, chat);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double q = 0.0;
+        if (is_free(free_mask, i)) {
+            for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
+                const int32_t ent = inc[t];
+                const uint32_t u = (uint32_t)ent & ~kSignBit;
+                const int k = (int)(u & 7u);
+                const ElemVec<TT> v = V[u >> 3];
+                const TT c = sc[3 * k] * v.a + sc[3 * k + 1] * v.b + sc[3 * k + 2] * v.c;
+                q += ent < 0 ? -(double)c : (double)c;
+            }
+        }
+        y[i] = (TT)q;
+    }
+}
+
+template <typename TT>
+const TT *chat_ptr(const ElemTopology &top);
+template <>
+const double *chat_ptr<double>(const ElemTopology &top) {
+    return top.chat64.p;
+}
+template <>
+const float *chat_ptr<float>(const ElemTopology &top) {
+    return top.chat32.p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- topology
+
+int build_elem_topology(ElemTopology &top, int32_t n, const ElemBlock *blocks, int n_blocks, const double *ctab_host,
+                        int32_t n_orient, cudaStream_t s, bool *usable) {
+    *usable = false;
+    SNP_REQUIRE(n > 0 && n_orient >= 1 && ctab_host != nullptr, "element topology: bad arguments");
+    int64_t ne = 0;
+    for (int b = 0; b < n_blocks; ++b) ne = ne > blocks[b].offset + blocks[b].count ? ne : blocks[b].offset + blocks[b].count;
+    if (ne <= 0 || ne >= ((int64_t)1 << 28)) return SNP_OK;  // (e << 3 | k) must fit in 31 bits
+    // every orientation's curls must be +-(orientation 0's), edge by edge
+    std::vector<int8_t> sgn((size_t)n_orient * 6, 1);
+    for (int o = 0; o < n_orient; ++o)
+        for (int j = 0; j < 6; ++j) {
+            const double *c = ctab_host + ((size_t)o * 6 + j) * 3;
+            const double *c0 = ctab_host + (size_t)j * 3;
+            bool plus = true, minus = true;
+            for (int k = 0; k < 3; ++k) {
+                plus = plus && (c[k] == c0[k]);
+                minus = minus && (c[k] == -c0[k]);
+            }
+            if (!plus && !minus) return SNP_OK;
+            sgn[(size_t)o * 6 + j] = plus ? 1 : -1;
+        }
+    DevBuf<int8_t> d_sgn;
+    DevBuf<int> bad;
+    SNP_TRY(d_sgn.alloc(sgn.size()));
+    SNP_TRY(bad.alloc(1));
+    SNP_CUDA_TRY(cudaMemcpyAsync(d_sgn.p, sgn.data(), sgn.size(), cudaMemcpyHostToDevice, s));
+    SNP_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    SNP_TRY(top.edof.alloc(6 * ne));
+    SNP_CUDA_TRY(cudaMemsetAsync(top.edof.p, 0, sizeof(int32_t) * 6 * ne, s));
+    for (int b = 0; b < n_blocks; ++b) {
+        if (blocks[b].count == 0) continue;
+        k_edof<<<stride_grid(blocks[b].count, 256, 8), 256, 0, s>>>(blocks[b].count, blocks[b].offset, ne,
+                                                                     blocks[b].gids, blocks[b].orient, d_sgn.p,
+                                                                     n_orient, n, top.edof.p, bad.p);
+        SNP_LAUNCH_CHECK();
+    }
+    // incidence: stable radix sort of (DoF, entry) pairs keeps each DoF's entries in (e, k) order
+    const int64_t m = 6 * ne;
+    DevBuf<int32_t> key, key2, val, cnt;
+    SNP_TRY(key.alloc(m));
+    SNP_TRY(key2.alloc(m));
+    SNP_TRY(val.alloc(m));
+    SNP_TRY(top.inc.alloc(m));
+    SNP_TRY(cnt.alloc((size_t)n + 1));
+    SNP_TRY(top.inc_ptr.alloc((size_t)n + 1));
+    SNP_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * ((size_t)n + 1), s));
+    k_inc_keys<<<stride_grid(m, 256, 8), 256, 0, s>>>(ne, top.edof.p, key.p, val.p, cnt.p);
+    SNP_LAUNCH_CHECK();
+    int end_bit = 1;
+    while (end_bit < 31 && ((int64_t)1 << end_bit) < (int64_t)n) ++end_bit;
+    cub::DoubleBuffer<int32_t> dk(key.p, key2.p);
+    cub::DoubleBuffer<int32_t> dv(val.p, top.inc.p);
+    size_t tb_sort = 0, tb_scan = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, dk, dv, (int)m, 0, end_bit, s);
+    cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, cnt.p, top.inc_ptr.p, n + 1, s);
+    DevBuf<unsigned char> temp;
+    SNP_TRY(temp.alloc(tb_sort > tb_scan ? tb_sort : tb_scan));
+    SNP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.p, tb_sort, dk, dv, (int)m, 0, end_bit, s));
+    if (dv.Current() != top.inc.p)
+        SNP_CUDA_TRY(cudaMemcpyAsync(top.inc.p, dv.Current(), sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, s));
+    SNP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp.p, tb_scan, cnt.p, top.inc_ptr.p, n + 1, s));
+    double c64[18];
+    float c32[18];
+    for (int t = 0; t < 18; ++t) {
+        c64[t] = ctab_host[t];
+        c32[t] = (float)ctab_host[t];
+    }
+    SNP_TRY(top.chat64.alloc(18));
+    SNP_TRY(top.chat32.alloc(18));
+    SNP_CUDA_TRY(cudaMemcpyAsync(top.chat64.p, c64, sizeof(c64), cudaMemcpyHostToDevice, s));
+    SNP_CUDA_TRY(cudaMemcpyAsync(top.chat32.p, c32, sizeof(c32), cudaMemcpyHostToDevice, s));
+    int hbad = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    SNP_REQUIRE(hbad == 0, "element topology: a DoF index or orientation is out of range");
+    top.n_elems = ne;
+    top.n = n;
+    *usable = true;
+    return SNP_OK;
+}
+
+int elem_sum_to_dofs(const ElemTopology &top, const double *Fe, const double *De, const double *rhs_extra,
+                     double *F, double *diag, cudaStream_t s) {
+    SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "element sums: topology not built");
+    k_sum_to_dofs<<<stride_grid(top.n, kEBlock, 8), kEBlock, 0, s>>>(top.n, top.n_elems, top.inc_ptr.p, top.inc.p, Fe,
+                                                                    De, rhs_extra, F, diag);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+// ---------------------------------------------------------------- PCG engine
+
+template <typename TT>
+ElemPcg<TT>::~ElemPcg() {
+    drop_graph();
+}
+
+template <typename TT>
+void ElemPcg<TT>::drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+}
+
+template <typename TT>
+int ElemPcg<TT>::reserve(int32_t n_, int64_t ne_) {
+    if (n_ == n && ne_ == ne && G.p) return SNP_OK;
+    drop_graph();
+    n = n_;
+    ne = ne_;
+    SNP_TRY(G.alloc(n));
+    SNP_TRY(R.alloc(n));
+    SNP_TRY(D.alloc(n));
+    SNP_TRY(V.alloc(ne));
+    const int gmax = sm_count() * 8 + 1;
+    SNP_TRY(part.alloc(3 * (size_t)gmax));
+    SNP_TRY(st.alloc(1));
+    SNP_TRY(hst.alloc(1));
+    SNP_TRY(bad.alloc(1));
+    SNP_CUDA_TRY(cudaMemset(st.p, 0, sizeof(PcgState)));
+    return SNP_OK;
+}
+
+template <typename TT>
+int ElemPcg<TT>::launch_iteration(const ElemTopology &top, const TT *T, const uint8_t *free_mask, cudaStream_t s,
+                                  int use_cond, cudaGraphConditionalHandle cond) {
+    const TT *chat = chat_ptr<TT>(top);
+    k_epass1<TT><<<wave_grid(k_epass1<TT>, ne, kEBlock), kEBlock, 0, s>>>(ne, top.edof.p, T, chat, G.p, V.p, st.p,
+                                                                         part.p);
+    SNP_LAUNCH_CHECK();
+    k_epass2<TT><<<wave_grid(k_epass2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, top.inc.p, chat,
+                                                                        V.p, G.p, R.p, D.p, st.p, part.p, use_cond,
+                                                                        cond);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+template <typename TT>
+int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask) {
+    drop_graph();
+    const char *env = getenv("SNP_PCG_GRAPH");
+    if (env && env[0] == '0') return SNP_OK;
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return SNP_OK;
+    }
+    cudaGraphConditionalHandle h;
+    cudaGraphNode_t node;
+    cudaGraphNodeParams cp = {};
+    bool ok = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&node, g, nullptr, 0, &cp) == cudaSuccess;
+    }
+    cudaStream_t cs = nullptr;
+    if (ok) ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            int rc = launch_iteration(top, T, free_mask, cs, 1, h);
+            cudaGraph_t out = nullptr;
+            cudaError_t e = cudaStreamEndCapture(cs, &out);
+            ok = (rc == SNP_OK) && e == cudaSuccess;
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+    if (cs) cudaStreamDestroy(cs);
+    if (!ok) {
+        cudaGetLastError();
+        clear_error();
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        cudaGraphDestroy(g);
+        return SNP_OK;
+    }
+    graph = g;
+    key_top = &top;
+    key_T = T;
+    key_fm = free_mask;
+    return SNP_OK;
+}
+
+template <typename TT>
+int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag, const uint8_t *free_mask,
+                       const double *b, double b_scale, double *h, double rtol, double atol, int64_t maxit,
+                       cudaStream_t s, int64_t *its, double *res, int *status) {
+    SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "element PCG: topology not built");
+    SNP_TRY(reserve(top.n, top.n_elems));
+    if (maxit < 0) maxit = 10 * (int64_t)n;
+    SNP_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    k_einit<TT><<<wave_grid(k_einit<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, b, b_scale, diag, G.p, R.p,
+                                                                      D.p, st.p, part.p, rtol, atol, (long long)maxit,
+                                                                      bad.p);
+    SNP_LAUNCH_CHECK();
+    launches += 1;
+    int hbad = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hbad) {
+        if (status) *status = SNP_ZERO_PIVOT;
+        return fail(SNP_ZERO_PIVOT, "element PCG: zero or non-finite Jacobian diagonal on a free DoF");
+    }
+    int64_t chunk_launches = -1;
+    const bool same = exec && key_top == &top && key_T == T && key_fm == free_mask;
+    if (!same) SNP_TRY(build_graph(top, T, free_mask));
+    if (exec) {
+        SNP_CUDA_TRY(cudaGraphLaunch(exec, s));
+    } else {
+        const int chunk = 32;
+        int64_t launched = 0;
+        while (true) {
+            for (int k = 0; k < chunk; ++k) SNP_TRY(launch_iteration(top, T, free_mask, s, 0, 0));
+            launched += chunk;
+            SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+            SNP_CUDA_TRY(cudaStreamSynchronize(s));
+            if (hst.p->done || launched > maxit + chunk) break;
+        }
+        chunk_launches = 2 * launched;
+    }
+    k_eextract<TT><<<stride_grid(n, kEBlock, 8), kEBlock, 0, s>>>(n, R.p, h);
+    SNP_LAUNCH_CHECK();
+    SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+    SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    const PcgState &H = *hst.p;
+    launches += 1 + (chunk_launches >= 0 ? chunk_launches : 2 * (H.iter > 0 ? H.iter : 1));
+    if (its) *its = H.iter;
+    if (res) *res = sqrt(H.rr);
+    int stt = SNP_OK;
+    if (H.done == 2) stt = SNP_NOT_CONVERGED;
+    else if (H.done == 3) stt = SNP_NAN_DETECTED;
+    if (status) *status = stt;
+    return SNP_OK;
+}
+
+template <typename TT>
+int ElemPcg<TT>::apply(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const TT *x, TT *y,
+                       cudaStream_t s) {
+    SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "element operator: topology not built");
+    SNP_TRY(reserve(top.n, top.n_elems));
+    const TT *chat = chat_ptr<TT>(top);
+    k_eapply1<TT><<<wave_grid(k_eapply1<TT>, ne, kEBlock), kEBlock, 0, s>>>(ne, top.edof.p, T, chat, free_mask, x, V.p);
+    SNP_LAUNCH_CHECK();
+    k_eapply2<TT><<<wave_grid(k_eapply2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, top.inc.p,
+                                                                          chat, V.p, y);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+template struct ElemPcg<double>;
+template struct ElemPcg<float>;
+
+}  // namespace snp

@@ -21,6 +21,7 @@
 #include "snp_common.cuh"
 #include "snp_internal.cuh"
 #include "snp_krylov.cuh"
+#include "snp_reduce.cuh"
 
 namespace snp {
 
@@ -28,29 +29,8 @@ namespace {
 
 constexpr int kVecBlock = 256;
 constexpr int kSpmvBlock = 256;
-
-__device__ __forceinline__ bool is_free(const uint8_t *free_mask, int64_t i) { return free_mask == nullptr || free_mask[i]; }
-
-// The block that takes the last ticket reduces `part[0 .. nparts)` (stride `width`).
-__device__ __forceinline__ bool last_block(unsigned int *counter) {
-    __shared__ bool s_last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned int t = atomicInc(counter, gridDim.x - 1);
-        s_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    return s_last;
-}
-
-template <typename T>
-__device__ double reduce_parts(const T *part, int nparts, int width, int comp, double *sh) {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < nparts; i += blockDim.x) v += (double)__ldcg(part + (int64_t)i * width + comp);
-    v = block_sum(v, sh);
-    return v;  // valid in thread 0
-}
+constexpr int kSpmvUnroll = 4;  // matrix entries per lane and pass
+constexpr int kVecIlp = 4;      // vector elements per thread and pass
 
 // y = A x restricted to free rows/cols; TPR threads per row.  DOT: also p.y partial sums.
 template <typename VT, typename XT, int TPR, bool MASKCOL, bool DOT>
@@ -72,9 +52,26 @@ __global__ void __launch_bounds__(kSpmvBlock)
         const bool fr = valid && is_free(free_mask, row);
         if (fr) {
             const int b = __ldg(rp + row), e = __ldg(rp + row + 1);
-            for (int k = b + lane; k < e; k += TPR) {
-                const int c = __ldg(ci + k);
-                if (!MASKCOL || is_free(free_mask, c)) s += (double)__ldg(v + k) * (double)__ldg(x + c);
+            // kSpmvUnroll independent index/value loads per lane before any gather; the matrix
+            // is streamed (evict-first) so the gathered vector stays in L2
+            for (int k0 = b; k0 < e; k0 += TPR * kSpmvUnroll) {
+                int c[kSpmvUnroll];
+                VT a[kSpmvUnroll];
+#pragma unroll
+                for (int u = 0; u < kSpmvUnroll; ++u) {
+                    const int k = k0 + lane + u * TPR;
+                    if (k < e) {
+                        c[u] = __ldcs(ci + k);
+                        a[u] = __ldcs(v + k);
+                    } else {
+                        c[u] = -1;
+                        a[u] = VT(0);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kSpmvUnroll; ++u)
+                    if (c[u] >= 0 && (!MASKCOL || is_free(free_mask, c[u])))
+                        s += (double)a[u] * (double)__ldg(x + c[u]);
             }
         }
 #pragma unroll
@@ -97,37 +94,65 @@ __global__ void __launch_bounds__(kSpmvBlock)
     }
 }
 
+// x += alpha p, r -= alpha q, z = dinv r on free rows; r.z and r.r reduced by the last block,
+// which also forms beta and the convergence flag.  kVecIlp independent elements per thread.
 template <typename XT>
 __global__ void __launch_bounds__(kVecBlock)
     k_update(int32_t n, const uint8_t *__restrict__ free_mask, XT *__restrict__ x, XT *__restrict__ r,
              XT *__restrict__ z, const XT *__restrict__ p, const XT *__restrict__ q, const XT *__restrict__ dinv,
              PcgState *st, double *part, int use_cond, cudaGraphConditionalHandle cond) {
-    __shared__ double sh[32];
+    __shared__ double sh2[2][32];
     if (st->done) {
         if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
         return;
     }
     const XT alpha = (XT)st->alpha;
     double rz = 0.0, rr = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (is_free(free_mask, i)) {
-            x[i] += alpha * p[i];
-            const XT ri = r[i] - alpha * q[i];
-            const XT zi = dinv[i] * ri;
-            r[i] = ri;
-            z[i] = zi;
-            rz += (double)ri * (double)zi;
-            rr += (double)ri * (double)ri;
+    for (int64_t base = (int64_t)blockIdx.x * kVecBlock * kVecIlp; base < n;
+         base += (int64_t)gridDim.x * kVecBlock * kVecIlp) {
+        XT pv[kVecIlp], rv[kVecIlp], qv[kVecIlp], dv[kVecIlp], xv[kVecIlp];
+        bool f[kVecIlp];
+#pragma unroll
+        for (int j = 0; j < kVecIlp; ++j) {
+            const int64_t i = base + threadIdx.x + (int64_t)j * kVecBlock;
+            f[j] = i < n && is_free(free_mask, i);
+            if (f[j]) {
+                pv[j] = p[i];
+                rv[j] = r[i];
+                qv[j] = q[i];
+                dv[j] = dinv[i];
+                xv[j] = x[i];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kVecIlp; ++j) {
+            if (f[j]) {
+                const int64_t i = base + threadIdx.x + (int64_t)j * kVecBlock;
+                const XT ri = rv[j] - alpha * qv[j];
+                const XT zi = dv[j] * ri;
+                x[i] = xv[j] + alpha * pv[j];
+                r[i] = ri;
+                z[i] = zi;
+                rz += (double)ri * (double)zi;
+                rr += (double)ri * (double)ri;
+            }
         }
     }
-    const double brz = block_sum(rz, sh);
-    if (threadIdx.x == 0) part[2 * blockIdx.x] = brz;
-    const double brr = block_sum(rr, sh);
-    if (threadIdx.x == 0) part[2 * blockIdx.x + 1] = brr;
+    block_sum2(rz, rr, sh2);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = rz;
+        part[2 * blockIdx.x + 1] = rr;
+    }
     if (last_block(&st->counter)) {
-        const double rz_new = reduce_parts(part, gridDim.x, 2, 0, sh);
-        const double rr_new = reduce_parts(part, gridDim.x, 2, 1, sh);
+        double a = 0.0, b = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+            a += __ldcg(part + 2 * i);
+            b += __ldcg(part + 2 * i + 1);
+        }
+        __syncthreads();
+        block_sum2(a, b, sh2);
         if (threadIdx.x == 0) {
+            const double rz_new = a, rr_new = b;
             st->beta = rz_new / st->rz;
             st->rz = rz_new;
             st->rr = rr_new;
@@ -142,14 +167,32 @@ __global__ void __launch_bounds__(kVecBlock)
     }
 }
 
+// p = z + beta p on free rows, kVecIlp independent elements per thread.
 template <typename XT>
 __global__ void __launch_bounds__(kVecBlock)
     k_pupdate(int32_t n, const uint8_t *__restrict__ free_mask, XT *__restrict__ p, const XT *__restrict__ z,
               const PcgState *st) {
     if (st->done) return;
     const XT beta = (XT)st->beta;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        if (is_free(free_mask, i)) p[i] = z[i] + beta * p[i];
+    for (int64_t base = (int64_t)blockIdx.x * kVecBlock * kVecIlp; base < n;
+         base += (int64_t)gridDim.x * kVecBlock * kVecIlp) {
+        XT zv[kVecIlp], pv[kVecIlp];
+        bool f[kVecIlp];
+#pragma unroll
+        for (int j = 0; j < kVecIlp; ++j) {
+            const int64_t i = base + threadIdx.x + (int64_t)j * kVecBlock;
+            f[j] = i < n && is_free(free_mask, i);
+            if (f[j]) {
+                zv[j] = z[i];
+                pv[j] = p[i];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kVecIlp; ++j) {
+            const int64_t i = base + threadIdx.x + (int64_t)j * kVecBlock;
+            if (f[j]) p[i] = zv[j] + beta * pv[j];
+        }
+    }
 }
 
 // r = b - q (free rows), z = dinv r, p = z; x = 0 on non-free rows; partials of r.z, r.r, b.b
@@ -253,58 +296,127 @@ int find_diag(int32_t n, const int32_t *rp, const int32_t *ci, int32_t *diag, cu
     return SNP_OK;
 }
 
+// lanes per row: each lane takes kSpmvUnroll entries per pass, so rows of up to
+// kSpmvUnroll * TPR entries finish in one pass
 int choose_tpr(int64_t nnz, int32_t n) {
     const double avg = n > 0 ? (double)nnz / n : 0.0;
-    if (avg > 48) return 32;
-    if (avg > 24) return 16;
-    if (avg > 10) return 8;
+    if (avg > 96) return 32;
+    if (avg > 48) return 16;
+    if (avg > 24) return 8;
     return 4;
+}
+
+template <typename VT, typename XT, int TPR, bool MASKCOL, bool DOT>
+static void spmv_launch(int32_t n, const int32_t *rp, const int32_t *ci, const VT *v, const uint8_t *fm, const XT *x,
+                        XT *y, PcgState *st, double *part, cudaStream_t s) {
+    const int64_t groups = kSpmvBlock / TPR;
+    auto kern = k_spmv<VT, XT, TPR, MASKCOL, DOT>;
+    const int grid = wave_grid(kern, (n + groups - 1) / groups * kSpmvBlock, kSpmvBlock);
+    kern<<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part);
 }
 
 template <typename VT, typename XT, bool MASKCOL, bool DOT>
 static int spmv_dispatch(int tpr, int32_t n, const int32_t *rp, const int32_t *ci, const VT *v, const uint8_t *fm,
-                         const XT *x, XT *y, PcgState *st, double *part, int grid, cudaStream_t s) {
+                         const XT *x, XT *y, PcgState *st, double *part, cudaStream_t s) {
     switch (tpr) {
-        case 4: k_spmv<VT, XT, 4, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
-        case 8: k_spmv<VT, XT, 8, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
-        case 16: k_spmv<VT, XT, 16, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
-        default: k_spmv<VT, XT, 32, MASKCOL, DOT><<<grid, kSpmvBlock, 0, s>>>(n, rp, ci, v, fm, x, y, st, part); break;
+        case 4: spmv_launch<VT, XT, 4, MASKCOL, DOT>(n, rp, ci, v, fm, x, y, st, part, s); break;
+        case 8: spmv_launch<VT, XT, 8, MASKCOL, DOT>(n, rp, ci, v, fm, x, y, st, part, s); break;
+        case 16: spmv_launch<VT, XT, 16, MASKCOL, DOT>(n, rp, ci, v, fm, x, y, st, part, s); break;
+        default: spmv_launch<VT, XT, 32, MASKCOL, DOT>(n, rp, ci, v, fm, x, y, st, part, s); break;
     }
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }
 
-int spmv_grid(int32_t n, int tpr) {
-    const int64_t groups = kSpmvBlock / tpr;
-    return stride_grid((n + groups - 1) / groups * kSpmvBlock, kSpmvBlock, 8);
+// y = A x with A in SELL-C-sigma order: one warp per 32-row slice, one thread per row, four
+// independent coalesced (column, value) loads per thread before the gathers.  DOT as k_spmv.
+template <typename VT, typename XT, bool MASKCOL, bool DOT>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmv_sell(int64_t n_slices, const int64_t *__restrict__ off, const int32_t *__restrict__ srow,
+                const int32_t *__restrict__ col, const VT *__restrict__ v, const uint8_t *__restrict__ free_mask,
+                const XT *__restrict__ x, XT *__restrict__ y, PcgState *st, double *part) {
+    __shared__ double sh[32];
+    if (DOT && st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    double dot = 0.0;
+    for (int64_t sl = warp; sl < n_slices; sl += nwarps) {
+        const int32_t row = __ldg(srow + sl * 32 + lane);
+        if (row < 0) continue;
+        const int64_t o = __ldg(off + sl);
+        const int L = (int)((__ldg(off + sl + 1) - o) >> 5);
+        const bool fr = is_free(free_mask, row);
+        double sum = 0.0;
+        if (fr) {
+            const VT *vp = v + o + lane;
+            const int32_t *cp = col + o + lane;
+            int k = 0;
+            for (; k + kSpmvUnroll <= L; k += kSpmvUnroll) {
+                int c[kSpmvUnroll];
+                VT a[kSpmvUnroll];
+#pragma unroll
+                for (int u = 0; u < kSpmvUnroll; ++u) {
+                    c[u] = __ldcs(cp + (int64_t)(k + u) * 32);
+                    a[u] = __ldcs(vp + (int64_t)(k + u) * 32);
+                }
+#pragma unroll
+                for (int u = 0; u < kSpmvUnroll; ++u)
+                    if (!MASKCOL || is_free(free_mask, c[u])) sum += (double)a[u] * (double)__ldg(x + c[u]);
+            }
+            for (; k < L; ++k) {
+                const int c = __ldcs(cp + (int64_t)k * 32);
+                if (!MASKCOL || is_free(free_mask, c)) sum += (double)__ldcs(vp + (int64_t)k * 32) * (double)__ldg(x + c);
+            }
+        }
+        y[row] = fr ? (XT)sum : (XT)0;
+        if (DOT && fr) dot += (double)x[row] * sum;
+    }
+    if (DOT) {
+        dot = block_sum(dot, sh);
+        if (threadIdx.x == 0) part[blockIdx.x] = dot;
+        if (last_block(&st->counter)) {
+            const double pq = reduce_parts(part, gridDim.x, 1, 0, sh);
+            if (threadIdx.x == 0) {
+                st->pq = pq;
+                st->alpha = st->rz / pq;
+            }
+        }
+    }
+}
+
+// Launch the SpMV for A's layout (SELL when present, else CSR with TPR lanes per row).
+template <typename VT, typename XT, bool MASKCOL, bool DOT>
+static int spmv_run(const CsrView<VT> &A, const uint8_t *fm, const XT *x, XT *y, PcgState *st, double *part,
+                    cudaStream_t s) {
+    if (A.sell_off) {
+        auto kern = k_spmv_sell<VT, XT, MASKCOL, DOT>;
+        const int grid = wave_grid(kern, A.n_slices * 32, kSpmvBlock);
+        kern<<<grid, kSpmvBlock, 0, s>>>(A.n_slices, A.sell_off, A.sell_row, A.sell_col, A.v, fm, x, y, st, part);
+        SNP_LAUNCH_CHECK();
+        return SNP_OK;
+    }
+    const int tpr = choose_tpr(A.nnz, A.n);
+    return spmv_dispatch<VT, XT, MASKCOL, DOT>(tpr, A.n, A.rp, A.ci, A.v, fm, x, y, st, part, s);
 }
 
 int spmv_f64(const CsrView<double> &A, const uint8_t *free_mask, const double *x, double *y, cudaStream_t s) {
-    const int tpr = choose_tpr(A.nnz, A.n);
-    const int grid = spmv_grid(A.n, tpr);
     if (free_mask)
-        return spmv_dispatch<double, double, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, y, nullptr, nullptr,
-                                                          grid, s);
-    return spmv_dispatch<double, double, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, y, nullptr, nullptr, grid, s);
+        return spmv_run<double, double, true, false>(A, free_mask, x, y, nullptr, nullptr, s);
+    return spmv_run<double, double, false, false>(A, nullptr, x, y, nullptr, nullptr, s);
 }
 
 int spmv_f32(const CsrView<float> &A, const uint8_t *free_mask, const float *x, float *y, cudaStream_t s) {
-    const int tpr = choose_tpr(A.nnz, A.n);
-    const int grid = spmv_grid(A.n, tpr);
     if (free_mask)
-        return spmv_dispatch<float, float, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, y, nullptr, nullptr,
-                                                        grid, s);
-    return spmv_dispatch<float, float, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, y, nullptr, nullptr, grid, s);
+        return spmv_run<float, float, true, false>(A, free_mask, x, y, nullptr, nullptr, s);
+    return spmv_run<float, float, false, false>(A, nullptr, x, y, nullptr, nullptr, s);
 }
 
 // float32 matrix applied to a float64 vector with float64 accumulation (refinement residuals)
 int spmv_f32_f64(const CsrView<float> &A, const uint8_t *free_mask, const double *x, double *y, cudaStream_t s) {
-    const int tpr = choose_tpr(A.nnz, A.n);
-    const int grid = spmv_grid(A.n, tpr);
     if (free_mask)
-        return spmv_dispatch<float, double, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, y, nullptr, nullptr,
-                                                         grid, s);
-    return spmv_dispatch<float, double, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, y, nullptr, nullptr, grid, s);
+        return spmv_run<float, double, true, false>(A, free_mask, x, y, nullptr, nullptr, s);
+    return spmv_run<float, double, false, false>(A, nullptr, x, y, nullptr, nullptr, s);
 }
 
 // ------------------------------------------------------------------ PCG engine
@@ -362,14 +474,13 @@ int Pcg<VT, XT>::set_jacobi(const CsrView<VT> &A, const int32_t *diag_pos, const
 template <typename VT, typename XT>
 int Pcg<VT, XT>::launch_iteration(const CsrView<VT> &A, const uint8_t *free_mask, XT *x, cudaStream_t s, int use_cond,
                                   cudaGraphConditionalHandle cond) {
-    const int tpr = choose_tpr(A.nnz, A.n);
-    const int g_spmv = spmv_grid(A.n, tpr);
-    if (free_mask) SNP_TRY((spmv_dispatch<VT, XT, false, true>(tpr, A.n, A.rp, A.ci, A.v, free_mask, p.p, q.p, st.p, part.p, g_spmv, s)));
-    else SNP_TRY((spmv_dispatch<VT, XT, false, true>(tpr, A.n, A.rp, A.ci, A.v, nullptr, p.p, q.p, st.p, part.p, g_spmv, s)));
-    const int g = stride_grid(A.n, kVecBlock, 8);
-    k_update<XT><<<g, kVecBlock, 0, s>>>(A.n, free_mask, x, r.p, z.p, p.p, q.p, dinv.p, st.p, part.p, use_cond, cond);
+    if (free_mask) SNP_TRY((spmv_run<VT, XT, false, true>(A, free_mask, p.p, q.p, st.p, part.p, s)));
+    else SNP_TRY((spmv_run<VT, XT, false, true>(A, nullptr, p.p, q.p, st.p, part.p, s)));
+    const int64_t nt = (A.n + kVecIlp - 1) / kVecIlp;
+    k_update<XT><<<wave_grid(k_update<XT>, nt, kVecBlock), kVecBlock, 0, s>>>(A.n, free_mask, x, r.p, z.p, p.p, q.p,
+                                                                             dinv.p, st.p, part.p, use_cond, cond);
     SNP_LAUNCH_CHECK();
-    k_pupdate<XT><<<g, kVecBlock, 0, s>>>(A.n, free_mask, p.p, z.p, st.p);
+    k_pupdate<XT><<<wave_grid(k_pupdate<XT>, nt, kVecBlock), kVecBlock, 0, s>>>(A.n, free_mask, p.p, z.p, st.p);
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }
@@ -435,13 +546,10 @@ int Pcg<VT, XT>::solve(const CsrView<VT> &A, const uint8_t *free_mask, const XT 
     // initial residual
     const int g = stride_grid(A.n, kVecBlock, 8);
     if (!zero_x) {
-        const int tpr = choose_tpr(A.nnz, A.n);
         if (free_mask)
-            SNP_TRY((spmv_dispatch<VT, XT, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, q.p, nullptr, nullptr,
-                                                         spmv_grid(A.n, tpr), s)));
+            SNP_TRY((spmv_run<VT, XT, true, false>(A, free_mask, x, q.p, nullptr, nullptr, s)));
         else
-            SNP_TRY((spmv_dispatch<VT, XT, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, q.p, nullptr, nullptr,
-                                                          spmv_grid(A.n, tpr), s)));
+            SNP_TRY((spmv_run<VT, XT, false, false>(A, nullptr, x, q.p, nullptr, nullptr, s)));
         launches += 1;
     }
     k_init<XT><<<g, kVecBlock, 0, s>>>(A.n, free_mask, b, x, r.p, z.p, p.p, q.p, dinv.p, st.p, part.p, rtol, atol,
@@ -494,22 +602,22 @@ int pcg_on_buffers(const CsrView<double> &A, const uint8_t *free_mask, const dou
     SNP_CUDA_TRY(cudaMemsetAsync(B.bad, 0, sizeof(int), s));
     SNP_TRY(find_diag(A.n, A.rp, A.ci, B.diag, s));
     const int gv = stride_grid(A.n, kVecBlock, 8);
-    SNP_REQUIRE(gv <= B.max_blocks, "pcg: %d blocks exceed the %d partial-sum slots", gv, B.max_blocks);
+    const int64_t nt = (A.n + kVecIlp - 1) / kVecIlp;
+    const int gu = wave_grid(k_update<double>, nt, kVecBlock);
+    const int gp = wave_grid(k_pupdate<double>, nt, kVecBlock);
+    SNP_REQUIRE(gv <= B.max_blocks && gu <= B.max_blocks, "pcg: %d blocks exceed the %d partial-sum slots",
+                gv > gu ? gv : gu, B.max_blocks);
     k_dinv<double, double><<<gv, kVecBlock, 0, s>>>(A.n, B.diag, A.v, free_mask, B.dinv, B.bad);
     SNP_LAUNCH_CHECK();
     int hbad = 0;
     SNP_CUDA_TRY(cudaMemcpyAsync(&hbad, B.bad, sizeof(int), cudaMemcpyDeviceToHost, s));
     SNP_CUDA_TRY(cudaStreamSynchronize(s));
     if (hbad) return fail(SNP_ZERO_PIVOT, "pcg: zero or missing diagonal entry on a free row");
-    const int tpr = choose_tpr(A.nnz, A.n);
-    const int gs = spmv_grid(A.n, tpr);
-    SNP_REQUIRE(gs <= B.max_blocks, "pcg: %d blocks exceed the %d partial-sum slots", gs, B.max_blocks);
+
     if (free_mask)
-        SNP_TRY((spmv_dispatch<double, double, true, false>(tpr, A.n, A.rp, A.ci, A.v, free_mask, x, B.q, nullptr,
-                                                             nullptr, gs, s)));
+        SNP_TRY((spmv_run<double, double, true, false>(A, free_mask, x, B.q, nullptr, nullptr, s)));
     else
-        SNP_TRY((spmv_dispatch<double, double, false, false>(tpr, A.n, A.rp, A.ci, A.v, nullptr, x, B.q, nullptr,
-                                                              nullptr, gs, s)));
+        SNP_TRY((spmv_run<double, double, false, false>(A, nullptr, x, B.q, nullptr, nullptr, s)));
     k_init<double><<<gv, kVecBlock, 0, s>>>(A.n, free_mask, b, x, B.r, B.z, B.p, B.q, B.dinv, B.st, B.part, rtol, atol,
                                             (long long)maxit, 0);
     SNP_LAUNCH_CHECK();
@@ -524,14 +632,12 @@ int pcg_on_buffers(const CsrView<double> &A, const uint8_t *free_mask, const dou
         if (H.done || launched > maxit + chunk) break;
         for (int k = 0; k < chunk; ++k) {
             if (free_mask)
-                SNP_TRY((spmv_dispatch<double, double, false, true>(tpr, A.n, A.rp, A.ci, A.v, free_mask, B.p, B.q, B.st,
-                                                                     B.part, gs, s)));
+                SNP_TRY((spmv_run<double, double, false, true>(A, free_mask, B.p, B.q, B.st, B.part, s)));
             else
-                SNP_TRY((spmv_dispatch<double, double, false, true>(tpr, A.n, A.rp, A.ci, A.v, nullptr, B.p, B.q, B.st,
-                                                                     B.part, gs, s)));
-            k_update<double><<<gv, kVecBlock, 0, s>>>(A.n, free_mask, x, B.r, B.z, B.p, B.q, B.dinv, B.st, B.part, 0, 0);
+                SNP_TRY((spmv_run<double, double, false, true>(A, nullptr, B.p, B.q, B.st, B.part, s)));
+            k_update<double><<<gu, kVecBlock, 0, s>>>(A.n, free_mask, x, B.r, B.z, B.p, B.q, B.dinv, B.st, B.part, 0, 0);
             SNP_LAUNCH_CHECK();
-            k_pupdate<double><<<gv, kVecBlock, 0, s>>>(A.n, free_mask, B.p, B.z, B.st);
+            k_pupdate<double><<<gp, kVecBlock, 0, s>>>(A.n, free_mask, B.p, B.z, B.st);
             SNP_LAUNCH_CHECK();
         }
         launched += chunk;

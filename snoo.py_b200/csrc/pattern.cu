@@ -156,6 +156,133 @@ int pattern_create(const int32_t *elem_dofs, int64_t n_elems, int32_t dpe, int32
     return SNP_OK;
 }
 
+// ------------------------------------------------------------------ SELL-C-sigma layout
+
+namespace {
+
+constexpr int kSellC = 32;
+constexpr int kSellSigma = 256;
+
+// key = window * 256 + (255 - min(length, 255)): ascending sort = windows in order, longest first
+__global__ void k_sell_keys(int32_t n, const int32_t *__restrict__ rp, uint32_t *__restrict__ key,
+                            int32_t *__restrict__ row) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        int len = rp[r + 1] - rp[r];
+        if (len > 255) len = 255;
+        key[r] = (uint32_t)(r / kSellSigma) * 256u + (uint32_t)(255 - len);
+        row[r] = (int32_t)r;
+    }
+}
+
+// slot rows and slice widths (entries of the longest row of each slice)
+__global__ void k_sell_slices(int32_t n, int64_t n_slices, const int32_t *__restrict__ rp,
+                              const int32_t *__restrict__ sorted_row, int32_t *__restrict__ slice_row,
+                              int64_t *__restrict__ width) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n_slices; s += (int64_t)gridDim.x * blockDim.x) {
+        int w = 0;
+        for (int l = 0; l < kSellC; ++l) {
+            const int64_t i = s * kSellC + l;
+            const int32_t r = i < n ? sorted_row[i] : -1;
+            slice_row[s * kSellC + l] = r;
+            if (r >= 0) {
+                const int len = rp[r + 1] - rp[r];
+                w = len > w ? len : w;
+            }
+        }
+        width[s] = (int64_t)w * kSellC;
+    }
+}
+
+// one thread per slot: column indices (padding: the slot's own row) and CSR -> SELL positions
+__global__ void k_sell_fill(int64_t n_slices, const int64_t *__restrict__ off, const int32_t *__restrict__ slice_row,
+                            const int32_t *__restrict__ rp, const int32_t *__restrict__ ci, int32_t *__restrict__ col,
+                            int32_t *__restrict__ csr2sell) {
+    const int64_t total = n_slices * kSellC;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = t / kSellC;
+        const int lane = (int)(t - s * kSellC);
+        const int64_t o = off[s];
+        const int L = (int)((off[s + 1] - o) / kSellC);
+        const int32_t r = slice_row[t];
+        const int b = r >= 0 ? rp[r] : 0;
+        const int len = r >= 0 ? rp[r + 1] - b : 0;
+        for (int k = 0; k < L; ++k) {
+            const int64_t pos = o + (int64_t)k * kSellC + lane;
+            if (k < len) {
+                col[pos] = ci[b + k];
+                csr2sell[b + k] = (int32_t)pos;
+            } else {
+                col[pos] = r >= 0 ? r : 0;
+            }
+        }
+    }
+}
+
+__global__ void k_gather_i32(int64_t n, const int32_t *__restrict__ map, const int32_t *__restrict__ idx,
+                             int32_t *__restrict__ out) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t i = idx[t];
+        out[t] = i >= 0 ? map[i] : -1;
+    }
+}
+
+}  // namespace
+
+int build_sell(const snp_pattern *pat, SellLayout &S, cudaStream_t st) {
+    SNP_REQUIRE(pat != nullptr, "build_sell: pattern is NULL");
+    const int32_t n = pat->n_rows;
+    const int64_t n_slices = (n + kSellC - 1) / kSellC;
+    S.n_slices = n_slices;
+    DevBuf<uint32_t> key, key2;
+    DevBuf<int32_t> row, row2;
+    DevBuf<int64_t> width;
+    DevBuf<unsigned char> temp;
+    SNP_TRY(key.alloc(n));
+    SNP_TRY(key2.alloc(n));
+    SNP_TRY(row.alloc(n));
+    SNP_TRY(row2.alloc(n));
+    SNP_TRY(width.alloc(n_slices + 1));
+    SNP_TRY(S.slice_off.alloc(n_slices + 1));
+    SNP_TRY(S.slice_row.alloc(n_slices * kSellC));
+    k_sell_keys<<<stride_grid(n, 256, 8), 256, 0, st>>>(n, pat->row_ptr.p, key.p, row.p);
+    SNP_LAUNCH_CHECK();
+    size_t tb_sort = 0, tb_scan = 0;
+    cub::DoubleBuffer<uint32_t> dk(key.p, key2.p);
+    cub::DoubleBuffer<int32_t> dv(row.p, row2.p);
+    cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, dk, dv, n, 0, 32, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, width.p, S.slice_off.p, n_slices + 1, st);
+    SNP_TRY(temp.alloc(tb_sort > tb_scan ? tb_sort : tb_scan));
+    SNP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.p, tb_sort, dk, dv, n, 0, 32, st));
+    SNP_CUDA_TRY(cudaMemsetAsync(width.p + n_slices, 0, sizeof(int64_t), st));
+    k_sell_slices<<<stride_grid(n_slices, 256, 8), 256, 0, st>>>(n, n_slices, pat->row_ptr.p, dv.Current(),
+                                                                 S.slice_row.p, width.p);
+    SNP_LAUNCH_CHECK();
+    SNP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp.p, tb_scan, width.p, S.slice_off.p, n_slices + 1, st));
+    int64_t total = 0;
+    SNP_CUDA_TRY(cudaMemcpyAsync(&total, S.slice_off.p + n_slices, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SNP_CUDA_TRY(cudaStreamSynchronize(st));
+    SNP_REQUIRE(total < (int64_t)0x7fffffff, "build_sell: %lld stored entries exceed the 32-bit slot range",
+                (long long)total);
+    S.total = total;
+    SNP_TRY(S.col.alloc(total));
+    SNP_TRY(S.csr2sell.alloc(pat->nnz > 0 ? pat->nnz : 1));
+    SNP_TRY(S.diag.alloc(n));
+    const int64_t n_slot = pat->n_elems * pat->dpe * pat->dpe;
+    SNP_TRY(S.slots.alloc(n_slot > 0 ? n_slot : 1));
+    k_sell_fill<<<stride_grid(n_slices * kSellC, 256, 16), 256, 0, st>>>(n_slices, S.slice_off.p, S.slice_row.p,
+                                                                        pat->row_ptr.p, pat->col_idx.p, S.col.p,
+                                                                        S.csr2sell.p);
+    SNP_LAUNCH_CHECK();
+    k_gather_i32<<<stride_grid(n, 256, 8), 256, 0, st>>>(n, S.csr2sell.p, pat->diag_pos.p, S.diag.p);
+    SNP_LAUNCH_CHECK();
+    if (n_slot > 0) {
+        k_gather_i32<<<stride_grid(n_slot, 256, 16), 256, 0, st>>>(n_slot, S.csr2sell.p, pat->slots.p, S.slots.p);
+        SNP_LAUNCH_CHECK();
+    }
+    SNP_CUDA_TRY(cudaStreamSynchronize(st));
+    return SNP_OK;
+}
+
 }  // namespace snp
 
 extern "C" {

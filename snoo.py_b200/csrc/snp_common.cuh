@@ -50,6 +50,20 @@ inline int stride_grid(int64_t n, int block, int per_sm) {
     return (int)(need < cap ? need : cap);
 }
 
+// Blocks of `block` threads (with `smem` dynamic shared bytes) of `kernel` that one SM holds
+// at once (occupancy API, cached per kernel and device; at most 8, at least 1).
+int resident_blocks(const void *kernel, int block, size_t smem);
+
+// Grid for a grid-stride kernel: enough blocks for n_threads, capped at one full wave of
+// resident blocks, so no block waits for a second wave.
+template <typename Kernel>
+inline int wave_grid(Kernel kernel, int64_t n_threads, int block, size_t smem = 0) {
+    int64_t need = (n_threads + block - 1) / block;
+    if (need < 1) need = 1;
+    const int64_t cap = (int64_t)sm_count() * resident_blocks(reinterpret_cast<const void *>(kernel), block, smem);
+    return (int)(need < cap ? need : cap);
+}
+
 constexpr double kNu0 = 1.0 / 4.0 / 3.14159265358979323846 * 1e7;  // vacuum reluctance
 
 // ---------------------------------------------------------------- material laws

@@ -98,14 +98,41 @@ struct CurlArgs {
     float *J32;
     double *rhs;
     double *F;
+    // element-tensor outputs (launch_curlcurl_tensor), all [k * t_stride + e] with the
+    // pointers already offset to this material: S_e in float64 or float32 (components
+    // xx xy xz yy yz zz), and per element edge k its residual term Fe and Jacobian
+    // diagonal term De (summed per DoF afterwards, in a fixed order)
+    double *T64;
+    float *T32;
+    int64_t t_stride;
+    double *Fe;
+    double *De;
 };
 
 // Launch the fused assembly for one material.  Tables must be affine (checked by the caller).
 int launch_curlcurl(const CurlArgs &a, cudaStream_t st);
 
+// Element tensors of the Newton Jacobian for one material: S_e = Jm^T (kfac I + M) Jm with
+// J_e,jk = chat_j . S_e chat_k (chat_j: reference curls of the element's orientation), plus
+// the element terms of diag(J) and of F = K(x) x - rhs(x).  Tables must be affine.
+int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st);
+
 // Validate that d_phi and curls do not vary across quadrature points; sets *affine.
 int check_affine_tables(const double *curls, int32_t n_orient, const double *d_phi, int32_t nq, cudaStream_t st,
                         bool *affine);
+
+// SELL-C-sigma copy of a CSR pattern (C = 32 rows per slice, rows sorted by length within
+// windows of sigma rows, each slice stored column-major and padded to its longest row).
+struct SellLayout {
+    int64_t n_slices = 0;
+    int64_t total = 0;                   // stored entries including padding
+    DevBuf<int64_t> slice_off;           // [n_slices + 1] element offset of each slice
+    DevBuf<int32_t> slice_row;           // [n_slices * 32] original row of each slot (-1: padding row)
+    DevBuf<int32_t> col;                 // [total] column index (padding: the slot's own row, value 0)
+    DevBuf<int32_t> csr2sell;            // [nnz] SELL position of each CSR position
+    DevBuf<int32_t> diag;                // [n_rows] SELL position of each row's diagonal (-1: none)
+    DevBuf<int32_t> slots;               // [n_elems * dpe * dpe] slot map into the SELL values
+};
 
 }  // namespace snp
 
@@ -116,3 +143,8 @@ struct snp_pattern {
     int32_t dpe = 0;
     snp::DevBuf<int32_t> row_ptr, col_idx, slots, diag_pos;
 };
+
+namespace snp {
+// Build the SELL layout of a pattern (and its slot map) on the device.
+int build_sell(const snp_pattern *pat, SellLayout &S, cudaStream_t st);
+}  // namespace snp

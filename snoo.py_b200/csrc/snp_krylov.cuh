@@ -8,6 +8,8 @@
 
 namespace snp {
 
+// A square sparse matrix: CSR (rp, ci, v), or, when sell_off is set, the SELL-C-sigma layout
+// of the same pattern with the values v stored in SELL order (rp/ci still describe the CSR).
 template <typename VT>
 struct CsrView {
     int32_t n;
@@ -15,6 +17,10 @@ struct CsrView {
     const int32_t *rp;
     const int32_t *ci;
     const VT *v;
+    int64_t n_slices = 0;
+    const int64_t *sell_off = nullptr;
+    const int32_t *sell_row = nullptr;
+    const int32_t *sell_col = nullptr;
 };
 
 // Device-resident CG state, written only by the last block of each reduction.
@@ -81,6 +87,101 @@ struct Pcg {
     int launch_iteration(const CsrView<VT> &A, const uint8_t *free_mask, XT *x, cudaStream_t s, int use_cond,
                          cudaGraphConditionalHandle cond);
     int build_graph(const CsrView<VT> &A, const uint8_t *free_mask, XT *x, cudaStream_t s);
+};
+
+// ------------------------------------------------------------------ matrix-free Jacobian
+//
+// The Newton Jacobian of first-order Nedelec curl-curl on affine tetrahedra is stored per
+// element as the 3x3 symmetric tensor S_e (six numbers): J_e,jk = s_j s_k chat_j . S_e chat_k,
+// chat_j the reference curls of orientation 0 and s_j = +-1 the element's edge signs.  A
+// product y = J x is two passes without atomics:
+//   element pass  u_e = sum_j s_j x_j chat_j,  v_e = S_e u_e          (stores v_e)
+//   DoF pass      y_i = sum over incident (e, k) of s_k chat_k . v_e  (gathers v_e)
+
+// Element topology of the operator: DoFs with edge signs and the DoF -> (element, local
+// edge) incidence, built once per mesh.
+struct ElemTopology {
+    int64_t n_elems = 0;
+    int32_t n = 0;
+    DevBuf<int32_t> edof;     // [6][n_elems]  DoF, bit 31 set when the edge function is negated
+    DevBuf<int32_t> inc_ptr;  // [n + 1]
+    DevBuf<int32_t> inc;      // [6 n_elems]   (e << 3 | k), bit 31 = sign, grouped by DoF
+    DevBuf<double> chat64;    // [18] reference curls of orientation 0
+    DevBuf<float> chat32;
+};
+
+// One material's elements: gids [count][6], orientation index [count], placed at `offset`.
+struct ElemBlock {
+    const int32_t *gids;
+    const int32_t *orient;
+    int64_t count;
+    int64_t offset;
+};
+
+// Build the topology.  ctab_host: curls at quadrature point 0, [n_orient][6][3].  Sets
+// *usable = false (and builds nothing) when the orientation tables are not sign flips of
+// orientation 0 or the mesh exceeds the 32-bit incidence encoding.
+int build_elem_topology(ElemTopology &top, int32_t n, const ElemBlock *blocks, int n_blocks, const double *ctab_host,
+                        int32_t n_orient, cudaStream_t s, bool *usable);
+
+// Per-DoF CG state, split by who reads it: the element pass gathers {z, p} (16 bytes in
+// float64, two DoFs per 32-byte sector); {r, x} and 1/diag are read only by the DoF's own
+// thread in the DoF pass.
+// Per-DoF sums of element-edge terms [6][n_elems] in incidence order (deterministic):
+// F_i = sum Fe - rhs_extra_i (rhs_extra may be NULL), diag_i = sum De.
+int elem_sum_to_dofs(const ElemTopology &top, const double *Fe, const double *De, const double *rhs_extra,
+                     double *F, double *diag, cudaStream_t s);
+
+template <typename TT>
+struct alignas(2 * sizeof(TT)) DofPair {
+    TT a, b;
+};
+
+template <typename TT>
+struct alignas(4 * sizeof(TT)) ElemVec {
+    TT a, b, c, pad;
+};
+
+// Jacobi-PCG on the matrix-free Jacobian (values TT = double or float; sums in double),
+// scipy cg's stopping rule, iteration loop in a CUDA-graph conditional WHILE node.
+template <typename TT>
+struct ElemPcg {
+    int32_t n = 0;
+    int64_t ne = 0;
+    DevBuf<DofPair<TT>> G;  // {z, p}
+    DevBuf<DofPair<TT>> R;  // {r, x}
+    DevBuf<TT> D;           // 1 / diag(J)
+    DevBuf<ElemVec<TT>> V;
+    DevBuf<double> part;
+    DevBuf<PcgState> st;
+    HostBuf<PcgState> hst;
+    DevBuf<int> bad;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void *key_top = nullptr;
+    const TT *key_T = nullptr;
+    const uint8_t *key_fm = nullptr;
+    int64_t launches = 0;
+
+    ElemPcg() = default;
+    ElemPcg(const ElemPcg &) = delete;
+    ElemPcg &operator=(const ElemPcg &) = delete;
+    ~ElemPcg();
+    int reserve(int32_t n, int64_t ne);
+    void drop_graph();
+    // Solve J h = b_scale * b on the free DoFs from h = 0 with Jacobi from diag; h (float64)
+    // gets the iterate, 0 on constrained DoFs.  SNP_ZERO_PIVOT for a zero/non-finite
+    // diagonal entry on a free DoF.
+    int solve(const ElemTopology &top, const TT *T, const double *diag, const uint8_t *free_mask, const double *b,
+              double b_scale, double *h, double rtol, double atol, int64_t maxit, cudaStream_t s, int64_t *its,
+              double *res, int *status);
+    // y = J x on the free rows and columns (0 on constrained rows).
+    int apply(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const TT *x, TT *y, cudaStream_t s);
+
+   private:
+    int launch_iteration(const ElemTopology &top, const TT *T, const uint8_t *free_mask, cudaStream_t s, int use_cond,
+                         cudaGraphConditionalHandle cond);
+    int build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask);
 };
 
 }  // namespace snp

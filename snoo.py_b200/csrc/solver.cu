@@ -14,8 +14,10 @@
 // Jacobian values and the CG run in float32 while F, the update and the norms stay float64
 // (the Newton loop is the iterative refinement of the float32 solves).
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "snp_common.cuh"
@@ -171,6 +173,17 @@ struct snp_solver {
     bool has_extra = false;
     std::vector<std::unique_ptr<snp::Material>> mats;
     snp_pattern *pat = nullptr;
+    // storage of the Newton loop's Jacobian: element tensors (matrix-free), or an assembled
+    // CSR / SELL-C-sigma matrix; reference-semantics solves and exports always use the CSR
+    int layout = SNP_LAYOUT_CSR;
+    snp::SellLayout sell;
+    bool use_sell = false;
+    snp::ElemTopology etop;
+    snp::DevBuf<double> T64, Jdiag, Fe, De;
+    snp::DevBuf<float> T32;
+    snp::ElemPcg<double> epcg64;
+    snp::ElemPcg<float> epcg32;
+    int j_valid[2] = {0, 0};  // the float64 / float32 Newton Jacobian is current
     bool finalized = false;
     snp::DevBuf<double> J, F, b, xw, h, part, res;
     snp::DevBuf<float> J32, b32, h32;
@@ -216,9 +229,82 @@ struct snp_solver {
         return SNP_OK;
     }
 
-    // J (f64 or f32), F = K x - rhs - rhs_extra; optional K and rhs.
-    int assemble(const double *x, double *Kv, double *Jv, float *J32v, double *rhsv, double *Fv) {
-        const int64_t nnz = pat->nnz;
+    // The Newton Jacobian's matrix view (SELL when use_sell) over values v.
+    template <typename VT>
+    snp::CsrView<VT> jacobian_view(const VT *v) const {
+        snp::CsrView<VT> A{n, pat->nnz, pat->row_ptr.p, pat->col_idx.p, v};
+        if (use_sell) {
+            A.n_slices = sell.n_slices;
+            A.sell_off = sell.slice_off.p;
+            A.sell_row = sell.slice_row.p;
+            A.sell_col = sell.col.p;
+        }
+        return A;
+    }
+
+    int apply_jacobian(int precision, const void *x, void *y, cudaStream_t st) {
+        if (layout == SNP_LAYOUT_ELEM) {
+            if (precision == 0)
+                return epcg64.apply(etop, T64.p, free_mask.p, static_cast<const double *>(x), static_cast<double *>(y), st);
+            return epcg32.apply(etop, T32.p, free_mask.p, static_cast<const float *>(x), static_cast<float *>(y), st);
+        }
+        if (precision == 0)
+            return snp::spmv_f64(jacobian_view<double>(J.p), free_mask.p, static_cast<const double *>(x),
+                                 static_cast<double *>(y), st);
+        return snp::spmv_f32(jacobian_view<float>(J32.p), free_mask.p, static_cast<const float *>(x),
+                             static_cast<float *>(y), st);
+    }
+
+    // Element tensors (float64 or float32), diag(J) and F = K x - rhs - rhs_extra at x.
+    int assemble_elem(const double *x, bool f32, double *Fv) {
+        const int64_t E = n_elems_total();
+        j_valid[f32 ? 1 : 0] = 1;
+        for (auto &m : mats) {
+            snp::CurlArgs a{};
+            a.n_elems = m->count;
+            a.nodes = nodes.p;
+            a.cells = m->cells.p;
+            a.gids = m->gids.p;
+            a.orient = m->orient.p;
+            a.ctab = curls.p;
+            a.n_orient = n_orient;
+            a.dphi0 = dphi.p;
+            a.w = w.p;
+            a.nq = nq;
+            a.x = x;
+            a.Bs = m->has_bs ? m->Bs.p : nullptr;
+            a.n_int = m->n_int;
+            a.rel_c = m->relc.p;
+            a.rel_x = m->relx.p;
+            a.T64 = f32 ? nullptr : T64.p + m->offset;
+            a.T32 = f32 ? T32.p + m->offset : nullptr;
+            a.t_stride = E;
+            a.Fe = Fe.p + m->offset;
+            a.De = De.p + m->offset;
+            SNP_TRY(snp::launch_curlcurl_tensor(a, stream));
+            if (m->count) ++launches;
+        }
+        SNP_TRY(snp::elem_sum_to_dofs(etop, Fe.p, De.p, has_extra ? rhs_extra.p : nullptr, Fv, Jdiag.p, stream));
+        ++launches;
+        return SNP_OK;
+    }
+
+    // Newton-loop assembly at x in the solver's layout: Jacobian (precision f32 or not) and F.
+    int assemble_newton(const double *x, bool f32) {
+        if (layout == SNP_LAYOUT_ELEM) return assemble_elem(x, f32, F.p);
+        return assemble(x, nullptr, f32 ? nullptr : J.p, f32 ? J32.p : nullptr, nullptr, F.p, true);
+    }
+
+    // J (f64 or f32), F = K x - rhs - rhs_extra; optional K and rhs.  With sell_order the
+    // matrix outputs are written in the SELL layout (the Newton loop's Jacobian), else in CSR.
+    int assemble(const double *x, double *Kv, double *Jv, float *J32v, double *rhsv, double *Fv,
+                 bool sell_order = false) {
+        const bool so = sell_order && use_sell;
+        const int64_t nnz = so ? sell.total : pat->nnz;
+        // the assembled Newton Jacobian is what jacobian_apply uses unless the layout is matrix-free
+        const bool newton_j = sell_order && layout != SNP_LAYOUT_ELEM;
+        if (Jv == J.p) j_valid[0] = newton_j;
+        if (J32v == J32.p) j_valid[1] = newton_j;
         if (Kv) SNP_CUDA_TRY(cudaMemsetAsync(Kv, 0, sizeof(double) * nnz, stream));
         if (Jv) SNP_CUDA_TRY(cudaMemsetAsync(Jv, 0, sizeof(double) * nnz, stream));
         if (J32v) SNP_CUDA_TRY(cudaMemsetAsync(J32v, 0, sizeof(float) * nnz, stream));
@@ -241,7 +327,7 @@ struct snp_solver {
             a.n_int = m->n_int;
             a.rel_c = m->relc.p;
             a.rel_x = m->relx.p;
-            a.slots = pat->slots.p + 36 * m->offset;
+            a.slots = (so ? sell.slots.p : pat->slots.p) + 36 * m->offset;
             a.K = Kv;
             a.J = Jv;
             a.J32 = J32v;
@@ -269,10 +355,13 @@ struct snp_solver {
         launches = 0;
         pcg64.launches = 0;
         pcg32.launches = 0;
+        epcg64.launches = 0;
+        epcg32.launches = 0;
         const int grid = snp::stride_grid(n, snp::kVB, 4);
         SNP_CUDA_TRY(cudaEventRecord(ev[2], stream));
-        snp::CsrView<double> A{n, pat->nnz, pat->row_ptr.p, pat->col_idx.p, J.p};
-        snp::CsrView<float> A32{n, pat->nnz, pat->row_ptr.p, pat->col_idx.p, J32.p};
+        const snp::CsrView<double> A = jacobian_view(J.p);
+        const snp::CsrView<float> A32 = jacobian_view(J32.p);
+        const int32_t *diag = use_sell ? sell.diag.p : pat->diag_pos.p;
         const int64_t cg_maxit = o.cg_maxiter < 0 ? 10 * n_free : o.cg_maxiter;
         double st3[3];
         int status = SNP_OK;
@@ -280,7 +369,7 @@ struct snp_solver {
             SNP_REQUIRE(o.precision == 0, "mode 0 (reference semantics) runs in float64 only");
             for (int it = 0; it < o.max_newton; ++it) {
                 SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
-                SNP_TRY(assemble(x, nullptr, J.p, nullptr, nullptr, F.p));
+                SNP_TRY(assemble(x, nullptr, J.p, nullptr, nullptr, F.p, true));
                 SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
                 // b = J x - (K x - rhs)
                 SNP_TRY(snp::spmv_f64(A, nullptr, x, b.p, stream));
@@ -299,7 +388,7 @@ struct snp_solver {
                     break;
                 }
                 bool zp = false;
-                SNP_TRY(pcg64.set_jacobi(A, pat->diag_pos.p, free_mask.p, stream, &zp));
+                SNP_TRY(pcg64.set_jacobi(A, diag, free_mask.p, stream, &zp));
                 if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
                 SNP_CUDA_TRY(cudaMemcpyAsync(xw.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
                 SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
@@ -329,7 +418,7 @@ struct snp_solver {
             SNP_LAUNCH_CHECK();
             ++launches;
             SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
-            SNP_TRY(assemble(x, nullptr, f32 ? nullptr : J.p, f32 ? J32.p : nullptr, nullptr, F.p));
+            SNP_TRY(assemble_newton(x, f32));
             SNP_TRY(vstats(F.p, nullptr, true, st3));
             SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
             SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
@@ -366,8 +455,16 @@ struct snp_solver {
                 int st = SNP_OK;
                 bool zp = false;
                 SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
-                if (f32) {
-                    SNP_TRY(pcg32.set_jacobi(A32, pat->diag_pos.p, free_mask.p, stream, &zp));
+                if (layout == SNP_LAYOUT_ELEM) {
+                    const int rc = f32 ? epcg32.solve(etop, T32.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0,
+                                                      cg_maxit, stream, &its, &rn, &st)
+                                       : epcg64.solve(etop, T64.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0,
+                                                      cg_maxit, stream, &its, &rn, &st);
+                    if (rc == SNP_ZERO_PIVOT)
+                        return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
+                    SNP_TRY(rc);
+                } else if (f32) {
+                    SNP_TRY(pcg32.set_jacobi(A32, diag, free_mask.p, stream, &zp));
                     if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
                     snp::k_neg_free_f32<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, F.p, b32.p);
                     SNP_LAUNCH_CHECK();
@@ -376,7 +473,7 @@ struct snp_solver {
                     SNP_LAUNCH_CHECK();
                     launches += 2;
                 } else {
-                    SNP_TRY(pcg64.set_jacobi(A, pat->diag_pos.p, free_mask.p, stream, &zp));
+                    SNP_TRY(pcg64.set_jacobi(A, diag, free_mask.p, stream, &zp));
                     if (zp) return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
                     snp::k_neg_free<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, F.p, b.p);
                     SNP_LAUNCH_CHECK();
@@ -403,7 +500,7 @@ struct snp_solver {
                     snp::k_axpy_free<<<grid, snp::kVB, 0, stream>>>(n, free_mask.p, x, h.p, alpha, xw.p);
                     SNP_LAUNCH_CHECK();
                     ++launches;
-                    SNP_TRY(assemble(xw.p, nullptr, f32 ? nullptr : J.p, f32 ? J32.p : nullptr, nullptr, F.p));
+                    SNP_TRY(assemble_newton(xw.p, f32));
                     if (ls > 0) S.residual_evals += 1;
                     if (!o.line_search) break;
                     double g = 0.0;
@@ -429,7 +526,7 @@ struct snp_solver {
         SNP_CUDA_TRY(cudaEventSynchronize(ev[3]));
         S.t_total_ms = elapsed(2, 3);
         S.status = status;
-        S.kernel_launches = launches + pcg64.launches + pcg32.launches;
+        S.kernel_launches = launches + pcg64.launches + pcg32.launches + epcg64.launches + epcg32.launches;
         return status == SNP_OK ? SNP_OK : snp::fail(status, "Newton did not reach the tolerance in %d steps", o.max_newton);
     }
 };
@@ -533,7 +630,37 @@ int snp_solver_finalize(snp_solver *s) {
             SNP_CUDA_TRY(cudaMemcpyAsync(all.p + 6 * m->offset, m->gids.p, sizeof(int32_t) * 6 * m->count,
                                          cudaMemcpyDeviceToDevice, st));
     SNP_TRY(snp::pattern_create(all.p, E, 6, s->n, st, &s->pat));
-    const int64_t nnz = s->pat->nnz;
+    int64_t nnz = s->pat->nnz;
+    // Newton-loop Jacobian layout: SNP_JACOBIAN = elem (default) | csr | sell
+    const char *env = getenv("SNP_JACOBIAN");
+    const std::string want = env ? env : "elem";
+    s->layout = want == "csr" ? SNP_LAYOUT_CSR : want == "sell" ? SNP_LAYOUT_SELL : SNP_LAYOUT_ELEM;
+    if (s->layout == SNP_LAYOUT_ELEM) {
+        std::vector<double> ctab((size_t)s->n_orient * 18);
+        for (int o = 0; o < s->n_orient; ++o)
+            SNP_CUDA_TRY(cudaMemcpyAsync(ctab.data() + (size_t)o * 18, s->curls.p + (size_t)o * s->nq * 18,
+                                         18 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SNP_CUDA_TRY(cudaStreamSynchronize(st));
+        std::vector<snp::ElemBlock> blocks;
+        for (auto &m : s->mats) blocks.push_back(snp::ElemBlock{m->gids.p, m->orient.p, m->count, m->offset});
+        bool usable = false;
+        SNP_TRY(snp::build_elem_topology(s->etop, s->n, blocks.data(), (int)blocks.size(), ctab.data(), s->n_orient,
+                                         st, &usable));
+        if (usable) {
+            SNP_TRY(s->T64.alloc(6 * E));
+            SNP_TRY(s->Fe.alloc(6 * E));
+            SNP_TRY(s->De.alloc(6 * E));
+            SNP_TRY(s->T32.alloc(6 * E));
+            SNP_TRY(s->Jdiag.alloc(s->n));
+        } else {
+            s->layout = SNP_LAYOUT_CSR;
+        }
+    }
+    s->use_sell = s->layout == SNP_LAYOUT_SELL;
+    if (s->use_sell) {
+        SNP_TRY(snp::build_sell(s->pat, s->sell, st));
+        if (s->sell.total > nnz) nnz = s->sell.total;
+    }
     SNP_TRY(s->J.alloc(nnz));
     SNP_TRY(s->J32.alloc(nnz));
     SNP_TRY(s->F.alloc(s->n));
@@ -584,6 +711,24 @@ int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *
     int rc = s->assemble(x, K_vals, J_vals, nullptr, rhs, F);
     s->stream = keep;
     return rc;
+}
+
+int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void *y, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_jacobian_apply: solver missing or not finalized");
+    SNP_REQUIRE(precision == 0 || precision == 1, "snp_solver_jacobian_apply: precision must be 0 or 1");
+    SNP_REQUIRE(x != nullptr && y != nullptr, "snp_solver_jacobian_apply: x or y is NULL");
+    SNP_REQUIRE(s->j_valid[precision], "snp_solver_jacobian_apply: no %s Newton Jacobian (run a solve first)",
+                precision ? "float32" : "float64");
+    return s->apply_jacobian(precision, x, y, stream ? snp::as_stream(stream) : s->stream);
+}
+
+int snp_solver_jacobian_layout(const snp_solver *s, int *layout) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && layout != nullptr && s->finalized,
+                "snp_solver_jacobian_layout: solver missing or not finalized");
+    *layout = s->layout;
+    return SNP_OK;
 }
 
 int snp_solver_pattern(const snp_solver *s, const snp_pattern **pat) {

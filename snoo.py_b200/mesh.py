@@ -437,6 +437,44 @@ def _coil_terminals(mesh, ctag, zs):
     return t1, t2
 
 
+def bar_conductor_mesh(target_tets=20000, jitter=0.1, seed=3, box=(0.6, 0.6, 0.8), bar=0.1, ring=(0.3, 0.5),
+                       ring_length=0.4):
+    """A straight conductor bar along z through the whole box inside a square iron ring.
+
+    The bar (|x|, |y| < bar/2, all z) is volume TAG_COIL_1; its terminals are its node sets on
+    the two z faces of the box, which carry the Dirichlet condition, so the source current
+    enters and leaves through the boundary (a consistent total-potential problem).  The iron
+    ring (inner/outer half widths ring, |z| < ring_length/2) is TAG_IRON, the rest TAG_AIR.
+    """
+    bx, by, bz = (0.5 * b for b in box)
+    hb, ri, ro, lz = 0.5 * bar, 0.5 * ring[0], 0.5 * ring[1], 0.5 * ring_length
+    xb = sorted({-bx, -ro, -ri, -hb, hb, ri, ro, bx})
+    zb = sorted({-bz, -lz, lz, bz})
+    lo, hi = 0.002, 0.5
+    for _ in range(60):
+        mid = np.sqrt(lo * hi)
+        xs, zs = _graded_lines(xb, mid, mid, (-bx, bx)), _graded_lines(zb, mid, mid, (-bz, bz))
+        if 6 * (len(xs) - 1) ** 2 * (len(zs) - 1) > target_tets:
+            lo = mid
+        else:
+            hi = mid
+    xs, zs = _graded_lines(xb, hi, hi, (-bx, bx)), _graded_lines(zb, hi, hi, (-bz, bz))
+    ys = xs.copy()
+    cx, cz = 0.5 * (xs[1:] + xs[:-1]), 0.5 * (zs[1:] + zs[:-1])
+    X, Y, Z = np.meshgrid(cx, cx, cz, indexing="ij")
+    dom = np.full(X.shape, TAG_AIR, dtype=np.int32)
+    ring_m = (np.maximum(np.abs(X), np.abs(Y)) > ri) & (np.maximum(np.abs(X), np.abs(Y)) < ro) & (np.abs(Z) < lz)
+    dom[ring_m] = TAG_IRON
+    dom[(np.abs(X) < hb) & (np.abs(Y) < hb)] = TAG_COIL_1
+    fixed = [np.flatnonzero(np.isin(np.round(a, 12), np.round(b, 12))) for a, b in ((xs, xb), (ys, xb), (zs, zb))]
+    mesh = tensor_grid_mesh(xs, ys, zs, dom, jitter=jitter, seed=seed, fixed_planes=fixed)
+    coil_nodes = mesh.domain_nodes_mask(TAG_COIL_1)
+    z = mesh.nodes[:, 2]
+    mesh.coil_terminals = {TAG_COIL_1: (np.flatnonzero(coil_nodes & (np.abs(z + bz) < 1e-12)),
+                                        np.flatnonzero(coil_nodes & (np.abs(z - bz) < 1e-12)))}
+    return mesh
+
+
 def kuhn_microbench_mesh(nx=120, ny=120, nz=116, jitter=0.2, iron_fraction=0.4, seed=11):
     """Unit-spacing structured grid split into 6 tets per cell, jittered nodes, seeded
     per-element iron/air flags (iron with probability ``iron_fraction``)."""

@@ -87,6 +87,23 @@ class DeviceNewton:
                   _lib.ptr(out["rhs"]), _lib.ptr(out["F"]), _lib.stream_ptr(self._stream))
         return out
 
+    @property
+    def jacobian_layout(self):
+        """Storage of the residual-mode Newton loop's Jacobian, chosen when the solver was
+        finalized from the environment variable SNP_JACOBIAN: "elem" (matrix-free element
+        tensors, the default), "csr" or "sell" (SELL-C-sigma, C=32, sigma=256)."""
+        v = ctypes.c_int(-1)
+        _lib.call("snp_solver_jacobian_layout", self.handle, ctypes.byref(v))
+        return {0: "csr", 1: "sell", 2: "elem"}[v.value]
+
+    def jacobian_apply(self, x, y, precision="fp64"):
+        """y = J x on the free DoFs with the Newton Jacobian of the last solve of that precision
+        ("fp64": float64 vectors; "mixed": the float32 Jacobian and float32 vectors)."""
+        prec = {"fp64": 0, "mixed": 1}[precision]
+        _lib.call("snp_solver_jacobian_apply", self.handle, prec, _lib.ptr(x), _lib.ptr(y),
+                  _lib.stream_ptr(self._stream))
+        return y
+
     def __del__(self):
         try:
             if getattr(self, "handle", None) is not None and _lib._lib is not None:
