@@ -127,17 +127,18 @@ def bytes_pcg_iteration(nnz, n, vb=8, xb=8):
 
 
 def bytes_elem_apply(ne, n, tb=8):
-    """y = J x with the matrix-free Jacobian: per element its six DoF words and six tensor
-    entries (6*4 + 6*tb), per DoF its incidence (six entries per element, 4 B each, plus the
-    row pointer) and x read once, y written once.  The element results v_e are an
-    intermediate and not counted."""
-    return ne * (24 + 6 * tb) + ne * 24 + (n + 1) * 4 + 2 * n * tb
+    """y = J x with the matrix-free Jacobian: per element its six DoF words, six tensor
+    entries and six incidence-slot indices (6*4 + 6*tb + 6*4), per DoF the slot-range pointer,
+    x read once and y written once.  The edge terms passed between the two passes through
+    their slots (6*tb per element, written and read) are an intermediate and not counted."""
+    return ne * (24 + 6 * tb + 24) + (n + 1) * 4 + 2 * n * tb
 
 
 def bytes_elem_pcg_iteration(ne, n, tb=8):
     """One matrix-free PCG iteration (element pass + DoF pass): the operator data as in
-    bytes_elem_apply, the DoF states {r, p, dinv, x} read once and {r, p, x} written once."""
-    return ne * (24 + 6 * tb) + ne * 24 + (n + 1) * 4 + 7 * n * tb
+    bytes_elem_apply; per DoF {z, p}, {r, x} and 1/diag read once, {z, p} and {r, x} written
+    once (9 words)."""
+    return ne * (24 + 6 * tb + 24) + (n + 1) * 4 + 9 * n * tb
 
 
 def run_ours(args):

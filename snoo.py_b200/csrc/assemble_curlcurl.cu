@@ -452,8 +452,9 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
                 for (int c = r; c < 3; ++c) S[t++] = Jm[r] * P[c] + Jm[3 + r] * P[3 + c] + Jm[6 + r] * P[6 + c];
         }
+        const int64_t eb = eslot(a.t_offset + e, 0);
 #pragma unroll
-        for (int t = 0; t < 6; ++t) T[t * a.t_stride + e] = (TT)S[t];
+        for (int t = 0; t < 6; ++t) T[eb + 32 * t] = (TT)S[t];
         // G = kfac Jm^T (Jm bh) - Jm^T Rs;  F_j = chat_j . G
         double G[3];
 #pragma unroll
@@ -466,8 +467,8 @@ __global__ void __launch_bounds__(kBlock)
             const double sh0 = S[0] * h0 + S[1] * h1 + S[2] * h2;
             const double sh1 = S[1] * h0 + S[3] * h1 + S[4] * h2;
             const double sh2 = S[2] * h0 + S[4] * h1 + S[5] * h2;
-            a.Fe[j * a.t_stride + e] = h0 * G[0] + h1 * G[1] + h2 * G[2];
-            a.De[j * a.t_stride + e] = h0 * sh0 + h1 * sh1 + h2 * sh2;
+            a.Fe[eb + 32 * j] = h0 * G[0] + h1 * G[1] + h2 * G[2];
+            a.De[eb + 32 * j] = h0 * sh0 + h1 * sh1 + h2 * sh2;
         }
     }
 }

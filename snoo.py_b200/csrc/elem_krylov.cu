@@ -7,13 +7,14 @@
 // kept as six numbers per element plus the fixed topology, and a product is two passes:
 //
 //   element pass  p_j formed on the fly, u_e = sum_j s_j p_j chat_j, v_e = S_e u_e, p.q
-//                 partial sums (p.J p = sum_e u_e . v_e); stores v_e
-//   DoF pass      q_i = sum_(e,k) s_k chat_k . v_e over the DoF's incident elements, then the
-//                 CG update of the DoF: p = z + beta p, x += alpha p, r -= alpha q,
+//                 partial sums (p.J p = sum_e u_e . v_e); each edge term s_k chat_k . v_e
+//                 is stored in the slot that (e, k) holds in the DoF-ordered incidence list
+//   DoF pass      q_i = sum of DoF i's slots (a contiguous range, no gathers), then the CG
+//                 update of the DoF: p = z + beta p, x += alpha p, r -= alpha q,
 //                 z = dinv r, r.z and r.r partial sums
 //
-// Neither pass uses atomics; every sum runs in a fixed order, so the iteration is
-// deterministic.  The per-DoF CG state is split so the element pass gathers only {z, p}
+// Every slot has one writer and every sum runs in a fixed order, so the iteration is
+// deterministic without atomics.  The per-DoF CG state is split so the element pass gathers only {z, p}
 // (16 bytes per DoF in float64).  The direction p_k = z_k + beta p_(k-1) is formed in both
 // passes by the same rounded expression, so both see the same p.
 #include <cstdio>
@@ -32,16 +33,11 @@ namespace snp {
 namespace {
 
 constexpr int kEBlock = 256;
-#ifndef SNP_INC_UNROLL
-#define SNP_INC_UNROLL 4
-#endif
-#ifndef SNP_PASS1_PREFETCH
-#define SNP_PASS1_PREFETCH 1
-#endif
-constexpr int kIncUnroll = SNP_INC_UNROLL;    // incidence gathers in flight per lane in the DoF pass
-constexpr int kWarpSlab = 256;                // incidence terms staged per warp (shared memory)
-constexpr bool kPass1Prefetch = SNP_PASS1_PREFETCH;  // element pass loads element e+stride before e's gathers
 constexpr uint32_t kSignBit = 0x80000000u;
+#ifndef SNP_PASS1_MIN_BLOCKS
+#define SNP_PASS1_MIN_BLOCKS 4
+#endif
+constexpr int kPass1MinBlocks = SNP_PASS1_MIN_BLOCKS;  // resident blocks per SM the element pass asks for
 
 // p = z + beta p_old, rounded the same way wherever it is formed
 __device__ __forceinline__ double pnext(double beta, double p_old, double z) { return __fma_rn(beta, p_old, z); }
@@ -65,7 +61,7 @@ __global__ void k_edof(int64_t count, int64_t offset, int64_t ne, const int32_t 
                 atomicExch(bad, 1);
                 continue;
             }
-            edof[(int64_t)k * ne + offset + e] = (int32_t)((uint32_t)g | (sgn[6 * o + k] < 0 ? kSignBit : 0u));
+            edof[eslot(offset + e, k)] = (int32_t)((uint32_t)g | (sgn[6 * o + k] < 0 ? kSignBit : 0u));
         }
     }
 }
@@ -77,7 +73,7 @@ __global__ void k_inc_keys(int64_t ne, const int32_t *__restrict__ edof, int32_t
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = t / 6;
         const int k = (int)(t - 6 * e);
-        const uint32_t d = (uint32_t)edof[(int64_t)k * ne + e];
+        const uint32_t d = (uint32_t)edof[eslot(e, k)];
         const int32_t g = (int32_t)(d & ~kSignBit);
         key[t] = g;
         val[t] = (int32_t)(((uint32_t)e << 3) | (uint32_t)k | (d & kSignBit));
@@ -94,13 +90,32 @@ __global__ void k_sum_to_dofs(int32_t n, int64_t ne, const int32_t *__restrict__
         double f = 0.0, d = 0.0;
         for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
             const uint32_t u = (uint32_t)inc[t] & ~kSignBit;
-            const int64_t idx = (int64_t)(u & 7u) * ne + (u >> 3);
+            const int64_t idx = eslot(u >> 3, (int)(u & 7u));
             f += Fe[idx];
             d += De[idx];
         }
         F[i] = rhs_extra ? f - rhs_extra[i] : f;
         diag[i] = d;
     }
+}
+
+// slot of every (e, k) in the DoF-ordered incidence list
+__global__ void k_inc_pos(int64_t m, int64_t ne, const int32_t *__restrict__ inc, int32_t *__restrict__ pos) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t u = (uint32_t)inc[t] & ~kSignBit;
+        pos[eslot(u >> 3, (int)(u & 7u))] = (int32_t)t;
+    }
+}
+
+// Edge term s chat_k . v of one element edge, rounded the same way wherever it is formed.
+template <typename TT>
+__device__ __forceinline__ TT edge_term(const TT *sc, int k, bool neg, TT v0, TT v1, TT v2) {
+    TT c;
+    if constexpr (sizeof(TT) == 8)
+        c = __fma_rn(sc[3 * k + 2], v2, __fma_rn(sc[3 * k + 1], v1, __dmul_rn(sc[3 * k], v0)));
+    else
+        c = __fmaf_rn(sc[3 * k + 2], v2, __fmaf_rn(sc[3 * k + 1], v1, __fmul_rn(sc[3 * k], v0)));
+    return neg ? -c : c;
 }
 
 // ---------------------------------------------------------------- PCG kernels
@@ -166,68 +181,83 @@ __device__ __forceinline__ void load_chat(TT *sc, const TT *chat) {
     __syncthreads();
 }
 
-// element pass of a CG iteration: p from the DoF states, v_e = S_e u_e, p.J p -> alpha.
-// The next element's DoF words and tensor are loaded before this element's gathers.
+// element pass of a CG iteration: p from the DoF states, v_e = S_e u_e, p.J p -> alpha, and
+// the six edge terms into their incidence slots.  Two lanes per element, three edges each:
+// each lane gathers three DoF states, the halves of u_e meet through one shuffle, and each
+// lane stores its three edge terms (half the registers of one lane per element, so twice
+// the resident warps keep the same number of gathers in flight).
 template <typename TT>
-__global__ void __launch_bounds__(kEBlock)
-    k_epass1(int64_t ne, const int32_t *__restrict__ edof, const TT *__restrict__ T, const TT *__restrict__ chat,
-             const DofPair<TT> *__restrict__ G, ElemVec<TT> *__restrict__ V, PcgState *st, double *part) {
+__global__ void __launch_bounds__(kEBlock, kPass1MinBlocks)
+    k_epass1(int64_t ne, const int32_t *__restrict__ edof, const int32_t *__restrict__ pos,
+             const TT *__restrict__ T, const TT *__restrict__ chat, const DofPair<TT> *__restrict__ G,
+             TT *__restrict__ Y, PcgState *st, double *part) {
     __shared__ TT sc[18];
     __shared__ double sh[32];
     if (st->done) return;
     load_chat(sc, chat);
     const TT beta = (TT)st->beta;
+    const int lane = threadIdx.x & 31;
+    const int h = lane & 1;  // edges 3h .. 3h+2
     double dot = 0.0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int32_t nd[6];
-    TT nt[6];
+    // a warp takes 16 consecutive elements per pass; the loop bound is uniform across the warp
+    const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5) * 16;
+#pragma unroll 1
+    for (int64_t e0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 16; e0 < ne; e0 += wstride) {
+        const int64_t e = e0 + (lane >> 1);
+        const bool valid = e < ne;
+        const int64_t eb = eslot(valid ? e : 0, 0);
+        // every streamed word of this pass is requested before the gathers: the lane's three
+        // DoF words, slots and tensor components (the partner lane holds the other three)
+        int32_t d[3], ps[3];
+        TT th[3];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        nd[k] = e < ne ? __ldcs(edof + (int64_t)k * ne + e) : 0;
-        nt[k] = e < ne ? __ldcs(T + (int64_t)k * ne + e) : TT(0);
-    }
-    for (; e < ne; e += stride) {
-        int32_t d[6];
-        TT t[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            d[k] = nd[k];
-            t[k] = nt[k];
+        for (int j = 0; j < 3; ++j) {
+            d[j] = valid ? __ldcs(edof + eb + 32 * (3 * h + j)) : 0;
+            ps[j] = valid ? __ldcs(pos + eb + 32 * (3 * h + j)) : 0;
+            th[j] = valid ? __ldcs(T + eb + 32 * (3 * h + j)) : TT(0);
         }
-        DofPair<TT> w[6];
+        DofPair<TT> w[3];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) w[k] = G[(uint32_t)d[k] & ~kSignBit];
-        if (kPass1Prefetch) {
-            const int64_t en = e + stride;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                nd[k] = en < ne ? __ldcs(edof + (int64_t)k * ne + en) : 0;
-                nt[k] = en < ne ? __ldcs(T + (int64_t)k * ne + en) : TT(0);
-            }
-        }
+        for (int j = 0; j < 3; ++j) w[j] = G[(uint32_t)d[j] & ~kSignBit];
         TT u0 = TT(0), u1 = TT(0), u2 = TT(0);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            TT pk = pnext(beta, w[k].b, w[k].a);
-            if (d[k] < 0) pk = -pk;
-            u0 += pk * sc[3 * k];
-            u1 += pk * sc[3 * k + 1];
-            u2 += pk * sc[3 * k + 2];
+        for (int j = 0; j < 3; ++j) {
+            TT pk = pnext(beta, w[j].b, w[j].a);
+            if (d[j] < 0) pk = -pk;
+            const TT *c = sc + 3 * (3 * h + j);
+            u0 += pk * c[0];
+            u1 += pk * c[1];
+            u2 += pk * c[2];
         }
+        if (!valid) u0 = u1 = u2 = TT(0);
+        // u_e = (edges 0-2) + (edges 3-5), added in that order on both lanes
+        const TT o0 = __shfl_xor_sync(0xffffffffu, u0, 1);
+        const TT o1 = __shfl_xor_sync(0xffffffffu, u1, 1);
+        const TT o2 = __shfl_xor_sync(0xffffffffu, u2, 1);
+        if (h) {
+            u0 = o0 + u0;
+            u1 = o1 + u1;
+            u2 = o2 + u2;
+        } else {
+            u0 = u0 + o0;
+            u1 = u1 + o1;
+            u2 = u2 + o2;
+        }
+        TT t[6];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const TT other = __shfl_xor_sync(0xffffffffu, th[j], 1);
+            t[j] = h ? other : th[j];
+            t[3 + j] = h ? th[j] : other;
+        }
+        if (!valid) continue;
         const TT v0 = t[0] * u0 + t[1] * u1 + t[2] * u2;
         const TT v1 = t[1] * u0 + t[3] * u1 + t[4] * u2;
         const TT v2 = t[2] * u0 + t[4] * u1 + t[5] * u2;
-        dot += (double)u0 * (double)v0 + (double)u1 * (double)v1 + (double)u2 * (double)v2;
-        V[e] = ElemVec<TT>{v0, v1, v2, TT(0)};
-        if (!kPass1Prefetch) {
-            const int64_t en = e + stride;
+        if (!h) dot += (double)u0 * (double)v0 + (double)u1 * (double)v1 + (double)u2 * (double)v2;
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                nd[k] = en < ne ? __ldcs(edof + (int64_t)k * ne + en) : 0;
-                nt[k] = en < ne ? __ldcs(T + (int64_t)k * ne + en) : TT(0);
-            }
-        }
+        for (int j = 0; j < 3; ++j)
+            Y[ps[j]] = edge_term(sc, 3 * h + j, d[j] < 0, v0, v1, v2);
     }
     dot = block_sum(dot, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = dot;
@@ -240,111 +270,27 @@ __global__ void __launch_bounds__(kEBlock)
     }
 }
 
-// Signed contribution s_k chat_k . v_e of one incidence entry, rounded the same way on
-// every path that forms it.
-template <typename TT>
-__device__ __forceinline__ double inc_term(const TT *sc, int32_t ent, const ElemVec<TT> &v) {
-    const int k = (int)((uint32_t)ent & 7u);
-    TT c;
-    if constexpr (sizeof(TT) == 8)
-        c = __fma_rn(sc[3 * k + 2], v.c, __fma_rn(sc[3 * k + 1], v.b, __dmul_rn(sc[3 * k], v.a)));
-    else
-        c = __fmaf_rn(sc[3 * k + 2], v.c, __fmaf_rn(sc[3 * k + 1], v.b, __fmul_rn(sc[3 * k], v.a)));
-    return ent < 0 ? -(double)c : (double)c;
-}
-
-// q_i = sum over the incidence entries of DoF i, in entry order.  A warp takes 32 consecutive
-// DoFs; when their entries fit in the warp's shared-memory slab, the lanes stride over the
-// flattened entry range (coalesced entry loads, kIncUnroll gathers in flight per lane, no
-// divergence from uneven list lengths) and each lane then sums its own DoF's terms from
-// shared memory.  Otherwise each lane walks its own list.  Both give the same bits.
-template <typename TT>
-__device__ __forceinline__ double warp_gather_q(bool valid, int b0, int b1, const int32_t *__restrict__ inc,
-                                                const TT *sc, const ElemVec<TT> *__restrict__ V, double *slab) {
-    const int lane = threadIdx.x & 31;
-    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    const int last = 31 - __clz(vmask);
-    const int rb = __shfl_sync(0xffffffffu, b0, 0);
-    const int re = __shfl_sync(0xffffffffu, b1, last);
-    const int cnt = re - rb;
-    double q = 0.0;
-    if (cnt <= kWarpSlab) {
-        for (int t0 = lane; t0 < cnt; t0 += 32 * kIncUnroll) {
-            int32_t ent[kIncUnroll];
-            ElemVec<TT> v[kIncUnroll];
-#pragma unroll
-            for (int u = 0; u < kIncUnroll; ++u) {
-                const int t = t0 + 32 * u;
-                ent[u] = t < cnt ? __ldcs(inc + rb + t) : 0;
-            }
-#pragma unroll
-            for (int u = 0; u < kIncUnroll; ++u) v[u] = V[((uint32_t)ent[u] & ~kSignBit) >> 3];
-#pragma unroll
-            for (int u = 0; u < kIncUnroll; ++u) {
-                const int t = t0 + 32 * u;
-                if (t < cnt) slab[t] = inc_term(sc, ent[u], v[u]);
-            }
-        }
-        __syncwarp();
-        if (valid)
-            for (int t = b0 - rb; t < b1 - rb; ++t) q += slab[t];
-        __syncwarp();
-    } else if (valid) {
-        for (int t = b0; t < b1; ++t) {
-            const int32_t ent = inc[t];
-            q += inc_term(sc, ent, V[((uint32_t)ent & ~kSignBit) >> 3]);
-        }
-    }
-    return q;
-}
-
-// DoF pass of a CG iteration: q_i gathered from v_e, then the update of DoF i
+// DoF pass of a CG iteration: q_i = sum of the DoF's incidence slots, then the update of DoF i
 template <typename TT>
 __global__ void __launch_bounds__(kEBlock)
     k_epass2(int32_t n, const uint8_t *__restrict__ free_mask, const int32_t *__restrict__ inc_ptr,
-             const int32_t *__restrict__ inc, const TT *__restrict__ chat, const ElemVec<TT> *__restrict__ V,
-             DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R, const TT *__restrict__ D, PcgState *st,
-             double *part, int use_cond, cudaGraphConditionalHandle cond) {
-    __shared__ TT sc[18];
+             const TT *__restrict__ Y, DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R,
+             const TT *__restrict__ D, PcgState *st, double *part, int use_cond, cudaGraphConditionalHandle cond) {
     __shared__ double sh2[2][32];
-    __shared__ double s_slab[kEBlock / 32][kWarpSlab];
     if (st->done) {
         if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
         return;
     }
-    load_chat(sc, chat);
     const TT alpha = (TT)st->alpha, beta = (TT)st->beta;
-    double *slab = s_slab[threadIdx.x >> 5];
     double rz = 0.0, rr = 0.0;
-    // the loop bound is uniform across each warp (32 consecutive DoFs per warp and pass); the
-    // next pass's list bounds and this pass's own-row state are loaded ahead of the gathers
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
-    int nb0 = 0, nb1 = 0;
-    if (base + (threadIdx.x & 31) < n) {
-        nb0 = __ldcs(inc_ptr + base + (threadIdx.x & 31));
-        nb1 = __ldcs(inc_ptr + base + (threadIdx.x & 31) + 1);
-    }
-    for (; base < n; base += stride) {
-        const int64_t i = base + (threadIdx.x & 31);
-        const bool valid = i < n;
-        const int b0 = nb0, b1 = nb1;
-        const bool upd = valid && is_free(free_mask, i);
-        DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
-        TT dv = TT(0);
-        if (upd) {
-            g = G[i];
-            rx = R[i];
-            dv = D[i];
-        }
-        // lanes past the end carry an empty list, so their slab range is empty too
-        nb0 = nb1 = 0;
-        if (i + stride < n) {
-            nb0 = __ldcs(inc_ptr + i + stride);
-            nb1 = __ldcs(inc_ptr + i + stride + 1);
-        }
-        const double q = warp_gather_q(valid, b0, b1, inc, sc, V, slab);
-        if (!upd) continue;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (!is_free(free_mask, i)) continue;
+        const DofPair<TT> g = G[i];
+        const DofPair<TT> rx = R[i];
+        const TT dv = D[i];
+        const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
+        double q = 0.0;
+        for (int t = b0; t < b1; ++t) q += (double)Y[t];
         const TT p = pnext(beta, g.b, g.a);
         const TT r = rx.a - alpha * (TT)q;
         const TT z = dv * r;
@@ -392,49 +338,44 @@ __global__ void k_eextract(int32_t n, const DofPair<TT> *__restrict__ R, double 
 
 template <typename TT>
 __global__ void __launch_bounds__(kEBlock)
-    k_eapply1(int64_t ne, const int32_t *__restrict__ edof, const TT *__restrict__ T, const TT *__restrict__ chat,
-              const uint8_t *__restrict__ free_mask, const TT *__restrict__ x, ElemVec<TT> *__restrict__ V) {
+    k_eapply1(int64_t ne, const int32_t *__restrict__ edof, const int32_t *__restrict__ pos,
+              const TT *__restrict__ T, const TT *__restrict__ chat, const uint8_t *__restrict__ free_mask,
+              const TT *__restrict__ x, TT *__restrict__ Y) {
     __shared__ TT sc[18];
     load_chat(sc, chat);
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t eb = eslot(e, 0);
+        int32_t d[6];
         TT u0 = TT(0), u1 = TT(0), u2 = TT(0);
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            const int32_t d = edof[(int64_t)k * ne + e];
-            const uint32_t g = (uint32_t)d & ~kSignBit;
+            d[k] = edof[eb + 32 * k];
+            const uint32_t g = (uint32_t)d[k] & ~kSignBit;
             TT xk = is_free(free_mask, g) ? x[g] : TT(0);
-            if (d < 0) xk = -xk;
+            if (d[k] < 0) xk = -xk;
             u0 += xk * sc[3 * k];
             u1 += xk * sc[3 * k + 1];
             u2 += xk * sc[3 * k + 2];
         }
         TT t[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) t[k] = T[(int64_t)k * ne + e];
-        V[e] = ElemVec<TT>{t[0] * u0 + t[1] * u1 + t[2] * u2, t[1] * u0 + t[3] * u1 + t[4] * u2,
-                           t[2] * u0 + t[4] * u1 + t[5] * u2, TT(0)};
+        for (int k = 0; k < 6; ++k) t[k] = T[eb + 32 * k];
+        const TT v0 = t[0] * u0 + t[1] * u1 + t[2] * u2;
+        const TT v1 = t[1] * u0 + t[3] * u1 + t[4] * u2;
+        const TT v2 = t[2] * u0 + t[4] * u1 + t[5] * u2;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) Y[pos[eb + 32 * k]] = edge_term(sc, k, d[k] < 0, v0, v1, v2);
     }
 }
 
 template <typename TT>
 __global__ void __launch_bounds__(kEBlock)
     k_eapply2(int32_t n, const uint8_t *__restrict__ free_mask, const int32_t *__restrict__ inc_ptr,
-              const int32_t *__restrict__ inc, const TT *__restrict__ chat, const ElemVec<TT> *__restrict__ V,
-              TT *__restrict__ y) {
-    __shared__ TT sc[18];
-    load_chat(sc, chat);
+              const TT *__restrict__ Y, TT *__restrict__ y) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double q = 0.0;
-        if (is_free(free_mask, i)) {
-            for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
-                const int32_t ent = inc[t];
-                const uint32_t u = (uint32_t)ent & ~kSignBit;
-                const int k = (int)(u & 7u);
-                const ElemVec<TT> v = V[u >> 3];
-                const TT c = sc[3 * k] * v.a + sc[3 * k + 1] * v.b + sc[3 * k + 2] * v.c;
-                q += ent < 0 ? -(double)c : (double)c;
-            }
-        }
+        if (is_free(free_mask, i))
+            for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) q += (double)Y[t];
         y[i] = (TT)q;
     }
 }
@@ -481,8 +422,8 @@ int build_elem_topology(ElemTopology &top, int32_t n, const ElemBlock *blocks, i
     SNP_TRY(bad.alloc(1));
     SNP_CUDA_TRY(cudaMemcpyAsync(d_sgn.p, sgn.data(), sgn.size(), cudaMemcpyHostToDevice, s));
     SNP_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
-    SNP_TRY(top.edof.alloc(6 * ne));
-    SNP_CUDA_TRY(cudaMemsetAsync(top.edof.p, 0, sizeof(int32_t) * 6 * ne, s));
+    SNP_TRY(top.edof.alloc(eslots_size(ne)));
+    SNP_CUDA_TRY(cudaMemsetAsync(top.edof.p, 0, sizeof(int32_t) * eslots_size(ne), s));
     for (int b = 0; b < n_blocks; ++b) {
         if (blocks[b].count == 0) continue;
         k_edof<<<stride_grid(blocks[b].count, 256, 8), 256, 0, s>>>(blocks[b].count, blocks[b].offset, ne,
@@ -515,6 +456,10 @@ int build_elem_topology(ElemTopology &top, int32_t n, const ElemBlock *blocks, i
     if (dv.Current() != top.inc.p)
         SNP_CUDA_TRY(cudaMemcpyAsync(top.inc.p, dv.Current(), sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, s));
     SNP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp.p, tb_scan, cnt.p, top.inc_ptr.p, n + 1, s));
+    SNP_TRY(top.pos.alloc(eslots_size(ne)));
+    SNP_CUDA_TRY(cudaMemsetAsync(top.pos.p, 0, sizeof(int32_t) * eslots_size(ne), s));
+    k_inc_pos<<<stride_grid(m, 256, 8), 256, 0, s>>>(m, ne, top.inc.p, top.pos.p);
+    SNP_LAUNCH_CHECK();
     double c64[18];
     float c32[18];
     for (int t = 0; t < 18; ++t) {
@@ -568,7 +513,7 @@ int ElemPcg<TT>::reserve(int32_t n_, int64_t ne_) {
     SNP_TRY(G.alloc(n));
     SNP_TRY(R.alloc(n));
     SNP_TRY(D.alloc(n));
-    SNP_TRY(V.alloc(ne));
+    SNP_TRY(Y.alloc(6 * ne));
     const int gmax = sm_count() * 8 + 1;
     SNP_TRY(part.alloc(3 * (size_t)gmax));
     SNP_TRY(st.alloc(1));
@@ -582,12 +527,11 @@ template <typename TT>
 int ElemPcg<TT>::launch_iteration(const ElemTopology &top, const TT *T, const uint8_t *free_mask, cudaStream_t s,
                                   int use_cond, cudaGraphConditionalHandle cond) {
     const TT *chat = chat_ptr<TT>(top);
-    k_epass1<TT><<<wave_grid(k_epass1<TT>, ne, kEBlock), kEBlock, 0, s>>>(ne, top.edof.p, T, chat, G.p, V.p, st.p,
-                                                                         part.p);
+    k_epass1<TT><<<wave_grid(k_epass1<TT>, 2 * ne, kEBlock), kEBlock, 0, s>>>(ne, top.edof.p, top.pos.p, T, chat, G.p,
+                                                                         Y.p, st.p, part.p);
     SNP_LAUNCH_CHECK();
-    k_epass2<TT><<<wave_grid(k_epass2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, top.inc.p, chat,
-                                                                        V.p, G.p, R.p, D.p, st.p, part.p, use_cond,
-                                                                        cond);
+    k_epass2<TT><<<wave_grid(k_epass2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, Y.p, G.p, R.p,
+                                                                        D.p, st.p, part.p, use_cond, cond);
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }
@@ -700,10 +644,10 @@ int ElemPcg<TT>::apply(const ElemTopology &top, const TT *T, const uint8_t *free
     SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "element operator: topology not built");
     SNP_TRY(reserve(top.n, top.n_elems));
     const TT *chat = chat_ptr<TT>(top);
-    k_eapply1<TT><<<wave_grid(k_eapply1<TT>, ne, kEBlock), kEBlock, 0, s>>>(ne, top.edof.p, T, chat, free_mask, x, V.p);
+    k_eapply1<TT><<<wave_grid(k_eapply1<TT>, ne, kEBlock), kEBlock, 0, s>>>(ne, top.edof.p, top.pos.p, T, chat,
+                                                                           free_mask, x, Y.p);
     SNP_LAUNCH_CHECK();
-    k_eapply2<TT><<<wave_grid(k_eapply2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, top.inc.p,
-                                                                          chat, V.p, y);
+    k_eapply2<TT><<<wave_grid(k_eapply2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, Y.p, y);
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }

@@ -8,6 +8,13 @@
 
 namespace snp {
 
+// Arrays of six values per element (one per element edge, or the six components of a
+// symmetric 3x3 tensor) are stored in blocks of 32 elements: value k of element e sits at
+// ((e / 32) * 6 + k) * 32 + e % 32.  A warp's 32 consecutive elements read each k as one
+// coalesced row, and the six rows lie at fixed offsets from one base address.
+__host__ __device__ __forceinline__ int64_t eslot(int64_t e, int k) { return ((e >> 5) * 6 + k) * 32 + (e & 31); }
+__host__ __device__ __forceinline__ int64_t eslots_size(int64_t n_elems) { return ((n_elems + 31) >> 5) * 192; }
+
 // Owning device allocation (cudaMalloc'd; freed on destruction).
 template <typename T>
 struct DevBuf {
@@ -98,13 +105,13 @@ struct CurlArgs {
     float *J32;
     double *rhs;
     double *F;
-    // element-tensor outputs (launch_curlcurl_tensor), all [k * t_stride + e] with the
-    // pointers already offset to this material: S_e in float64 or float32 (components
-    // xx xy xz yy yz zz), and per element edge k its residual term Fe and Jacobian
-    // diagonal term De (summed per DoF afterwards, in a fixed order)
+    // element-tensor outputs (launch_curlcurl_tensor), element-edge arrays indexed by
+    // eslot(t_offset + e, k): S_e in float64 or float32 (components xx xy xz yy yz zz), and
+    // per element edge k its residual term Fe and Jacobian diagonal term De (summed per DoF
+    // afterwards, in a fixed order)
     double *T64;
     float *T32;
-    int64_t t_stride;
+    int64_t t_offset;
     double *Fe;
     double *De;
 };

@@ -95,17 +95,19 @@ struct Pcg {
 // element as the 3x3 symmetric tensor S_e (six numbers): J_e,jk = s_j s_k chat_j . S_e chat_k,
 // chat_j the reference curls of orientation 0 and s_j = +-1 the element's edge signs.  A
 // product y = J x is two passes without atomics:
-//   element pass  u_e = sum_j s_j x_j chat_j,  v_e = S_e u_e          (stores v_e)
-//   DoF pass      y_i = sum over incident (e, k) of s_k chat_k . v_e  (gathers v_e)
+//   element pass  u_e = sum_j s_j x_j chat_j,  v_e = S_e u_e, and the six edge terms
+//                 y_e,k = s_k chat_k . v_e stored at their slots of the DoF-ordered incidence
+//   DoF pass      y_i = sum of the DoF's slots, a contiguous range
 
 // Element topology of the operator: DoFs with edge signs and the DoF -> (element, local
 // edge) incidence, built once per mesh.
 struct ElemTopology {
     int64_t n_elems = 0;
     int32_t n = 0;
-    DevBuf<int32_t> edof;     // [6][n_elems]  DoF, bit 31 set when the edge function is negated
+    DevBuf<int32_t> edof;     // eslot(e, k): DoF, bit 31 set when the edge function is negated
     DevBuf<int32_t> inc_ptr;  // [n + 1]
     DevBuf<int32_t> inc;      // [6 n_elems]   (e << 3 | k), bit 31 = sign, grouped by DoF
+    DevBuf<int32_t> pos;      // eslot(e, k): slot of (e, k) in that DoF-ordered list
     DevBuf<double> chat64;    // [18] reference curls of orientation 0
     DevBuf<float> chat32;
 };
@@ -127,7 +129,7 @@ int build_elem_topology(ElemTopology &top, int32_t n, const ElemBlock *blocks, i
 // Per-DoF CG state, split by who reads it: the element pass gathers {z, p} (16 bytes in
 // float64, two DoFs per 32-byte sector); {r, x} and 1/diag are read only by the DoF's own
 // thread in the DoF pass.
-// Per-DoF sums of element-edge terms [6][n_elems] in incidence order (deterministic):
+// Per-DoF sums of element-edge terms (indexed by eslot) in incidence order (deterministic):
 // F_i = sum Fe - rhs_extra_i (rhs_extra may be NULL), diag_i = sum De.
 int elem_sum_to_dofs(const ElemTopology &top, const double *Fe, const double *De, const double *rhs_extra,
                      double *F, double *diag, cudaStream_t s);
@@ -137,10 +139,6 @@ struct alignas(2 * sizeof(TT)) DofPair {
     TT a, b;
 };
 
-template <typename TT>
-struct alignas(4 * sizeof(TT)) ElemVec {
-    TT a, b, c, pad;
-};
 
 // Jacobi-PCG on the matrix-free Jacobian (values TT = double or float; sums in double),
 // scipy cg's stopping rule, iteration loop in a CUDA-graph conditional WHILE node.
@@ -151,7 +149,7 @@ struct ElemPcg {
     DevBuf<DofPair<TT>> G;  // {z, p}
     DevBuf<DofPair<TT>> R;  // {r, x}
     DevBuf<TT> D;           // 1 / diag(J)
-    DevBuf<ElemVec<TT>> V;
+    DevBuf<TT> Y;           // [6 n_elems] element-edge terms in DoF-ordered slots
     DevBuf<double> part;
     DevBuf<PcgState> st;
     HostBuf<PcgState> hst;

@@ -257,7 +257,6 @@ struct snp_solver {
 
     // Element tensors (float64 or float32), diag(J) and F = K x - rhs - rhs_extra at x.
     int assemble_elem(const double *x, bool f32, double *Fv) {
-        const int64_t E = n_elems_total();
         j_valid[f32 ? 1 : 0] = 1;
         for (auto &m : mats) {
             snp::CurlArgs a{};
@@ -276,11 +275,11 @@ struct snp_solver {
             a.n_int = m->n_int;
             a.rel_c = m->relc.p;
             a.rel_x = m->relx.p;
-            a.T64 = f32 ? nullptr : T64.p + m->offset;
-            a.T32 = f32 ? T32.p + m->offset : nullptr;
-            a.t_stride = E;
-            a.Fe = Fe.p + m->offset;
-            a.De = De.p + m->offset;
+            a.T64 = f32 ? nullptr : T64.p;
+            a.T32 = f32 ? T32.p : nullptr;
+            a.t_offset = m->offset;
+            a.Fe = Fe.p;
+            a.De = De.p;
             SNP_TRY(snp::launch_curlcurl_tensor(a, stream));
             if (m->count) ++launches;
         }
@@ -647,10 +646,10 @@ int snp_solver_finalize(snp_solver *s) {
         SNP_TRY(snp::build_elem_topology(s->etop, s->n, blocks.data(), (int)blocks.size(), ctab.data(), s->n_orient,
                                          st, &usable));
         if (usable) {
-            SNP_TRY(s->T64.alloc(6 * E));
-            SNP_TRY(s->Fe.alloc(6 * E));
-            SNP_TRY(s->De.alloc(6 * E));
-            SNP_TRY(s->T32.alloc(6 * E));
+            SNP_TRY(s->T64.alloc(snp::eslots_size(E)));
+            SNP_TRY(s->Fe.alloc(snp::eslots_size(E)));
+            SNP_TRY(s->De.alloc(snp::eslots_size(E)));
+            SNP_TRY(s->T32.alloc(snp::eslots_size(E)));
             SNP_TRY(s->Jdiag.alloc(s->n));
         } else {
             s->layout = SNP_LAYOUT_CSR;
