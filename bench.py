@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the assembly microbenchmark and the 4M-tet mixed-precision accuracy run")
     return ap.parse_args()
 
 
@@ -139,6 +141,20 @@ def bytes_elem_pcg_iteration(ne, n, tb=8):
     bytes_elem_apply; per DoF {z, p}, {r, x} and 1/diag read once, {z, p} and {r, x} written
     once (9 words)."""
     return ne * (24 + 6 * tb + 24) + (n + 1) * 4 + 9 * n * tb
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one matrix-free PCG iteration,
+# k_epass1 + k_epass2, from ncu captures of the 1,164,240-tet workload (cold cache: ncu
+# flushes L2 before every replay pass, so slot values and DoF states that stay in L2 between
+# the two passes of a live run are counted as DRAM traffic here).  Summaries and commands:
+# profiles/elem_pcg_passes_window_frame_1p2M.md.  Scaled by the element count for other sizes.
+MEASURED_TRAFFIC = {"ne": 1_164_240, "fp64": (143.15e6 + 129.10e6), "mixed": (100.94e6 + 62.43e6)}
+
+
+def measured_traffic(layout, precision, ne):
+    if layout != "elem" or precision not in MEASURED_TRAFFIC:
+        return None
+    return MEASURED_TRAFFIC[precision] * ne / MEASURED_TRAFFIC["ne"]
 
 
 def run_ours(args):
@@ -278,7 +294,8 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"kernel": kern_name, "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "bytes_per_launch": b_it, "launch_ms": it_ms, "traffic": None,
+                     "peak_kind": peak_kind, "bytes_per_launch": b_it, "launch_ms": it_ms,
+                     "traffic": measured_traffic(layout, args.precision, ne),
                      "spmv_alone": {"achieved": spmv_gbs, "frac": spmv_gbs / peak, "ms": spmv_ms,
                                     "bytes": b_apply, "layout": layout},
                      "spmv_csr_f64": {"achieved": csr_gbs, "frac": csr_gbs / peak, "ms": csr_ms,
@@ -288,11 +305,122 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and not args.no_extras:
+        del eng, solver, x, J, y, xv, yv, pat, fm
+        torch.cuda.empty_cache()
+        line["assembly_microbench"] = assembly_microbench()
+        torch.cuda.empty_cache()
+        line["mixed_precision_4m"] = mixed_precision_accuracy()
+        torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def mixed_precision_accuracy(tets=4_000_000, n_probes=1000):
+    """The same window-frame yoke at ~4M tets solved to the 1e-8 Newton residual twice: in
+    float64, and with float32 element tensors and float32 CG inside the float64 Newton loop
+    (the Newton residual and update stay float64, so each Newton step refines the float32
+    inner solve).  Reported: B error at 1000 seeded aperture probes of the mixed solve against
+    the float64 solve, and Newton / CG counts and times of both."""
+    import torch
+
+    import snoopy_b200 as S
+    from snoopy_b200 import mesh as M
+
+    t0 = time.perf_counter()
+    msh, coils, rel = workload(tets)
+    solver = S.RedMVPSolver(msh, coils, [M.TAG_IRON], [M.TAG_AIR], [rel], max_newton_iterations=60, quad_order=2)
+    solver.verbose = False
+    solver.newton_engine()
+    probes = msh.geometry.aperture_probes(n_probes)
+    el, _ = msh.locate(probes)
+    setup_s = time.perf_counter() - t0
+    out = {"workload": f"window-frame yoke, {msh.num_elements} tets / {msh.num_dofs} edge DoFs, Q=4",
+           "setup_s": setup_s, "probes": n_probes}
+    B = {}
+    for prec in ("fp64", "mixed"):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        xs, st = solver.solve_to_residual(RTOL, precision=prec, max_newton=60, return_device=True)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t
+        B[prec] = solver.evaluate_B(xs, probes, el)
+        out[prec] = {"newton": st["newton_iterations"], "cg": st["cg_iterations"], "rel_res": st["rel_res"],
+                     "solve_s": wall, "krylov_ms": st["t_krylov_ms"], "assembly_ms": st["t_assemble_ms"]}
+    d = np.linalg.norm(B["mixed"] - B["fp64"], axis=1)
+    out["b_err_max_rel"] = float(d.max() / np.linalg.norm(B["fp64"], axis=1).max())
+    out["b_err_rms_rel"] = float(np.sqrt(np.mean(d ** 2)) / np.sqrt(np.mean(np.sum(B["fp64"] ** 2, axis=1))))
+    del solver
+    return out
+
+
+def assembly_microbench(reps=5, warmup=3, seed=5):
+    """Assembly-only microbenchmark: the structured 120 x 120 x 116 grid split into 6 tets
+    per cell (10,022,400 tets), nodes jittered by U[-0.2, 0.2] x spacing, edge DoFs
+    x ~ N(0, 1e-3), seeded 40% iron flags (PCHIP atan B-H) against air, no Dirichlet mask,
+    4-point rule, float64.  Two Newton assemblies at x are timed (CUDA events, after warm-up):
+
+    * csr: the drop-in path, J = K + dK scattered into the fixed CSR through the slot map
+      plus the residual F (``snp_solver_assemble``, the value zeroing included);
+    * tensors: the matrix-free path of the Newton loop, S_e per element plus F and diag(J)
+      summed per DoF (``snp_solver_assemble_tensors``).
+
+    Algorithmic bytes: csr E*(16 cells + 24 DoFs + 4 orientation + 144 slots) + 24N + 8n (x)
+    + 8nnz (J) + 8n (F); tensors E*(16 + 24 + 4 + 48 S_e) + 24N + 8n + 16n (F, diag).
+    Every element is read once per call; the 1.9e8-entry matrix and the slot map exceed L2.
+    """
+    import torch
+
+    import snoopy_b200 as S
+    from snoopy_b200 import _lib
+    from snoopy_b200 import materials as MAT
+    from snoopy_b200 import mesh as M
+    from snoopy_b200.curl_curl_assembler import CurlCurlAssembler
+    from snoopy_b200.device import upload, zeros
+    from snoopy_b200.newton import DeviceNewton
+
+    t0 = time.perf_counter()
+    msh = M.kuhn_microbench_mesh()
+    E, N, n = msh.num_elements, msh.nodes.shape[0], msh.num_dofs
+    asm = CurlCurlAssembler(msh, [M.TAG_IRON, M.TAG_AIR], [MAT.atan_reluctance(), S.ConstantReluctance(1e7 / (4 * np.pi))])
+    eng = DeviceNewton(asm, np.ones(n, dtype=np.uint8), (), quad_order=2)
+    nnz = eng.pattern.nnz
+    x = upload(np.random.default_rng(seed).normal(0.0, 1e-3, n), np.float64)
+    J = zeros(nnz)
+    F = zeros(n)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_csr = timed(lambda: _lib.call("snp_solver_assemble", eng.handle, _lib.ptr(x), None, _lib.ptr(J), None,
+                                     _lib.ptr(F), _lib.stream_ptr()))
+    ms_t = timed(lambda: eng.assemble_tensors(x, "fp64", F))
+    peak, peak_kind = measured_peaks()
+    b_csr = E * (16 + 24 + 4 + 144) + 24 * N + 8 * n + 8 * nnz + 8 * n
+    b_t = E * (16 + 24 + 4 + 48) + 24 * N + 8 * n + 16 * n
+    out = {"workload": f"Kuhn grid 120x120x116 x 6 = {E} tets, {N} nodes, {n} edge DoFs, nnz {nnz}, "
+                       f"40% iron, x ~ N(0, 1e-3), Q=4, f64",
+           "setup_s": setup_s, "peak_gbs": peak, "peak_kind": peak_kind}
+    for name, ms, b in (("csr", ms_csr, b_csr), ("tensors", ms_t, b_t)):
+        gbs = b / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "gelem_per_s": E / (ms / 1e3) / 1e9, "bytes": b, "achieved_gbs": gbs,
+                     "frac": gbs / peak}
+    del eng, asm, J, F, x
+    return out
 
 
 # ---------------------------------------------------------------------------- CPU reference

@@ -262,6 +262,13 @@ int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *
 #define SNP_LAYOUT_ELEM 2
 int snp_solver_jacobian_layout(const snp_solver *s, int *layout);
 
+/* Matrix-free Newton assembly at x (device, [n_dofs]): the element tensors of the Jacobian
+ * (float64 for precision 0, float32 for 1; afterwards snp_solver_jacobian_apply with that
+ * precision applies J(x)) and, when F is not NULL, the residual F = K(x) x - rhs(x) - rhs_extra
+ * ([n_dofs], device).  Needs the SNP_LAYOUT_ELEM layout.  Replaces, for the Newton loop, the
+ * K/dK/rhs assembly of compute_K_dK_Hcurl[_red] (fem_c/ctools.c:960-1388). */
+int snp_solver_assemble_tensors(snp_solver *s, const double *x, int precision, double *F, void *stream);
+
 /* y = J x on the free rows and columns (y = 0 on constrained rows) with the Newton Jacobian
  * the solver holds from its last solve, in the layout the solver's Krylov loop uses.
  * precision 0: the float64 Jacobian, x/y double[n]; precision 1: the float32 Jacobian of a

@@ -80,6 +80,7 @@ _SIGS = {
     "snp_solver_pattern": [_vp, _pp],
     "snp_solver_jacobian_apply": [_vp, ctypes.c_int, _vp, _vp, _vp],
     "snp_solver_jacobian_layout": [_vp, ctypes.POINTER(ctypes.c_int)],
+    "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
     "snp_solver_destroy": [_vp],
 }
 _RESTYPES = {"snp_last_error": ctypes.c_char_p, "snp_version": ctypes.c_int}

@@ -712,6 +712,19 @@ int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *
     return rc;
 }
 
+int snp_solver_assemble_tensors(snp_solver *s, const double *x, int precision, double *F, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_assemble_tensors: solver missing or not finalized");
+    SNP_REQUIRE(s->layout == SNP_LAYOUT_ELEM, "snp_solver_assemble_tensors: the solver's Jacobian layout is not elem");
+    SNP_REQUIRE(precision == 0 || precision == 1, "snp_solver_assemble_tensors: precision must be 0 or 1");
+    SNP_REQUIRE(x != nullptr, "snp_solver_assemble_tensors: x is NULL");
+    cudaStream_t keep = s->stream;
+    if (stream) s->stream = snp::as_stream(stream);
+    int rc = s->assemble_elem(x, precision == 1, F ? F : s->F.p);
+    s->stream = keep;
+    return rc;
+}
+
 int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void *y, void *stream) {
     snp::clear_error();
     SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_jacobian_apply: solver missing or not finalized");

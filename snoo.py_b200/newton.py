@@ -96,6 +96,14 @@ class DeviceNewton:
         _lib.call("snp_solver_jacobian_layout", self.handle, ctypes.byref(v))
         return {0: "csr", 1: "sell", 2: "elem"}[v.value]
 
+    def assemble_tensors(self, x, precision="fp64", F=None):
+        """Matrix-free Newton assembly at x (element tensors of J(x), and F(x) into ``F`` when
+        given); afterwards ``jacobian_apply(..., precision)`` applies J(x)."""
+        x_d = x if hasattr(x, "data_ptr") else upload(x, np.float64)
+        _lib.call("snp_solver_assemble_tensors", self.handle, _lib.ptr(x_d), {"fp64": 0, "mixed": 1}[precision],
+                  _lib.ptr(F), _lib.stream_ptr(self._stream))
+        return F
+
     def jacobian_apply(self, x, y, precision="fp64"):
         """y = J x on the free DoFs with the Newton Jacobian of the last solve of that precision
         ("fp64": float64 vectors; "mixed": the float32 Jacobian and float32 vectors)."""

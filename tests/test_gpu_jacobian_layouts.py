@@ -145,3 +145,33 @@ def test_element_layout_multi_pass_grid():
         out[layout] = solver.curl_curl_factory.compute_B_at_points(x, probes, el)
     err = np.linalg.norm(out["elem"] - out["csr"], axis=1).max() / np.linalg.norm(out["csr"], axis=1).max()
     assert err < 1e-6, err
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_assemble_tensors_at_any_iterate(precision):
+    """snp_solver_assemble_tensors at a random iterate: J(x) z and F(x) against the CSR
+    assembly of the same x (the reduced formulation with a source field)."""
+    msh, solver, eng = _solver("elem")
+    n = msh.num_dofs
+    rng = np.random.default_rng(9)
+    x = upload(rng.normal(0.0, 2e-3, n), np.float64)
+    F = torch.zeros(n, dtype=torch.float64, device="cuda")
+    eng.assemble_tensors(x, precision, F)
+    ref = eng.assemble(x, J=True, F=True, rhs=True)
+    Jc = eng.pattern.to_scipy(ref["J"], drop_zeros=False)
+    mask = solver.make_boundary_mask()
+    z = rng.standard_normal(n)
+    zf = np.where(mask, z, 0.0)
+    want = np.where(mask, Jc @ zf, 0.0)
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    yd = torch.zeros(n, dtype=dt, device="cuda")
+    eng.jacobian_apply(upload(z, np.float64).to(dt), yd, precision)
+    got = yd.double().cpu().numpy()
+    scale = np.abs(Jc) @ np.abs(zf)
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    assert (np.abs(got - want) / (scale + 1e-300))[mask].max() <= tol
+    # F: same float64 terms summed in another order; bound by the terms' magnitudes
+    Fg, Fr = F.cpu().numpy(), ref["F"].cpu().numpy()
+    Kabs = np.abs(Jc) @ np.abs(x.cpu().numpy())
+    rhs = np.abs(ref["rhs"].cpu().numpy())
+    assert np.all(np.abs(Fg - Fr) <= 1e-12 * (Kabs + rhs) + 1e-13 * np.abs(Fr).max())
