@@ -281,6 +281,37 @@ int snp_solver_pattern(const snp_solver *s, const snp_pattern **pat);
 
 int snp_solver_destroy(snp_solver *s);
 
+/* ---------------------------------------------------------------- warm-start surrogate
+ * Dense kernels of the learned warm start: an MLP that maps design parameters to POD
+ * coefficients of the converged edge-DoF vector.  None has a counterpart in the reference
+ * (snoo.py has no surrogate); BF16 arrays are passed as raw 16-bit words. */
+
+/* C[M,N] = A[M,K] . B[N,K]^T (+ bias[N]) on the tcgen05 tensor cores: A, B row-major BF16
+ * with K contiguous (K and lda, ldb multiples of 8, A and B 16-byte aligned), FP32
+ * accumulation.  Outputs (either may be NULL): C FP32 [M, ldc]; H BF16 [M, ldh] = act(C)
+ * with act 0 = identity, 1 = GELU (0.5 z (1 + erf(z / sqrt 2))).  *err (device int, caller
+ * zeroes it) is set to 1 if a tensor-core wait timed out.  Asynchronous on the stream. */
+int snp_gemm_bf16(int32_t M, int32_t N, int32_t K, const void *A, int32_t lda, const void *B, int32_t ldb,
+                  const float *bias, int32_t act, float *C, int32_t ldc, void *H, int32_t ldh, int32_t *err,
+                  void *stream);
+
+/* dZ = dH * GELU'(Z), element-wise over count values; BF16 and/or FP32 output. */
+int snp_gelu_backward(int64_t count, const float *dH, const float *Z, void *dZ_bf16, float *dZ_f32, void *stream);
+
+/* out[c][r] = in[r][c] for a rows x cols BF16 matrix (row strides ldi, ldo). */
+int snp_transpose_bf16(int32_t rows, int32_t cols, const void *in, int32_t ldi, void *out, int32_t ldo, void *stream);
+
+/* out[c] = sum_r in[r][c] (FP32; bias gradients). */
+int snp_col_sum(int32_t rows, int32_t cols, const float *in, int32_t ld, float *out, void *stream);
+
+/* One Adam step (bias-corrected, step >= 1) on FP32 weights w with gradient g and moments m,
+ * v; refreshes the BF16 copy w_bf16 when not NULL. */
+int snp_adam_step(int64_t count, float *w, const float *g, float *m, float *v, void *w_bf16, float lr, float beta1,
+                  float beta2, float eps, int32_t step, void *stream);
+
+/* BF16 (round to nearest even) copy of count FP32 values. */
+int snp_f32_to_bf16(int64_t count, const float *in, void *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,6 +81,14 @@ _SIGS = {
     "snp_solver_jacobian_apply": [_vp, ctypes.c_int, _vp, _vp, _vp],
     "snp_solver_jacobian_layout": [_vp, ctypes.POINTER(ctypes.c_int)],
     "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
+    "snp_gemm_bf16": [_c_i32, _c_i32, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp,
+                      _vp],
+    "snp_gelu_backward": [_c_i64, _vp, _vp, _vp, _vp, _vp],
+    "snp_transpose_bf16": [_c_i32, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp],
+    "snp_col_sum": [_c_i32, _c_i32, _vp, _c_i32, _vp, _vp],
+    "snp_adam_step": [_c_i64, _vp, _vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                      ctypes.c_float, _c_i32, _vp],
+    "snp_f32_to_bf16": [_c_i64, _vp, _vp, _vp],
     "snp_solver_destroy": [_vp],
 }
 _RESTYPES = {"snp_last_error": ctypes.c_char_p, "snp_version": ctypes.c_int}

@@ -1,0 +1,339 @@
+// Dense kernels of the warm-start surrogate (an MLP on POD coefficients): a BF16 GEMM on the
+// 5th-generation tensor cores (tcgen05.mma, FP32 accumulator in tensor memory) with a fused
+// bias / GELU epilogue, and the element-wise kernels of its training step.
+//
+// GEMM  C[M,N] = A[M,K] . B[N,K]^T  (+ bias[N]),  A and B row-major BF16 with K contiguous.
+// One CTA of 128 threads computes a 128 x NT tile (NT <= 256, a multiple of 16): K is walked
+// in chunks of 64; each chunk of A (128 x 64) and B (NT x 64) is copied into shared memory in
+// the no-swizzle K-major layout the MMA reads (8-row x 16-byte core matrices: element (r, k)
+// of a chunk at ((k / 8) * (rows / 8) + r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2 bytes), then
+// one thread issues four 128 x NT x 16 MMAs and commits them to an mbarrier that every thread
+// waits on.  The epilogue reads the accumulator back with tcgen05.ld (warp w owns TMEM lanes
+// 32w .. 32w+31 = tile rows) and writes FP32 C and/or BF16 act(C).
+//
+// Every wait on the mbarrier is bounded: after kMaxSpin polls the CTA records an error in
+// *err (a device flag the caller reads when it synchronises), stops issuing work, frees its
+// tensor memory and returns.  The kernel asks for more
+// than half of an SM's shared memory, so one CTA (holding 256 TMEM columns) runs per SM and
+// the allocation never waits on another CTA.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "snp_common.cuh"
+#include "snp_internal.cuh"
+
+namespace snp {
+
+namespace {
+
+constexpr int kGemmThreads = 128;
+constexpr int kTileM = 128;
+constexpr int kChunkK = 64;
+constexpr int kMaxNT = 256;
+constexpr int kTmemCols = 256;
+constexpr size_t kGemmSmem = 120 * 1024;  // > half of the SM: one CTA per SM
+constexpr long long kMaxSpin = 1ll << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: no swizzle, K-major canonical layout.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 accumulator, M x N.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int m, int n) {
+    return (1u << 4)                      // accumulator F32
+           | (1u << 7)                    // A BF16
+           | (1u << 10)                   // B BF16
+           | ((uint32_t)(n >> 3) << 17)   // N / 8
+           | ((uint32_t)(m >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kMaxSpin; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+// Copy rows [r0, r0 + rows) x K-chunk [k0, k0 + 64) of a row-major BF16 matrix (ld elements,
+// rows_total x k_total) into the canonical layout; out-of-range elements become zero.
+__device__ __forceinline__ void load_chunk(uint8_t *dst, const __nv_bfloat16 *src, int ld, int r0, int rows,
+                                           int rows_total, int k0, int k_total) {
+    const int vecs = rows * (kChunkK / 8);
+    for (int v = threadIdx.x; v < vecs; v += kGemmThreads) {
+        const int r = v / (kChunkK / 8);
+        const int kc = v - r * (kChunkK / 8);
+        const int gr = r0 + r, gk = k0 + 8 * kc;
+        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+        if (gr < rows_total && gk < k_total)  // k_total is a multiple of 8 (checked on the host)
+            val = *reinterpret_cast<const uint4 *>(src + (int64_t)gr * ld + gk);
+        *reinterpret_cast<uint4 *>(dst + (kc * (rows / 8) + r / 8) * 128 + (r % 8) * 16) = val;
+    }
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    k_gemm_bf16(int M, int N, int K, const __nv_bfloat16 *__restrict__ A, int lda,
+                const __nv_bfloat16 *__restrict__ B, int ldb, const float *__restrict__ bias, int act,
+                float *__restrict__ C, int ldc, __nv_bfloat16 *__restrict__ H, int ldh, int nt, int *err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ int failed;
+    uint8_t *sa = smem;                                  // 128 x 64 BF16 = 16 KiB
+    uint8_t *sb = smem + kTileM * kChunkK * 2;           // nt x 64 BF16 <= 32 KiB
+    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * nt;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        failed = 0;
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base_slot;
+    const uint32_t idesc = instr_desc_bf16(kTileM, nt);
+    const uint32_t bar_addr = smem_u32(&bar);
+    const int n_chunks = (K + kChunkK - 1) / kChunkK;
+
+    for (int c = 0; c < n_chunks; ++c) {
+        load_chunk(sa, A, lda, m0, kTileM, M, c * kChunkK, K);
+        load_chunk(sb, B, ldb, n0, nt, N, c * kChunkK, K);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+#pragma unroll
+            for (int s = 0; s < kChunkK / 16; ++s) {
+                // MMA step s covers k-chunks 2s and 2s+1 of 8 elements each
+                const uint64_t da = smem_desc(a0 + 2 * s * (kTileM / 8) * 128, (kTileM / 8) * 128, 128);
+                const uint64_t db = smem_desc(b0 + 2 * s * (nt / 8) * 128, (nt / 8) * 128, 128);
+                const uint32_t accumulate = (c > 0 || s > 0) ? 1u : 0u;
+                const uint32_t no_mask = 0u;  // disable-output-lane mask: every lane written
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(no_mask));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_addr)
+                         : "memory");
+        }
+        // every thread waits for the chunk's MMAs before the buffers are refilled
+        if (!mbar_wait(bar_addr, (uint32_t)(c & 1))) atomicExch(&failed, 1);
+        __syncthreads();
+        if (failed) break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+
+    if (!failed) {
+        const int row = m0 + 32 * warp + lane;
+        for (int c8 = 0; c8 < nt / 8; ++c8) {
+            uint32_t v[8];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(8 * c8);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int col = n0 + 8 * c8 + j;
+                    if (col < N) {
+                        float z = __uint_as_float(v[j]);
+                        if (bias) z += bias[col];
+                        if (C) C[(int64_t)row * ldc + col] = z;
+                        if (H) H[(int64_t)row * ldh + col] = __float2bfloat16_rn(act == 1 ? gelu(z) : z);
+                    }
+                }
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
+// dZ = dH * GELU'(Z) (FP32 in, BF16 out for the next GEMMs, FP32 copy optional)
+__global__ void k_gelu_backward(int64_t count, const float *__restrict__ dH, const float *__restrict__ Z,
+                                __nv_bfloat16 *__restrict__ dZb, float *__restrict__ dZf) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const float z = Z[i];
+        const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+        const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+        const float g = dH[i] * (cdf + z * pdf);
+        if (dZb) dZb[i] = __float2bfloat16_rn(g);
+        if (dZf) dZf[i] = g;
+    }
+}
+
+// out[c, r] = in[r, c] (BF16, rows x cols -> cols x rows, ld = row length)
+__global__ void k_transpose_bf16(int rows, int cols, const __nv_bfloat16 *__restrict__ in, int ldi,
+                                 __nv_bfloat16 *__restrict__ out, int ldo) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = r0 + j, c = c0 + threadIdx.x;
+        tile[j][threadIdx.x] = (r < rows && c < cols) ? in[(int64_t)r * ldi + c] : __float2bfloat16_rn(0.f);
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int c = c0 + j, r = r0 + threadIdx.x;
+        if (c < cols && r < rows) out[(int64_t)c * ldo + r] = tile[threadIdx.x][j];
+    }
+}
+
+// column sums of a rows x cols FP32 matrix (bias gradients), one block per column group
+__global__ void k_col_sum(int rows, int cols, const float *__restrict__ in, int ld, float *__restrict__ out) {
+    __shared__ float sh[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    float s = 0.f;
+    if (c < cols)
+        for (int r = threadIdx.y; r < rows; r += blockDim.y) s += in[(int64_t)r * ld + c];
+    sh[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < cols) {
+        float t = 0.f;
+        for (int j = 0; j < (int)blockDim.y; ++j) t += sh[j][threadIdx.x];
+        out[c] = t;
+    }
+}
+
+// Adam step on FP32 master weights, refreshing their BF16 copy.
+__global__ void k_adam(int64_t count, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, __nv_bfloat16 *__restrict__ wb, float lr, float b1, float b2, float eps,
+                       float bc1, float bc2) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+        w[i] = wi;
+        if (wb) wb[i] = __float2bfloat16_rn(wi);
+    }
+}
+
+__global__ void k_f32_to_bf16(int64_t count, const float *__restrict__ a, __nv_bfloat16 *__restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = __float2bfloat16_rn(a[i]);
+}
+
+}  // namespace
+
+}  // namespace snp
+
+extern "C" {
+
+int snp_gemm_bf16(int32_t M, int32_t N, int32_t K, const void *A, int32_t lda, const void *B, int32_t ldb,
+                  const float *bias, int32_t act, float *C, int32_t ldc, void *H, int32_t ldh, int32_t *err,
+                  void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(M >= 0 && N >= 0 && K >= 0, "snp_gemm_bf16: negative size");
+    if (M == 0 || N == 0) return SNP_OK;
+    SNP_REQUIRE(A && B && err, "snp_gemm_bf16: A, B or err is NULL");
+    SNP_REQUIRE(C || H, "snp_gemm_bf16: no output (C and H are NULL)");
+    SNP_REQUIRE(K % 8 == 0 && K > 0, "snp_gemm_bf16: K = %d must be a positive multiple of 8 (pad with zeros)", K);
+    SNP_REQUIRE(lda % 8 == 0 && ldb % 8 == 0 && lda >= K && ldb >= K,
+                "snp_gemm_bf16: lda/ldb must be multiples of 8 and >= K");
+    SNP_REQUIRE(((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0, "snp_gemm_bf16: A and B must be 16-byte aligned");
+    SNP_REQUIRE(!C || ldc >= N, "snp_gemm_bf16: ldc < N");
+    SNP_REQUIRE(!H || ldh >= N, "snp_gemm_bf16: ldh < N");
+    SNP_REQUIRE(act == 0 || act == 1, "snp_gemm_bf16: act must be 0 (none) or 1 (GELU)");
+    // N tile: the whole N when it fits, else 256-wide tiles (both multiples of 16)
+    const int nt = N <= snp::kMaxNT ? ((N + 15) / 16) * 16 : snp::kMaxNT;
+    cudaStream_t s = snp::as_stream(stream);
+    SNP_CUDA_TRY(cudaFuncSetAttribute(snp::k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)snp::kGemmSmem));
+    dim3 grid((M + snp::kTileM - 1) / snp::kTileM, (N + nt - 1) / nt);
+    snp::k_gemm_bf16<<<grid, snp::kGemmThreads, snp::kGemmSmem, s>>>(
+        M, N, K, static_cast<const __nv_bfloat16 *>(A), lda, static_cast<const __nv_bfloat16 *>(B), ldb, bias, act, C,
+        ldc, static_cast<__nv_bfloat16 *>(H), ldh, nt, err);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int snp_gelu_backward(int64_t count, const float *dH, const float *Z, void *dZ_bf16, float *dZ_f32, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(count >= 0 && dH && Z && (dZ_bf16 || dZ_f32), "snp_gelu_backward: bad arguments");
+    if (count == 0) return SNP_OK;
+    snp::k_gelu_backward<<<snp::stride_grid(count, 256, 8), 256, 0, snp::as_stream(stream)>>>(
+        count, dH, Z, static_cast<__nv_bfloat16 *>(dZ_bf16), dZ_f32);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int snp_transpose_bf16(int32_t rows, int32_t cols, const void *in, int32_t ldi, void *out, int32_t ldo, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(rows >= 0 && cols >= 0 && in && out && ldi >= cols && ldo >= rows, "snp_transpose_bf16: bad arguments");
+    if (rows == 0 || cols == 0) return SNP_OK;
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+    snp::k_transpose_bf16<<<grid, block, 0, snp::as_stream(stream)>>>(
+        rows, cols, static_cast<const __nv_bfloat16 *>(in), ldi, static_cast<__nv_bfloat16 *>(out), ldo);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int snp_col_sum(int32_t rows, int32_t cols, const float *in, int32_t ld, float *out, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(rows >= 0 && cols >= 0 && in && out && ld >= cols, "snp_col_sum: bad arguments");
+    if (cols == 0) return SNP_OK;
+    dim3 grid((cols + 31) / 32), block(32, 8);
+    snp::k_col_sum<<<grid, block, 0, snp::as_stream(stream)>>>(rows, cols, in, ld, out);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int snp_adam_step(int64_t count, float *w, const float *g, float *m, float *v, void *w_bf16, float lr, float beta1,
+                  float beta2, float eps, int32_t step, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(count >= 0 && w && g && m && v && step >= 1, "snp_adam_step: bad arguments");
+    if (count == 0) return SNP_OK;
+    const float bc1 = 1.f - powf(beta1, (float)step), bc2 = 1.f - powf(beta2, (float)step);
+    snp::k_adam<<<snp::stride_grid(count, 256, 8), 256, 0, snp::as_stream(stream)>>>(
+        count, w, g, m, v, static_cast<__nv_bfloat16 *>(w_bf16), lr, beta1, beta2, eps, bc1, bc2);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int snp_f32_to_bf16(int64_t count, const float *in, void *out, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(count >= 0 && in && out, "snp_f32_to_bf16: bad arguments");
+    if (count == 0) return SNP_OK;
+    snp::k_f32_to_bf16<<<snp::stride_grid(count, 256, 8), 256, 0, snp::as_stream(stream)>>>(
+        count, in, static_cast<__nv_bfloat16 *>(out));
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+}  // extern "C"
