@@ -226,7 +226,10 @@ typedef struct {
     double cg_rtol;          /* mode 0: scipy default 1e-5; mode 1: cap of the adaptive forcing term */
     int32_t precision;       /* 0: float64 throughout; 1: float32 Jacobian + Krylov inside float64 Newton */
     int32_t verbose;         /* print one line per Newton step to stdout */
-    int32_t line_search;     /* mode 1: Armijo backtracking on ||F_free|| (quadratic interpolation, factor in [0.1, 0.5]) */
+    int32_t line_search;     /* mode 1: step length where the energy slope F(x + a h).h has halved (safeguarded secant) */
+    double res_ref;          /* mode 1: > 0 replaces ||F_free(x0)|| in the criterion (pass ||F_free(0)|| to hold a
+                                warm start to the zero-start target); a start with ||F_free(x0)|| > res_ref is
+                                replaced by x0 = 0 (stats.start_dropped) */
 } snp_solve_opts;
 
 /* Solve statistics (host struct). */
@@ -239,6 +242,7 @@ typedef struct {
     int32_t status;
     int64_t kernel_launches;     /* this library's kernels launched by the solve (graph nodes counted per execution) */
     int32_t residual_evals;      /* extra residual-only assemblies of the line search */
+    int32_t start_dropped;       /* 1 when the initial guess was replaced by 0 (see res_ref) */
 } snp_solve_stats;
 
 /* x[n_dofs] (device): in = initial guess, out = solution.  Synchronises. */
@@ -276,6 +280,15 @@ int snp_solver_assemble_tensors(snp_solver *s, const double *x, int precision, d
  * No counterpart in the reference (Jacobian-vector product of the Newton step). */
 int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void *y, void *stream);
 
+/* Replace the node coordinates (device f64[n_nodes][3]) of a solver's mesh: same topology,
+ * moved nodes (a morphed geometry).  The CSR pattern, element topology and materials stay.
+ * No counterpart in the reference (it rebuilds everything per geometry). */
+int snp_solver_set_nodes(snp_solver *s, const double *nodes, void *stream);
+
+/* Replace the source field of material `material` (device f64[n_elems][n_quad][3], the
+ * material must have been added with one), e.g. after moving the coils or nodes. */
+int snp_solver_set_source(snp_solver *s, int32_t material, const double *B_s, void *stream);
+
 /* The solver's CSR pattern (owned by the solver). */
 int snp_solver_pattern(const snp_solver *s, const snp_pattern **pat);
 
@@ -308,6 +321,10 @@ int snp_col_sum(int32_t rows, int32_t cols, const float *in, int32_t ld, float *
  * v; refreshes the BF16 copy w_bf16 when not NULL. */
 int snp_adam_step(int64_t count, float *w, const float *g, float *m, float *v, void *w_bf16, float lr, float beta1,
                   float beta2, float eps, int32_t step, void *stream);
+
+/* dY = scale * (Y - T) over count values (gradient of a mean-squared error), with an
+ * optional BF16 copy. */
+int snp_mse_grad(int64_t count, const float *Y, const float *T, float scale, float *dY, void *dY_bf16, void *stream);
 
 /* BF16 (round to nearest even) copy of count FP32 values. */
 int snp_f32_to_bf16(int64_t count, const float *in, void *out, void *stream);

@@ -31,13 +31,14 @@ STATUS = {0: "SNP_OK", 1: "SNP_BAD_ARG", 2: "SNP_CUDA_ERROR", 3: "SNP_NOT_CONVER
 
 class SolveOpts(ctypes.Structure):
     _fields_ = [("mode", _c_i32), ("tol", _c_f64), ("cg_maxiter", _c_i64), ("max_newton", _c_i32),
-                ("cg_rtol", _c_f64), ("precision", _c_i32), ("verbose", _c_i32), ("line_search", _c_i32)]
+                ("cg_rtol", _c_f64), ("precision", _c_i32), ("verbose", _c_i32), ("line_search", _c_i32),
+                ("res_ref", _c_f64)]
 
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("newton_iterations", _c_i32), ("cg_iterations", _c_i64), ("res0", _c_f64), ("res", _c_f64),
                 ("t_assemble_ms", _c_f64), ("t_krylov_ms", _c_f64), ("t_total_ms", _c_f64), ("status", _c_i32),
-                ("kernel_launches", _c_i64), ("residual_evals", _c_i32)]
+                ("kernel_launches", _c_i64), ("residual_evals", _c_i32), ("start_dropped", _c_i32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -81,6 +82,8 @@ _SIGS = {
     "snp_solver_jacobian_apply": [_vp, ctypes.c_int, _vp, _vp, _vp],
     "snp_solver_jacobian_layout": [_vp, ctypes.POINTER(ctypes.c_int)],
     "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
+    "snp_solver_set_nodes": [_vp, _vp, _vp],
+    "snp_solver_set_source": [_vp, _c_i32, _vp, _vp],
     "snp_gemm_bf16": [_c_i32, _c_i32, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp,
                       _vp],
     "snp_gelu_backward": [_c_i64, _vp, _vp, _vp, _vp, _vp],
@@ -89,6 +92,7 @@ _SIGS = {
     "snp_adam_step": [_c_i64, _vp, _vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                       ctypes.c_float, _c_i32, _vp],
     "snp_f32_to_bf16": [_c_i64, _vp, _vp, _vp],
+    "snp_mse_grad": [_c_i64, _vp, _vp, ctypes.c_float, _vp, _vp, _vp],
     "snp_solver_destroy": [_vp],
 }
 _RESTYPES = {"snp_last_error": ctypes.c_char_p, "snp_version": ctypes.c_int}

@@ -244,6 +244,16 @@ __global__ void k_adam(int64_t count, float *__restrict__ w, const float *__rest
     }
 }
 
+// Mean-squared-error gradient dY = scale * (Y - T) with a BF16 copy (the next GEMMs' input).
+__global__ void k_mse_grad(int64_t count, const float *__restrict__ Y, const float *__restrict__ T, float scale,
+                           float *__restrict__ dY, __nv_bfloat16 *__restrict__ dYb) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        const float g = scale * (Y[i] - T[i]);
+        dY[i] = g;
+        if (dYb) dYb[i] = __float2bfloat16_rn(g);
+    }
+}
+
 __global__ void k_f32_to_bf16(int64_t count, const float *__restrict__ a, __nv_bfloat16 *__restrict__ b) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
         b[i] = __float2bfloat16_rn(a[i]);
@@ -322,6 +332,16 @@ int snp_adam_step(int64_t count, float *w, const float *g, float *m, float *v, v
     const float bc1 = 1.f - powf(beta1, (float)step), bc2 = 1.f - powf(beta2, (float)step);
     snp::k_adam<<<snp::stride_grid(count, 256, 8), 256, 0, snp::as_stream(stream)>>>(
         count, w, g, m, v, static_cast<__nv_bfloat16 *>(w_bf16), lr, beta1, beta2, eps, bc1, bc2);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int snp_mse_grad(int64_t count, const float *Y, const float *T, float scale, float *dY, void *dY_bf16, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(count >= 0 && Y && T && dY, "snp_mse_grad: bad arguments");
+    if (count == 0) return SNP_OK;
+    snp::k_mse_grad<<<snp::stride_grid(count, 256, 8), 256, 0, snp::as_stream(stream)>>>(
+        count, Y, T, scale, dY, static_cast<__nv_bfloat16 *>(dY_bf16));
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }

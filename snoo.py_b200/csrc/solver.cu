@@ -423,8 +423,20 @@ struct snp_solver {
             SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
             S.t_assemble_ms += elapsed(0, 1);
             double fn = std::sqrt(st3[0]);
-            F0 = fn;
             S.res0 = fn;
+            if (o.res_ref > 0.0 && !(fn <= o.res_ref)) {
+                // a start worse than x = 0 (by the zero-start residual) is dropped for x = 0
+                SNP_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
+                SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+                SNP_TRY(assemble_newton(x, f32));
+                SNP_TRY(vstats(F.p, nullptr, true, st3));
+                SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
+                S.t_assemble_ms += elapsed(0, 1);
+                fn = std::sqrt(st3[0]);
+                S.start_dropped = 1;
+            }
+            F0 = o.res_ref > 0.0 ? o.res_ref : fn;
             for (int it = 0;; ++it) {
                 if (!(fn == fn)) return snp::fail(SNP_NAN_DETECTED, "Newton step %d: non-finite residual", it);
                 S.res = fn;
@@ -740,6 +752,27 @@ int snp_solver_jacobian_layout(const snp_solver *s, int *layout) {
     SNP_REQUIRE(s != nullptr && layout != nullptr && s->finalized,
                 "snp_solver_jacobian_layout: solver missing or not finalized");
     *layout = s->layout;
+    return SNP_OK;
+}
+
+int snp_solver_set_nodes(snp_solver *s, const double *nodes, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && nodes != nullptr, "snp_solver_set_nodes: NULL argument");
+    SNP_CUDA_TRY(cudaMemcpyAsync(s->nodes.p, nodes, sizeof(double) * 3 * s->n_nodes, cudaMemcpyDeviceToDevice,
+                                 stream ? snp::as_stream(stream) : s->stream));
+    s->j_valid[0] = s->j_valid[1] = 0;
+    return SNP_OK;
+}
+
+int snp_solver_set_source(snp_solver *s, int32_t material, const double *B_s, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && B_s != nullptr, "snp_solver_set_source: NULL argument");
+    SNP_REQUIRE(material >= 0 && material < (int32_t)s->mats.size(), "snp_solver_set_source: no material %d", material);
+    snp::Material &m = *s->mats[material];
+    SNP_REQUIRE(m.has_bs, "snp_solver_set_source: material %d was added without a source field", material);
+    SNP_CUDA_TRY(cudaMemcpyAsync(m.Bs.p, B_s, sizeof(double) * m.count * s->nq * 3, cudaMemcpyDeviceToDevice,
+                                 stream ? snp::as_stream(stream) : s->stream));
+    s->j_valid[0] = s->j_valid[1] = 0;
     return SNP_OK;
 }
 

@@ -48,11 +48,13 @@ class DeviceNewton:
         self.pattern = Pattern(None, 0, 6, self.n, handle=p, owned=False)
 
     def solve(self, x0=None, mode=MODE_RESIDUAL, tol=1e-8, cg_maxiter=-1, max_newton=25, cg_rtol=None, precision=0,
-              verbose=False, x_out=None, raise_on_failure=True, line_search=None):
+              verbose=False, x_out=None, raise_on_failure=True, line_search=None, res_ref=0.0):
         """Run Newton from ``x0`` (zeros if None).  Returns (x CUDA tensor, stats dict).
 
-        ``line_search`` (default: on in residual mode, off in reference mode) damps each step by
-        Armijo backtracking on ||F_free||."""
+        ``line_search`` (default: on in residual mode, off in reference mode) takes the step
+        length where the energy slope F(x + a h).h has halved.  ``res_ref`` > 0 (residual mode)
+        replaces ||F_free(x0)|| in the stopping rule, e.g. ||F_free(0)|| so that a warm start is
+        held to the zero-start target; a start whose residual exceeds it is replaced by 0."""
         if line_search is None:
             line_search = mode == MODE_RESIDUAL
         t = torch()
@@ -68,11 +70,12 @@ class DeviceNewton:
         if cg_rtol is None:
             cg_rtol = 1e-5 if mode == MODE_REFERENCE else 0.1
         opts = _lib.SolveOpts(int(mode), float(tol), int(cg_maxiter), int(max_newton), float(cg_rtol), int(precision),
-                              1 if verbose else 0, 1 if line_search else 0)
+                              1 if verbose else 0, 1 if line_search else 0, float(res_ref))
         st = _lib.SolveStats()
         rc = _lib.load().snp_solver_solve(self.handle, _lib.ptr(x), ctypes.byref(opts), ctypes.byref(st))
         stats = st.as_dict()
-        stats["rel_res"] = stats["res"] / stats["res0"] if stats["res0"] > 0 else 0.0
+        ref = res_ref if res_ref > 0 else stats["res0"]
+        stats["rel_res"] = stats["res"] / ref if ref > 0 else 0.0
         if rc != 0 and (raise_on_failure or rc not in (3,)):
             _lib.check(rc)
         stats["converged"] = rc == 0
@@ -95,6 +98,22 @@ class DeviceNewton:
         v = ctypes.c_int(-1)
         _lib.call("snp_solver_jacobian_layout", self.handle, ctypes.byref(v))
         return {0: "csr", 1: "sell", 2: "elem"}[v.value]
+
+    def set_nodes(self, nodes_dev):
+        """Move the mesh nodes (device float64 [N, 3]); topology, pattern and materials stay."""
+        _lib.call("snp_solver_set_nodes", self.handle, _lib.ptr(nodes_dev), _lib.stream_ptr(self._stream))
+
+    def set_source(self, material, B_s_dev):
+        """Replace material ``material``'s source field (device float64 [E_m * Q * 3])."""
+        _lib.call("snp_solver_set_source", self.handle, int(material), _lib.ptr(B_s_dev), _lib.stream_ptr(self._stream))
+
+    def residual_norm(self, x):
+        """||F_free(x)|| (float64), via the matrix-free assembly."""
+        t = torch()
+        F = zeros(self.n)[: self.n]
+        self.assemble_tensors(x, "fp64", F)
+        fm = self.free_mask.to(t.bool)
+        return float(t.linalg.vector_norm(F[fm]).item())
 
     def assemble_tensors(self, x, precision="fp64", F=None):
         """Matrix-free Newton assembly at x (element tensors of J(x), and F(x) into ``F`` when

@@ -145,3 +145,48 @@ def test_restatement_vs_live_reference(oracle_mod, rel):
     assert_csr_close(a[0], b[0], 1e-12, atol_rel=1e-15)
     assert_csr_close(a[1], b[1], 1e-12, atol_rel=1e-15)
     assert rel_max(a[2], b[2]) < 1e-13
+
+
+def test_mlp_oracle_backward_matches_finite_differences():
+    """The MLP oracle's own backward pass against central differences of its forward pass
+    (float64, no BF16 rounding): the oracle that checks the device gradients is itself pinned."""
+    import mlp_oracle as MO
+
+    rng = np.random.default_rng(0)
+    sizes = [9, 8, 8, 4]
+    W = [rng.normal(0, 0.5, (sizes[i + 1], sizes[i])) for i in range(3)]
+    b = [rng.normal(0, 0.1, sizes[i + 1]) for i in range(3)]
+    X = rng.normal(0, 1, (5, 9))
+    T = rng.normal(0, 1, (5, 4))
+    grads, _ = MO.backward(W, b, X, T)
+
+    def loss():
+        Y, _ = MO.forward(W, b, X)
+        return float(np.mean((Y - T) ** 2))
+
+    h = 1e-6
+    for l in range(3):
+        for (i, j) in [(0, 0), (1, 3), (sizes[l + 1] - 1, sizes[l] - 1)]:
+            W[l][i, j] += h
+            lp = loss()
+            W[l][i, j] -= 2 * h
+            lm = loss()
+            W[l][i, j] += h
+            assert abs((lp - lm) / (2 * h) - grads[l][0][i, j]) < 1e-7
+        b[l][0] += h
+        lp = loss()
+        b[l][0] -= 2 * h
+        lm = loss()
+        b[l][0] += h
+        assert abs((lp - lm) / (2 * h) - grads[l][1][0]) < 1e-7
+
+
+def test_bf16_rounding_is_nearest_even():
+    import mlp_oracle as MO
+
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, -2.5, 3.14159265], dtype=np.float32)
+    r = MO.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0  # tie between 1 and 1 + 2^-7 goes to even (1.0)
+    assert r[2] == 1.0 + 2 ** -7        # above the tie rounds up
+    assert r[3] == -2.5
+    assert abs(r[4] - 3.140625) < 1e-12
