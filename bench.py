@@ -44,7 +44,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the assembly microbenchmark and the 4M-tet mixed-precision accuracy run")
+                    help="skip the assembly microbenchmark, the 4M-tet mixed-precision accuracy run and the "
+                         "warm-start study at the bench size")
+    ap.add_argument("--warm-start-family", action="store_true",
+                    help="only the learned-warm-start study on the 300k-tet morphed family "
+                         "(4000 training / 500 held-out members); prints its own JSON line")
     return ap.parse_args()
 
 
@@ -312,11 +316,81 @@ def run_ours(args):
         torch.cuda.empty_cache()
         line["mixed_precision_4m"] = mixed_precision_accuracy()
         torch.cuda.empty_cache()
+        line["mixed_warm_start"] = warm_start_study(args.tets, n_train=160, n_test=8)
+        torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs=None, seed=0):
+    """Learned warm start on a morphed-yoke family (fixed topology, 8 shape parameters + coil
+    current density).  Untimed: ``n_train`` zero-start mixed-precision solves, POD to
+    ``n_modes`` modes, MLP training on the tensor-core kernels.  Timed (CUDA events around each
+    solve; moving the solver to a member is not timed): ``n_test`` held-out members solved
+    three ways to ||F_free|| <= 1e-8 ||F_free(0)||: plain float64 from zero, mixed precision
+    from zero, and mixed precision from the network's prediction (inference and reconstruction
+    inside the timed region)."""
+    import torch
+
+    from snoopy_b200 import morph
+    from snoopy_b200 import surrogate as SG
+
+    t0 = time.perf_counter()
+    fam = morph.YokeMorphFamily(base_tets=base_tets, seed=7)
+    ms = SG.MorphedSolver(fam)
+    P = fam.sample(n_train + n_test, seed=seed + 101)
+    P_train, P_test = P[:n_train], P[n_train:]
+    setup_s = time.perf_counter() - t0
+    modes = min(n_modes, n_train - 1)
+    ws = SG.WarmStart(ms, n_modes=modes, hidden=hidden, seed=seed)
+    snaps, st_train = ws.generate(P_train, precision="mixed")
+    ws.fit(P_train, snaps, epochs=epochs, batch=min(256, (n_train // 8) * 8), lr=2e-3, seed=seed)
+    del snaps
+    torch.cuda.empty_cache()
+    stream = torch.cuda.current_stream()
+    rows = {"fp64_zero": [], "mixed_zero": [], "mixed_warm": []}
+    surr_err, proj_err, b_err = [], [], []
+    probes = fam.geometry.aperture_probes(200, margin=0.03)
+    el, _ = fam.mesh.locate(probes)
+    for p in P_test:
+        ref = ms.set_member(p)
+        for name in rows:
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            x0 = ws.predict(p)[0] if name == "mixed_warm" else None
+            x, st = ms.solve(x0, rtol=RTOL, precision="fp64" if name == "fp64_zero" else "mixed", res_ref=ref)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            rows[name].append((e0.elapsed_time(e1), st["newton_iterations"], st["cg_iterations"], st["rel_res"],
+                               st["start_dropped"]))
+            if name == "fp64_zero":
+                x_ref = x.clone()
+                B_ref = ms.solver.curl_curl_factory.compute_B_at_points(x, probes, el)
+            elif name == "mixed_warm":
+                nrm = float(torch.linalg.vector_norm(x_ref).item())
+                surr_err.append(float(torch.linalg.vector_norm(x0 - x_ref).item()) / nrm)
+                proj_err.append(float(torch.linalg.vector_norm(ws.project(x_ref) - x_ref).item()) / nrm)
+                Bw = ms.solver.curl_curl_factory.compute_B_at_points(x, probes, el)
+                b_err.append(float(np.linalg.norm(Bw - B_ref, axis=1).max() / np.linalg.norm(B_ref, axis=1).max()))
+    out = {"workload": f"morphed window-frame yoke family, {fam.mesh.num_elements} tets / {fam.mesh.num_dofs} DoFs, "
+                       f"8 shape parameters + J, {n_train} training / {n_test} held-out members",
+           "setup_s": setup_s, "generate_s": ws.timings["generate_s"], "fit_s": ws.timings["fit_s"],
+           "pod_modes": modes, "pod_energy": ws.pod_energy, "train_loss_first_last": [ws.history[0][1], ws.history[-1][1]],
+           "train_newton_mean": float(np.mean([s["newton_iterations"] for s in st_train])),
+           "surrogate_rel_err_mean": float(np.mean(surr_err)), "pod_floor_rel_err_mean": float(np.mean(proj_err)),
+           "warm_vs_fp64_B_err_max": float(np.max(b_err))}
+    for name, r in rows.items():
+        r = np.array(r, dtype=np.float64)
+        out[name] = {"solves_per_s": len(r) / (r[:, 0].sum() / 1e3), "ms_mean": float(r[:, 0].mean()),
+                     "newton_mean": float(r[:, 1].mean()), "cg_mean": float(r[:, 2].mean()),
+                     "rel_res_max": float(r[:, 3].max()), "starts_dropped": int(r[:, 4].sum())}
+    out["speedup_mixed_warm_vs_fp64_zero"] = out["mixed_warm"]["solves_per_s"] / out["fp64_zero"]["solves_per_s"]
+    del ws, ms, fam
+    return out
 
 
 def mixed_precision_accuracy(tets=4_000_000, n_probes=1000):
@@ -521,9 +595,22 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_warm_start_family(args):
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    res = warm_start_study(300_000, n_train=4000, n_test=500)
+    line = {"metric": "warm-started vs zero-start nonlinear solves/s, morphed 300k-tet yoke family",
+            "value": res["mixed_warm"]["solves_per_s"], "unit": UNIT, "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f32+f64 (bf16 MLP)", "data": "synthetic (seeded morphed-yoke family)", "config": res}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.warm_start_family:
+        run_warm_start_family(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

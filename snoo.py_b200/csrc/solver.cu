@@ -424,8 +424,9 @@ struct snp_solver {
             S.t_assemble_ms += elapsed(0, 1);
             double fn = std::sqrt(st3[0]);
             S.res0 = fn;
-            if (o.res_ref > 0.0 && !(fn <= o.res_ref)) {
-                // a start worse than x = 0 (by the zero-start residual) is dropped for x = 0
+            if (o.res_ref > 0.0 && !(fn <= o.res_ref * (1.0 + 1e-9))) {
+                // a start worse than x = 0 (by the zero-start residual, up to rounding of the
+                // two evaluations) is dropped for x = 0
                 SNP_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, stream));
                 SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
                 SNP_TRY(assemble_newton(x, f32));

@@ -245,16 +245,23 @@ class WarmStart:
         self.timings["generate_s"] = time.perf_counter() - t0
         return snaps, stats
 
-    def fit(self, params, snapshots, epochs=300, batch=256, lr=2e-3, seed=0):
+    def fit(self, params, snapshots, epochs=None, batch=256, lr=2e-3, seed=0, steps=6000):
+        """POD of the snapshots, then Adam with a cosine-decayed learning rate for ``epochs``
+        passes over the data (default: as many as make about ``steps`` steps)."""
         t = torch()
         t0 = time.perf_counter()
         self.mean, self.U, coeffs, self.pod_energy = pod(snapshots, self.n_modes)
+        # one scale for every mode (not a per-mode standardisation): the network's squared
+        # error then equals the DoF-space error of the reconstruction (the modes are
+        # orthonormal), so training weights each mode by its energy
         self.c_mu = coeffs.mean(0)
-        self.c_sd = coeffs.std(0).clamp_min(1e-30)
+        self.c_sd = ((coeffs - self.c_mu) ** 2).mean().sqrt().clamp_min(1e-30)
         T = ((coeffs - self.c_mu) / self.c_sd).float()
         X = self.mlp.input_bf16(t.as_tensor(np.asarray(params), dtype=t.float32, device="cuda"))
         S = len(params)
         batch = max(8, min(batch, (S // 8) * 8))
+        if epochs is None:
+            epochs = max(1, -(-steps // max(1, S // batch)))
         rng = np.random.default_rng(seed)
         self.history = []
         for ep in range(epochs):
