@@ -266,6 +266,16 @@ int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *
 #define SNP_LAYOUT_ELEM 2
 int snp_solver_jacobian_layout(const snp_solver *s, int *layout);
 
+/* Solve `count` independent problems concurrently: instance i runs snp_solver_solve(solvers[i],
+ * x[i], &opts[i], &stats[i]) on its own host thread (at most n_threads at a time; <= 0: one
+ * per instance), each on the stream its solver was created with, so the GPU overlaps the
+ * instances' kernels.  status[i] (may be NULL) receives each instance's status; the return
+ * value is the first failure's, with its message.  Solvers must be distinct and should have
+ * distinct streams (a shared stream serialises them).  The reference solves one design per
+ * process (red_mvp_solver.py:121-224); this is the batched form. */
+int snp_solver_solve_many(snp_solver *const *solvers, int32_t count, double *const *x, const snp_solve_opts *opts,
+                          snp_solve_stats *stats, int32_t n_threads, int32_t *status);
+
 /* Matrix-free Newton assembly at x (device, [n_dofs]): the element tensors of the Jacobian
  * (float64 for precision 0, float32 for 1; afterwards snp_solver_jacobian_apply with that
  * precision applies J(x)) and, when F is not NULL, the residual F = K(x) x - rhs(x) - rhs_extra

@@ -83,6 +83,7 @@ _SIGS = {
     "snp_solver_jacobian_layout": [_vp, ctypes.POINTER(ctypes.c_int)],
     "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
     "snp_solver_set_nodes": [_vp, _vp, _vp],
+    "snp_solver_solve_many": [_vp, _c_i32, _vp, _vp, _vp, _c_i32, _vp],
     "snp_solver_set_source": [_vp, _c_i32, _vp, _vp],
     "snp_gemm_bf16": [_c_i32, _c_i32, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp,
                       _vp],

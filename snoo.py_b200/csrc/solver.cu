@@ -13,11 +13,13 @@
 // step J h = -F solved by CG to an Eisenstat-Walker forcing tolerance; with precision 1 the
 // Jacobian values and the CG run in float32 while F, the update and the norms stay float64
 // (the Newton loop is the iterative refinement of the float32 solves).
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "snp_common.cuh"
@@ -711,6 +713,45 @@ int snp_solver_solve(snp_solver *s, double *x, const snp_solve_opts *opts, snp_s
     snp_solve_stats tmp;
     snp_solve_stats &S = stats ? *stats : tmp;
     return s->solve(x, *opts, S);
+}
+
+int snp_solver_solve_many(snp_solver *const *solvers, int32_t count, double *const *x, const snp_solve_opts *opts,
+                          snp_solve_stats *stats, int32_t n_threads, int32_t *status) {
+    snp::clear_error();
+    SNP_REQUIRE(count >= 0, "snp_solver_solve_many: negative count");
+    if (count == 0) return SNP_OK;
+    SNP_REQUIRE(solvers && x && opts, "snp_solver_solve_many: NULL argument");
+    for (int32_t i = 0; i < count; ++i) {
+        SNP_REQUIRE(solvers[i] && solvers[i]->finalized && x[i], "snp_solver_solve_many: instance %d missing", i);
+        for (int32_t j = 0; j < i; ++j)
+            SNP_REQUIRE(solvers[j] != solvers[i], "snp_solver_solve_many: instances %d and %d share a solver", j, i);
+    }
+    int dev = 0;
+    SNP_CUDA_TRY(cudaGetDevice(&dev));
+    const int32_t nt = (n_threads <= 0 || n_threads > count) ? count : n_threads;
+    std::atomic<int32_t> next{0};
+    std::vector<int> rc((size_t)count, SNP_OK);
+    std::vector<std::string> msg((size_t)count);
+    auto worker = [&]() {
+        if (cudaSetDevice(dev) != cudaSuccess) cudaGetLastError();
+        for (;;) {
+            const int32_t i = next.fetch_add(1);
+            if (i >= count) break;
+            snp_solve_stats tmp;
+            rc[i] = snp_solver_solve(solvers[i], x[i], &opts[i], stats ? &stats[i] : &tmp);
+            if (rc[i] != SNP_OK) msg[i] = snp_last_error();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int32_t t = 0; t < nt; ++t) pool.emplace_back(worker);
+    for (auto &th : pool) th.join();
+    int first = -1;
+    for (int32_t i = 0; i < count; ++i) {
+        if (status) status[i] = rc[i];
+        if (rc[i] != SNP_OK && first < 0) first = i;
+    }
+    if (first >= 0) return snp::fail(rc[first], "instance %d: %s", first, msg[first].c_str());
+    return SNP_OK;
 }
 
 int snp_solver_assemble(snp_solver *s, const double *x, double *K_vals, double *J_vals, double *rhs, double *F,

@@ -58,7 +58,7 @@ class MVPSolver:
         if self._newton is None or self._rhs_key != key:
             rhs_mvp = self.compute_source_rhs(phi_list)
             self._newton = DeviceNewton(self.curl_curl_factory, self.make_boundary_mask(), (), self.quad_order,
-                                        rhs_extra=rhs_mvp)
+                                        rhs_extra=rhs_mvp, stream=getattr(self, "stream", None))
             self._rhs_key = key
         return self._newton
 

@@ -20,6 +20,10 @@ class DeviceNewton:
 
     def __init__(self, assembler, free_mask, source_fields=(), quad_order=2, rhs_extra=None, stream=None):
         _lib.require_cuda()
+        if stream is not None:
+            # inputs uploaded on torch's current stream must be complete before the solver's
+            # own stream copies them
+            torch().cuda.synchronize()
         self.assembler = assembler
         self.n = assembler.num_dofs
         d = assembler._device_state()
@@ -69,6 +73,8 @@ class DeviceNewton:
             x.zero_()
         if cg_rtol is None:
             cg_rtol = 1e-5 if mode == MODE_REFERENCE else 0.1
+        if self._stream is not None:
+            t.cuda.current_stream().synchronize()  # x was prepared on torch's stream
         opts = _lib.SolveOpts(int(mode), float(tol), int(cg_maxiter), int(max_newton), float(cg_rtol), int(precision),
                               1 if verbose else 0, 1 if line_search else 0, float(res_ref))
         st = _lib.SolveStats()

@@ -76,7 +76,7 @@ class RedMVPSolver:
     def newton_engine(self):
         if self._newton is None:
             self._newton = DeviceNewton(self.curl_curl_factory, self.make_boundary_mask(), self.compute_source_fields(),
-                                        self.quad_order)
+                                        self.quad_order, stream=getattr(self, "stream", None))
         return self._newton
 
     def solve(self, tolerance=1e-4, x_0=np.zeros((0,)), maxiter=-1, apply_gauge=False):
