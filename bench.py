@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the assembly microbenchmark, the 4M-tet mixed-precision accuracy run and the "
                          "warm-start study at the bench size")
+    ap.add_argument("--batched", action="store_true",
+                    help="only the batched-variants study (128 seeded yoke variants, 30k-600k tets, half "
+                         "reduced, half total potential); prints its own JSON line")
     ap.add_argument("--warm-start-family", action="store_true",
                     help="only the learned-warm-start study on the 300k-tet morphed family "
                          "(4000 training / 500 held-out members); prints its own JSON line")
@@ -595,6 +598,48 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, n=128):
+    """128 seeded variants (BASELINE's batched configuration): every instance solved to the 1e-8
+    residual one after another, then all of them concurrently through snp_solver_solve_many,
+    in float64 and in mixed precision.  Throughput is instances per second of wall time
+    (host clock around each whole batch, after a synchronize), so the overlap between
+    instances counts."""
+    import torch
+
+    from snoopy_b200 import batch as B
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.perf_counter()
+    V = B.sample_variants(n, seed=0)
+    inst = [B.Instance(v) for v in V]
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    tets = sum(i.num_elements for i in inst)
+    dofs = sum(i.n for i in inst)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        B.solve_many(inst[:8], precision=prec)  # warm-up: graphs and work buffers of a few instances
+        t = time.perf_counter()
+        seq = B.solve_one_by_one(inst, precision=prec)
+        t_seq = time.perf_counter() - t
+        x_seq = [i.x.clone() for i in inst]
+        t = time.perf_counter()
+        par = B.solve_many(inst, precision=prec)
+        t_par = time.perf_counter() - t
+        same = all(bool(torch.equal(a, i.x)) for a, i in zip(x_seq, inst))
+        res[prec] = {"one_by_one_s": t_seq, "batched_s": t_par, "one_by_one_per_s": n / t_seq, "batched_per_s": n / t_par,
+                     "speedup": t_seq / t_par, "identical_answers": same,
+                     "max_rel_res": max(s["rel_res"] for s in par), "newton_mean": float(np.mean([s["newton_iterations"] for s in par])),
+                     "cg_mean": float(np.mean([s["cg_iterations"] for s in par]))}
+        del x_seq
+    line = {"metric": "batched nonlinear solves/s, 128 seeded yoke variants (30k-600k tets) to 1e-8 residual",
+            "value": res["mixed"]["batched_per_s"], "unit": "solves/s", "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f32+f64", "data": "synthetic (seeded variant family)",
+            "config": {"instances": n, "tets_total": tets, "dofs_total": dofs, "setup_s": setup_s,
+                       "batching": "one host thread and CUDA stream per instance (snp_solver_solve_many)", **res}}
+    print(json.dumps(line), flush=True)
+
+
 def run_warm_start_family(args):
     import torch
 
@@ -610,6 +655,8 @@ if __name__ == "__main__":
     a = parse()
     if a.warm_start_family:
         run_warm_start_family(a)
+    elif a.batched:
+        run_batched(a)
     elif a.impl == "reference":
         run_reference(a)
     else:

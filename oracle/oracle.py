@@ -602,11 +602,13 @@ def newton_residual(assembler, mask, source_fields=(), rtol=1e-8, x_0=None, cg_r
         stats["cg"].append(its[0])
         if line_search == "energy":
             # F is the gradient of the magnetic energy W (convex for a monotone B-H law), so
-            # phi'(a) = F(x + a h) . h increases along h: accept the full step when
-            # phi'(1) <= 0.5 |phi'(0)|, else find phi'(a) ~ 0 by a safeguarded secant
+            # phi'(a) = F(x + a h) . h increases along h: keep the full step unless
+            # phi'(1) > 0.5 |phi'(0)|, else bracket phi'(a) ~ 0 by a safeguarded secant and
+            # accept |phi'(a)| <= 0.5 |phi'(0)| (undershoots raise the lower end)
             g0 = float(F[mask] @ h)
-            a_lo, g_lo, a_hi, g_hi = 0.0, g0, None, None
+            a_lo, g_lo, a_hi, g_hi = 0.0, g0, 1.0, 0.0
             alpha = 1.0
+            c = 0.5 * abs(g0)
             for ls in range(12):
                 xt = x.copy()
                 xt[mask] += alpha * h
@@ -614,9 +616,14 @@ def newton_residual(assembler, mask, source_fields=(), rtol=1e-8, x_0=None, cg_r
                 stats["assemblies"] += 1
                 Ft = Kt @ xt - rt
                 g = float(Ft[mask] @ h)
-                if g <= 0.5 * abs(g0) or ls == 11:
+                if g != g or ls == 11:
                     break
-                a_hi, g_hi = alpha, g
+                if (g <= c) if ls == 0 else (abs(g) <= c):
+                    break
+                if g < -c:
+                    a_lo, g_lo = alpha, g
+                else:
+                    a_hi, g_hi = alpha, g
                 a_new = a_lo - g_lo * (a_hi - a_lo) / (g_hi - g_lo)
                 width = a_hi - a_lo
                 alpha = min(max(a_new, a_lo + 0.01 * width), a_hi - 0.01 * width)

@@ -504,7 +504,7 @@ struct snp_solver {
                 // energy's slope phi'(a) = F(x + a h) . h has fallen to 0.5 |phi'(0)|; F is
                 // the gradient of the magnetic energy, convex for a monotone B-H law, so
                 // phi' increases along h and a safeguarded secant brackets the step
-                double alpha = 1.0, g0 = 0.0, a_lo = 0.0, g_lo = 0.0;
+                double alpha = 1.0, g0 = 0.0, a_lo = 0.0, g_lo = 0.0, a_hi = 1.0, g_hi = 0.0;
                 SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
                 if (o.line_search) {
                     SNP_TRY(vdot(F.p, h.p, &g0));
@@ -519,8 +519,19 @@ struct snp_solver {
                     if (!o.line_search) break;
                     double g = 0.0;
                     SNP_TRY(vdot(F.p, h.p, &g));
-                    if (!(g > 0.5 * std::fabs(g0)) || ls >= 11) break;
-                    const double a_hi = alpha, g_hi = g;
+                    // the full step is kept unless it overshoots (slope above +0.5 |phi'(0)|);
+                    // inside the bracket a trial must have |phi'| <= 0.5 |phi'(0)|, an undershoot
+                    // raising the lower end and an overshoot lowering the upper end
+                    const double c = 0.5 * std::fabs(g0);
+                    if (!(g == g) || ls >= 11) break;
+                    if (ls == 0 ? !(g > c) : std::fabs(g) <= c) break;
+                    if (g < -c) {
+                        a_lo = alpha;
+                        g_lo = g;
+                    } else {
+                        a_hi = alpha;
+                        g_hi = g;
+                    }
                     const double a_new = a_lo - g_lo * (a_hi - a_lo) / (g_hi - g_lo);
                     const double width = a_hi - a_lo;
                     alpha = std::fmin(std::fmax(a_new, a_lo + 0.01 * width), a_hi - 0.01 * width);
