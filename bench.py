@@ -164,6 +164,40 @@ def measured_traffic(layout, precision, ne):
     return MEASURED_TRAFFIC[precision] * ne / MEASURED_TRAFFIC["ne"]
 
 
+# ---------------------------------------------------------------------------- ranks
+
+def max_over_ranks(value, device="cpu"):
+    """The largest of a float over all ranks of the default process group (the value itself
+    when no group is initialised): every multi-GPU time is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_throughput(units_per_rank, ms_local, device="cpu"):
+    """Units processed by all ranks per second of the slowest rank's timed interval."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size() if (dist.is_available() and dist.is_initialized()) else 1
+    return world * units_per_rank / (max_over_ranks(ms_local, device) / 1e3)
+
+
+def partition_by_size(sizes, world):
+    """Greedy balance of independent instances over ranks: largest first, each to the rank
+    with the least work so far (ties to the lower rank).  Returns each rank's indices."""
+    parts = [[] for _ in range(world)]
+    load = [0.0] * world
+    for i in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -211,11 +245,8 @@ def run_ours(args):
         dist.barrier()
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, "cuda")
+    value = whole_job_throughput(args.steps, ms, "cuda")
 
     # dominant kernel: the PCG iteration (the two passes of the matrix-free operator, or the
     # assembled-matrix kernels), timed by the solver's CUDA events around every Krylov solve
@@ -275,10 +306,7 @@ def run_ours(args):
         t1 = time.perf_counter()
         e2e_times.append(t1 - t0)
     e2e_s = float(np.median(e2e_times))
-    tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = world / float(tt.item())
+    e2e_value = whole_job_throughput(1, 1e3 * e2e_s, "cuda")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -600,7 +628,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def batched_study(n=128):
+def batched_study(n=128, rank=0, world=1):
     """Seeded yoke variants (BASELINE's batched configuration: 30k-600k tets, half reduced, half
     total potential): every instance solved to the 1e-8 residual one after another, then all
     of them concurrently through snp_solver_solve_many, in float64 and in mixed precision.
@@ -612,21 +640,31 @@ def batched_study(n=128):
 
     t0 = time.perf_counter()
     V = B.sample_variants(n, seed=0)
+    if world > 1:  # independent instances: each rank takes a greedy size-balanced share
+        V = [V[i] for i in partition_by_size([v["tets"] for v in V], world)[rank]]
     inst = [B.Instance(v) for v in V]
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     tets = sum(i.num_elements for i in inst)
     dofs = sum(i.n for i in inst)
     res = {}
+    import torch.distributed as dist
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
     for prec in ("fp64", "mixed"):
         B.solve_many(inst[:8], precision=prec)  # warm-up: graphs and work buffers of a few instances
+        barrier()
         t = time.perf_counter()
         seq = B.solve_one_by_one(inst, precision=prec)
-        t_seq = time.perf_counter() - t
+        t_seq = max_over_ranks(time.perf_counter() - t, "cuda")
         x_seq = [i.x.clone() for i in inst]
+        barrier()
         t = time.perf_counter()
         par = B.solve_many(inst, precision=prec)
-        t_par = time.perf_counter() - t
+        t_par = max_over_ranks(time.perf_counter() - t, "cuda")
         same = all(bool(torch.equal(a, i.x)) for a, i in zip(x_seq, inst))
         res[prec] = {"one_by_one_s": t_seq, "batched_s": t_par, "one_by_one_per_s": n / t_seq, "batched_per_s": n / t_par,
                      "speedup": t_seq / t_par, "identical_answers": same,
@@ -634,19 +672,31 @@ def batched_study(n=128):
                      "cg_mean": float(np.mean([s["cg_iterations"] for s in par]))}
         del x_seq
     del inst
-    return {"instances": n, "tets_total": tets, "dofs_total": dofs, "setup_s": setup_s,
-            "batching": "one host thread and CUDA stream per instance (snp_solver_solve_many)", **res}
+    return {"instances": n, "ranks": world, "tets_this_rank": tets, "dofs_this_rank": dofs, "setup_s": setup_s,
+            "batching": "one host thread and CUDA stream per instance (snp_solver_solve_many)"
+                        + (f"; instances split over {world} ranks by size, max time over ranks" if world > 1 else ""),
+            **res}
 
 
 def run_batched(args, n=128):
     import torch
+    import torch.distributed as dist
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    res = batched_study(n)
-    line = {"metric": "batched nonlinear solves/s, 128 seeded yoke variants (30k-600k tets) to 1e-8 residual",
-            "value": res["mixed"]["batched_per_s"], "unit": "solves/s", "higher_is_better": True, "n_gpus": 1,
-            "dtype": "f32+f64", "data": "synthetic (seeded variant family)", "config": res}
-    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    res = batched_study(n, rank, world)
+    if rank == 0:
+        line = {"metric": "batched nonlinear solves/s, 128 seeded yoke variants (30k-600k tets) to 1e-8 residual",
+                "value": res["mixed"]["batched_per_s"], "unit": "solves/s", "higher_is_better": True,
+                "n_gpus": world, "scaling": "strong", "dtype": "f32+f64", "data": "synthetic (seeded variant family)",
+                "config": res}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_warm_start_family(args):
