@@ -105,6 +105,24 @@ int snp_curlcurl_assemble_f32(const snp_pattern *pat, int64_t elem_offset, int64
                               int32_t n_int, const double *rel_c, const double *rel_x,
                               float *J_vals, void *stream);
 
+/* Diluted steel.  Replaces fem_c.compute_stiffness_and_jacobi_matrix_curl_curl_diluted
+ * (fem_c/interface_c.pyx:698-926) -> compute_K_dK_Hcurl_red_dil (fem_c/ctools.c:1565-1759).
+ * As snp_curlcurl_assemble, and with B_s the reluctance at each quadrature point is
+ * nu = s PCHIP(s |B|), nu' = s^2 PCHIP'(s |B|) with s = (c_num + z m_num) / (c_den + z m_den),
+ * z = sum_i phi[q][i] Z_i the point's z coordinate; phi is device f64[n_quad][4] (the nodal
+ * basis at the points) and dilution host f64[4] = {c_num, m_num, c_den, m_den}.  Without
+ * B_s the plain kernel runs and phi/dilution are not read (the reference's air branch,
+ * interface_c.pyx:874-886). */
+int snp_curlcurl_assemble_diluted(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems,
+                                  const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                                  const int32_t *orientations, const double *curls, int32_t n_orient,
+                                  const double *phi, const double *d_phi, const double *w, int32_t n_quad,
+                                  const double *x, const double *B_s,
+                                  int32_t n_int, const double *rel_c, const double *rel_x,
+                                  const double *dilution,
+                                  double *K_vals, double *dK_vals, double *J_vals, double *rhs, double *F,
+                                  void *stream);
+
 /* Reduced rhs only.  Replaces fem_c.compute_rhs_Hcurl_red_c (fem_c/interface_c.pyx:377-552)
  * -> compute_rhs_Hcurl_red (fem_c/ctools.c:1390-1497).  Accumulates into rhs[n]. */
 int snp_curlcurl_rhs_red(int64_t n_elems, const double *nodes, const int32_t *cells, const int32_t *glob_ids,
@@ -298,6 +316,12 @@ int snp_solver_set_nodes(snp_solver *s, const double *nodes, void *stream);
 /* Replace the source field of material `material` (device f64[n_elems][n_quad][3], the
  * material must have been added with one), e.g. after moving the coils or nodes. */
 int snp_solver_set_source(snp_solver *s, int32_t material, const double *B_s, void *stream);
+
+/* Diluted steel for material `material` (RedMVPSolverDiluted, snoopy/red_mvp_solver_diluted.py):
+ * phi device f64[n_quad][4] (nodal basis at the quadrature points, copied) and dilution host
+ * f64[4] = {c_num, m_num, c_den, m_den}; dilution NULL switches it off again.  Applies to a
+ * material with a source field only, as in the reference.  Not while a solve is running. */
+int snp_solver_set_dilution(snp_solver *s, int32_t material, const double *phi, const double *dilution);
 
 /* The solver's CSR pattern (owned by the solver). */
 int snp_solver_pattern(const snp_solver *s, const snp_pattern **pat);

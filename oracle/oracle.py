@@ -88,6 +88,11 @@ class _Rel(ctypes.Structure):
                 ("coefficients", _dp), ("knots", _dp)]
 
 
+class _Dil(ctypes.Structure):
+    _fields_ = [("c_num", ctypes.c_double), ("m_num", ctypes.c_double), ("c_den", ctypes.c_double),
+                ("m_den", ctypes.c_double)]
+
+
 _LIBS = {}
 
 
@@ -118,7 +123,7 @@ def lib(backend="oracle"):
                             ctypes.c_double, ctypes.c_double, _dp]
         L.or_curlcurl.restype = _i64
         L.or_curlcurl.argtypes = [_i64, ctypes.c_int, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp,
-                                  ctypes.c_int, _dp, _dp, _ip, _ip, _dp, _dp, _dp, _dp, _dp]
+                                  ctypes.c_int, _dp, _dp, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.or_rhs_red.restype = ctypes.c_int
         L.or_rhs_red.argtypes = [_i64, ctypes.c_int, _dp, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp,
                                  ctypes.c_int, _dp, _dp, _dp]
@@ -140,6 +145,9 @@ def lib(backend="oracle"):
         L.compute_K_dK_Hcurl_red.restype = None
         L.compute_K_dK_Hcurl_red.argtypes = [P(_Triplets), P(_Triplets), _dp, _ip, P(_Rel), P(_Mesh), P(_Quad),
                                              _dp, _dp, _ip, _dp, _dp]
+        L.compute_K_dK_Hcurl_red_dil.restype = None
+        L.compute_K_dK_Hcurl_red_dil.argtypes = [P(_Triplets), P(_Triplets), _dp, P(_Dil), _ip, P(_Rel), P(_Mesh),
+                                                 P(_Quad), _dp, _dp, _dp, _ip, _dp, _dp]
         L.compute_rhs_Hcurl_red.restype = None
         L.compute_rhs_Hcurl_red.argtypes = [_dp, _ip, P(_Rel), P(_Mesh), P(_Quad), _dp, _dp, _ip, _dp, _dp, ctypes.c_int]
         L.compute_B_Hcurl.restype = None
@@ -231,11 +239,14 @@ def mu_eval(permeability, H, backend="oracle"):
 # ------------------------------------------------------------------ fem_c_mod restatement
 
 def curl_curl_triplets(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_s, reluctance, q, w,
-                       num_dofs, num_el_dofs, backend="oracle", scales=None):
+                       num_dofs, num_el_dofs, backend="oracle", scales=None, phi=None, dilution=None):
     """Triplets (i, j, vK, vdK) and rhs of one material, as the C kernels emit them.
 
     ``scales``: an optional dict that receives "K" and "dK", the per-triplet sums of term
-    magnitudes (restatement only), the scale of any evaluation order's rounding error."""
+    magnitudes (restatement only), the scale of any evaluation order's rounding error.
+    ``phi``/``dilution``: diluted steel (``compute_K_dK_Hcurl_red_dil``, ctools.c:1565-1759),
+    used only with a source field, as ``interface_c.pyx:874-901`` does; ``dilution`` is any
+    object with ``c_num, m_num, c_den, m_den``."""
     if num_el_dofs != 6:
         raise ValueError("only first-order edge elements (6 DoFs) are supported")
     nodes_c, cells_c, gid_c = _f64(nodes), _i32(cells), _i32(glob_ids)
@@ -252,13 +263,19 @@ def curl_curl_triplets(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_
     rhs = np.zeros(num_dofs)
     n_int, rc, rx = reluctance_arrays(reluctance)
     L = lib(backend)
+    dil = None
+    if dilution is not None and len(Bs_c) > 0:
+        dil = np.array([dilution.c_num, dilution.m_num, dilution.c_den, dilution.m_den], dtype=np.float64)
+        phi_c = _f64(phi)
+        assert len(phi_c) == 4 * Q, "phi must hold 4 nodal basis values per quadrature point"
     if backend == "oracle":
         bs_ptr = _d(Bs_c) if len(Bs_c) > 0 else None
         sK = np.empty(nt) if scales is not None else None
         sdK = np.empty(nt) if scales is not None else None
         got = L.or_curlcurl(E, Q, _d(nodes_c), _i(cells_c), _i(gid_c), _i(or_c), _d(curls_c), _d(dphi_c),
                             _d(w_c), _d(x_c), bs_ptr, n_int, _d(rc), _d(rx), _i(ti), _i(tj), _d(vK), _d(vdK), _d(rhs),
-                            _d(sK) if sK is not None else None, _d(sdK) if sdK is not None else None)
+                            _d(sK) if sK is not None else None, _d(sdK) if sdK is not None else None,
+                            _d(phi_c) if dil is not None else None, _d(dil) if dil is not None else None)
         assert got == nt, got
         if scales is not None:
             scales["K"], scales["dK"] = sK, sdK
@@ -270,7 +287,12 @@ def curl_curl_triplets(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_
         rel = _Rel(reluctance.get_type_spec(), n_int, _d(rc), _d(rx))
         msh = _Mesh(len(nodes_c) // 3, E, 4, _d(nodes_c), _i(cells_c))
         quad = _Quad(Q, _d(q_c), _d(w_c))
-        if len(Bs_c) == 0:
+        if dil is not None:
+            dc = _Dil(*[float(v) for v in dil])
+            L.compute_K_dK_Hcurl_red_dil(ctypes.byref(tK), ctypes.byref(tdK), _d(rhs), ctypes.byref(dc), _i(gid_c),
+                                         ctypes.byref(rel), ctypes.byref(msh), ctypes.byref(quad), _d(curls_c),
+                                         _d(phi_c), _d(dphi_c), _i(or_c), _d(x_c), _d(Bs_c))
+        elif len(Bs_c) == 0:
             L.compute_K_dK_Hcurl(ctypes.byref(tK), ctypes.byref(tdK), _i(gid_c), ctypes.byref(rel), ctypes.byref(msh),
                                  ctypes.byref(quad), _d(curls_c), _d(dphi_c), _i(or_c), _d(x_c))
         else:
@@ -286,6 +308,19 @@ def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls,
     """(K, dK, rhs) of one material (``interface_c.pyx:162-374``)."""
     ti, tj, vK, vdK, rhs = curl_curl_triplets(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_s,
                                               reluctance, q, w, num_dofs, num_el_dofs, backend)
+    K = csr_array((vK, (ti, tj)), shape=(num_dofs, num_dofs))
+    dK = csr_array((vdK, (ti, tj)), shape=(num_dofs, num_dofs))
+    return K, dK, rhs
+
+
+def compute_stiffness_and_jacobi_matrix_curl_curl_diluted(nodes, cells, glob_ids, curls, phi, d_phi, orientations,
+                                                          x, B_s, reluctance, dilution, q, w, num_dofs, num_el_dofs,
+                                                          backend="oracle"):
+    """(K, dK, rhs) of one diluted-steel material (``interface_c.pyx:698-926``): the diluted
+    reduced kernel with a source field, the plain kernel without one."""
+    ti, tj, vK, vdK, rhs = curl_curl_triplets(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_s,
+                                              reluctance, q, w, num_dofs, num_el_dofs, backend, phi=phi,
+                                              dilution=dilution)
     K = csr_array((vK, (ti, tj)), shape=(num_dofs, num_dofs))
     dK = csr_array((vdK, (ti, tj)), shape=(num_dofs, num_dofs))
     return K, dK, rhs
@@ -400,14 +435,15 @@ class OracleCurlCurlAssembler:
     (``curl_curl_assembler.py:815-932``) over explicit arrays.
 
     ``materials``: list of dicts with 0-based ``cells`` [E_m, 4], ``glob_ids`` [E_m, 6],
-    ``orientations`` [E_m] and ``reluctance``.
+    ``orientations`` [E_m] and ``reluctance``, optionally ``dilution`` (diluted steel, the
+    loop of ``curl_curl_assembler_diluted.py:204-300``; needs ``phi``).
     """
 
-    def __init__(self, nodes, materials, num_dofs, w, q, d_phi, curls, backend="oracle"):
+    def __init__(self, nodes, materials, num_dofs, w, q, d_phi, curls, backend="oracle", phi=None):
         self.nodes = nodes
         self.materials = materials
         self.num_dofs = num_dofs
-        self.w, self.q, self.d_phi, self.curls = w, q, d_phi, curls
+        self.w, self.q, self.d_phi, self.curls, self.phi = w, q, d_phi, curls, phi
         self.backend = backend
         self.timings = {"kernel": 0.0, "csr": 0.0}
 
@@ -422,7 +458,8 @@ class OracleCurlCurlAssembler:
             t0 = time.perf_counter()
             ti, tj, vK, vdK, this_rhs = curl_curl_triplets(self.nodes, mat["cells"], mat["glob_ids"], self.curls,
                                                            self.d_phi, mat["orientations"], x, B_s,
-                                                           mat["reluctance"], self.q, self.w, n, 6, self.backend)
+                                                           mat["reluctance"], self.q, self.w, n, 6, self.backend,
+                                                           phi=self.phi, dilution=mat.get("dilution"))
             t1 = time.perf_counter()
             this_K = csr_array((vK, (ti, tj)), shape=(n, n))
             this_dK = csr_array((vdK, (ti, tj)), shape=(n, n))
@@ -447,7 +484,7 @@ class OracleCurlCurlAssembler:
             sc = {}
             ti, tj, _, _, _ = curl_curl_triplets(self.nodes, mat["cells"], mat["glob_ids"], self.curls, self.d_phi,
                                                  mat["orientations"], x, B_s, mat["reluctance"], self.q, self.w, n, 6,
-                                                 "oracle", scales=sc)
+                                                 "oracle", scales=sc, phi=self.phi, dilution=mat.get("dilution"))
             sK = sK + csr_array((sc["K"], (ti, tj)), shape=(n, n))
             sJ = sJ + csr_array((sc["K"] + sc["dK"], (ti, tj)), shape=(n, n))
         return sK, sJ

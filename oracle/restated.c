@@ -169,13 +169,19 @@ static double or_dot(const double *a, const double *b) { return a[0] * b[0] + a[
  * sK/sdK (optional) receive, per triplet, the sum of the magnitudes of the terms that make
  * it up (|nu| |cu| |cv| |w| / |det| and |nu'| |cu| |cv| |B| |w| / |det|): the scale of the
  * rounding error any evaluation order makes, used as the comparison scale in the tests.
+ * phi/dil (optional, reduced kernel only): diluted steel (compute_K_dK_Hcurl_red_dil,
+ * ctools.c:1565-1759).  phi[Q][4] holds the nodal basis at the quadrature points, the point's
+ * z is sum_i phi_i Z_i (evaluate_finite_element, ctools.c:480-504), the dilution factor
+ * s = (c_num + z m_num) / (c_den + z m_den) (eval_dilution, ctools.c:124-128) with
+ * dil = {c_num, m_num, c_den, m_den}, and nu = s PCHIP(s |B|), nu' = s^2 PCHIP'(s |B|).
  * Returns the number of triplets written, or -1 on a bad argument. */
 int64_t or_curlcurl(int64_t E, int Q, const double *nodes, const int *cells, const int *glob_ids,
                     const int *orient, const double *curls, const double *dphi, const double *w,
                     const double *x, const double *B_s, int n_int, const double *rel_c,
                     const double *rel_x, int *ti, int *tj, double *vK, double *vdK, double *rhs,
-                    double *sK, double *sdK)
+                    double *sK, double *sdK, const double *phi, const double *dil)
 {
+    if (dil && (!phi || !B_s)) return -1;
     if (Q <= 0 || Q > OR_MAXQ) return -1;
     const double nu0 = 1.0 / 4.0 / M_PI * 1e7;
     double J[OR_MAXQ][9], Jinv[9], det[OR_MAXQ], B[OR_MAXQ][3], Bm[OR_MAXQ], nu[OR_MAXQ], dnu[OR_MAXQ];
@@ -196,7 +202,15 @@ int64_t or_curlcurl(int64_t E, int Q, const double *nodes, const int *cells, con
                 for (int d = 0; d < 3; ++d) B[q][d] += c[d] * x[g[j]] / det[q];
             }
             Bm[q] = sqrt(or_dot(B[q], B[q]));
-            nu[q] = or_pchip(n_int, rel_c, rel_x, Bm[q], &dnu[q]);
+            if (dil) {
+                double z = 0.0;
+                for (int i = 0; i < 4; ++i) z += phi[4 * q + i] * nodes[3 * cell[i] + 2];
+                const double sf = (dil[0] + z * dil[1]) / (dil[2] + z * dil[3]);
+                nu[q] = sf * or_pchip(n_int, rel_c, rel_x, sf * Bm[q], &dnu[q]);
+                dnu[q] *= sf * sf;
+            } else {
+                nu[q] = or_pchip(n_int, rel_c, rel_x, Bm[q], &dnu[q]);
+            }
         }
         for (int j = 0; j < 6; ++j) {
             for (int k = j; k < 6; ++k) {

@@ -8,8 +8,10 @@ Drop-in pieces, with the reference's names and call signatures:
 * ``RedMVPSolver``               ``snoopy/red_mvp_solver.py``
 * ``MVPSolver``                  ``snoopy/mvp_solver.py``
 * ``LaplaceSubdomainSolver``     ``snoopy/laplace_subdomain_solver.py``
-* ``Reluctance``, ``ConstantReluctance``, ``Permeability``, ``ConstantPermeability``
-                                 ``snoopy/materials.py``
+* ``CurlCurlAssemblerDiluted``  ``snoopy/curl_curl_assembler_diluted.py``
+* ``RedMVPSolverDiluted``        ``snoopy/red_mvp_solver_diluted.py``
+* ``Reluctance``, ``ConstantReluctance``, ``Permeability``, ``ConstantPermeability``,
+  ``Dilution``                   ``snoopy/materials.py``
 * ``RacetrackCoil``              ``snoopy/racetrack_coil.py``
 
 gmsh is replaced by ``mesh.TetMesh`` and its generators, and by ``finite_element``'s tables.
@@ -17,7 +19,7 @@ All arithmetic runs in ``libsnoopy_b200.so`` (CUDA, sm_100a); there is no CPU fa
 """
 
 from . import finite_element, materials, mesh
-from .materials import ConstantPermeability, ConstantReluctance, Permeability, Reluctance
+from .materials import ConstantPermeability, ConstantReluctance, Dilution, Permeability, Reluctance
 from .mesh import TetMesh, kuhn_microbench_mesh, window_frame_mesh
 from .racetrack_coil import RacetrackCoil
 
@@ -38,6 +40,14 @@ def __getattr__(name):
         from .red_mvp_solver import RedMVPSolver
 
         return RedMVPSolver
+    if name == "CurlCurlAssemblerDiluted":
+        from .curl_curl_assembler_diluted import CurlCurlAssemblerDiluted
+
+        return CurlCurlAssemblerDiluted
+    if name == "RedMVPSolverDiluted":
+        from .red_mvp_solver_diluted import RedMVPSolverDiluted
+
+        return RedMVPSolverDiluted
     if name == "MVPSolver":
         from .mvp_solver import MVPSolver
 

@@ -56,6 +56,8 @@ _SIGS = {
     "snp_pattern_destroy": [_vp],
     "snp_curlcurl_assemble": [_vp, _c_i64, _c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp,
                               _c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "snp_curlcurl_assemble_diluted": [_vp, _c_i64, _c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _vp, _c_i32,
+                                      _vp, _vp, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snp_curlcurl_assemble_f32": [_vp, _c_i64, _c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp,
                                   _c_i32, _vp, _vp, _vp, _vp],
     "snp_curlcurl_rhs_red": [_c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp,
@@ -85,6 +87,7 @@ _SIGS = {
     "snp_solver_set_nodes": [_vp, _vp, _vp],
     "snp_solver_solve_many": [_vp, _c_i32, _vp, _vp, _vp, _c_i32, _vp],
     "snp_solver_set_source": [_vp, _c_i32, _vp, _vp],
+    "snp_solver_set_dilution": [_vp, _c_i32, _vp, _vp],
     "snp_gemm_bf16": [_c_i32, _c_i32, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp,
                       _vp],
     "snp_gelu_backward": [_c_i64, _vp, _vp, _vp, _vp, _vp],

@@ -12,6 +12,10 @@
 //   dK_jk     = sum_q [|B_q| >= 1e-14] nu'_q w_q (c_j . B_q)(c_k . B_q) / (det |B_q|)
 //   rhs_j     = sum_q (nu0 - nu_q) (c_j . B_s,q) w_q     (reduced kernel, ctools.c:1332-1335)
 //
+// Diluted steel (compute_K_dK_Hcurl_red_dil, fem_c/ctools.c:1565-1759), reduced kernel only:
+//   z_q = sum_i phi_i(q) Z_i,  s_q = (c_num + z_q m_num) / (c_den + z_q m_den)
+//   nu_q = s_q PCHIP(s_q |B_q|),  nu'_q = s_q^2 PCHIP'(s_q |B_q|)
+//
 // For first-order tetrahedra d_phi and the curls do not depend on the quadrature point,
 // so Jm, det and c_j are computed once per element and the sums over q factor:
 // K_jk = (c_j . c_k) * sum_q nu_q w_q / det.  Without a source field B is constant over
@@ -30,7 +34,7 @@ namespace {
 constexpr int kBlock = 128;
 
 struct SmemLayout {
-    int off_ctab, off_dphi, off_w, off_relc, off_relx, total;
+    int off_ctab, off_dphi, off_w, off_phi, off_relc, off_relx, total;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int n_orient, int nq, int n_int) {
@@ -42,6 +46,8 @@ __host__ __device__ inline SmemLayout smem_layout(int n_orient, int nq, int n_in
     o += 12;
     L.off_w = o;
     o += nq;
+    L.off_phi = o;
+    o += 4 * nq;
     int nc = n_int < 0 ? 1 : 4 * n_int;
     int nx = n_int < 0 ? 1 : n_int + 1;
     L.off_relc = o;
@@ -57,9 +63,28 @@ __device__ __forceinline__ void red_add(T *p, T v) {
     atomicAdd(p, v);
 }
 
+// nu and nu' at one quadrature point; DIL: diluted steel with the point's nodal basis ph[4]
+// and the element's node z coordinates Zn[4]
+template <bool DIL>
+__device__ __forceinline__ double nu_at(const CurlArgs &a, const double *relc, const double *relx, const double *ph,
+                                        const double (&Zn)[4], double bm, double &dnu) {
+    if constexpr (!DIL) {
+        return pchip_eval<double>(a.n_int, relc, relx, bm, dnu);
+    } else {
+        double z = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) z += ph[i] * Zn[i];
+        const double sf = (a.dil[0] + z * a.dil[1]) / (a.dil[2] + z * a.dil[3]);
+        const double nu = sf * pchip_eval<double>(a.n_int, relc, relx, sf * bm, dnu);
+        dnu *= sf * sf;
+        return nu;
+    }
+}
+
 // HAS_BS: reduced formulation with a source field at each quadrature point.
 // NQ: compile-time number of quadrature points (0 = runtime count).
-template <bool HAS_BS, int NQ, typename VT>
+// DIL: diluted steel (with HAS_BS only).
+template <bool HAS_BS, int NQ, typename VT, bool DIL>
 __global__ void __launch_bounds__(kBlock)
     k_curlcurl(CurlArgs a, int quad_stride_ctab) {
     extern __shared__ double sm[];
@@ -67,6 +92,7 @@ __global__ void __launch_bounds__(kBlock)
     double *s_ctab = sm + L.off_ctab;
     double *s_dphi = sm + L.off_dphi;
     double *s_w = sm + L.off_w;
+    double *s_phi = sm + L.off_phi;
     double *s_relc = sm + L.off_relc;
     double *s_relx = sm + L.off_relx;
     // stage tables: curls at q = 0 for every orientation, d_phi at q = 0, weights, PCHIP
@@ -76,6 +102,8 @@ __global__ void __launch_bounds__(kBlock)
     }
     for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = a.dphi0[t];
     for (int t = threadIdx.x; t < a.nq; t += blockDim.x) s_w[t] = a.w[t];
+    if (a.phi)
+        for (int t = threadIdx.x; t < 4 * a.nq; t += blockDim.x) s_phi[t] = a.phi[t];
     const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
     const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
     for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
@@ -90,7 +118,7 @@ __global__ void __launch_bounds__(kBlock)
         const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
         const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
         // Jacobian J[k][l] = sum_i X[i][k] dphi[i][l]
-        double Jm[9];
+        double Jm[9], Zn[4];
 #pragma unroll
         for (int r = 0; r < 9; ++r) Jm[r] = 0.0;
 #pragma unroll
@@ -98,6 +126,7 @@ __global__ void __launch_bounds__(kBlock)
             const double X0 = __ldg(a.nodes + 3 * (int64_t)cidx[i]);
             const double X1 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 1);
             const double X2 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 2);
+            Zn[i] = X2;
 #pragma unroll
             for (int l = 0; l < 3; ++l) {
                 const double d = s_dphi[3 * i + l];
@@ -191,7 +220,7 @@ __global__ void __launch_bounds__(kBlock)
                 const double B0 = s0 + Bc[0], B1 = s1 + Bc[1], B2 = s2 + Bc[2];
                 const double bm = sqrt(B0 * B0 + B1 * B1 + B2 * B2);
                 double dnu;
-                const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, bm, dnu);
+                const double nu = nu_at<DIL>(a, s_relc, s_relx, s_phi + 4 * q, Zn, bm, dnu);
                 const double wq = s_w[q];
                 kfac += nu * wq;
                 const double aq = (bm >= 1e-14) ? dnu * wq * idet / bm : 0.0;
@@ -255,6 +284,7 @@ __global__ void __launch_bounds__(kBlock)
     double *s_ctab = sm + L.off_ctab;
     double *s_dphi = sm + L.off_dphi;
     double *s_w = sm + L.off_w;
+    double *s_phi = sm + L.off_phi;
     double *s_relc = sm + L.off_relc;
     double *s_relx = sm + L.off_relx;
     for (int t = threadIdx.x; t < a.n_orient * 18; t += blockDim.x) {
@@ -263,6 +293,8 @@ __global__ void __launch_bounds__(kBlock)
     }
     for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = a.dphi0[t];
     for (int t = threadIdx.x; t < a.nq; t += blockDim.x) s_w[t] = a.w[t];
+    if (a.phi)
+        for (int t = threadIdx.x; t < 4 * a.nq; t += blockDim.x) s_phi[t] = a.phi[t];
     const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
     const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
     for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
@@ -327,7 +359,7 @@ __global__ void k_check_affine(const double *curls, int n_orient, const double *
 //   (K x)_j = chat_j . (kfac Jm^T Jm bh),   rhs_j = chat_j . (Jm^T sum_q rq B_s,q).
 // One pass over the quadrature points; S_e and the six element terms of F and of diag(J)
 // are written once per element (no atomics; the DoF sums follow in a fixed order).
-template <bool HAS_BS, int NQ, typename TT>
+template <bool HAS_BS, int NQ, typename TT, bool DIL>
 __global__ void __launch_bounds__(kBlock)
     k_curlcurl_tensor(CurlArgs a, int quad_stride_ctab, TT *__restrict__ T) {
     extern __shared__ double sm[];
@@ -335,6 +367,7 @@ __global__ void __launch_bounds__(kBlock)
     double *s_ctab = sm + L.off_ctab;
     double *s_dphi = sm + L.off_dphi;
     double *s_w = sm + L.off_w;
+    double *s_phi = sm + L.off_phi;
     double *s_relc = sm + L.off_relc;
     double *s_relx = sm + L.off_relx;
     for (int t = threadIdx.x; t < a.n_orient * 18; t += blockDim.x) {
@@ -343,6 +376,8 @@ __global__ void __launch_bounds__(kBlock)
     }
     for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = a.dphi0[t];
     for (int t = threadIdx.x; t < a.nq; t += blockDim.x) s_w[t] = a.w[t];
+    if (a.phi)
+        for (int t = threadIdx.x; t < 4 * a.nq; t += blockDim.x) s_phi[t] = a.phi[t];
     const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
     const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
     for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
@@ -356,7 +391,7 @@ __global__ void __launch_bounds__(kBlock)
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x) {
         const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
         const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
-        double Jm[9];
+        double Jm[9], Zn[4];
 #pragma unroll
         for (int r = 0; r < 9; ++r) Jm[r] = 0.0;
 #pragma unroll
@@ -364,6 +399,7 @@ __global__ void __launch_bounds__(kBlock)
             const double X0 = __ldg(a.nodes + 3 * (int64_t)cidx[i]);
             const double X1 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 1);
             const double X2 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 2);
+            Zn[i] = X2;
 #pragma unroll
             for (int l = 0; l < 3; ++l) {
                 const double d = s_dphi[3 * i + l];
@@ -420,7 +456,7 @@ __global__ void __launch_bounds__(kBlock)
                 const double B0 = s0 + Bc[0], B1 = s1 + Bc[1], B2 = s2 + Bc[2];
                 const double bm = sqrt(B0 * B0 + B1 * B1 + B2 * B2);
                 double dnu;
-                const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, bm, dnu);
+                const double nu = nu_at<DIL>(a, s_relc, s_relx, s_phi + 4 * q, Zn, bm, dnu);
                 const double wq = s_w[q];
                 kfac += nu * wq;
                 const double aq = (bm >= 1e-14) ? dnu * wq * idet / bm : 0.0;
@@ -473,10 +509,10 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
-template <bool HAS_BS, int NQ, typename TT>
+template <bool HAS_BS, int NQ, typename TT, bool DIL = false>
 int launch_tensor_t(const CurlArgs &a, TT *T, cudaStream_t st, size_t smem, int qstride) {
     if (a.n_elems == 0) return SNP_OK;
-    auto kern = k_curlcurl_tensor<HAS_BS, NQ, TT>;
+    auto kern = k_curlcurl_tensor<HAS_BS, NQ, TT, DIL>;
     if (smem > 48 * 1024) SNP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<wave_grid(kern, a.n_elems, kBlock, smem), kBlock, smem, st>>>(a, qstride, T);
     SNP_LAUNCH_CHECK();
@@ -490,21 +526,23 @@ int launch_tensor(const CurlArgs &a, TT *T, cudaStream_t st, size_t smem, int qs
         if (a.nq == 4) return launch_tensor_t<false, 4, TT>(a, T, st, smem, qstride);
         return launch_tensor_t<false, 0, TT>(a, T, st, smem, qstride);
     }
+    if (a.phi) {
+        if (a.nq == 4) return launch_tensor_t<true, 4, TT, true>(a, T, st, smem, qstride);
+        return launch_tensor_t<true, 0, TT, true>(a, T, st, smem, qstride);
+    }
     if (a.nq == 1) return launch_tensor_t<true, 1, TT>(a, T, st, smem, qstride);
     if (a.nq == 4) return launch_tensor_t<true, 4, TT>(a, T, st, smem, qstride);
     if (a.nq == 5) return launch_tensor_t<true, 5, TT>(a, T, st, smem, qstride);
     return launch_tensor_t<true, 0, TT>(a, T, st, smem, qstride);
 }
 
-template <bool HAS_BS, int NQ>
+template <bool HAS_BS, int NQ, bool DIL = false>
 int launch_t(const CurlArgs &a, cudaStream_t st, size_t smem, int qstride) {
     if (a.n_elems == 0) return SNP_OK;
-    if (smem > 48 * 1024) {
-        SNP_CUDA_TRY(cudaFuncSetAttribute(k_curlcurl<HAS_BS, NQ, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
-    }
+    auto kern = k_curlcurl<HAS_BS, NQ, double, DIL>;
+    if (smem > 48 * 1024) SNP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = stride_grid(a.n_elems, kBlock, 16);
-    k_curlcurl<HAS_BS, NQ, double><<<grid, kBlock, smem, st>>>(a, qstride);
+    kern<<<grid, kBlock, smem, st>>>(a, qstride);
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }
@@ -534,6 +572,10 @@ int launch_curlcurl(const CurlArgs &a, cudaStream_t st) {
         if (a.nq == 1) return launch_t<false, 1>(a, st, smem, qstride);
         if (a.nq == 4) return launch_t<false, 4>(a, st, smem, qstride);
         return launch_t<false, 0>(a, st, smem, qstride);
+    }
+    if (a.phi) {
+        if (a.nq == 4) return launch_t<true, 4, true>(a, st, smem, qstride);
+        return launch_t<true, 0, true>(a, st, smem, qstride);
     }
     if (a.nq == 1) return launch_t<true, 1>(a, st, smem, qstride);
     if (a.nq == 4) return launch_t<true, 4>(a, st, smem, qstride);
@@ -607,6 +649,31 @@ int snp_curlcurl_assemble(const snp_pattern *pat, int64_t elem_offset, int64_t n
     snp::CurlArgs a;
     SNP_TRY(snp::fill_args(a, pat, elem_offset, n_elems, nodes, cells, glob_ids, orientations, curls, n_orient, d_phi,
                            w, n_quad, x, B_s, n_int, rel_c, rel_x));
+    a.K = K_vals;
+    a.dK = dK_vals;
+    a.J = J_vals;
+    a.rhs = rhs;
+    a.F = F;
+    return snp::launch_curlcurl(a, snp::as_stream(stream));
+}
+
+int snp_curlcurl_assemble_diluted(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,
+                                  const int32_t *cells, const int32_t *glob_ids, const int32_t *orientations,
+                                  const double *curls, int32_t n_orient, const double *phi, const double *d_phi,
+                                  const double *w, int32_t n_quad, const double *x, const double *B_s, int32_t n_int,
+                                  const double *rel_c, const double *rel_x, const double *dilution, double *K_vals,
+                                  double *dK_vals, double *J_vals, double *rhs, double *F, void *stream) {
+    snp::clear_error();
+    const bool want_mat = K_vals || dK_vals || J_vals;
+    SNP_REQUIRE(!want_mat || pat != nullptr, "snp_curlcurl_assemble_diluted: matrix outputs need a pattern");
+    snp::CurlArgs a;
+    SNP_TRY(snp::fill_args(a, pat, elem_offset, n_elems, nodes, cells, glob_ids, orientations, curls, n_orient, d_phi,
+                           w, n_quad, x, B_s, n_int, rel_c, rel_x));
+    if (B_s != nullptr) {
+        SNP_REQUIRE(phi != nullptr && dilution != nullptr, "snp_curlcurl_assemble_diluted: phi and dilution are required");
+        a.phi = phi;
+        for (int i = 0; i < 4; ++i) a.dil[i] = dilution[i];
+    }
     a.K = K_vals;
     a.dK = dK_vals;
     a.J = J_vals;

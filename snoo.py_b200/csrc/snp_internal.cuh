@@ -114,6 +114,10 @@ struct CurlArgs {
     int64_t t_offset;
     double *Fe;
     double *De;
+    // diluted steel (reduced formulation only): phi[Q][4] nodal basis at the quadrature
+    // points or null; dil = {c_num, m_num, c_den, m_den}, s(z) = (c_num + z m_num) / (c_den + z m_den)
+    const double *phi;
+    double dil[4];
 };
 
 // Launch the fused assembly for one material.  Tables must be affine (checked by the caller).

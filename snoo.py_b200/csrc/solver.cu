@@ -14,6 +14,7 @@
 // Jacobian values and the CG run in float32 while F, the update and the norms stay float64
 // (the Newton loop is the iterative refinement of the float32 solves).
 #include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -37,6 +38,10 @@ struct Material {
     DevBuf<int32_t> cells, gids, orient;
     DevBuf<double> relc, relx, Bs;
     bool has_bs = false;
+    // diluted steel: nodal basis at the quadrature points [Q][4] and {c_num, m_num, c_den, m_den}
+    DevBuf<double> phi;
+    bool diluted = false;
+    double dil[4] = {0.0, 0.0, 1.0, 0.0};
 };
 
 // res[0] += sum over free i of v[i]^2 (deterministic last-block reduction)
@@ -277,6 +282,10 @@ struct snp_solver {
             a.n_int = m->n_int;
             a.rel_c = m->relc.p;
             a.rel_x = m->relx.p;
+            if (m->diluted && m->has_bs) {
+                a.phi = m->phi.p;
+                for (int i = 0; i < 4; ++i) a.dil[i] = m->dil[i];
+            }
             a.T64 = f32 ? nullptr : T64.p;
             a.T32 = f32 ? T32.p : nullptr;
             a.t_offset = m->offset;
@@ -328,6 +337,10 @@ struct snp_solver {
             a.n_int = m->n_int;
             a.rel_c = m->relc.p;
             a.rel_x = m->relx.p;
+            if (m->diluted && m->has_bs) {
+                a.phi = m->phi.p;
+                for (int i = 0; i < 4; ++i) a.dil[i] = m->dil[i];
+            }
             a.slots = (so ? sell.slots.p : pat->slots.p) + 36 * m->offset;
             a.K = Kv;
             a.J = Jv;
@@ -814,6 +827,26 @@ int snp_solver_set_nodes(snp_solver *s, const double *nodes, void *stream) {
     SNP_CUDA_TRY(cudaMemcpyAsync(s->nodes.p, nodes, sizeof(double) * 3 * s->n_nodes, cudaMemcpyDeviceToDevice,
                                  stream ? snp::as_stream(stream) : s->stream));
     s->j_valid[0] = s->j_valid[1] = 0;
+    return SNP_OK;
+}
+
+int snp_solver_set_dilution(snp_solver *s, int32_t material, const double *phi, const double *dilution) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr, "snp_solver_set_dilution: solver is NULL");
+    SNP_REQUIRE(material >= 0 && material < (int32_t)s->mats.size(), "snp_solver_set_dilution: no material %d", material);
+    auto &m = *s->mats[material];
+    if (dilution == nullptr) {
+        m.diluted = false;
+        return SNP_OK;
+    }
+    SNP_REQUIRE(phi != nullptr, "snp_solver_set_dilution: phi is NULL");
+    SNP_REQUIRE(std::isfinite(dilution[0]) && std::isfinite(dilution[1]) && std::isfinite(dilution[2]) &&
+                    std::isfinite(dilution[3]),
+                "snp_solver_set_dilution: coefficients must be finite");
+    if (!m.phi.p) SNP_TRY(m.phi.alloc((size_t)4 * s->nq));
+    SNP_CUDA_TRY(cudaMemcpyAsync(m.phi.p, phi, sizeof(double) * 4 * s->nq, cudaMemcpyDeviceToDevice, s->stream));
+    for (int i = 0; i < 4; ++i) m.dil[i] = dilution[i];
+    m.diluted = true;
     return SNP_OK;
 }
 

@@ -23,6 +23,8 @@ def upload(a, dtype):
     """numpy-like -> contiguous 1-D device tensor of ``dtype`` (np.float64 / np.int32 / np.uint8 / np.float32)."""
     t = torch()
     arr = np.ascontiguousarray(np.asarray(a, dtype=dtype).reshape(-1))
+    if not arr.flags.writeable:
+        arr = arr.copy()
     return t.from_numpy(arr).to(device(), non_blocking=False)
 
 

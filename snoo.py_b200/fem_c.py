@@ -104,6 +104,47 @@ def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls,
     return pat.to_scipy(K), pat.to_scipy(dK), rhs[: int(num_dofs)].cpu().numpy()
 
 
+def compute_stiffness_and_jacobi_matrix_curl_curl_diluted(nodes, cells, glob_ids, curls, phi, d_phi, orientations, x,
+                                                          B_s, reluctance, dilution, q, w, num_dofs, num_el_dofs):
+    """Curl-curl Newton system of diluted steel (``interface_c.pyx:698-926``).
+
+    With ``B_s`` the reluctance at each quadrature point is s nu(s |B|) with the dilution
+    factor s(z) of ``dilution`` (``materials.Dilution``); ``B_s`` empty selects the plain
+    kernel, as the reference does for air.
+    :return: ``(K, dK, rhs)``: scipy CSR (num_dofs x num_dofs) and float64[num_dofs].
+    """
+    _lib.require_cuda()
+    if num_el_dofs != 6:
+        raise ValueError("only first-order edge elements (6 DoFs per element) are supported")
+    if np.asarray(d_phi).shape[1] != 4:
+        raise ValueError("only 4-node tetrahedra are supported")
+    nq = _n_quad(w)
+    if np.asarray(phi).size != 4 * nq:
+        raise ValueError("phi must hold the 4 nodal basis functions at every quadrature point")
+    check_affine(curls, d_phi, nq)
+    n_orient = int(np.asarray(curls).size // (nq * 18))
+    _check_mesh(nodes, cells, glob_ids, num_dofs, orientations, n_orient)
+    cells_d = upload(cells, np.int32)
+    num_el = cells_d.numel() // 4
+    gids_d = upload(glob_ids, np.int32)
+    pat = Pattern(gids_d, num_el, 6, int(num_dofs))
+    n_int, rc, rx = reluctance_tables(reluctance)
+    B_s = np.asarray(B_s)
+    bs_d = upload(B_s, np.float64) if B_s.size > 0 else None
+    dil = (ctypes.c_double * 4)(dilution.c_num, dilution.m_num, dilution.c_den, dilution.m_den)
+    K = zeros(pat.nnz)
+    dK = zeros(pat.nnz)
+    rhs = zeros(int(num_dofs))
+    nodes_d, or_d, curls_d = upload(nodes, np.float64), upload(orientations, np.int32), upload(curls, np.float64)
+    phi_d, dphi_d, w_d, x_d = (upload(phi, np.float64), upload(d_phi, np.float64), upload(w, np.float64),
+                               upload(x, np.float64))
+    _lib.call("snp_curlcurl_assemble_diluted", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d),
+              _lib.ptr(gids_d), _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(phi_d), _lib.ptr(dphi_d),
+              _lib.ptr(w_d), nq, _lib.ptr(x_d), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), dil, _lib.ptr(K),
+              _lib.ptr(dK), None, _lib.ptr(rhs), None, _lib.stream_ptr())
+    return pat.to_scipy(K), pat.to_scipy(dK), rhs[: int(num_dofs)].cpu().numpy()
+
+
 def compute_rhs_Hcurl_red_c(nodes, cells, glob_ids, curls, d_phi, orientations, B_s, reluctance, x, q, w, num_dofs,
                             num_el_dofs):
     """rhs of the reduced vector potential formulation (``interface_c.pyx:377-552``)."""

@@ -12,6 +12,7 @@ Cython layer uses (``fem_c/interface_c.pyx:57-68, 226-234``): ``get_type_spec()`
   with H_min where the spline's slope vanishes in the first interval
   (``materials.py:30-62, 184-197``).
 * ``ConstantPermeability``: type 0 (``materials.py:210-269``).
+* ``Dilution``: the linear-in-z iron fraction of diluted steel (``materials.py:538-599``).
 
 ``atan_bh_table`` makes the B-H table of the saturating law
 B(H) = mu0 H + Js (2/pi) atan(pi mu0 (mu_r - 1) H / (2 Js)); ``Reluctance.from_bh`` fits
@@ -154,6 +155,49 @@ class ConstantPermeability:
 
     def get_type_spec(self):
         return 0
+
+
+class Dilution:
+    """Diluted steel: the iron fills only part of a magnet's cross section, and the part
+    changes linearly along z (``snoopy/materials.py:538-599``).
+
+    Each of the four x boundaries (middle gap, core, void, yoke) runs on a straight line
+    from x_1 at z = z_pos to x_2 at z = z_pos + z_len, x(z) = c + m z.  The dilution factor
+    is a ratio of two widths, s(z) = (c_num + z m_num) / (c_den + z m_den): for magnet type 1
+    (yoke - void) / (core - gap), for type 3 the inverse.  The curl-curl kernels evaluate s at
+    every quadrature point and use nu = s PCHIP(s |B|), nu' = s^2 PCHIP'(s |B|)
+    (``fem_c/ctools.c:1665-1680``).
+    """
+
+    def __init__(self, x_mgap_1, x_core_1, x_void_1, x_yoke_1, x_mgap_2, x_core_2, x_void_2, x_yoke_2, z_pos, z_len,
+                 mag_type=1):
+        def line(x1, x2):
+            return (x1 * (z_len + z_pos) - x2 * z_pos) / z_len, (x2 - x1) / z_len
+
+        c_gap, m_gap = line(x_mgap_1, x_mgap_2)
+        c_core, m_core = line(x_core_1, x_core_2)
+        c_void, m_void = line(x_void_1, x_void_2)
+        c_yoke, m_yoke = line(x_yoke_1, x_yoke_2)
+        outer = (c_yoke - c_void, m_yoke - m_void)
+        inner = (c_core - c_gap, m_core - m_gap)
+        if mag_type == 1:
+            num, den = outer, inner
+        elif mag_type == 3:
+            num, den = inner, outer
+        else:
+            raise ValueError(f"magnet type {mag_type} unknown (1 or 3)")
+        self.c_num, self.m_num = num
+        self.c_den, self.m_den = den
+        self.mag_type = mag_type
+
+    def coefficients(self):
+        """(c_num, m_num, c_den, m_den), the order the C interface takes them in."""
+        return (float(self.c_num), float(self.m_num), float(self.c_den), float(self.m_den))
+
+    def evaluate(self, z):
+        """s(z), as ``eval_dilution`` (``fem_c/ctools.c:124-128``)."""
+        z = np.asarray(z, dtype=np.float64)
+        return (self.c_num + z * self.m_num) / (self.c_den + z * self.m_den)
 
 
 def atan_bh(H, mu_r=3000.0, Js=1.9):

@@ -41,6 +41,11 @@ class DeviceNewton:
             n_int, rc, rx = d["rel"][n]
             _lib.call("snp_solver_add_material", self.handle, _lib.ptr(m["cells"]), _lib.ptr(m["gids"]),
                       _lib.ptr(m["orient"]), m["count"], n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(bs[n]))
+        # diluted steel (CurlCurlAssemblerDiluted): the factor s(z) enters every assembly
+        for n, dil in enumerate(getattr(assembler, "dilutions", [])[: len(d["mats"])]):
+            if dil is not None:
+                coef = (ctypes.c_double * 4)(dil.c_num, dil.m_num, dil.c_den, dil.m_den)
+                _lib.call("snp_solver_set_dilution", self.handle, n, _lib.ptr(tb.phi_d), coef)
         if rhs_extra is not None:
             r = rhs_extra if hasattr(rhs_extra, "data_ptr") else upload(rhs_extra, np.float64)
             _lib.call("snp_solver_set_rhs", self.handle, _lib.ptr(r))

@@ -5,7 +5,8 @@ into ``oracle/_ref/``) with the Cython layer's marshalling (``oracle/oracle.py``
 "ref") on small seeded inputs, and stores inputs and outputs in ``golden_small.npz``:
 
 * curl-curl K, dK (CSR with explicit zeros, as ``csr_array((v,(i,j)))`` returns them) and rhs,
-  plain kernel (air) and reduced kernel (iron with a source field), 4-point rule;
+  plain kernel (air) and reduced kernel (iron with a source field), 4-point rule; the
+  diluted-steel reduced kernel (``compute_K_dK_Hcurl_red_dil``) on the iron;
 * grad-grad K, dK with a B-spline permeability and with a constant one;
 * B at quadrature points; Biot-Savart of a racetrack coil's segments;
 * PCHIP nu, nu' and B-spline mu, mu' at sample points.
@@ -46,6 +47,36 @@ def golden_inputs(seed=3):
     return msh, w, q, dphi, phi, curls, x, iron, air, Bs, xn
 
 
+DILUTION_CASES = [(0.0, 0.30, 0.35, 0.75, 0.02, 0.40, 0.45, 0.80, -0.25, 0.5, 1),
+                  (0.0, 0.30, 0.35, 0.75, 0.02, 0.40, 0.45, 0.80, -0.25, 0.5, 3),
+                  (0.05, 0.62, 0.70, 1.45, 0.11, 0.93, 1.02, 2.10, 3.0, 4.5, 1),
+                  (0.05, 0.62, 0.70, 1.45, 0.11, 0.93, 1.02, 2.10, 3.0, 4.5, 3)]
+
+
+def reference_dilution_coefficients():
+    """(c_num, m_num, c_den, m_den) of the reference's own ``snoopy/materials.py`` Dilution for
+    every case of DILUTION_CASES (its plotting import is stubbed: nothing plots here)."""
+    import importlib.util
+    import types
+
+    for name in ("matplotlib", "matplotlib.pyplot"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    spec = importlib.util.spec_from_file_location("_ref_materials", "/root/reference/snoopy/materials.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    out = []
+    for c in DILUTION_CASES:
+        d = mod.Dilution(*c)
+        out.append([d.c_num, d.m_num, d.c_den, d.m_den])
+    return np.array(out)
+
+
+def golden_dilution():
+    """Magnet type 1 with an iron fraction changing over z in [-0.25, 0.25]: s = 4/3 at the
+    entrance, 35/38 at the exit."""
+    return MAT.Dilution(0.0, 0.30, 0.35, 0.75, 0.02, 0.40, 0.45, 0.80, z_pos=-0.25, z_len=0.5, mag_type=1)
+
+
 def main():
     O.lib("ref")
     msh, w, q, dphi, phi, curls, x, iron, air, Bs, xn = golden_inputs()
@@ -69,6 +100,19 @@ def main():
             out[f"cc_{name}_{tag}_indices"] = A.indices
             out[f"cc_{name}_{tag}_data"] = A.data
         out[f"cc_{name}_rhs"] = rhs
+    # diluted steel (type 1): iron fraction running linearly over the iron's z extent
+    dil = golden_dilution()
+    out["dil_coef"] = np.array(dil.coefficients())
+    out["dil_cases"] = np.array(DILUTION_CASES, dtype=np.float64)
+    out["dil_cases_ref"] = reference_dilution_coefficients()
+    K, dK, rhs = O.compute_stiffness_and_jacobi_matrix_curl_curl_diluted(
+        msh.nodes, msh.cells[iron], msh.elem_edges[iron], curls, phi, dphi, msh.orientations[iron], x, Bs, rel, dil, q,
+        w, n, 6, backend="ref")
+    for tag, A in (("K", K), ("dK", dK)):
+        out[f"cc_iron_dil_{tag}_indptr"] = A.indptr
+        out[f"cc_iron_dil_{tag}_indices"] = A.indices
+        out[f"cc_iron_dil_{tag}_data"] = A.data
+    out["cc_iron_dil_rhs"] = rhs
     out["rhs_red"] = O.compute_rhs_Hcurl_red_c(msh.nodes, msh.cells[iron], msh.elem_edges[iron], curls, dphi,
                                                msh.orientations[iron], Bs, rel, x, q, w, n, 6, backend="ref")
     for name, pm in (("bspline", perm), ("const", S.ConstantPermeability(1.0))):

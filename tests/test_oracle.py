@@ -83,6 +83,41 @@ def test_curlcurl_matches_reference(golden, oracle_mod, rel, name):
         assert not ref_rhs.any() and not rhs.any()
 
 
+def test_dilution_coefficients_match_reference(golden):
+    for case, ref in zip(golden["dil_cases"], golden["dil_cases_ref"]):
+        d = MAT.Dilution(*case[:10], mag_type=int(case[10]))
+        np.testing.assert_allclose(d.coefficients(), ref, rtol=1e-15, atol=0)
+    with pytest.raises(ValueError):
+        MAT.Dilution(*golden["dil_cases"][0][:10], mag_type=2)
+
+
+def test_curlcurl_diluted_matches_reference(golden, oracle_mod, rel):
+    g = golden
+    n = int(g["num_dofs"])
+    el = g["iron"]
+    dil = MAT.Dilution(0, 0, 0, 0, 0, 0, 0, 0, 0.0, 1.0)
+    dil.c_num, dil.m_num, dil.c_den, dil.m_den = g["dil_coef"]
+    K, dK, rhs = oracle_mod.compute_stiffness_and_jacobi_matrix_curl_curl_diluted(
+        g["nodes"], g["cells"][el], g["glob_ids"][el], g["curls"], g["phi"], g["d_phi"], g["orientations"][el], g["x"],
+        g["B_s"], rel, dil, g["q"], g["w"], n, 6)
+    assert_same_pattern(K, csr_from(g, "cc_iron_dil_K", n))
+    # same operation order as the reference: bitwise apart from summation of duplicates
+    assert_csr_close(K, csr_from(g, "cc_iron_dil_K", n), 1e-14, atol_rel=1e-16)
+    assert_csr_close(dK, csr_from(g, "cc_iron_dil_dK", n), 1e-14, atol_rel=1e-16)
+    assert rel_max(rhs, g["cc_iron_dil_rhs"]) < 1e-14
+    # the dilution changes the answer (s runs from 4/3 to 35/38 over the iron)
+    K0, _, _ = oracle_mod.compute_stiffness_and_jacobi_matrix_curl_curl(
+        g["nodes"], g["cells"][el], g["glob_ids"][el], g["curls"], g["d_phi"], g["orientations"][el], g["x"],
+        g["B_s"], rel, g["q"], g["w"], n, 6)
+    assert rel_max(K.data, K0.data) > 1e-3
+    # without a source field the plain kernel runs, as in the reference's air branch
+    Ka, _, ra = oracle_mod.compute_stiffness_and_jacobi_matrix_curl_curl_diluted(
+        g["nodes"], g["cells"][el], g["glob_ids"][el], g["curls"], g["phi"], g["d_phi"], g["orientations"][el], g["x"],
+        np.zeros((0, 3)), rel, dil, g["q"], g["w"], n, 6)
+    assert_csr_close(Ka, csr_from(g, "cc_iron_plain_K", n), 1e-13, atol_rel=1e-15)
+    assert not ra.any()
+
+
 def test_rhs_red_matches_reference(golden, oracle_mod, rel):
     g = golden
     el = g["iron"]
@@ -145,6 +180,30 @@ def test_restatement_vs_live_reference(oracle_mod, rel):
     assert_csr_close(a[0], b[0], 1e-12, atol_rel=1e-15)
     assert_csr_close(a[1], b[1], 1e-12, atol_rel=1e-15)
     assert rel_max(a[2], b[2]) < 1e-13
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference C not compiled here")
+def test_diluted_restatement_vs_live_reference(oracle_mod, rel):
+    """Diluted reduced kernel on fresh inputs, magnet type 3, 5-point rule."""
+    msh = M.window_frame_mesh(3000, jitter=0.2, seed=98)
+    w, q = FE.quadrature_rule(3)
+    dphi = FE.evaluate_basis_derivative(q)
+    phi = FE.evaluate_basis(q)
+    curls, _ = FE.curl_edge_basis_functions(q)
+    rng = np.random.default_rng(6)
+    x = rng.normal(0, 5e-3, msh.num_dofs)
+    el = msh.domain_elements(M.TAG_IRON)
+    Bs = rng.normal(0, 1.0, (len(el) * len(w), 3))
+    dil = MAT.Dilution(0.01, 0.28, 0.33, 0.70, 0.03, 0.42, 0.47, 0.85, -0.3, 0.6, mag_type=3)
+    n = msh.num_dofs
+    args = (msh.nodes, msh.cells[el], msh.elem_edges[el], curls, phi, dphi, msh.orientations[el], x, Bs, rel, dil, q,
+            w, n, 6)
+    a = oracle_mod.compute_stiffness_and_jacobi_matrix_curl_curl_diluted(*args)
+    b = oracle_mod.compute_stiffness_and_jacobi_matrix_curl_curl_diluted(*args, backend="ref")
+    assert_same_pattern(a[0], b[0])
+    assert_csr_close(a[0], b[0], 1e-14, atol_rel=1e-16)
+    assert_csr_close(a[1], b[1], 1e-14, atol_rel=1e-16)
+    assert rel_max(a[2], b[2]) < 1e-14
 
 
 def test_mlp_oracle_backward_matches_finite_differences():
