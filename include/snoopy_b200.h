@@ -163,6 +163,45 @@ int snp_b_at_elements(int64_t n_points, const int32_t *elem, const double *nodes
                       int32_t n_orient, const double *d_phi, int32_t n_quad, const double *x, double *B,
                       void *stream);
 
+/* ---------------------------------------------------------------- field maps
+ * Mesh index for point location and nodal output.  Replaces gmsh's point location
+ * (get_element_by_coordinates in snoopy/evaluators.py:155-295, 297-410) and the Python loop of
+ * CurlCurlAssembler.compute_nodal_fields (snoopy/curl_curl_assembler.py:2089-2196).  Built once
+ * per mesh (device copies of nodes[N][3] and cells[E][4]; cells are checked): a uniform bucket
+ * grid with cell edge >= the largest element extent, elements bucketed by centroid, and the
+ * node -> element incidence. */
+typedef struct snp_mesh_index snp_mesh_index;
+
+int snp_mesh_index_create(const double *nodes, int64_t n_nodes, const int32_t *cells, int64_t n_elems,
+                          void *stream, snp_mesh_index **out);
+
+/* Grid shape (nb[3] buckets, origin bmin[3], cell edges h[3]) and the fullest bucket's size;
+ * any output may be NULL. */
+int snp_mesh_index_info(const snp_mesh_index *mi, int32_t *nb, double *bmin, double *h, int32_t *max_bucket);
+
+/* For each point (device f64[n_points][3]): the element holding it, elem[i] (-1 when the best
+ * candidate's smallest barycentric coordinate is below -tol, or the point is not finite), and,
+ * when bary is not NULL, its barycentric coordinates bary[i][4] in the element's node order
+ * (0 outside).  Among elements holding a point (faces, edges) the one with the largest smallest
+ * coordinate wins, ties to the lower element index. */
+int snp_mesh_index_locate(const snp_mesh_index *mi, const double *points, int64_t n_points, double tol,
+                          int32_t *elem, double *bary, void *stream);
+
+/* nodal[v][c] = mean of elem_values[e][c] over the elements e of node v with elem_mask[e] != 0
+ * (all elements when elem_mask is NULL), summed in element order; 0 for a node with none
+ * (compute_nodal_fields, curl_curl_assembler.py:2185-2196). */
+int snp_mesh_index_nodal_average(const snp_mesh_index *mi, const double *elem_values, int32_t n_comp,
+                                 const uint8_t *elem_mask, double *nodal, void *stream);
+
+/* out[i][c] = sum_k bary[i][k] nodal[s][cells[elem[i]][k]][c] with s = point_set[i] (0 when
+ * point_set is NULL); 0 for elem[i] outside [0, E) or s outside [0, n_sets).  nodal holds
+ * n_sets arrays of N x n_comp values (evaluate_interpolation, snoopy/evaluators.py:297-410). */
+int snp_mesh_index_interpolate(const snp_mesh_index *mi, int64_t n_points, const int32_t *elem,
+                               const double *bary, const double *nodal, int32_t n_comp, int32_t n_sets,
+                               const int32_t *point_set, double *out, void *stream);
+
+int snp_mesh_index_destroy(snp_mesh_index *mi);
+
 /* Source rhs of the total-potential formulation from a nodal electric potential x_p[N]:
  * rhs[g_k] += sum_q (J^-T w_hat_k) . (J^-T grad_hat phi) w_q det, with the edge basis
  * functions basis[n_orient][Q][6][3] (not their curls).  Replaces the pure-Python

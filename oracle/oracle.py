@@ -26,6 +26,8 @@ The glue around them restates the reference's Python/Cython layers:
 * ``newton_residual``: the same loop driven to a relative Newton residual
   ||F_free(x)|| / ||F_free(x0)|| with F(x) = K(x) x - rhs(x) and a tight inner CG.
 * ``laplace_subdomain_solve``                        ``snoopy/laplace_subdomain_solver.py:117-158``
+* ``locate_points``, ``element_B``, ``nodal_fields``, ``interpolate_nodal``: field-map output
+  (``snoopy/evaluators.py:155-410``, ``snoopy/curl_curl_assembler.py:2089-2196``)
 """
 
 import ctypes
@@ -733,4 +735,108 @@ def laplace_subdomain_solve(nodes, cells, term_tags, subdomain_mask, Phi, tags_t
     x[mask_c] = x_c
     out = x_l.copy()
     out[np.flatnonzero(keep)] = x
+    return out
+
+
+# ------------------------------------------------------------------ field maps
+
+def locate_points(nodes, cells, points, tol=1e-12):
+    """Element index (-1 outside) and barycentric coordinates of each point.
+
+    The bucket search of the device mesh index, in numpy: elements bucketed by centroid on a
+    uniform grid whose cell is at least the largest element extent, the 27 buckets around the
+    point searched, the candidate with the largest smallest barycentric coordinate kept (the
+    first one on ties; coordinates by LU solve).  The reference locates with gmsh's
+    ``get_element_by_coordinates`` (``snoopy/evaluators.py:155-295``).
+    """
+    nodes = np.asarray(nodes, dtype=np.float64).reshape(-1, 3)
+    cells = np.asarray(cells, dtype=np.int64).reshape(-1, 4)
+    pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+    p = nodes[cells]  # [E,4,3]
+    ext = (p.max(axis=1) - p.min(axis=1)).max()
+    cen = p.mean(axis=1)
+    bmin = nodes.min(axis=0)
+    bmax = nodes.max(axis=0)
+    nb = np.maximum(1, np.floor((bmax - bmin) / ext).astype(np.int64))
+    h = (bmax - bmin) / nb
+    cb = np.minimum(((cen - bmin) / h).astype(np.int64), nb - 1)
+    key = cb[:, 0] + nb[0] * (cb[:, 1] + nb[1] * cb[:, 2])
+    order = np.argsort(key, kind="stable")
+    skey = key[order]
+    elem = np.full(pts.shape[0], -1, dtype=np.int64)
+    bary = np.zeros((pts.shape[0], 4))
+    fin = np.isfinite(pts).all(axis=1)
+    r = np.where(fin[:, None], (pts - bmin) / h, -10.0)
+    ip = np.floor(np.clip(r, -2.0, nb + 1.0)).astype(np.int64)
+    offs = np.array([(i, j, k) for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)])
+    for n, x in enumerate(pts):
+        if not fin[n]:
+            continue
+        b = ip[n] + offs
+        ok = np.all((b >= 0) & (b < nb), axis=1)
+        b = b[ok]
+        keys = b[:, 0] + nb[0] * (b[:, 1] + nb[1] * b[:, 2])
+        lo = np.searchsorted(skey, keys, side="left")
+        hi = np.searchsorted(skey, keys, side="right")
+        cand = np.concatenate([order[a:c] for a, c in zip(lo, hi)]) if len(keys) else np.zeros(0, np.int64)
+        if cand.size == 0:
+            continue
+        pc = p[cand]
+        T = np.stack([pc[:, 1] - pc[:, 0], pc[:, 2] - pc[:, 0], pc[:, 3] - pc[:, 0]], axis=2)
+        lam123 = np.linalg.solve(T, (x - pc[:, 0])[:, :, None])[:, :, 0]
+        lam = np.concatenate([1.0 - lam123.sum(axis=1, keepdims=True), lam123], axis=1)
+        score = lam.min(axis=1)
+        best = int(np.argmax(score))
+        if score[best] >= -tol:
+            elem[n] = cand[best]
+            bary[n] = lam[best]
+    return elem, bary
+
+
+def element_B(nodes, cells, glob_ids, orientations, curls, n_orient, d_phi, x):
+    """B = sum_k J curl_hat_k x_k / det in every listed element, at the first point of the
+    tables (first order: constant), the loop body of ``compute_nodal_fields``
+    (``snoopy/curl_curl_assembler.py:2160-2183``)."""
+    nodes = np.asarray(nodes, dtype=np.float64).reshape(-1, 3)
+    cells = np.asarray(cells, dtype=np.int64).reshape(-1, 4)
+    gids = np.asarray(glob_ids, dtype=np.int64).reshape(-1, 6)
+    ori = np.asarray(orientations, dtype=np.int64).reshape(-1)
+    dphi = np.asarray(d_phi, dtype=np.float64).reshape(-1, 4, 3)[0]
+    ct = np.asarray(curls, dtype=np.float64).reshape(int(n_orient), -1, 6, 3)[:, 0]  # [n_orient, 6, 3], first point
+    X = nodes[cells]                                   # [E, 4, 3]
+    J = np.einsum("eik,il->ekl", X, dphi)              # J[k][l] = sum_i X_i[k] dphi_i[l]
+    det = np.linalg.det(J)
+    xv = np.asarray(x, dtype=np.float64)[gids]         # [E, 6]
+    B = np.zeros((len(cells), 3))
+    for k in range(6):
+        B += np.einsum("ekl,el->ek", J, ct[ori, k]) * (xv[:, k] / det)[:, None]
+    return B
+
+
+def nodal_fields(num_nodes, cells, B_elem):
+    """Element values averaged at the nodes (``compute_nodal_fields``,
+    ``snoopy/curl_curl_assembler.py:2185-2196``): per node the sum over its listed elements
+    divided by their number; nodes with none keep 0."""
+    cells = np.asarray(cells, dtype=np.int64).reshape(-1, 4)
+    out = np.zeros((num_nodes, B_elem.shape[1]))
+    mult = np.zeros(num_nodes, dtype=np.int64)
+    for i in range(4):
+        np.add.at(out, cells[:, i], B_elem)
+        np.add.at(mult, cells[:, i], 1)
+    m = mult != 0
+    out[m] /= mult[m][:, None]
+    return out
+
+
+def interpolate_nodal(cells, elem, bary, nodal_sets, point_set):
+    """sum_i phi_i v[cells[e][i]] at located points (``evaluate_interpolation``,
+    ``snoopy/evaluators.py:390-406``), v = nodal_sets[point_set[p]]; 0 for unlocated points."""
+    cells = np.asarray(cells, dtype=np.int64).reshape(-1, 4)
+    nc = nodal_sets[0].reshape(len(nodal_sets[0]), -1).shape[1]
+    out = np.zeros((len(elem), nc))
+    for p, (e, s) in enumerate(zip(elem, point_set)):
+        if e < 0 or s < 0:
+            continue
+        v = nodal_sets[s].reshape(-1, nc)
+        out[p] = bary[p] @ v[cells[e]]
     return out

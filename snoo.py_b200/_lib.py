@@ -88,6 +88,12 @@ _SIGS = {
     "snp_solver_solve_many": [_vp, _c_i32, _vp, _vp, _vp, _c_i32, _vp],
     "snp_solver_set_source": [_vp, _c_i32, _vp, _vp],
     "snp_solver_set_dilution": [_vp, _c_i32, _vp, _vp],
+    "snp_mesh_index_create": [_vp, _c_i64, _vp, _c_i64, _vp, _vp],
+    "snp_mesh_index_info": [_vp, _vp, _vp, _vp, _vp],
+    "snp_mesh_index_locate": [_vp, _vp, _c_i64, ctypes.c_double, _vp, _vp, _vp],
+    "snp_mesh_index_nodal_average": [_vp, _vp, _c_i32, _vp, _vp, _vp],
+    "snp_mesh_index_interpolate": [_vp, _c_i64, _vp, _vp, _vp, _c_i32, _c_i32, _vp, _vp, _vp],
+    "snp_mesh_index_destroy": [_vp],
     "snp_gemm_bf16": [_c_i32, _c_i32, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp, _c_i32, _vp,
                       _vp],
     "snp_gelu_backward": [_c_i64, _vp, _vp, _vp, _vp, _vp],

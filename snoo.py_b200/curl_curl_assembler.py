@@ -204,6 +204,36 @@ class CurlCurlAssembler:
                       _lib.ptr(w_t), nq, _lib.ptr(xp), _lib.ptr(rhs), _lib.stream_ptr())
         return rhs[: self.num_dofs].cpu().numpy()
 
+    def element_B_device(self, x):
+        """Device [E, 3]: B = curl A in every element of the mesh (first order: constant)."""
+        d = self._device_state()
+        tb = self.tables(1)
+        x_d = x if hasattr(x, "data_ptr") else upload(x, np.float64)
+        if "all" not in d:
+            d["all"] = (upload(self.mesh.cells, np.int32), upload(self.mesh.elem_edges, np.int32),
+                        upload(self.mesh.orientations, np.int32))
+        if "arange" not in d:
+            d["arange"] = upload(np.arange(self.mesh.num_elements), np.int32)
+        cells_d, gids_d, or_d = d["all"]
+        E = self.mesh.num_elements
+        B = zeros(3 * E)[: 3 * E]
+        _lib.call("snp_b_at_elements", E, _lib.ptr(d["arange"]), _lib.ptr(d["nodes"]), _lib.ptr(cells_d),
+                  _lib.ptr(gids_d), _lib.ptr(or_d), _lib.ptr(tb.curls_d), tb.n_orient, _lib.ptr(tb.d_phi_d), tb.nq,
+                  _lib.ptr(x_d), _lib.ptr(B), _lib.stream_ptr())
+        return B.view(E, 3)
+
+    def compute_nodal_fields(self, x, mat_ids):
+        """B at the mesh nodes by averaging the element fields of the materials ``mat_ids``
+        (volume tags) around each node (``curl_curl_assembler.py:2089-2196``); nodes outside
+        them get 0.  Returns float64 [N, 3] (numpy)."""
+        mask = np.zeros(self.mesh.num_elements, dtype=np.uint8)
+        for mid in mat_ids:
+            n = list(self.volume_tags).index(mid)
+            mask[self._elems[n]] = 1
+        B = self.element_B_device(x)
+        out = self.mesh.index().nodal_average(B, 3, upload(mask, np.uint8))
+        return out.cpu().numpy()
+
     def compute_B_at_points(self, x, points, elements=None):
         """B = curl A at arbitrary points (element constant for first order); points outside give 0."""
         d = self._device_state()

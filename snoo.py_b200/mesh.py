@@ -162,49 +162,26 @@ class TetMesh:
         c = self.cells if elems is None else self.cells[elems]
         return self.nodes[c].mean(axis=1)
 
+    def index(self):
+        """Device ``MeshIndex`` (bucket grid + node incidence) of this mesh, rebuilt when the
+        node coordinates change."""
+        from .mesh_index import MeshIndex
+
+        key = (self.nodes.shape, self.cells.shape, float(np.add.reduce(self.nodes, axis=None)),
+               int(self.cells[:: max(1, len(self.cells) // 64)].sum()))
+        if getattr(self, "_index_key", None) != key:
+            self._index = MeshIndex(self.nodes, self.cells)
+            self._index_key = key
+        return self._index
+
     def locate(self, points, tol=1e-12):
-        """Element index and barycentric coordinates of each point (-1 if outside).
+        """Element index (-1 outside) and barycentric coordinates of each point, on the device.
 
         Elements are bucketed by centroid on a uniform grid whose cell is at least the
         largest element extent, so a point's element lies in the 27 buckets around it.
         Replaces gmsh's point location used by ``evaluators.py:155-295``.
         """
-        pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
-        p = self.nodes[self.cells]  # [E,4,3]
-        ext = (p.max(axis=1) - p.min(axis=1)).max()
-        cen = p.mean(axis=1)
-        bmin = self.nodes.min(axis=0)
-        bmax = self.nodes.max(axis=0)
-        nb = np.maximum(1, np.floor((bmax - bmin) / ext).astype(np.int64))
-        h = (bmax - bmin) / nb
-        cb = np.minimum(((cen - bmin) / h).astype(np.int64), nb - 1)
-        key = cb[:, 0] + nb[0] * (cb[:, 1] + nb[1] * cb[:, 2])
-        order = np.argsort(key, kind="stable")
-        skey = key[order]
-        elem = np.full(pts.shape[0], -1, dtype=np.int64)
-        bary = np.zeros((pts.shape[0], 4))
-        ip = np.floor((pts - bmin) / h).astype(np.int64)
-        offs = np.array([(i, j, k) for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)])
-        for n, x in enumerate(pts):
-            b = ip[n] + offs
-            ok = np.all((b >= 0) & (b < nb), axis=1)
-            b = b[ok]
-            keys = b[:, 0] + nb[0] * (b[:, 1] + nb[1] * b[:, 2])
-            lo = np.searchsorted(skey, keys, side="left")
-            hi = np.searchsorted(skey, keys, side="right")
-            cand = np.concatenate([order[a:c] for a, c in zip(lo, hi)]) if len(keys) else np.zeros(0, np.int64)
-            if cand.size == 0:
-                continue
-            pc = p[cand]
-            T = np.stack([pc[:, 1] - pc[:, 0], pc[:, 2] - pc[:, 0], pc[:, 3] - pc[:, 0]], axis=2)
-            lam123 = np.linalg.solve(T, (x - pc[:, 0])[:, :, None])[:, :, 0]
-            lam = np.concatenate([1.0 - lam123.sum(axis=1, keepdims=True), lam123], axis=1)
-            score = lam.min(axis=1)
-            best = int(np.argmax(score))
-            if score[best] >= -tol:
-                elem[n] = cand[best]
-                bary[n] = lam[best]
-        return elem, bary
+        return self.index().locate(points, tol)
 
 
 def tensor_grid_mesh(xs, ys, zs, cell_domain, jitter=0.0, seed=0, fixed_planes=None):

@@ -96,10 +96,11 @@ def test_dirichlet_edges_on_box_surface(msh):
     assert len(ids) > 0
 
 
-def test_locate_points(msh):
+def test_locate_points(msh, oracle_mod):
+    """The oracle's bucket search (the checker of the device mesh index)."""
     rng = np.random.default_rng(0)
     pts = rng.uniform([-0.5, -0.5, -0.6], [0.5, 0.5, 0.6], (200, 3))
-    el, bary = msh.locate(pts)
+    el, bary = oracle_mod.locate_points(msh.nodes, msh.cells, pts)
     assert (el >= 0).all()
     rec = np.einsum("pi,pid->pd", bary, msh.nodes[msh.cells[el]])
     np.testing.assert_allclose(rec, pts, atol=1e-12)
