@@ -162,6 +162,37 @@ class TetMesh:
         c = self.cells if elems is None else self.cells[elems]
         return self.nodes[c].mean(axis=1)
 
+    def get_cotree_dofs(self):
+        """Tree-cotree split of the edges (``mesh_tools.py:468-566``): 0-based edge ids of a
+        spanning tree of the node graph and of the remaining (cotree) edges.
+
+        The reference takes networkx's minimum spanning tree of the unit-weight edge graph,
+        i.e. any spanning tree.  Here the tree spans the outer boundary's nodes first (boundary
+        edges are preferred), so that fixing the tree edges on top of the Dirichlet boundary
+        removes exactly the gradient null space of the interior nodes.
+        """
+        from scipy.sparse import coo_matrix
+        from scipy.sparse.csgraph import connected_components, minimum_spanning_tree
+
+        n = self.num_nodes
+        m = self.num_dofs
+        w = np.full(m, 2.0)
+        w[self.boundary_edge_ids()] = 1.0
+        # edge id + 1 rides along in the weight's fraction so that the tree's edges come back
+        # by id (weights stay ordered: boundary < interior)
+        ids = np.arange(m, dtype=np.float64)
+        G = coo_matrix((w + (ids + 1.0) / (2.0 * (m + 1)), (self.edges[:, 0], self.edges[:, 1])), shape=(n, n)).tocsr()
+        ncomp, _ = connected_components(G, directed=False)
+        if ncomp != 1:
+            raise ValueError("The input graph must be connected.")
+        T = minimum_spanning_tree(G).tocoo()
+        frac = T.data - np.floor(T.data)
+        tree = np.rint(frac * 2.0 * (m + 1) - 1.0).astype(np.int64)
+        tree = np.sort(tree)
+        mask = np.ones(m, dtype=bool)
+        mask[tree] = False
+        return tree, np.flatnonzero(mask)
+
     def index(self):
         """Device ``MeshIndex`` (bucket grid + node incidence) of this mesh, rebuilt when the
         node coordinates change."""

@@ -53,21 +53,24 @@ class MVPSolver:
                                                                          select_mat=[i])
         return rhs
 
-    def _engine(self, phi_list):
-        key = tuple(float(p) for p in phi_list)
+    def _engine(self, phi_list, apply_gauge=False):
+        key = (tuple(float(p) for p in phi_list), bool(apply_gauge))
         if self._newton is None or self._rhs_key != key:
             rhs_mvp = self.compute_source_rhs(phi_list)
-            self._newton = DeviceNewton(self.curl_curl_factory, self.make_boundary_mask(), (), self.quad_order,
-                                        rhs_extra=rhs_mvp, stream=getattr(self, "stream", None))
+            mask = self.make_boundary_mask()
+            if apply_gauge:
+                # tree-cotree gauge: the spanning tree's edges are fixed too (mvp_solver.py:257-260)
+                tree_dofs, _ = self.curl_curl_factory.mesh.get_cotree_dofs()
+                mask[tree_dofs] = False
+            self._newton = DeviceNewton(self.curl_curl_factory, mask, (), self.quad_order, rhs_extra=rhs_mvp,
+                                        stream=getattr(self, "stream", None))
             self._rhs_key = key
         return self._newton
 
     def solve_nonlin(self, phi_list, tolerance=1e-4, x_0=np.zeros((0,)), maxiter=-1, apply_gauge=False,
                      plot_current_density=False):
         """Newton with the reference's increment test; returns float64[num_dofs] (numpy)."""
-        if apply_gauge:
-            raise NotImplementedError("the tree-cotree gauge (apply_gauge=True) is not implemented")
-        eng = self._engine(phi_list)
+        eng = self._engine(phi_list, apply_gauge)
         x0 = None if len(x_0) == 0 else np.asarray(x_0, dtype=np.float64)
         if self.verbose:
             print("***********************")

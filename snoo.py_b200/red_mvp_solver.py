@@ -73,7 +73,21 @@ class RedMVPSolver:
             self._source_fields = fields
         return self._source_fields
 
-    def newton_engine(self):
+    def gauge_mask(self):
+        """Free-DoF mask of the tree-cotree gauged formulation: the Dirichlet edges and the
+        spanning tree's edges are fixed (``red_mvp_solver.py:169-171``)."""
+        mask = self.make_boundary_mask()
+        tree_dofs, _ = self.curl_curl_factory.mesh.get_cotree_dofs()
+        mask[tree_dofs] = False
+        return mask
+
+    def newton_engine(self, apply_gauge=False):
+        if apply_gauge:
+            if getattr(self, "_newton_gauged", None) is None:
+                self._newton_gauged = DeviceNewton(self.curl_curl_factory, self.gauge_mask(),
+                                                   self.compute_source_fields(), self.quad_order,
+                                                   stream=getattr(self, "stream", None))
+            return self._newton_gauged
         if self._newton is None:
             self._newton = DeviceNewton(self.curl_curl_factory, self.make_boundary_mask(), self.compute_source_fields(),
                                         self.quad_order, stream=getattr(self, "stream", None))
@@ -84,9 +98,7 @@ class RedMVPSolver:
 
         :return: the solution vector, float64[num_dofs] (numpy).
         """
-        if apply_gauge:
-            raise NotImplementedError("the tree-cotree gauge (apply_gauge=True) is not implemented")
-        eng = self.newton_engine()
+        eng = self.newton_engine(apply_gauge)
         x0 = None if len(x_0) == 0 else np.asarray(x_0, dtype=np.float64)
         if self.verbose:
             print("***********************")

@@ -120,3 +120,25 @@ def test_coil_terminals_split_ring():
         t1, t2 = m.coil_terminals[tag]
         assert len(t1) > 0 and len(t2) > 0
         assert not np.intersect1d(t1, t2).size
+
+
+def test_cotree_split_is_a_spanning_tree(msh):
+    tree, cotree = msh.get_cotree_dofs()
+    assert len(tree) == msh.num_nodes - 1 and len(tree) + len(cotree) == msh.num_dofs
+    assert not np.intersect1d(tree, cotree).size
+    parent = np.arange(msh.num_nodes)
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    for e in tree:  # acyclic with N - 1 edges: spanning
+        a, b = find(msh.edges[e, 0]), find(msh.edges[e, 1])
+        assert a != b
+        parent[a] = b
+    # the tree spans the outer boundary's nodes through boundary edges first
+    bnd = msh.boundary_edge_ids()
+    n_bnodes = len(np.unique(msh.edges[bnd].ravel()))
+    assert np.isin(tree, bnd).sum() == n_bnodes - 1
