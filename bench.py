@@ -386,6 +386,7 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
     stream = torch.cuda.current_stream()
     rows = {"fp64_zero": [], "mixed_zero": [], "mixed_warm": []}
     surr_err, proj_err, b_err = [], [], []
+    warm_x = []
     probes = fam.geometry.aperture_probes(200, margin=0.03)
     el, _ = fam.mesh.locate(probes)
     for p in P_test:
@@ -404,6 +405,7 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
                 x_ref = x.clone()
                 B_ref = ms.solver.curl_curl_factory.compute_B_at_points(x, probes, el)
             elif name == "mixed_warm":
+                warm_x.append(x.clone())
                 nrm = float(torch.linalg.vector_norm(x_ref).item())
                 surr_err.append(float(torch.linalg.vector_norm(x0 - x_ref).item()) / nrm)
                 proj_err.append(float(torch.linalg.vector_norm(ws.project(x_ref) - x_ref).item()) / nrm)
@@ -422,6 +424,34 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
                      "newton_mean": float(r[:, 1].mean()), "cg_mean": float(r[:, 2].mean()),
                      "rel_res_max": float(r[:, 3].max()), "starts_dropped": int(r[:, 4].sum())}
     out["speedup_mixed_warm_vs_fp64_zero"] = out["mixed_warm"]["solves_per_s"] / out["fp64_zero"]["solves_per_s"]
+    # the same warm-started mixed solves, `batch` members at a time: one solver per member, each
+    # on its own stream and host thread (snp_solver_solve_many); wall clock around each batch's
+    # predictions and solves (moving the solvers to their members is not timed, as above)
+    batch = min(4, len(P_test))
+    if batch > 1:
+        extra = [SG.MorphedSolver(fam, stream=torch.cuda.Stream()) for _ in range(batch)]
+        wall, stats, same = 0.0, [], True
+        for c0 in range(0, len(P_test), batch):
+            chunk = list(range(c0, min(c0 + batch, len(P_test))))
+            mss = extra[: len(chunk)]
+            refs = [m.set_member(P_test[i]) for m, i in zip(mss, chunk)]
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            x0s = [ws.predict(P_test[i])[0] for i in chunk]
+            xs, st = SG.solve_members_at_once(mss, x0s, refs, rtol=RTOL, precision="mixed")
+            torch.cuda.synchronize()
+            wall += time.perf_counter() - t1
+            stats += st
+            same = same and all(torch.equal(x, warm_x[i]) for x, i in zip(xs, chunk))
+        out["mixed_warm_batched"] = {
+            "members_at_once": batch, "solves_per_s": len(P_test) / wall,
+            "newton_mean": float(np.mean([s_["newton_iterations"] for s_ in stats])),
+            "cg_mean": float(np.mean([s_["cg_iterations"] for s_ in stats])),
+            "rel_res_max": float(max(s_["rel_res"] for s_ in stats)),
+            "identical_to_one_at_a_time": bool(same)}
+        out["speedup_mixed_warm_batched_vs_fp64_zero"] = (out["mixed_warm_batched"]["solves_per_s"]
+                                                          / out["fp64_zero"]["solves_per_s"])
+        del extra
     del ws, ms, fam
     return out
 

@@ -84,6 +84,7 @@ class DeviceNewton:
                               1 if verbose else 0, 1 if line_search else 0, float(res_ref))
         st = _lib.SolveStats()
         rc = _lib.load().snp_solver_solve(self.handle, _lib.ptr(x), ctypes.byref(opts), ctypes.byref(st))
+        self._leave()
         stats = st.as_dict()
         ref = res_ref if res_ref > 0 else stats["res0"]
         stats["rel_res"] = stats["res"] / ref if ref > 0 else 0.0
@@ -92,13 +93,26 @@ class DeviceNewton:
         stats["converged"] = rc == 0
         return x, stats
 
+    def _enter(self):
+        """Work queued on torch's current stream (inputs of the next call) precedes the solver's
+        own stream."""
+        if self._stream is not None:
+            self._stream.wait_stream(torch().cuda.current_stream())
+
+    def _leave(self):
+        """Torch's current stream waits for what the last call queued on the solver's stream."""
+        if self._stream is not None:
+            torch().cuda.current_stream().wait_stream(self._stream)
+
     def assemble(self, x, K=False, J=True, rhs=False, F=True):
         x_d = x if hasattr(x, "data_ptr") else upload(x, np.float64)
         nnz = self.pattern.nnz
         out = {"K": zeros(nnz) if K else None, "J": zeros(nnz) if J else None, "rhs": zeros(self.n) if rhs else None,
                "F": zeros(self.n) if F else None}
+        self._enter()
         _lib.call("snp_solver_assemble", self.handle, _lib.ptr(x_d), _lib.ptr(out["K"]), _lib.ptr(out["J"]),
                   _lib.ptr(out["rhs"]), _lib.ptr(out["F"]), _lib.stream_ptr(self._stream))
+        self._leave()
         return out
 
     @property
@@ -112,11 +126,15 @@ class DeviceNewton:
 
     def set_nodes(self, nodes_dev):
         """Move the mesh nodes (device float64 [N, 3]); topology, pattern and materials stay."""
+        self._enter()
         _lib.call("snp_solver_set_nodes", self.handle, _lib.ptr(nodes_dev), _lib.stream_ptr(self._stream))
+        self._leave()
 
     def set_source(self, material, B_s_dev):
         """Replace material ``material``'s source field (device float64 [E_m * Q * 3])."""
+        self._enter()
         _lib.call("snp_solver_set_source", self.handle, int(material), _lib.ptr(B_s_dev), _lib.stream_ptr(self._stream))
+        self._leave()
 
     def residual_norm(self, x):
         """||F_free(x)|| (float64), via the matrix-free assembly."""
@@ -130,16 +148,20 @@ class DeviceNewton:
         """Matrix-free Newton assembly at x (element tensors of J(x), and F(x) into ``F`` when
         given); afterwards ``jacobian_apply(..., precision)`` applies J(x)."""
         x_d = x if hasattr(x, "data_ptr") else upload(x, np.float64)
+        self._enter()
         _lib.call("snp_solver_assemble_tensors", self.handle, _lib.ptr(x_d), {"fp64": 0, "mixed": 1}[precision],
                   _lib.ptr(F), _lib.stream_ptr(self._stream))
+        self._leave()
         return F
 
     def jacobian_apply(self, x, y, precision="fp64"):
         """y = J x on the free DoFs with the Newton Jacobian of the last solve of that precision
         ("fp64": float64 vectors; "mixed": the float32 Jacobian and float32 vectors)."""
         prec = {"fp64": 0, "mixed": 1}[precision]
+        self._enter()
         _lib.call("snp_solver_jacobian_apply", self.handle, prec, _lib.ptr(x), _lib.ptr(y),
                   _lib.stream_ptr(self._stream))
+        self._leave()
         return y
 
     def __del__(self):

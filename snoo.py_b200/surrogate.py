@@ -15,6 +15,7 @@ weights.  The POD basis is a setup step (float64 Gram matrix and eigendecomposit
 torch's cuBLAS/cuSOLVER calls).
 """
 
+import ctypes
 import math
 import time
 
@@ -182,7 +183,7 @@ class MorphedSolver:
     """One device Newton solver serving every member of a ``YokeMorphFamily``: moving a member
     in replaces the node coordinates and the coil source field, nothing else."""
 
-    def __init__(self, family, quad_order=2, max_newton=60):
+    def __init__(self, family, quad_order=2, max_newton=60, stream=None):
         from . import materials as MAT
         from . import mesh as M
         from .red_mvp_solver import RedMVPSolver
@@ -191,6 +192,8 @@ class MorphedSolver:
         self.solver = RedMVPSolver(family.mesh, family._base_coils, [M.TAG_IRON], [M.TAG_AIR],
                                    [MAT.atan_reluctance()], max_newton_iterations=max_newton, quad_order=quad_order)
         self.solver.verbose = False
+        if stream is not None:
+            self.solver.stream = stream
         self.eng = self.solver.newton_engine()
         self.n = family.mesh.num_dofs
         self.max_newton = max_newton
@@ -219,6 +222,41 @@ class MorphedSolver:
         prec = {"fp64": 0, "mixed": 1}[precision]
         return self.eng.solve(x0, mode=1, tol=rtol, max_newton=self.max_newton, precision=prec, cg_maxiter=50000,
                               res_ref=res_ref)
+
+
+def solve_members_at_once(msolvers, x0s, res_refs, rtol=1e-8, precision="mixed", n_threads=0):
+    """One Newton solve per ``MorphedSolver`` (each already moved to its member, each on its own
+    CUDA stream), all at once through ``snp_solver_solve_many``: every solve runs on a host
+    thread of its own, so the GPU overlaps their kernels.  ``x0s``: starting vectors (CUDA
+    float64 [n]) or None for zero starts; ``res_refs``: each member's ||F_free(0)||.
+    Returns the answers (new CUDA tensors) and per-solve stats dicts."""
+    k = len(msolvers)
+    t = torch()
+    xs = []
+    for ms, x0 in zip(msolvers, x0s):
+        x = zeros(ms.n)[: ms.n]
+        if x0 is not None:
+            x.copy_(x0)
+        xs.append(x)
+    t.cuda.synchronize()
+    prec = {"fp64": 0, "mixed": 1}[precision]
+    handles = (ctypes.c_void_p * k)(*[ms.eng.handle.value for ms in msolvers])
+    xp = (ctypes.c_void_p * k)(*[x.data_ptr() for x in xs])
+    opts = (_lib.SolveOpts * k)(*[_lib.SolveOpts(1, float(rtol), 50000, int(ms.max_newton), 0.1, prec, 0, 1,
+                                                 float(ref)) for ms, ref in zip(msolvers, res_refs)])
+    stats = (_lib.SolveStats * k)()
+    status = (ctypes.c_int32 * k)()
+    rc = _lib.load().snp_solver_solve_many(handles, k, xp, opts, stats, int(n_threads), status)
+    t.cuda.synchronize()
+    out = []
+    for i in range(k):
+        d = stats[i].as_dict()
+        d["rel_res"] = d["res"] / res_refs[i] if res_refs[i] > 0 else 0.0
+        d["status"] = int(status[i])
+        out.append(d)
+    if rc != 0:
+        _lib.check(rc)
+    return xs, out
 
 
 class WarmStart:

@@ -112,3 +112,21 @@ def test_bad_start_is_dropped(family_setup):
     bad = torch.full((ms.n,), 1e3, dtype=torch.float64, device="cuda")
     x, st = ms.solve(bad, rtol=1e-8, precision="fp64", res_ref=ref)
     assert st["start_dropped"] == 1 and st["rel_res"] <= 1e-8
+
+
+def test_members_solved_at_once_match_one_at_a_time(family_setup):
+    """Warm-started solves of several members at once (one solver, stream and host thread each)
+    give bitwise the answers of solving them one after another."""
+    fam, ms, P_train, P_test = family_setup
+    rng = np.random.default_rng(3)
+    mss = [SG.MorphedSolver(fam, stream=torch.cuda.Stream()) for _ in range(3)]
+    refs = [m.set_member(p) for m, p in zip(mss, P_test[:3])]
+    x0s = [torch.as_tensor(rng.normal(0, 1e-4, ms.n), device="cuda") for _ in range(3)]
+    xs, st = SG.solve_members_at_once(mss, x0s, refs, rtol=1e-8, precision="mixed")
+    for x, s, x0, p, r in zip(xs, st, x0s, P_test[:3], refs):
+        ref = ms.set_member(p)
+        assert ref == r
+        x1, s1 = ms.solve(x0, rtol=1e-8, precision="mixed", res_ref=ref)
+        assert s["rel_res"] <= 1e-8 and s["status"] == 0
+        assert s["newton_iterations"] == s1["newton_iterations"] and s["cg_iterations"] == s1["cg_iterations"]
+        assert torch.equal(x, x1)
