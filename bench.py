@@ -426,8 +426,9 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
     out["speedup_mixed_warm_vs_fp64_zero"] = out["mixed_warm"]["solves_per_s"] / out["fp64_zero"]["solves_per_s"]
     # the same warm-started mixed solves, `batch` members at a time: one solver per member, each
     # on its own stream and host thread (snp_solver_solve_many); wall clock around each batch's
-    # predictions and solves (moving the solvers to their members is not timed, as above)
-    batch = min(4, len(P_test))
+    # predictions and solves (moving the solvers to their members is not timed, as above).
+    # Smaller meshes leave more of the GPU idle per solve, so they run more members at once.
+    batch = min(8 if fam.mesh.num_elements < 600_000 else 4, len(P_test))
     if batch > 1:
         extra = [SG.MorphedSolver(fam, stream=torch.cuda.Stream()) for _ in range(batch)]
         wall, stats, same = 0.0, [], True
