@@ -495,8 +495,8 @@ def mixed_precision_accuracy(tets=4_000_000, n_probes=1000):
     return out
 
 
-def assembly_microbench(reps=5, warmup=3, seed=5):
-    """Assembly-only microbenchmark: the structured 120 x 120 x 116 grid split into 6 tets
+def assembly_microbench(reps=5, warmup=3, seed=5, grid=(120, 120, 116)):
+    """Assembly-only microbenchmark: the structured 120 x 120 x 116 grid (``grid``) split into 6 tets
     per cell (10,022,400 tets), nodes jittered by U[-0.2, 0.2] x spacing, edge DoFs
     x ~ N(0, 1e-3), seeded 40% iron flags (PCHIP atan B-H) against air, no Dirichlet mask,
     4-point rule, float64.  Two Newton assemblies at x are timed (CUDA events, after warm-up):
@@ -521,7 +521,7 @@ def assembly_microbench(reps=5, warmup=3, seed=5):
     from snoopy_b200.newton import DeviceNewton
 
     t0 = time.perf_counter()
-    msh = M.kuhn_microbench_mesh()
+    msh = M.kuhn_microbench_mesh(*grid)
     E, N, n = msh.num_elements, msh.nodes.shape[0], msh.num_dofs
     asm = CurlCurlAssembler(msh, [M.TAG_IRON, M.TAG_AIR], [MAT.atan_reluctance(), S.ConstantReluctance(1e7 / (4 * np.pi))])
     eng = DeviceNewton(asm, np.ones(n, dtype=np.uint8), (), quad_order=2)
@@ -550,7 +550,7 @@ def assembly_microbench(reps=5, warmup=3, seed=5):
     peak, peak_kind = measured_peaks()
     b_csr = E * (16 + 24 + 4 + 144) + 24 * N + 8 * n + 8 * nnz + 8 * n
     b_t = E * (16 + 24 + 4 + 48) + 24 * N + 8 * n + 16 * n
-    out = {"workload": f"Kuhn grid 120x120x116 x 6 = {E} tets, {N} nodes, {n} edge DoFs, nnz {nnz}, "
+    out = {"workload": f"Kuhn grid {grid[0]}x{grid[1]}x{grid[2]} x 6 = {E} tets, {N} nodes, {n} edge DoFs, nnz {nnz}, "
                        f"40% iron, x ~ N(0, 1e-3), Q=4, f64",
            "setup_s": setup_s, "peak_gbs": peak, "peak_kind": peak_kind}
     for name, ms, b in (("csr", ms_csr, b_csr), ("tensors", ms_t, b_t)):
