@@ -628,9 +628,10 @@ def cpu_baseline_sample(msh, coils, rel, assemblies_per_solve, cg_per_solve):
 
 # Work per solve of this workload, measured by running the whole solve on the CPU with the
 # reference's kernels and scipy's cg (oracle.newton_residual with forcing="ew" and
-# line_search="energy", the device solver's algorithm) on the 1.16M-tet mesh: 15 Newton steps,
-# 2988 CG iterations, 293 s on one core.  The device solver needs the same counts (15 and
-# about 3040); the reference arm projects its measured per-iteration times with them.
+# line_search="energy", the device solver's algorithm) on the 1.16M-tet mesh: 13 Newton steps,
+# 2868 CG iterations and 22 assemblies, 278 s on one core.  The device solver needs 13 steps and
+# 2652 CG iterations; the reference arm projects its measured per-iteration times with the
+# oracle's counts.
 REFERENCE_COUNTS = {"newton": 13.0, "assemblies": 22.0, "cg": 2868.0}
 
 
