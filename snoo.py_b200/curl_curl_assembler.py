@@ -136,10 +136,14 @@ class CurlCurlAssembler:
         return out
 
     # ---------------------------------------------------------------- reference API
-    def compute_stiffness_and_jacobi_matrix_c(self, x, quad_order=2, source_fields=[]):
-        """``(K, dK + K, rhs)`` like ``curl_curl_assembler.py:815-932``: scipy CSR without exact zeros."""
+    def compute_stiffness_and_jacobi_matrix_c(self, x, quad_order=2, source_fields=[], device=False):
+        """``(K, dK + K, rhs)`` like ``curl_curl_assembler.py:815-932``: scipy CSR without exact zeros.
+        With ``device=True``: torch sparse CSR tensors on the GPU with the full structural pattern
+        (exact zeros kept) and a CUDA rhs, nothing copied to the host."""
         out = self.assemble_device(x, quad_order, source_fields, K=True, J=True, rhs=True)
         pat = out["pattern"]
+        if device:
+            return pat.to_torch(out["K"]), pat.to_torch(out["J"]), out["rhs"][: self.num_dofs]
         K = pat.to_scipy(out["K"], drop_zeros=True)
         J = pat.to_scipy(out["J"], drop_zeros=True)
         return K, J, out["rhs"][: self.num_dofs].cpu().numpy()

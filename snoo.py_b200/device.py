@@ -84,6 +84,18 @@ class Pattern:
             A.eliminate_zeros()
         return A
 
+    def to_torch(self, values):
+        """Device ``torch.sparse_csr_tensor`` (float64 values, int32 indices) with this pattern and
+        the given device values; every structural entry is kept, exact zeros included.  The
+        index arrays are copies, so the tensor outlives the pattern."""
+        import warnings
+
+        t = torch()
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", UserWarning)  # torch's notes on sparse CSR being in beta
+            return t.sparse_csr_tensor(self.row_ptr.clone(), self.col_idx.clone(), values[: self.nnz],
+                                       size=(self.n_rows, self.n_rows))
+
     def __del__(self):
         try:
             if self._owned and self.handle is not None and _lib._lib is not None:

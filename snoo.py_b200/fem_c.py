@@ -39,10 +39,11 @@ def _check_mesh(nodes, cells, glob_ids=None, num_dofs=None, orientations=None, n
             raise ValueError("one orientation and six glob_ids per element are required")
 
 
-def compute_stiffness_and_jacobi_matrix(nodes, cells, d_phi, x, permeability, q, w):
+def compute_stiffness_and_jacobi_matrix(nodes, cells, d_phi, x, permeability, q, w, device=False):
     """Grad-grad stiffness matrix and Jacobian of the scalar potential (``interface_c.pyx:11-160``).
 
-    :return: ``(K, dK)`` scipy CSR (num_nodes x num_nodes).
+    :return: ``(K, dK)`` scipy CSR (num_nodes x num_nodes); with ``device=True`` torch sparse
+        CSR tensors on the GPU (same structure and values, nothing copied to the host).
     """
     _lib.require_cuda()
     nodes = np.asarray(nodes, dtype=np.float64)
@@ -65,15 +66,18 @@ def compute_stiffness_and_jacobi_matrix(nodes, cells, d_phi, x, permeability, q,
     _lib.call("snp_gradgrad_assemble", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d), _lib.ptr(dphi_d),
               _lib.ptr(w_d), nq, _lib.ptr(x_d), typ, k, n, _lib.ptr(t), _lib.ptr(c), hmin, muh, _lib.ptr(K),
               _lib.ptr(dK), None, _lib.stream_ptr())
+    if device:
+        return pat.to_torch(K), pat.to_torch(dK)
     return pat.to_scipy(K), pat.to_scipy(dK)
 
 
 def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_s,
-                                                  reluctance, q, w, num_dofs, num_el_dofs):
+                                                  reluctance, q, w, num_dofs, num_el_dofs, device=False):
     """Curl-curl stiffness matrix, Jacobian correction and reduced rhs (``interface_c.pyx:162-374``).
 
     ``B_s`` empty selects the plain kernel, otherwise the reduced one.
-    :return: ``(K, dK, rhs)``: scipy CSR (num_dofs x num_dofs) and float64[num_dofs].
+    :return: ``(K, dK, rhs)``: scipy CSR (num_dofs x num_dofs) and float64[num_dofs]; with
+        ``device=True`` torch sparse CSR tensors and a CUDA tensor, left on the GPU.
     """
     _lib.require_cuda()
     if num_el_dofs != 6:
@@ -101,17 +105,21 @@ def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls,
               _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(dphi_d), _lib.ptr(w_d), nq, _lib.ptr(x_d),
               _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(K), _lib.ptr(dK), None, _lib.ptr(rhs), None,
               _lib.stream_ptr())
+    if device:
+        return pat.to_torch(K), pat.to_torch(dK), rhs[: int(num_dofs)]
     return pat.to_scipy(K), pat.to_scipy(dK), rhs[: int(num_dofs)].cpu().numpy()
 
 
 def compute_stiffness_and_jacobi_matrix_curl_curl_diluted(nodes, cells, glob_ids, curls, phi, d_phi, orientations, x,
-                                                          B_s, reluctance, dilution, q, w, num_dofs, num_el_dofs):
+                                                          B_s, reluctance, dilution, q, w, num_dofs, num_el_dofs,
+                                                          device=False):
     """Curl-curl Newton system of diluted steel (``interface_c.pyx:698-926``).
 
     With ``B_s`` the reluctance at each quadrature point is s nu(s |B|) with the dilution
     factor s(z) of ``dilution`` (``materials.Dilution``); ``B_s`` empty selects the plain
     kernel, as the reference does for air.
-    :return: ``(K, dK, rhs)``: scipy CSR (num_dofs x num_dofs) and float64[num_dofs].
+    :return: ``(K, dK, rhs)``: scipy CSR (num_dofs x num_dofs) and float64[num_dofs]; with
+        ``device=True`` torch sparse CSR tensors and a CUDA tensor, left on the GPU.
     """
     _lib.require_cuda()
     if num_el_dofs != 6:
@@ -142,6 +150,8 @@ def compute_stiffness_and_jacobi_matrix_curl_curl_diluted(nodes, cells, glob_ids
               _lib.ptr(gids_d), _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(phi_d), _lib.ptr(dphi_d),
               _lib.ptr(w_d), nq, _lib.ptr(x_d), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), dil, _lib.ptr(K),
               _lib.ptr(dK), None, _lib.ptr(rhs), None, _lib.stream_ptr())
+    if device:
+        return pat.to_torch(K), pat.to_torch(dK), rhs[: int(num_dofs)]
     return pat.to_scipy(K), pat.to_scipy(dK), rhs[: int(num_dofs)].cpu().numpy()
 
 

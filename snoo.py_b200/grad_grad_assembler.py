@@ -97,8 +97,9 @@ class GradGradAssembler:
                       _lib.ptr(out["dK"]), _lib.ptr(out["J"]), _lib.stream_ptr())
         return out
 
-    def compute_stiffness_and_jacobi_matrix_c(self, x, mu_list, quad_order=8):
-        """``(K, J)`` (``matrix_assembly.py:1059-1135``), scipy CSR without exact zeros.
+    def compute_stiffness_and_jacobi_matrix_c(self, x, mu_list, quad_order=8, device=False):
+        """``(K, J)`` (``matrix_assembly.py:1059-1135``), scipy CSR without exact zeros; with
+        ``device=True`` torch sparse CSR tensors on the GPU (full structural pattern).
 
         The reference adds the running K to dK after every material (``dK += K`` inside the
         material loop), so J = dK + sum_n (K of materials 0..n).  This is kept as is: with one
@@ -120,4 +121,6 @@ class GradGradAssembler:
                       None, _lib.stream_ptr())
             Ksum += K
         J = dK + Ksum
+        if device:
+            return pat.to_torch(K), pat.to_torch(J)
         return pat.to_scipy(K, drop_zeros=True), pat.to_scipy(J, drop_zeros=True)
