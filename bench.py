@@ -661,7 +661,7 @@ def run_reference(args):
 
 
 def batched_study(n=128, rank=0, world=1):
-    """Seeded yoke variants (BASELINE's batched configuration: 30k-600k tets, half reduced, half
+    """Seeded yoke variants (the batched workload: 30k-600k tets, half reduced, half
     total potential): every instance solved to the 1e-8 residual one after another, then all
     of them concurrently through snp_solver_solve_many, in float64 and in mixed precision.
     Throughput is instances per second of wall time (host clock around each whole batch, after

@@ -3,7 +3,7 @@
 A small MLP maps a magnet's design parameters to the POD coefficients of its converged
 edge-DoF vector; Newton then starts from the reconstruction instead of from zero.  The
 network is trained on solutions this solver generates over a fixed-topology family
-(``morph.YokeMorphFamily``).  Zero-start Newton stays the judge: a warm-started solve is held
+(``morph.YokeMorphFamily``).  Zero-start Newton stays the yardstick: a warm-started solve is held
 to the zero-start residual target ||F_free(x)|| <= tol ||F_free(0)||, and a prediction whose
 residual exceeds ||F_free(0)|| is dropped for x = 0, so the network changes iteration counts,
 never the converged answer.
