@@ -13,6 +13,8 @@ Drop-in pieces, with the reference's names and call signatures:
 * ``Reluctance``, ``ConstantReluctance``, ``Permeability``, ``ConstantPermeability``,
   ``Dilution``                   ``snoopy/materials.py``
 * ``RacetrackCoil``              ``snoopy/racetrack_coil.py``
+* ``ship.get_vector_field_mag_1`` ``snoopy/SHiP_functions.py`` (template 1, meshed without gmsh)
+* ``evaluators``                 ``snoopy/evaluators.py``
 
 gmsh is replaced by ``mesh.TetMesh`` and its generators, and by ``finite_element``'s tables.
 All arithmetic runs in ``libsnoopy_b200.so`` (CUDA, sm_100a); there is no CPU fallback.

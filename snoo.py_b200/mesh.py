@@ -79,6 +79,9 @@ class TetMesh:
         self._boundary_node_mask = boundary_node_mask
         self._number_edges()
         self.physical_groups = {}
+        # (axis, value): outer-boundary planes that carry the natural condition (a symmetry
+        # plane of a model cut in half); every other outer face is "Dirichlet Boundary"
+        self.natural_planes = []
 
     # gmsh-model look-alike: solvers call gmsh_model.mesh
     @property
@@ -135,9 +138,26 @@ class TetMesh:
         b = uniq[counts == 1]
         return np.stack([b // (n * n), (b // n) % n, b % n], axis=1)
 
+    def dirichlet_faces(self):
+        """Outer boundary faces without those lying in a natural plane."""
+        f = self.boundary_faces()
+        if not self.natural_planes:
+            return f
+        scale = float(np.abs(self.nodes).max()) or 1.0
+        keep = np.ones(len(f), dtype=bool)
+        for axis, value in self.natural_planes:
+            keep &= ~np.all(np.abs(self.nodes[f, axis] - value) <= 1e-12 * scale, axis=1)
+        return f[keep]
+
+    def dirichlet_edge_ids(self):
+        """0-based ids of the edges on the Dirichlet part of the outer boundary."""
+        return self._edge_ids_of_faces(self.dirichlet_faces())
+
     def boundary_edge_ids(self):
         """0-based ids of the edges on the outer boundary surface."""
-        f = self.boundary_faces()
+        return self._edge_ids_of_faces(self.boundary_faces())
+
+    def _edge_ids_of_faces(self, f):
         pairs = np.concatenate([f[:, [0, 1]], f[:, [0, 2]], f[:, [1, 2]]])
         n = self.num_nodes
         keys = np.unique(pairs[:, 0] * n + pairs[:, 1])
@@ -149,13 +169,14 @@ class TetMesh:
     def get_edge_boundary_dofs(self, names=("Dirichlet Boundary",), element_order=1):
         """1-based Dirichlet edge DoFs, like ``mesh_tools.get_edge_boundary_dofs`` (``mesh_tools.py:350-427``).
 
-        The outer boundary of the mesh carries the name "Dirichlet Boundary".
+        The outer boundary of the mesh, without its natural planes, carries the name
+        "Dirichlet Boundary".
         """
         out = []
         for name in names:
             if name != "Dirichlet Boundary":
                 raise KeyError(f"unknown boundary {name!r}")
-            out.append(self.boundary_edge_ids() + 1)
+            out.append(self.dirichlet_edge_ids() + 1)
         return np.unique(np.concatenate(out)) if out else np.zeros(0, dtype=np.int64)
 
     def element_centroids(self, elems=None):
@@ -167,9 +188,9 @@ class TetMesh:
         spanning tree of the node graph and of the remaining (cotree) edges.
 
         The reference takes networkx's minimum spanning tree of the unit-weight edge graph,
-        i.e. any spanning tree.  Here the tree spans the outer boundary's nodes first (boundary
-        edges are preferred), so that fixing the tree edges on top of the Dirichlet boundary
-        removes exactly the gradient null space of the interior nodes.
+        i.e. any spanning tree.  Here the tree spans the Dirichlet boundary's nodes first (its
+        edges are preferred), so that fixing the tree edges on top of the Dirichlet edges
+        removes exactly the gradient null space of the other nodes.
         """
         from scipy.sparse import coo_matrix
         from scipy.sparse.csgraph import connected_components, minimum_spanning_tree
@@ -177,7 +198,7 @@ class TetMesh:
         n = self.num_nodes
         m = self.num_dofs
         w = np.full(m, 2.0)
-        w[self.boundary_edge_ids()] = 1.0
+        w[self.dirichlet_edge_ids()] = 1.0
         # edge id + 1 rides along in the weight's fraction so that the tree's edges come back
         # by id (weights stay ordered: boundary < interior)
         ids = np.arange(m, dtype=np.float64)

@@ -1,0 +1,241 @@
+"""SHiP magnet template 1 without gmsh (``snoopy/SHiP_functions.py:282-809``).
+
+``get_vector_field_mag_1`` keeps the reference driver's arguments, flow and return values:
+the template's iron (``geometry_tools.py:133-392``, or with ``use_diluted_steel`` the core plus
+a diluted return-yoke wing, ``geometry_tools.py:601-805``) in an air box, the racetrack
+filament coil(s) around the core, the reduced-potential Newton solve (``RedMVPSolver`` or
+``RedMVPSolverDiluted``), B = curl A_r + B_coil at the quadrature points of every element,
+optionally B at extra positions by nodal interpolation, and the iron mass, coil mass, power
+and current density of the design.
+
+The geometry is meshed by this module instead of gmsh's OCC kernel: every boundary of the
+template is a plane x = c + m z or y = c + m z between the magnet's entrance and exit, so the
+quarter model (x >= 0, y >= 0) is a tensor grid whose x and y grid lines follow those planes
+(linear in z inside the magnet, constant in front of and behind it), split into 6 tetrahedra
+per cell.  Cells inside iron get spacing ``0.2 lc`` across x and y (the reference's inner mesh
+size) and ``lc`` along z; the plane y = 0 carries the natural boundary condition, every other
+box face n x A = 0, as in the reference (``SHiP_functions.py:539-570``).  Plotting and the gmsh
+GUI flags are accepted and ignored.
+"""
+
+import json
+import os
+
+import numpy as np
+
+from . import mesh as M
+from .materials import Dilution, Reluctance
+from .racetrack_coil import RacetrackCoil
+
+TAG_WING = 5  # the diluted return-yoke wing
+
+
+def compute_J_opt(conductor_material_data, kappa_elec):
+    """Current density in A/mm^2 that balances conductor cost against the cost of its losses
+    (``SHiP_functions.py:260-279``): sqrt(kappa_cu rho_mass / (kappa_elec rho_el))."""
+    kappa_cu = conductor_material_data["material_cost(CHF/kg)"] + conductor_material_data["manufacturing_cost(CHF/kg)"]
+    dens = conductor_material_data["density(g/m3)"]
+    rho = conductor_material_data["resistivity(Ohm.m)"]
+    return np.sqrt(kappa_cu * dens * 1e-3 / kappa_elec / rho) * 1e-6
+
+
+def _value(parameters, name, df_index):
+    return float(np.asarray(parameters[name])[df_index])
+
+
+def mag_1_parameters(parameters, df_index=0):
+    """The template's geometry and coil parameters from one row of the SHiP parameter table."""
+    names = {"X_mgap": "Xmgap", "X_core": "Xcore", "X_void": "Xvoid", "X_yoke": "Xyoke", "Y_core": "Ycore",
+             "Y_void": "Yvoid", "Y_yoke": "Yyoke"}
+    g = {}
+    for key, col in names.items():
+        g[key + "_1"] = _value(parameters, f"{col}1(m)", df_index)
+        g[key + "_2"] = _value(parameters, f"{col}2(m)", df_index)
+    for key, col in (("Z_len", "Z_len(m)"), ("Z_pos", "Z_pos(m)"), ("delta_x", "delta_x(m)"),
+                     ("delta_y", "delta_y(m)"), ("delta_z", "delta_z(m)"), ("current", "NI(A)"),
+                     ("field_density", "field_density"), ("max_turns", "max_turns")):
+        g[key] = _value(parameters, col, df_index)
+    g["yoke_spacer"] = _value(parameters, "yoke_spacer(mm)", df_index) * 1e-3
+    g["ins"] = _value(parameters, "insulation(mm)", df_index) * 1e-3
+    g["coil_radius"] = 0.5 * _value(parameters, "coil_diam(mm)", df_index) * 1e-3
+    g["lim_x"] = max(g["X_yoke_1"], g["X_yoke_2"]) + g["delta_x"]
+    g["lim_y"] = max(g["Y_yoke_1"], g["Y_yoke_2"]) + g["delta_y"]
+    g["z_min"] = g["Z_pos"] - g["delta_z"]
+    g["z_max"] = g["Z_pos"] + g["Z_len"] + g["delta_z"]
+    return g
+
+
+def _axis(breaks_1, breaks_2, spacing, names):
+    """Grid lines of one axis of the template.
+
+    breaks_1 / breaks_2: breakpoints at the entrance / exit, spacing and names per interval.
+    Intervals of zero width at both ends are dropped; a width that vanishes at one end only
+    is rejected.  Returns, per grid line, its interval and fraction inside it, the interval
+    name of every cell, and the entrance / exit breakpoints kept."""
+    b1, b2, hs, nm = [breaks_1[0]], [breaks_2[0]], [], []
+    for i in range(len(names)):
+        w1 = breaks_1[i + 1] - breaks_1[i]
+        w2 = breaks_2[i + 1] - breaks_2[i]
+        if w1 == 0.0 and w2 == 0.0:
+            continue
+        if not (w1 > 0.0 and w2 > 0.0):
+            raise ValueError(f"template interval {names[i]!r} is empty or inverted at one end ({w1}, {w2})")
+        b1.append(breaks_1[i + 1])
+        b2.append(breaks_2[i + 1])
+        hs.append(spacing[i])
+        nm.append(names[i])
+    counts = [max(1, int(np.ceil(max(b1[i + 1] - b1[i], b2[i + 1] - b2[i]) / hs[i] - 1e-9))) for i in range(len(nm))]
+    line_iv, line_f = [], []
+    for i, c in enumerate(counts):
+        line_iv += [i] * c
+        line_f += [k / c for k in range(c)]
+    line_iv.append(len(counts) - 1)
+    line_f.append(1.0)
+    cell_names = np.repeat(np.array(nm, dtype=object), counts)
+    return np.array(line_iv), np.array(line_f), cell_names, np.array(b1), np.array(b2)
+
+
+def mag_1_mesh(g, lc=0.2, use_diluted_steel=False):
+    """Quarter-model tetrahedral mesh of template 1 (tags: iron 1, air 2, diluted wing 5)."""
+    lci = 0.2 * lc
+    Z1, Z2 = g["Z_pos"], g["Z_pos"] + g["Z_len"]
+    xb = lambda e: [0.0, g[f"X_mgap_{e}"], g[f"X_core_{e}"], g[f"X_void_{e}"], g[f"X_yoke_{e}"], g["lim_x"]]
+    xi, xf, xcell, xb1, xb2 = _axis(xb(1), xb(2), [lci, lci, lci, lci, lc], ["gap", "core", "void", "leg", "out"])
+    if use_diluted_steel:
+        yb = lambda e: [0.0, g[f"Y_core_{e}"], g[f"Y_void_{e}"], g[f"Y_yoke_{e}"], g["lim_y"]]
+        yi, yf, ycell, yb1, yb2 = _axis(yb(1), yb(2), [lci, lci, lci, lc], ["low", "mid", "top", "out"])
+    else:
+        yb = lambda e: [0.0, g[f"Y_core_{e}"], g[f"Y_yoke_{e}"], g["lim_y"]]
+        yi, yf, ycell, yb1, yb2 = _axis(yb(1), yb(2), [lci, lci, lc], ["low", "top", "out"])
+    zb = [g["z_min"], Z1, Z2, g["z_max"]]
+    zi, zf, zcell, zb1, _ = _axis(zb, zb, [lc, lc, lc], ["front", "magnet", "back"])
+    zs = zb1[zi] + zf * (zb1[np.minimum(zi + 1, len(zb1) - 1)] - zb1[zi])
+    # cell materials
+    nx, ny, nz = len(xcell), len(ycell), len(zcell)
+    X, Y, Z = np.meshgrid(xcell, ycell, zcell, indexing="ij")
+    inside = Z == "magnet"
+    if use_diluted_steel:
+        iron = inside & ((X == "core") & (Y != "out") | (X == "void") & np.isin(Y, ["mid", "top"]) |
+                         (X == "leg") & (Y == "top"))
+        wing = inside & (X == "leg") & np.isin(Y, ["low", "mid"])
+    else:
+        iron = inside & (np.isin(X, ["core", "leg"]) & (Y != "out") | (X == "void") & (Y == "top"))
+        wing = np.zeros_like(iron)
+    dom = np.full((nx, ny, nz), M.TAG_AIR, dtype=np.int32)
+    dom[iron] = M.TAG_IRON
+    dom[wing] = TAG_WING
+    ref = M.tensor_grid_mesh(np.arange(nx + 1.0), np.arange(ny + 1.0), np.arange(nz + 1.0), dom)
+    # map the reference grid onto the template: x and y lines follow their planes along z
+    I = np.rint(ref.nodes[:, 0]).astype(np.int64)
+    J = np.rint(ref.nodes[:, 1]).astype(np.int64)
+    K = np.rint(ref.nodes[:, 2]).astype(np.int64)
+    z = zs[K]
+    t = np.clip((z - Z1) / (Z2 - Z1), 0.0, 1.0)
+
+    def along(b1, b2, iv, f):
+        lo = b1[iv] + t * (b2[iv] - b1[iv])
+        hi_i = np.minimum(iv + 1, len(b1) - 1)
+        hi = b1[hi_i] + t * (b2[hi_i] - b1[hi_i])
+        return lo + f * (hi - lo)
+
+    nodes = np.stack([along(xb1, xb2, xi[I], xf[I]), along(yb1, yb2, yi[J], yf[J]), z], axis=1)
+    msh = M.TetMesh(nodes, ref.cells, ref.elem_domain)
+    msh.natural_planes = [(1, 0.0)]
+    return msh
+
+
+def _coils(g, J_tar, filling_factor):
+    """The template's racetrack coils, turn positions and the coil's electrical figures
+    (``SHiP_functions.py:572-658``)."""
+    X_mgap_1, X_mgap_2 = g["X_mgap_1"], g["X_mgap_2"]
+    X_core_1, X_core_2 = g["X_core_1"], g["X_core_2"]
+    Z_pos, Z_len = g["Z_pos"], g["Z_len"]
+    sp, ins, r = g["yoke_spacer"], g["ins"], g["coil_radius"]
+    current = g["current"]
+    slot_size = 2 * min(g["Y_core_1"], g["Y_core_2"])
+    num_cond = min(int(slot_size / 2 / (r + ins)), int(g["max_turns"]))
+    if num_cond < 1:
+        raise ValueError("the slot holds no conductor")
+    y = np.linspace(-0.5 * slot_size + r + ins, 0.5 * slot_size - r - ins, num_cond)
+    slot_size_horz = min(g["X_void_1"] - X_core_1, g["X_void_2"] - X_core_2)
+    A_geo = slot_size_horz * slot_size
+    A_cu = abs(current) / J_tar
+    A_coil = A_cu / filling_factor
+    current_density = 0.0 if current == 0.0 else abs(current) / min(A_geo, A_coil) / filling_factor
+    d = sp + ins + r
+    if X_mgap_1 == 0.0 or X_mgap_2 == 0.0:
+        kp = np.array([[-X_core_2 - d, Z_pos + Z_len], [-X_core_2, Z_pos + Z_len + d], [X_core_2, Z_pos + Z_len + d],
+                       [X_core_2 + d, Z_pos + Z_len], [X_core_1 + d, Z_pos], [X_core_1, Z_pos - d],
+                       [-X_core_1, Z_pos - d], [-X_core_1 - d, Z_pos]])
+        coils = [RacetrackCoil(kp, y, r, current / num_cond)]
+    else:
+        kp_1 = np.array([[X_mgap_2 - d, Z_pos + Z_len + r], [X_mgap_2, Z_pos + Z_len + d], [X_core_2, Z_pos + Z_len + d],
+                         [X_core_2 + d, Z_pos + Z_len], [X_core_1 + d, Z_pos], [X_core_1, Z_pos - d],
+                         [X_mgap_1, Z_pos - d], [X_mgap_1 - d, Z_pos]])
+        kp_2 = kp_1.copy()
+        kp_2[:, 0] *= -1.0
+        coils = [RacetrackCoil(kp_1, y, r, current / num_cond), RacetrackCoil(kp_2, y, r, current / num_cond)]
+    perimeter = sum(c.get_length() for c in coils)
+    return coils, A_cu, A_coil, perimeter, current_density
+
+
+def get_vector_field_mag_1(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh=False, plot_geo=False,
+                           plot_result=False, result_directory="none", result_spec="", eval_pos=np.zeros((0, 3)),
+                           materials_directory="files/materials", quad_order=8, max_coil_size=0.05,
+                           use_diluted_steel=False, kappa_elec=5.0):
+    """B of SHiP magnet template 1 (``SHiP_functions.py:282-809``).
+
+    :return: ``[points, B, M_iron, M_coil, Q, current_density]``: the quadrature points of every
+        element (``field_density`` order) and the total field there, the iron mass in g (the
+        quarter model's iron volume x 4 x density), the coil mass in g, the ohmic power in W
+        and the coil's current density in A/m^2.  With ``eval_pos``, B there (nodal
+        interpolation per domain) is written to ``B<result_spec>.csv``.
+    """
+    from .evaluators import evaluate_fem_solution_node_interpolation
+    from .red_mvp_solver import RedMVPSolver
+    from .red_mvp_solver_diluted import RedMVPSolverDiluted
+
+    reluctance_iron = Reluctance(os.path.join(materials_directory, str(np.asarray(parameters["material"])[df_index])))
+    with open(os.path.join(materials_directory, str(np.asarray(parameters["material"])[df_index]))) as f:
+        iron_material_data = json.load(f)
+    with open(os.path.join(materials_directory, str(np.asarray(parameters["coil_material"])[df_index]))) as f:
+        conductor_material_data = json.load(f)
+    J_tar_mm2 = _value(parameters, "J_tar(A/mm2)", df_index)
+    J_tar = (compute_J_opt(conductor_material_data, kappa_elec) if J_tar_mm2 < 0 else J_tar_mm2) * 1e6
+
+    g = mag_1_parameters(parameters, df_index)
+    msh = mag_1_mesh(g, lc=lc, use_diluted_steel=use_diluted_steel)
+    vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
+    iron_tags = [M.TAG_IRON, TAG_WING] if use_diluted_steel else [M.TAG_IRON]
+    M_iron = 4 * float(vol[np.isin(msh.elem_domain, iron_tags)].sum()) * iron_material_data["density(g/m3)"]
+
+    coils, A_cu, A_coil, perimeter, current_density = _coils(g, J_tar, conductor_material_data["filling_factor"])
+    M_coil = A_cu * perimeter * conductor_material_data["density(g/m3)"]
+    current = g["current"]
+    Q = 0.0 if current == 0 else abs(current * current) * perimeter * conductor_material_data["resistivity(Ohm.m)"] / A_cu
+
+    if use_diluted_steel:
+        dilution_wing = Dilution(g["X_mgap_1"], g["X_core_1"], g["X_void_1"], g["X_yoke_1"], g["X_mgap_2"],
+                                 g["X_core_2"], g["X_void_2"], g["X_yoke_2"], g["Z_pos"], g["Z_len"])
+        solver = RedMVPSolverDiluted(msh, coils, iron_tags, [M.TAG_AIR], [reluctance_iron, reluctance_iron],
+                                     [None, dilution_wing], quad_order=quad_order, max_newton_iterations=25)
+    else:
+        solver = RedMVPSolver(msh, coils, iron_tags, [M.TAG_AIR], [reluctance_iron], quad_order=quad_order,
+                              max_newton_iterations=25)
+    solver.verbose = False
+    x = np.zeros(solver.num_dofs_mvp) if current == 0.0 else solver.solve()
+    points, B_i = solver.curl_curl_factory.compute_B(x, quad_order=int(0.5 * g["field_density"]))
+    B_coil = 0.0 * B_i
+    for coil in coils:
+        B_coil += coil.compute_B(points)
+    if result_directory != "none":
+        np.save(os.path.join(result_directory, "x" + result_spec + ".npy"), x)
+    ret_vals = [points, B_i + B_coil, M_iron, M_coil, Q, current_density]
+    eval_pos = np.asarray(eval_pos, dtype=np.float64).reshape(-1, 3)
+    if eval_pos.shape[0] > 0:
+        B_tot = evaluate_fem_solution_node_interpolation(msh, eval_pos, solver, coils, x, iron_tags + [M.TAG_AIR])
+        name = "B" + result_spec + ".csv"
+        out = os.path.join(result_directory, name) if result_directory != "none" else name
+        header = "x(m),y(m),z(m),Bx(T),By(T),Bz(T)"
+        np.savetxt(out, np.append(eval_pos, B_tot, axis=1), delimiter=",", header=header, comments="")
+    return ret_vals

@@ -1,0 +1,80 @@
+"""SHiP template 1 meshed without gmsh: the quarter model's geometry, materials, boundary and
+coils (CPU), checked against their definitions."""
+
+import numpy as np
+import pytest
+
+from snoopy_b200 import mesh as M
+from snoopy_b200 import ship
+
+
+def template_parameters(X_mgap=(0.0, 0.0)):
+    """One design of the template (its own numbers, in the SHiP table's columns)."""
+    return {"yoke_type": ["Mag1"], "coil_material": ["cu_test.json"], "max_turns": [10], "J_tar(A/mm2)": [3.0],
+            "NI(A)": [4000.0], "coil_diam(mm)": [9.0], "insulation(mm)": [0.5], "yoke_spacer(mm)": [5.0],
+            "material": ["iron_test.json"], "field_density": [4], "delta_x(m)": [0.4], "delta_y(m)": [0.4],
+            "delta_z(m)": [0.5], "Z_pos(m)": [-2.0], "Z_len(m)": [4.0], "Xmgap1(m)": [X_mgap[0]],
+            "Xcore1(m)": [0.25], "Xvoid1(m)": [0.31], "Xyoke1(m)": [1.2], "Xmgap2(m)": [X_mgap[1]],
+            "Xcore2(m)": [0.28], "Xvoid2(m)": [0.34], "Xyoke2(m)": [1.3], "Ycore1(m)": [0.2], "Yvoid1(m)": [0.2],
+            "Yyoke1(m)": [0.5], "Ycore2(m)": [0.3], "Yvoid2(m)": [0.3], "Yyoke2(m)": [0.6]}
+
+
+def _iron_area(g, t, diluted):
+    """Cross-section area of the quarter model's iron (and wing) at fraction t of the length."""
+    v = {k: g[k + "_1"] + t * (g[k + "_2"] - g[k + "_1"]) for k in ("X_mgap", "X_core", "X_void", "X_yoke",
+                                                                     "Y_core", "Y_void", "Y_yoke")}
+    outer = (v["X_yoke"] - v["X_mgap"]) * v["Y_yoke"]
+    void = (v["X_void"] - v["X_core"]) * v["Y_core"]
+    return outer - void, (v["X_yoke"] - v["X_void"]) * v["Y_void"] if diluted else 0.0
+
+
+@pytest.mark.parametrize("diluted", [False, True])
+@pytest.mark.parametrize("X_mgap", [(0.0, 0.0), (0.05, 0.08)])
+def test_template_mesh_volumes_and_boundary(diluted, X_mgap):
+    g = ship.mag_1_parameters(template_parameters(X_mgap))
+    msh = ship.mag_1_mesh(g, lc=0.5, use_diluted_steel=diluted)
+    vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
+    assert (vol > 0).all()
+    box = (g["lim_x"] * g["lim_y"] * (g["z_max"] - g["z_min"]))
+    assert abs(vol.sum() - box) < 1e-9 * box
+    # planar boundaries: the tetrahedra fill the iron exactly; the area is quadratic in z (Simpson)
+    a = [_iron_area(g, t, diluted) for t in (0.0, 0.5, 1.0)]
+    iron = g["Z_len"] * (a[0][0] + 4 * a[1][0] + a[2][0]) / 6.0
+    wing = g["Z_len"] * (a[0][1] + 4 * a[1][1] + a[2][1]) / 6.0
+    if diluted:
+        iron -= wing  # the wing is cut out of the outer leg
+    got_iron = vol[msh.elem_domain == M.TAG_IRON].sum()
+    got_wing = vol[msh.elem_domain == ship.TAG_WING].sum()
+    assert abs(got_iron - iron) < 1e-9 * iron and abs(got_wing - wing) < 1e-9 * max(wing, 1.0)
+    # y = 0 is the symmetry plane: no Dirichlet edge lies in it unless it also bounds another face
+    d = msh.dirichlet_edge_ids()
+    b = msh.boundary_edge_ids()
+    on_plane = np.all(np.abs(msh.nodes[msh.edges[:, :]][:, :, 1]) < 1e-12, axis=1)
+    inner_plane = np.setdiff1d(np.flatnonzero(on_plane), np.flatnonzero(np.any(
+        (np.abs(msh.nodes[msh.edges][:, :, 0]) < 1e-12) | (np.abs(msh.nodes[msh.edges][:, :, 0] - g["lim_x"]) < 1e-12) |
+        (np.abs(msh.nodes[msh.edges][:, :, 2] - g["z_min"]) < 1e-12) |
+        (np.abs(msh.nodes[msh.edges][:, :, 2] - g["z_max"]) < 1e-12), axis=1) & on_plane))
+    assert len(inner_plane) > 0 and not np.isin(inner_plane, d).any() and np.isin(inner_plane, b).all()
+    assert len(d) < len(b)
+
+
+def test_template_coils():
+    for X_mgap, n_coils in (((0.0, 0.0), 1), ((0.05, 0.08), 2)):
+        g = ship.mag_1_parameters(template_parameters(X_mgap))
+        coils, A_cu, A_coil, perimeter, J = ship._coils(g, 3e6, 0.6)
+        assert len(coils) == n_coils
+        assert abs(A_cu - 4000.0 / 3e6) < 1e-15 and abs(A_coil - A_cu / 0.6) < 1e-15
+        slot = 2 * 0.2
+        n = min(int(slot / 2 / (4.5e-3 + 0.5e-3)), 10)
+        assert all(len(c.y) == n for c in coils)
+        assert abs(perimeter - sum(c.get_length() for c in coils)) < 1e-12
+        # the turns wrap the core: straight parts just outside the core's z ends
+        seg = coils[0].get_segments()
+        assert seg[:, 2].min() < g["Z_pos"] and seg[:, 2].max() > g["Z_pos"] + g["Z_len"]
+
+
+def test_compute_J_opt():
+    d = {"material_cost(CHF/kg)": 20.0, "manufacturing_cost(CHF/kg)": 80.0, "density(g/m3)": 8.9e6,
+         "resistivity(Ohm.m)": 1.7e-8}
+    J = ship.compute_J_opt(d, 5.0)
+    assert abs(J - np.sqrt(100.0 * 8.9e3 / 5.0 / 1.7e-8) * 1e-6) < 1e-12 * J
