@@ -1,9 +1,11 @@
-"""SHiP magnet template 1 without gmsh (``snoopy/SHiP_functions.py:282-809``).
+"""SHiP magnet templates 1 and 3 without gmsh (``snoopy/SHiP_functions.py:282-809, 1218-1711``).
 
-``get_vector_field_mag_1`` keeps the reference driver's arguments, flow and return values:
+``get_vector_field_mag_1`` and ``get_vector_field_mag_3`` keep the reference drivers' arguments,
+flow and return values:
 the template's iron (``geometry_tools.py:133-392``, or with ``use_diluted_steel`` the core plus
 a diluted return-yoke wing, ``geometry_tools.py:601-805``) in an air box, the racetrack
-filament coil(s) around the core, the reduced-potential Newton solve (``RedMVPSolver`` or
+filament coil(s) around the core (template 1) or the return-yoke legs (template 3), the
+reduced-potential Newton solve (``RedMVPSolver`` or
 ``RedMVPSolverDiluted``), B = curl A_r + B_coil at the quadrature points of every element,
 optionally B at extra positions by nodal interpolation, and the iron mass, coil mass, power
 and current density of the design.
@@ -95,9 +97,10 @@ def _axis(breaks_1, breaks_2, spacing, names):
     return np.array(line_iv), np.array(line_f), cell_names, np.array(b1), np.array(b2)
 
 
-def mag_1_mesh(g, lc=0.2, use_diluted_steel=False):
-    """Quarter-model tetrahedral mesh of template 1 (tags: iron 1, air 2, diluted wing 5)."""
-    lci = 0.2 * lc
+def mag_1_mesh(g, lc=0.2, use_diluted_steel=False, inner=0.2):
+    """Quarter-model tetrahedral mesh of templates 1 and 3 (one iron geometry; tags: iron 1,
+    air 2, diluted wing 5); ``inner`` x ``lc`` is the spacing across the iron."""
+    lci = inner * lc
     Z1, Z2 = g["Z_pos"], g["Z_pos"] + g["Z_len"]
     xb = lambda e: [0.0, g[f"X_mgap_{e}"], g[f"X_core_{e}"], g[f"X_void_{e}"], g[f"X_yoke_{e}"], g["lim_x"]]
     xi, xf, xcell, xb1, xb2 = _axis(xb(1), xb(2), [lci, lci, lci, lci, lc], ["gap", "core", "void", "leg", "out"])
@@ -144,9 +147,10 @@ def mag_1_mesh(g, lc=0.2, use_diluted_steel=False):
     return msh
 
 
-def _coils(g, J_tar, filling_factor):
+def _coils(g, J_tar, filling_factor, template=1):
     """The template's racetrack coils, turn positions and the coil's electrical figures
-    (``SHiP_functions.py:572-658``)."""
+    (template 1: around the core, ``SHiP_functions.py:572-658``; template 3: around the
+    return-yoke legs, ``SHiP_functions.py:1505-1562``)."""
     X_mgap_1, X_mgap_2 = g["X_mgap_1"], g["X_mgap_2"]
     X_core_1, X_core_2 = g["X_core_1"], g["X_core_2"]
     Z_pos, Z_len = g["Z_pos"], g["Z_len"]
@@ -163,7 +167,15 @@ def _coils(g, J_tar, filling_factor):
     A_coil = A_cu / filling_factor
     current_density = 0.0 if current == 0.0 else abs(current) / min(A_geo, A_coil) / filling_factor
     d = sp + ins + r
-    if X_mgap_1 == 0.0 or X_mgap_2 == 0.0:
+    if template == 3:
+        X_void_1, X_void_2, X_yoke_1, X_yoke_2 = g["X_void_1"], g["X_void_2"], g["X_yoke_1"], g["X_yoke_2"]
+        kp_1 = np.array([[X_void_2 - d, Z_pos + Z_len], [X_void_2, Z_pos + Z_len + d], [X_yoke_2, Z_pos + Z_len + d],
+                         [X_yoke_2 + d, Z_pos + Z_len], [X_yoke_1 + d, Z_pos], [X_yoke_1, Z_pos - d],
+                         [X_void_1, Z_pos - d], [X_void_1 - d, Z_pos]])
+        kp_2 = kp_1.copy()
+        kp_2[:, 0] *= -1.0
+        coils = [RacetrackCoil(kp_1, y, r, current / num_cond), RacetrackCoil(kp_2, y, r, current / num_cond)]
+    elif X_mgap_1 == 0.0 or X_mgap_2 == 0.0:
         kp = np.array([[-X_core_2 - d, Z_pos + Z_len], [-X_core_2, Z_pos + Z_len + d], [X_core_2, Z_pos + Z_len + d],
                        [X_core_2 + d, Z_pos + Z_len], [X_core_1 + d, Z_pos], [X_core_1, Z_pos - d],
                        [-X_core_1, Z_pos - d], [-X_core_1 - d, Z_pos]])
@@ -183,7 +195,25 @@ def get_vector_field_mag_1(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh
                            plot_result=False, result_directory="none", result_spec="", eval_pos=np.zeros((0, 3)),
                            materials_directory="files/materials", quad_order=8, max_coil_size=0.05,
                            use_diluted_steel=False, kappa_elec=5.0):
-    """B of SHiP magnet template 1 (``SHiP_functions.py:282-809``).
+    """B of SHiP magnet template 1 (``SHiP_functions.py:282-809``): coil around the core; see
+    ``_template`` for the return values."""
+    return _template(1, parameters, df_index, lc, result_directory, result_spec, eval_pos, materials_directory,
+                     quad_order, use_diluted_steel, kappa_elec)
+
+
+def get_vector_field_mag_3(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh=False, plot_geo=False,
+                           plot_result=False, result_directory="none", result_spec="", eval_pos=np.zeros((0, 3)),
+                           materials_directory="files/materials", quad_order=8, max_coil_size=0.05,
+                           use_diluted_steel=False, kappa_elec=5.0):
+    """B of SHiP magnet template 3 (``SHiP_functions.py:1218-1711``): template 1's iron (and
+    diluted wing), coils around the return-yoke legs."""
+    return _template(3, parameters, df_index, lc, result_directory, result_spec, eval_pos, materials_directory,
+                     quad_order, use_diluted_steel, kappa_elec)
+
+
+def _template(template, parameters, df_index, lc, result_directory, result_spec, eval_pos, materials_directory,
+              quad_order, use_diluted_steel, kappa_elec):
+    """Templates 1 and 3.
 
     :return: ``[points, B, M_iron, M_coil, Q, current_density]``: the quadrature points of every
         element (``field_density`` order) and the total field there, the iron mass in g (the
@@ -204,12 +234,15 @@ def get_vector_field_mag_1(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh
     J_tar = (compute_J_opt(conductor_material_data, kappa_elec) if J_tar_mm2 < 0 else J_tar_mm2) * 1e6
 
     g = mag_1_parameters(parameters, df_index)
-    msh = mag_1_mesh(g, lc=lc, use_diluted_steel=use_diluted_steel)
+    # iron spacing: 0.2 lc, except for template 3's plain yoke (0.3 lc, SHiP_functions.py:1435)
+    inner = 0.3 if (template == 3 and not use_diluted_steel) else 0.2
+    msh = mag_1_mesh(g, lc=lc, use_diluted_steel=use_diluted_steel, inner=inner)
     vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
     iron_tags = [M.TAG_IRON, TAG_WING] if use_diluted_steel else [M.TAG_IRON]
     M_iron = 4 * float(vol[np.isin(msh.elem_domain, iron_tags)].sum()) * iron_material_data["density(g/m3)"]
 
-    coils, A_cu, A_coil, perimeter, current_density = _coils(g, J_tar, conductor_material_data["filling_factor"])
+    coils, A_cu, A_coil, perimeter, current_density = _coils(g, J_tar, conductor_material_data["filling_factor"],
+                                                             template)
     M_coil = A_cu * perimeter * conductor_material_data["density(g/m3)"]
     current = g["current"]
     Q = 0.0 if current == 0 else abs(current * current) * perimeter * conductor_material_data["resistivity(Ohm.m)"] / A_cu

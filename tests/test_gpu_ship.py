@@ -50,3 +50,15 @@ def test_template_1_plain_and_diluted(materials_dir, tmp_path):
         out[diluted] = Be[:, 3:]
     # the diluted wing changes the field
     assert np.abs(out[True] - out[False]).max() > 1e-3 * np.abs(out[False]).max()
+
+
+def test_template_3(materials_dir, tmp_path):
+    P = template_parameters()
+    probes = np.array([[0.12, 0.1, 0.0], [0.8, 0.1, 0.0]])
+    pts, B, M_iron, M_coil, Q, J = ship.get_vector_field_mag_3(P, lc=0.4, eval_pos=probes, quad_order=2,
+                                                               materials_directory=materials_dir,
+                                                               result_directory=str(tmp_path), result_spec="_m3")
+    assert np.isfinite(B).all() and M_coil > 0 and Q > 0
+    Be = np.loadtxt(tmp_path / "B_m3.csv", delimiter=",", skiprows=1)[:, 3:]
+    # the coils sit around the legs: both the core and the leg carry flux along y
+    assert abs(Be[0, 1]) > 0.05 and abs(Be[1, 1]) > 0.05

@@ -73,6 +73,19 @@ def test_template_coils():
         assert seg[:, 2].min() < g["Z_pos"] and seg[:, 2].max() > g["Z_pos"] + g["Z_len"]
 
 
+def test_template_3_coils_wrap_the_legs():
+    g = ship.mag_1_parameters(template_parameters())
+    coils, _, _, perimeter, _ = ship._coils(g, 3e6, 0.6, template=3)
+    assert len(coils) == 2
+    d = 5e-3 + 0.5e-3 + 4.5e-3
+    seg = coils[0].get_segments()
+    xs = np.concatenate([seg[:, 0], seg[:, 3]])
+    assert xs.min() >= min(g["X_void_1"], g["X_void_2"]) - d - 1e-12
+    assert xs.max() <= max(g["X_yoke_1"], g["X_yoke_2"]) + d + 1e-12
+    seg2 = coils[1].get_segments()
+    assert np.allclose(seg2[:, [0, 3]], -seg[:, [0, 3]]) and np.allclose(seg2[:, [1, 2, 4, 5]], seg[:, [1, 2, 4, 5]])
+
+
 def test_compute_J_opt():
     d = {"material_cost(CHF/kg)": 20.0, "manufacturing_cost(CHF/kg)": 80.0, "density(g/m3)": 8.9e6,
          "resistivity(Ohm.m)": 1.7e-8}
