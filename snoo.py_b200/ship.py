@@ -1,6 +1,6 @@
-"""SHiP magnet templates 1 and 3 without gmsh (``snoopy/SHiP_functions.py:282-809, 1218-1711``).
+"""SHiP magnet templates 1, 2 and 3 without gmsh (``snoopy/SHiP_functions.py:282-1711``).
 
-``get_vector_field_mag_1`` and ``get_vector_field_mag_3`` keep the reference drivers' arguments,
+``get_vector_field_mag_1``, ``_mag_2`` and ``_mag_3`` keep the reference drivers' arguments,
 flow and return values:
 the template's iron (``geometry_tools.py:133-392``, or with ``use_diluted_steel`` the core plus
 a diluted return-yoke wing, ``geometry_tools.py:601-805``) in an air box, the racetrack
@@ -51,8 +51,10 @@ def mag_1_parameters(parameters, df_index=0):
              "Y_void": "Yvoid", "Y_yoke": "Yyoke"}
     g = {}
     for key, col in names.items():
-        g[key + "_1"] = _value(parameters, f"{col}1(m)", df_index)
-        g[key + "_2"] = _value(parameters, f"{col}2(m)", df_index)
+        for e in (1, 2):
+            name = f"{col}{e}(m)"
+            # template 2's table has no magnet gap: its core starts at x = 0
+            g[f"{key}_{e}"] = _value(parameters, name, df_index) if (key != "X_mgap" or name in parameters) else 0.0
     for key, col in (("Z_len", "Z_len(m)"), ("Z_pos", "Z_pos(m)"), ("delta_x", "delta_x(m)"),
                      ("delta_y", "delta_y(m)"), ("delta_z", "delta_z(m)"), ("current", "NI(A)"),
                      ("field_density", "field_density"), ("max_turns", "max_turns")):
@@ -100,8 +102,25 @@ def _axis(breaks_1, breaks_2, spacing, names):
 def mag_1_mesh(g, lc=0.2, use_diluted_steel=False, inner=0.2):
     """Quarter-model tetrahedral mesh of templates 1 and 3 (one iron geometry; tags: iron 1,
     air 2, diluted wing 5); ``inner`` x ``lc`` is the spacing across the iron."""
+    return template_mesh(g, 1, lc, use_diluted_steel, inner)
+
+
+def template_mesh(g, template=1, lc=0.2, use_diluted_steel=False, inner=0.2):
+    """Quarter-model tetrahedral mesh of a template (tags: iron 1, air 2, diluted wing 5).
+
+    Templates 1 and 3 (``geometry_tools.py:213-259``): core [X_mgap, X_core] x [0, Y_yoke],
+    top [X_core, X_void] x [Y_core, Y_yoke] and leg [X_void, X_yoke] x [0, Y_yoke]; with the
+    diluted wing (``geometry_tools.py:601-805``) the leg below Y_void is the wing.  Template 2
+    (``geometry_tools.py:392-500, 305-345``): core [0, X_core] x [0, Y_core], yoke
+    [0, X_yoke] x [Y_void, Y_yoke] and leg [X_void, X_yoke] x [0, Y_void]."""
     lci = inner * lc
     Z1, Z2 = g["Z_pos"], g["Z_pos"] + g["Z_len"]
+    if template == 2:
+        xb = lambda e: [0.0, g[f"X_core_{e}"], g[f"X_void_{e}"], g[f"X_yoke_{e}"], g["lim_x"]]
+        xi, xf, xcell, xb1, xb2 = _axis(xb(1), xb(2), [lci, lci, lci, lc], ["core", "void", "leg", "out"])
+        yb = lambda e: [0.0, g[f"Y_core_{e}"], g[f"Y_void_{e}"], g[f"Y_yoke_{e}"], g["lim_y"]]
+        yi, yf, ycell, yb1, yb2 = _axis(yb(1), yb(2), [lci, lci, lci, lc], ["low", "mid", "top", "out"])
+        return _finish(g, lc, xi, xf, xcell, xb1, xb2, yi, yf, ycell, yb1, yb2, template, use_diluted_steel)
     xb = lambda e: [0.0, g[f"X_mgap_{e}"], g[f"X_core_{e}"], g[f"X_void_{e}"], g[f"X_yoke_{e}"], g["lim_x"]]
     xi, xf, xcell, xb1, xb2 = _axis(xb(1), xb(2), [lci, lci, lci, lci, lc], ["gap", "core", "void", "leg", "out"])
     if use_diluted_steel:
@@ -110,6 +129,12 @@ def mag_1_mesh(g, lc=0.2, use_diluted_steel=False, inner=0.2):
     else:
         yb = lambda e: [0.0, g[f"Y_core_{e}"], g[f"Y_yoke_{e}"], g["lim_y"]]
         yi, yf, ycell, yb1, yb2 = _axis(yb(1), yb(2), [lci, lci, lc], ["low", "top", "out"])
+    return _finish(g, lc, xi, xf, xcell, xb1, xb2, yi, yf, ycell, yb1, yb2, template, use_diluted_steel)
+
+
+def _finish(g, lc, xi, xf, xcell, xb1, xb2, yi, yf, ycell, yb1, yb2, template, use_diluted_steel):
+    """z lines, cell materials and the mapped nodes of a template mesh."""
+    Z1, Z2 = g["Z_pos"], g["Z_pos"] + g["Z_len"]
     zb = [g["z_min"], Z1, Z2, g["z_max"]]
     zi, zf, zcell, zb1, _ = _axis(zb, zb, [lc, lc, lc], ["front", "magnet", "back"])
     zs = zb1[zi] + zf * (zb1[np.minimum(zi + 1, len(zb1) - 1)] - zb1[zi])
@@ -117,7 +142,11 @@ def mag_1_mesh(g, lc=0.2, use_diluted_steel=False, inner=0.2):
     nx, ny, nz = len(xcell), len(ycell), len(zcell)
     X, Y, Z = np.meshgrid(xcell, ycell, zcell, indexing="ij")
     inside = Z == "magnet"
-    if use_diluted_steel:
+    if template == 2:
+        iron = inside & ((X == "core") & (Y == "low") | (Y == "top") & (X != "out") |
+                         (X == "leg") & (Y != "out"))
+        wing = np.zeros_like(iron)
+    elif use_diluted_steel:
         iron = inside & ((X == "core") & (Y != "out") | (X == "void") & np.isin(Y, ["mid", "top"]) |
                          (X == "leg") & (Y == "top"))
         wing = inside & (X == "leg") & np.isin(Y, ["low", "mid"])
@@ -167,6 +196,8 @@ def _coils(g, J_tar, filling_factor, template=1):
     A_coil = A_cu / filling_factor
     current_density = 0.0 if current == 0.0 else abs(current) / min(A_geo, A_coil) / filling_factor
     d = sp + ins + r
+    if template == 2:
+        X_mgap_1 = X_mgap_2 = 0.0  # one coil around the core
     if template == 3:
         X_void_1, X_void_2, X_yoke_1, X_yoke_2 = g["X_void_1"], g["X_void_2"], g["X_yoke_1"], g["X_yoke_2"]
         kp_1 = np.array([[X_void_2 - d, Z_pos + Z_len], [X_void_2, Z_pos + Z_len + d], [X_yoke_2, Z_pos + Z_len + d],
@@ -211,6 +242,15 @@ def get_vector_field_mag_3(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh
                      quad_order, use_diluted_steel, kappa_elec)
 
 
+def get_vector_field_mag_2(parameters, df_index=0, lc=0.4, geo_th=1e-5, run_gmsh=False, plot_geo=False,
+                           plot_result=False, result_directory="none", result_spec="", eval_pos=np.zeros((0, 3)),
+                           materials_directory="files/materials", quad_order=8, max_coil_size=0.05, kappa_elec=5.0):
+    """B of SHiP magnet template 2, the superconducting one (``SHiP_functions.py:812-1217``):
+    an iron core [0, X_core] x [0, Y_core] inside an L-shaped yoke, one coil around the core."""
+    return _template(2, parameters, df_index, lc, result_directory, result_spec, eval_pos, materials_directory,
+                     quad_order, False, kappa_elec)
+
+
 def _template(template, parameters, df_index, lc, result_directory, result_spec, eval_pos, materials_directory,
               quad_order, use_diluted_steel, kappa_elec):
     """Templates 1 and 3.
@@ -234,9 +274,10 @@ def _template(template, parameters, df_index, lc, result_directory, result_spec,
     J_tar = (compute_J_opt(conductor_material_data, kappa_elec) if J_tar_mm2 < 0 else J_tar_mm2) * 1e6
 
     g = mag_1_parameters(parameters, df_index)
-    # iron spacing: 0.2 lc, except for template 3's plain yoke (0.3 lc, SHiP_functions.py:1435)
-    inner = 0.3 if (template == 3 and not use_diluted_steel) else 0.2
-    msh = mag_1_mesh(g, lc=lc, use_diluted_steel=use_diluted_steel, inner=inner)
+    # iron spacing: 0.2 lc, except 0.3 lc for template 2 and template 3's plain yoke
+    # (SHiP_functions.py:944-969, 1435)
+    inner = 0.3 if (template == 2 or (template == 3 and not use_diluted_steel)) else 0.2
+    msh = template_mesh(g, template, lc=lc, use_diluted_steel=use_diluted_steel, inner=inner)
     vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
     iron_tags = [M.TAG_IRON, TAG_WING] if use_diluted_steel else [M.TAG_IRON]
     M_iron = 4 * float(vol[np.isin(msh.elem_domain, iron_tags)].sum()) * iron_material_data["density(g/m3)"]
@@ -263,6 +304,9 @@ def _template(template, parameters, df_index, lc, result_directory, result_spec,
         B_coil += coil.compute_B(points)
     if result_directory != "none":
         np.save(os.path.join(result_directory, "x" + result_spec + ".npy"), x)
+        row = {k: np.asarray(v)[df_index] for k, v in dict(parameters).items()}
+        with open(os.path.join(result_directory, "parameters" + result_spec + ".csv"), "w") as f:
+            f.write(",".join(row) + "\n" + ",".join(str(v) for v in row.values()) + "\n")
     ret_vals = [points, B_i + B_coil, M_iron, M_coil, Q, current_density]
     eval_pos = np.asarray(eval_pos, dtype=np.float64).reshape(-1, 3)
     if eval_pos.shape[0] > 0:

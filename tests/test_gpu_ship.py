@@ -62,3 +62,18 @@ def test_template_3(materials_dir, tmp_path):
     Be = np.loadtxt(tmp_path / "B_m3.csv", delimiter=",", skiprows=1)[:, 3:]
     # the coils sit around the legs: both the core and the leg carry flux along y
     assert abs(Be[0, 1]) > 0.05 and abs(Be[1, 1]) > 0.05
+
+
+def test_template_2(materials_dir, tmp_path):
+    P = template_parameters()
+    for k in ("Xmgap1(m)", "Xmgap2(m)"):
+        del P[k]
+    P["Yvoid1(m)"], P["Yvoid2(m)"] = [0.25], [0.35]
+    probes = np.array([[0.12, 0.1, 0.0]])
+    pts, B, M_iron, M_coil, Q, J = ship.get_vector_field_mag_2(P, lc=0.4, eval_pos=probes, quad_order=2,
+                                                               materials_directory=materials_dir,
+                                                               result_directory=str(tmp_path), result_spec="_m2")
+    assert np.isfinite(B).all() and M_iron > 0 and M_coil > 0
+    Be = np.atleast_2d(np.loadtxt(tmp_path / "B_m2.csv", delimiter=",", skiprows=1))[0, 3:]
+    assert abs(Be[1]) > 5 * max(abs(Be[0]), abs(Be[2]))  # core field along y
+    assert (tmp_path / "parameters_m2.csv").exists()

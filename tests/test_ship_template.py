@@ -58,6 +58,28 @@ def test_template_mesh_volumes_and_boundary(diluted, X_mgap):
     assert len(d) < len(b)
 
 
+def test_template_2_mesh():
+    P = template_parameters()
+    for k in ("Xmgap1(m)", "Xmgap2(m)"):
+        del P[k]
+    P["Yvoid1(m)"], P["Yvoid2(m)"] = [0.25], [0.35]
+    g = ship.mag_1_parameters(P)
+    assert g["X_mgap_1"] == 0.0 and g["X_mgap_2"] == 0.0
+    msh = ship.template_mesh(g, 2, lc=0.5, inner=0.3)
+    vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
+    assert (vol > 0).all()
+
+    def area(t):
+        v = {k: g[k + "_1"] + t * (g[k + "_2"] - g[k + "_1"]) for k in ("X_core", "X_void", "X_yoke", "Y_core",
+                                                                         "Y_void", "Y_yoke")}
+        return (v["X_core"] * v["Y_core"] + v["X_yoke"] * (v["Y_yoke"] - v["Y_void"])
+                + (v["X_yoke"] - v["X_void"]) * v["Y_void"])
+
+    iron = g["Z_len"] * (area(0.0) + 4 * area(0.5) + area(1.0)) / 6.0
+    got = vol[msh.elem_domain == M.TAG_IRON].sum()
+    assert abs(got - iron) < 1e-9 * iron
+
+
 def test_template_coils():
     for X_mgap, n_coils in (((0.0, 0.0), 1), ((0.05, 0.08), 2)):
         g = ship.mag_1_parameters(template_parameters(X_mgap))
