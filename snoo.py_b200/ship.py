@@ -1,6 +1,6 @@
-"""SHiP magnet templates 1, 2 and 3 without gmsh (``snoopy/SHiP_functions.py:282-1711``).
+"""SHiP magnet templates 1 to 4 without gmsh (``snoopy/SHiP_functions.py:282-2138``).
 
-``get_vector_field_mag_1``, ``_mag_2`` and ``_mag_3`` keep the reference drivers' arguments,
+``get_vector_field_mag_1`` to ``_mag_4`` keep the reference drivers' arguments,
 flow and return values:
 the template's iron (``geometry_tools.py:133-392``, or with ``use_diluted_steel`` the core plus
 a diluted return-yoke wing, ``geometry_tools.py:601-805``) in an air box, the racetrack
@@ -29,7 +29,8 @@ from . import mesh as M
 from .materials import Dilution, Reluctance
 from .racetrack_coil import RacetrackCoil
 
-TAG_WING = 5  # the diluted return-yoke wing
+TAG_WING = 5  # the diluted return-yoke wing (templates 1 and 3)
+TAG_YOKE = 6  # template 4's yoke (its core carries tag 1, the dilutable part)
 
 
 def compute_J_opt(conductor_material_data, kappa_elec):
@@ -66,6 +67,22 @@ def mag_1_parameters(parameters, df_index=0):
     g["lim_y"] = max(g["Y_yoke_1"], g["Y_yoke_2"]) + g["delta_y"]
     g["z_min"] = g["Z_pos"] - g["delta_z"]
     g["z_max"] = g["Z_pos"] + g["Z_len"] + g["delta_z"]
+    return g
+
+
+def mag_4_parameters(parameters, df_index=0):
+    """Template 4's parameters: its six x boundaries X_A..X_F come from two table rows
+    (``SHiP_functions.py:1800-1815``): X_A, X_B, X_C = Xmgap, Xcore, Xvoid of row df_index and
+    X_D, X_E, X_F = Xcore, Xvoid, Xyoke of row df_index + 1."""
+    g = mag_1_parameters(parameters, df_index)
+    for e in (1, 2):
+        g[f"X_A_{e}"] = _value(parameters, f"Xmgap{e}(m)", df_index)
+        g[f"X_B_{e}"] = _value(parameters, f"Xcore{e}(m)", df_index)
+        g[f"X_C_{e}"] = _value(parameters, f"Xvoid{e}(m)", df_index)
+        g[f"X_D_{e}"] = _value(parameters, f"Xcore{e}(m)", df_index + 1)
+        g[f"X_E_{e}"] = _value(parameters, f"Xvoid{e}(m)", df_index + 1)
+        g[f"X_F_{e}"] = _value(parameters, f"Xyoke{e}(m)", df_index + 1)
+    g["lim_x"] = max(g["X_F_1"], g["X_F_2"]) + g["delta_x"]
     return g
 
 
@@ -115,6 +132,13 @@ def template_mesh(g, template=1, lc=0.2, use_diluted_steel=False, inner=0.2):
     [0, X_yoke] x [Y_void, Y_yoke] and leg [X_void, X_yoke] x [0, Y_void]."""
     lci = inner * lc
     Z1, Z2 = g["Z_pos"], g["Z_pos"] + g["Z_len"]
+    if template == 4:
+        xb = lambda e: [0.0] + [g[f"X_{c}_{e}"] for c in "ABCDEF"] + [g["lim_x"]]
+        xi, xf, xcell, xb1, xb2 = _axis(xb(1), xb(2), [lci] * 6 + [lc],
+                                        ["gap", "legA", "slot1", "core", "slot2", "legF", "out"])
+        yb = lambda e: [0.0, g[f"Y_core_{e}"], g[f"Y_yoke_{e}"], g["lim_y"]]
+        yi, yf, ycell, yb1, yb2 = _axis(yb(1), yb(2), [lci, lci, lc], ["low", "top", "out"])
+        return _finish(g, lc, xi, xf, xcell, xb1, xb2, yi, yf, ycell, yb1, yb2, template, use_diluted_steel)
     if template == 2:
         xb = lambda e: [0.0, g[f"X_core_{e}"], g[f"X_void_{e}"], g[f"X_yoke_{e}"], g["lim_x"]]
         xi, xf, xcell, xb1, xb2 = _axis(xb(1), xb(2), [lci, lci, lci, lc], ["core", "void", "leg", "out"])
@@ -142,6 +166,15 @@ def _finish(g, lc, xi, xf, xcell, xb1, xb2, yi, yf, ycell, yb1, yb2, template, u
     nx, ny, nz = len(xcell), len(ycell), len(zcell)
     X, Y, Z = np.meshgrid(xcell, ycell, zcell, indexing="ij")
     inside = Z == "magnet"
+    if template == 4:
+        # core [X_C, X_D] x [0, Y_core]; yoke [X_A, X_F] x [0, Y_yoke] without [X_B, X_E] x [0, Y_core]
+        iron = inside & (X == "core") & (Y == "low")
+        wing = inside & (np.isin(X, ["legA", "legF"]) & (Y != "out") |
+                         np.isin(X, ["slot1", "core", "slot2"]) & (Y == "top"))
+        dom = np.full((nx, ny, nz), M.TAG_AIR, dtype=np.int32)
+        dom[iron] = M.TAG_IRON
+        dom[wing] = TAG_YOKE
+        return _mapped(g, xi, xf, xb1, xb2, yi, yf, yb1, yb2, zs, nx, ny, nz, dom)
     if template == 2:
         iron = inside & ((X == "core") & (Y == "low") | (Y == "top") & (X != "out") |
                          (X == "leg") & (Y != "out"))
@@ -156,6 +189,12 @@ def _finish(g, lc, xi, xf, xcell, xb1, xb2, yi, yf, ycell, yb1, yb2, template, u
     dom = np.full((nx, ny, nz), M.TAG_AIR, dtype=np.int32)
     dom[iron] = M.TAG_IRON
     dom[wing] = TAG_WING
+    return _mapped(g, xi, xf, xb1, xb2, yi, yf, yb1, yb2, zs, nx, ny, nz, dom)
+
+
+def _mapped(g, xi, xf, xb1, xb2, yi, yf, yb1, yb2, zs, nx, ny, nz, dom):
+    """Split the reference grid into tetrahedra and move its nodes onto the template."""
+    Z1, Z2 = g["Z_pos"], g["Z_pos"] + g["Z_len"]
     ref = M.tensor_grid_mesh(np.arange(nx + 1.0), np.arange(ny + 1.0), np.arange(nz + 1.0), dom)
     # map the reference grid onto the template: x and y lines follow their planes along z
     I = np.rint(ref.nodes[:, 0]).astype(np.int64)
@@ -198,7 +237,20 @@ def _coils(g, J_tar, filling_factor, template=1):
     d = sp + ins + r
     if template == 2:
         X_mgap_1 = X_mgap_2 = 0.0  # one coil around the core
-    if template == 3:
+    if template == 4:
+        # slots on both sides of the core (SHiP_functions.py:1975-1976)
+        slot_size_horz = min(g["X_C_1"] - g["X_B_1"], g["X_C_2"] - g["X_B_2"], g["X_E_1"] - g["X_D_1"],
+                             g["X_E_2"] - g["X_D_2"])
+        A_geo = slot_size_horz * slot_size
+        current_density = 0.0 if current == 0.0 else abs(current) / min(A_geo, A_coil) / filling_factor
+        X_C_1, X_C_2, X_D_1, X_D_2 = g["X_C_1"], g["X_C_2"], g["X_D_1"], g["X_D_2"]
+        kp_1 = np.array([[X_C_2 - d, Z_pos + Z_len], [X_C_2, Z_pos + Z_len + d], [X_D_2, Z_pos + Z_len + d],
+                         [X_D_2 + d, Z_pos + Z_len], [X_D_1 + d, Z_pos], [X_D_1, Z_pos - d],
+                         [X_C_1, Z_pos - d], [X_C_1 - d, Z_pos]])
+        kp_2 = kp_1.copy()
+        kp_2[:, 0] *= -1.0
+        coils = [RacetrackCoil(kp_1, y, r, current / num_cond), RacetrackCoil(kp_2, y, r, current / num_cond)]
+    elif template == 3:
         X_void_1, X_void_2, X_yoke_1, X_yoke_2 = g["X_void_1"], g["X_void_2"], g["X_yoke_1"], g["X_yoke_2"]
         kp_1 = np.array([[X_void_2 - d, Z_pos + Z_len], [X_void_2, Z_pos + Z_len + d], [X_yoke_2, Z_pos + Z_len + d],
                          [X_yoke_2 + d, Z_pos + Z_len], [X_yoke_1 + d, Z_pos], [X_yoke_1, Z_pos - d],
@@ -242,6 +294,17 @@ def get_vector_field_mag_3(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh
                      quad_order, use_diluted_steel, kappa_elec)
 
 
+def get_vector_field_mag_4(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh=False, plot_geo=False,
+                           plot_result=False, result_directory="none", result_spec="", eval_pos=np.zeros((0, 3)),
+                           materials_directory="files/materials", quad_order=8, max_coil_size=0.05,
+                           use_diluted_steel=False, kappa_elec=5.0):
+    """B of SHiP magnet template 4 (``SHiP_functions.py:1712-2138``): a core [X_C, X_D] between
+    the two legs of a yoke (its boundaries from rows df_index and df_index + 1, see
+    ``mag_4_parameters``), coils around the core; ``use_diluted_steel`` dilutes the core."""
+    return _template(4, parameters, df_index, lc, result_directory, result_spec, eval_pos, materials_directory,
+                     quad_order, use_diluted_steel, kappa_elec)
+
+
 def get_vector_field_mag_2(parameters, df_index=0, lc=0.4, geo_th=1e-5, run_gmsh=False, plot_geo=False,
                            plot_result=False, result_directory="none", result_spec="", eval_pos=np.zeros((0, 3)),
                            materials_directory="files/materials", quad_order=8, max_coil_size=0.05, kappa_elec=5.0):
@@ -253,7 +316,7 @@ def get_vector_field_mag_2(parameters, df_index=0, lc=0.4, geo_th=1e-5, run_gmsh
 
 def _template(template, parameters, df_index, lc, result_directory, result_spec, eval_pos, materials_directory,
               quad_order, use_diluted_steel, kappa_elec):
-    """Templates 1 and 3.
+    """Templates 1 to 4.
 
     :return: ``[points, B, M_iron, M_coil, Q, current_density]``: the quadrature points of every
         element (``field_density`` order) and the total field there, the iron mass in g (the
@@ -273,13 +336,19 @@ def _template(template, parameters, df_index, lc, result_directory, result_spec,
     J_tar_mm2 = _value(parameters, "J_tar(A/mm2)", df_index)
     J_tar = (compute_J_opt(conductor_material_data, kappa_elec) if J_tar_mm2 < 0 else J_tar_mm2) * 1e6
 
-    g = mag_1_parameters(parameters, df_index)
-    # iron spacing: 0.2 lc, except 0.3 lc for template 2 and template 3's plain yoke
-    # (SHiP_functions.py:944-969, 1435)
-    inner = 0.3 if (template == 2 or (template == 3 and not use_diluted_steel)) else 0.2
+    g = mag_4_parameters(parameters, df_index) if template == 4 else mag_1_parameters(parameters, df_index)
+    # iron spacing: 0.2 lc, except 0.3 lc for template 2 and template 3's plain yoke and lc for
+    # template 4 (SHiP_functions.py:944-969, 1435, 1871)
+    if template == 4:
+        inner = 1.0
+    else:
+        inner = 0.3 if (template == 2 or (template == 3 and not use_diluted_steel)) else 0.2
     msh = template_mesh(g, template, lc=lc, use_diluted_steel=use_diluted_steel, inner=inner)
     vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
-    iron_tags = [M.TAG_IRON, TAG_WING] if use_diluted_steel else [M.TAG_IRON]
+    if template == 4:
+        iron_tags = [M.TAG_IRON, TAG_YOKE]
+    else:
+        iron_tags = [M.TAG_IRON, TAG_WING] if use_diluted_steel else [M.TAG_IRON]
     M_iron = 4 * float(vol[np.isin(msh.elem_domain, iron_tags)].sum()) * iron_material_data["density(g/m3)"]
 
     coils, A_cu, A_coil, perimeter, current_density = _coils(g, J_tar, conductor_material_data["filling_factor"],
@@ -288,14 +357,22 @@ def _template(template, parameters, df_index, lc, result_directory, result_spec,
     current = g["current"]
     Q = 0.0 if current == 0 else abs(current * current) * perimeter * conductor_material_data["resistivity(Ohm.m)"] / A_cu
 
-    if use_diluted_steel:
+    max_newton = 150 if template == 4 else 25
+    rels = [reluctance_iron] * len(iron_tags)
+    if use_diluted_steel and template == 4:
+        # template 4 dilutes its core (SHiP_functions.py:1850-1854, 2033-2038)
+        dil = Dilution(g["X_A_1"] + g["X_E_1"], g["X_B_1"] + g["X_F_1"], g["X_C_1"], g["X_D_1"],
+                       g["X_A_2"] + g["X_E_2"], g["X_B_2"] + g["X_F_2"], g["X_C_2"], g["X_D_2"], g["Z_pos"], g["Z_len"])
+        solver = RedMVPSolverDiluted(msh, coils, iron_tags, [M.TAG_AIR], rels, [dil, None], quad_order=quad_order,
+                                     max_newton_iterations=max_newton)
+    elif use_diluted_steel:
         dilution_wing = Dilution(g["X_mgap_1"], g["X_core_1"], g["X_void_1"], g["X_yoke_1"], g["X_mgap_2"],
                                  g["X_core_2"], g["X_void_2"], g["X_yoke_2"], g["Z_pos"], g["Z_len"])
-        solver = RedMVPSolverDiluted(msh, coils, iron_tags, [M.TAG_AIR], [reluctance_iron, reluctance_iron],
-                                     [None, dilution_wing], quad_order=quad_order, max_newton_iterations=25)
+        solver = RedMVPSolverDiluted(msh, coils, iron_tags, [M.TAG_AIR], rels, [None, dilution_wing],
+                                     quad_order=quad_order, max_newton_iterations=max_newton)
     else:
-        solver = RedMVPSolver(msh, coils, iron_tags, [M.TAG_AIR], [reluctance_iron], quad_order=quad_order,
-                              max_newton_iterations=25)
+        solver = RedMVPSolver(msh, coils, iron_tags, [M.TAG_AIR], rels, quad_order=quad_order,
+                              max_newton_iterations=max_newton)
     solver.verbose = False
     x = np.zeros(solver.num_dofs_mvp) if current == 0.0 else solver.solve()
     points, B_i = solver.curl_curl_factory.compute_B(x, quad_order=int(0.5 * g["field_density"]))

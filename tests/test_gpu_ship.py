@@ -9,7 +9,7 @@ import pytest
 from snoopy_b200 import materials as MAT
 from snoopy_b200 import mesh as M
 from snoopy_b200 import ship
-from test_ship_template import template_parameters
+from test_ship_template import template_4_parameters, template_parameters
 
 pytestmark = pytest.mark.gpu
 
@@ -77,3 +77,20 @@ def test_template_2(materials_dir, tmp_path):
     Be = np.atleast_2d(np.loadtxt(tmp_path / "B_m2.csv", delimiter=",", skiprows=1))[0, 3:]
     assert abs(Be[1]) > 5 * max(abs(Be[0]), abs(Be[2]))  # core field along y
     assert (tmp_path / "parameters_m2.csv").exists()
+
+
+def test_template_4(materials_dir, tmp_path):
+    P = template_4_parameters()
+    probes = np.array([[0.3, 0.1, 0.0]])
+    out = {}
+    for diluted in (False, True):
+        pts, B, M_iron, M_coil, Q, J = ship.get_vector_field_mag_4(P, lc=0.4, eval_pos=probes, quad_order=2,
+                                                                   materials_directory=materials_dir,
+                                                                   result_directory=str(tmp_path),
+                                                                   result_spec=f"_m4{int(diluted)}",
+                                                                   use_diluted_steel=diluted)
+        assert np.isfinite(B).all() and M_iron > 0
+        Be = np.atleast_2d(np.loadtxt(tmp_path / f"B_m4{int(diluted)}.csv", delimiter=",", skiprows=1))[0, 3:]
+        assert abs(Be[1]) > 5 * max(abs(Be[0]), abs(Be[2]))  # core field along y
+        out[diluted] = Be
+    assert np.abs(out[True] - out[False]).max() > 1e-3 * np.abs(out[False]).max()

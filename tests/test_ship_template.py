@@ -80,6 +80,40 @@ def test_template_2_mesh():
     assert abs(got - iron) < 1e-9 * iron
 
 
+def template_4_parameters():
+    """Two table rows: X_A, X_B, X_C from the first, X_D, X_E, X_F from the second."""
+    P = template_parameters()
+    two = {k: v * 2 for k, v in P.items()}
+    for e, (a, b, c, d_, e_, f) in ((1, (0.0, 0.1, 0.16, 0.46, 0.52, 0.9)), (2, (0.0, 0.12, 0.18, 0.5, 0.56, 1.0))):
+        two[f"Xmgap{e}(m)"] = [a, 0.0]
+        two[f"Xcore{e}(m)"] = [b, d_]
+        two[f"Xvoid{e}(m)"] = [c, e_]
+        two[f"Xyoke{e}(m)"] = [0.0, f]
+    return two
+
+
+def test_template_4_mesh():
+    g = ship.mag_4_parameters(template_4_parameters())
+    msh = ship.template_mesh(g, 4, lc=0.5, inner=1.0)
+    vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
+    assert (vol > 0).all()
+
+    def areas(t):
+        v = {k: g[k + "_1"] + t * (g[k + "_2"] - g[k + "_1"]) for k in ("X_A", "X_B", "X_C", "X_D", "X_E", "X_F",
+                                                                         "Y_core", "Y_yoke")}
+        core = (v["X_D"] - v["X_C"]) * v["Y_core"]
+        yoke = (v["X_F"] - v["X_A"]) * v["Y_yoke"] - (v["X_E"] - v["X_B"]) * v["Y_core"]
+        return core, yoke
+
+    a = [areas(t) for t in (0.0, 0.5, 1.0)]
+    core = g["Z_len"] * (a[0][0] + 4 * a[1][0] + a[2][0]) / 6.0
+    yoke = g["Z_len"] * (a[0][1] + 4 * a[1][1] + a[2][1]) / 6.0
+    assert abs(vol[msh.elem_domain == M.TAG_IRON].sum() - core) < 1e-9 * core
+    assert abs(vol[msh.elem_domain == ship.TAG_YOKE].sum() - yoke) < 1e-9 * yoke
+    coils, _, _, _, _ = ship._coils(g, 3e6, 0.6, template=4)
+    assert len(coils) == 2
+
+
 def test_template_coils():
     for X_mgap, n_coils in (((0.0, 0.0), 1), ((0.05, 0.08), 2)):
         g = ship.mag_1_parameters(template_parameters(X_mgap))
