@@ -31,6 +31,7 @@ from .racetrack_coil import RacetrackCoil
 
 TAG_WING = 5  # the diluted return-yoke wing (templates 1 and 3)
 TAG_YOKE = 6  # template 4's yoke (its core carries tag 1, the dilutable part)
+TAG_NC = 7  # the normal-conducting magnet of the NC/SC model (the superconducting one is tag 1)
 
 
 def compute_J_opt(conductor_material_data, kappa_elec):
@@ -215,6 +216,151 @@ def _mapped(g, xi, xf, xb1, xb2, yi, yf, yb1, yb2, zs, nx, ny, nz, dom):
     return msh
 
 
+class Magnet:
+    """One magnet of a multi-magnet model: its z range, its x and y boundaries at the entrance
+    and the exit (interior breakpoints, 0 and the box face are implied) with the names of the
+    intervals between them, a spacing across its iron, and ``tag(X, Y)`` giving the volume tag
+    (0 for air) of cells with interval names X, Y (arrays)."""
+
+    def __init__(self, z1, z2, x_names, x1, x2, y_names, y1, y2, tag, inner):
+        self.z1, self.z2 = float(z1), float(z2)
+        self.x = (list(x_names), list(x1), list(x2))
+        self.y = (list(y_names), list(y1), list(y2))
+        self.tag = tag
+        self.inner = inner
+
+
+def _chain(names, b1, b2, lim):
+    """A magnet's lines along one axis without zero-width intervals: entrance and exit
+    positions of its interior lines and the names of its intervals (from 0 to the box face)."""
+    k1, k2, nm = [0.0], [0.0], []
+    for i in range(len(b1)):
+        w1, w2 = b1[i] - k1[-1], b2[i] - k2[-1]
+        if w1 == 0.0 and w2 == 0.0:
+            continue
+        if not (w1 > 0.0 and w2 > 0.0):
+            raise ValueError(f"interval {names[i]!r} is empty or inverted at one end ({w1}, {w2})")
+        k1.append(b1[i])
+        k2.append(b2[i])
+        nm.append(names[i])
+    if not (lim > k1[-1] and lim > k2[-1]):
+        raise ValueError("the box does not contain the magnet")
+    nm.append(names[len(b1)])
+    return np.array(k1[1:]), np.array(k2[1:]), nm
+
+
+def _merged_axis(magnets, axis, lim, lc):
+    """Grid lines of one axis shared by several magnets.
+
+    Every magnet's lines take part; they are ordered by their mid-length positions (each
+    magnet's own order is kept).  Inside a magnet's z range its lines lie on its planes and the
+    other magnets' lines are spread evenly between their active neighbours; between magnets
+    every line moves linearly from one arrangement to the next.  Returns a function giving,
+    for a z value, the positions of the merged lines (0 and the box face included), the grid
+    lines (merged interval, fraction), and per magnet the name of its interval holding each
+    merged interval."""
+    chains = [_chain(*getattr(m, axis), lim) for m in magnets]
+    keys, owner = [], []
+    for mi, (k1, k2, _) in enumerate(chains):
+        for li in range(len(k1)):
+            keys.append((0.5 * (k1[li] + k2[li]), mi, li))
+            owner.append((mi, li))
+    order = sorted(range(len(keys)), key=lambda i: keys[i])
+    lines = [owner[i] for i in order]  # merged interior lines
+    L = len(lines) + 2
+
+    def arrangement(mi, t):
+        k1, k2, _ = chains[mi]
+        pos = np.full(L, np.nan)
+        pos[0], pos[-1] = 0.0, lim
+        for q, (m2, li) in enumerate(lines):
+            if m2 == mi:
+                pos[q + 1] = k1[li] + t * (k2[li] - k1[li])
+        act = np.flatnonzero(~np.isnan(pos))
+        for a, b in zip(act[:-1], act[1:]):
+            for j in range(a + 1, b):
+                pos[j] = pos[a] + (j - a) / (b - a) * (pos[b] - pos[a])
+        return pos
+
+    def positions(z):
+        if z <= magnets[0].z1:
+            return arrangement(0, 0.0)
+        for mi, m in enumerate(magnets):
+            if z <= m.z2:
+                if z >= m.z1:
+                    return arrangement(mi, (z - m.z1) / (m.z2 - m.z1))
+                prev = magnets[mi - 1]
+                s_ = (z - prev.z2) / (m.z1 - prev.z2)
+                return (1.0 - s_) * arrangement(mi - 1, 1.0) + s_ * arrangement(mi, 0.0)
+        return arrangement(len(magnets) - 1, 1.0)
+
+    # per magnet: the name of its interval that holds merged interval q
+    names = []
+    for mi, (k1, _, nm) in enumerate(chains):
+        count = 0
+        per = []
+        for q in range(L - 1):
+            per.append(nm[count])
+            if q < len(lines) and lines[q][0] == mi:
+                count += 1
+        names.append(np.array(per, dtype=object))
+    # spacing: the finest of the magnets whose lateral extent holds the interval
+    hs = np.full(L - 1, lc)
+    for mi, m in enumerate(magnets):
+        hs = np.where(names[mi] != "out", np.minimum(hs, m.inner), hs)
+    arr = [arrangement(mi, t) for mi in range(len(magnets)) for t in (0.0, 1.0)]
+    width = np.max([np.diff(a) for a in arr], axis=0)
+    counts = np.maximum(1, np.ceil(width / hs - 1e-9).astype(np.int64))
+    line_iv = np.concatenate([np.full(c, q) for q, c in enumerate(counts)] + [[L - 2]])
+    line_f = np.concatenate([np.arange(c) / c for c in counts] + [[1.0]])
+    cell_iv = np.repeat(np.arange(L - 1), counts)
+    return positions, line_iv, line_f, cell_iv, names
+
+
+def magnets_mesh(magnets, lim_x, lim_y, z_min, z_max, lc):
+    """Tetrahedral mesh of an air box [0, lim_x] x [0, lim_y] x [z_min, z_max] holding magnets
+    one after another along z (quarter model: y = 0 carries the natural condition)."""
+    magnets = sorted(magnets, key=lambda m: m.z1)
+    for a, b in zip(magnets[:-1], magnets[1:]):
+        if b.z1 < a.z2:
+            raise ValueError("magnets overlap along z")
+    xpos, xi, xf, xcell, xnames = _merged_axis(magnets, "x", lim_x, lc)
+    ypos, yi, yf, ycell, ynames = _merged_axis(magnets, "y", lim_y, lc)
+    zb = [z_min]
+    zseg = []
+    for mi, m in enumerate(magnets):
+        if m.z1 > zb[-1]:
+            zb.append(m.z1)
+            zseg.append(-1)
+        zb.append(m.z2)
+        zseg.append(mi)
+    zb.append(z_max)
+    zseg.append(-1)
+    zcount = [max(1, int(np.ceil((zb[i + 1] - zb[i]) / lc - 1e-9))) for i in range(len(zseg))]
+    zs = np.concatenate([zb[i] + (zb[i + 1] - zb[i]) * np.arange(c) / c for i, c in enumerate(zcount)] + [[z_max]])
+    zcell = np.repeat(np.array(zseg), zcount)
+    nx, ny, nz = len(xcell), len(ycell), len(zcell)
+    dom = np.full((nx, ny, nz), M.TAG_AIR, dtype=np.int32)
+    for mi, m in enumerate(magnets):
+        ks = np.flatnonzero(zcell == mi)
+        if len(ks) == 0:
+            continue
+        X, Y = np.meshgrid(xnames[mi][xcell], ynames[mi][ycell], indexing="ij")
+        tag = np.asarray(m.tag(X, Y), dtype=np.int32)
+        dom[:, :, ks] = np.where(tag[:, :, None] != 0, tag[:, :, None], M.TAG_AIR)
+    ref = M.tensor_grid_mesh(np.arange(nx + 1.0), np.arange(ny + 1.0), np.arange(nz + 1.0), dom)
+    I = np.rint(ref.nodes[:, 0]).astype(np.int64)
+    J = np.rint(ref.nodes[:, 1]).astype(np.int64)
+    K = np.rint(ref.nodes[:, 2]).astype(np.int64)
+    PX = np.array([xpos(z) for z in zs])  # [nz + 1, merged lines]
+    PY = np.array([ypos(z) for z in zs])
+    x = PX[K, xi[I]] + xf[I] * (PX[K, np.minimum(xi[I] + 1, PX.shape[1] - 1)] - PX[K, xi[I]])
+    y = PY[K, yi[J]] + yf[J] * (PY[K, np.minimum(yi[J] + 1, PY.shape[1] - 1)] - PY[K, yi[J]])
+    msh = M.TetMesh(np.stack([x, y, zs[K]], axis=1), ref.cells, ref.elem_domain)
+    msh.natural_planes = [(1, 0.0)]
+    return msh
+
+
 def _coils(g, J_tar, filling_factor, template=1):
     """The template's racetrack coils, turn positions and the coil's electrical figures
     (template 1: around the core, ``SHiP_functions.py:572-658``; template 3: around the
@@ -393,3 +539,98 @@ def _template(template, parameters, df_index, lc, result_directory, result_spec,
         header = "x(m),y(m),z(m),Bx(T),By(T),Bz(T)"
         np.savetxt(out, np.append(eval_pos, B_tot, axis=1), delimiter=",", header=header, comments="")
     return ret_vals
+
+
+def _tag_type_1(X, Y):
+    """Templates 1 and 3's iron (``geometry_tools.py:213-259``)."""
+    return (np.isin(X, ["core", "leg"]) & (Y != "out")) | ((X == "void") & (Y == "top"))
+
+
+def _tag_type_2(X, Y):
+    """Template 2's core and L-shaped yoke (``geometry_tools.py:305-345, 392-500``)."""
+    return ((X == "core") & (Y == "low")) | ((Y == "top") & (X != "out")) | ((X == "leg") & (Y != "out"))
+
+
+def get_vector_field_ncsc(parameters, df_index=0, lc=0.2, geo_th=1e-5, run_gmsh=False, plot_geo=False,
+                          plot_result=False, result_directory="none", result_spec="", eval_pos=np.zeros((0, 3)),
+                          materials_directory="files/materials", quad_order=8):
+    """B of the NC/SC model (``SHiP_functions.py:2139-2623``): a normal-conducting magnet with
+    template 1's yoke (row df_index) followed along z by a superconducting one with template
+    2's core and yoke (row df_index + 1), one coil around each core, in one air box.  The two
+    magnets' boundaries share one grid (``magnets_mesh``).
+
+    :return: ``[points, B, M_iron, M_coil, Q, J_tar]`` as the reference: the iron mass of the
+        superconducting magnet only, the coil mass and power of its coil, and its target
+        current density.
+    """
+    from .evaluators import evaluate_fem_solution_node_interpolation
+    from .red_mvp_solver import RedMVPSolver
+
+    row = df_index + 1
+    material = str(np.asarray(parameters["material"])[row])
+    reluctance_iron = Reluctance(os.path.join(materials_directory, material))
+    with open(os.path.join(materials_directory, material)) as f:
+        iron_material_data = json.load(f)
+    with open(os.path.join(materials_directory, str(np.asarray(parameters["coil_material"])[row]))) as f:
+        conductor_material_data = json.load(f)
+    J_tar = _value(parameters, "J_tar(A/mm2)", row) * 1e6
+    g1 = mag_1_parameters(parameters, df_index)
+    g2 = mag_1_parameters(parameters, row)
+    lim_x = max(g1["lim_x"], g2["lim_x"])
+    lim_y = max(g1["lim_y"], g2["lim_y"])
+    z_min, z_max = g1["z_min"], g2["z_max"]
+    e1 = lambda g, keys: ([g[f"{k}_1"] for k in keys], [g[f"{k}_2"] for k in keys])
+    x1 = e1(g1, ["X_mgap", "X_core", "X_void", "X_yoke"])
+    y1 = e1(g1, ["Y_core", "Y_yoke"])
+    x2 = e1(g2, ["X_core", "X_void", "X_yoke"])
+    y2 = e1(g2, ["Y_core", "Y_void", "Y_yoke"])
+    nc = Magnet(g1["Z_pos"], g1["Z_pos"] + g1["Z_len"], ["gap", "core", "void", "leg", "out"], *x1,
+                ["low", "top", "out"], *y1, lambda X, Y: np.where(_tag_type_1(X, Y), TAG_NC, 0), lc)
+    sc = Magnet(g2["Z_pos"], g2["Z_pos"] + g2["Z_len"], ["core", "void", "leg", "out"], *x2,
+                ["low", "mid", "top", "out"], *y2, lambda X, Y: np.where(_tag_type_2(X, Y), M.TAG_IRON, 0), lc)
+    msh = magnets_mesh([nc, sc], lim_x, lim_y, z_min, z_max, lc)
+    vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
+    M_iron = 4 * float(vol[msh.elem_domain == M.TAG_IRON].sum()) * iron_material_data["density(g/m3)"]
+
+    # coils (SHiP_functions.py:2427-2474): turns offset by spacer + insulation from each core
+    coils = []
+    for g in (g1, g2):
+        slot = 2 * min(g["Y_core_1"], g["Y_core_2"])
+        r, ins, sp = g["coil_radius"], g["ins"], g["yoke_spacer"]
+        n = min(int(slot / 2 / (r + ins)), int(g["max_turns"]))
+        if n < 1:
+            raise ValueError("a slot holds no conductor")
+        y = np.linspace(-0.5 * slot + r + ins, 0.5 * slot - r - ins, n)
+        d = sp + ins
+        X1, X2, Z1, Z2 = g["X_core_1"], g["X_core_2"], g["Z_pos"], g["Z_pos"] + g["Z_len"]
+        kp = np.array([[-X2 - d, Z2], [-X2, Z2 + d], [X2, Z2 + d], [X2 + d, Z2], [X1 + d, Z1], [X1, Z1 - d],
+                       [-X1, Z1 - d], [-X1 - d, Z1]])
+        coils.append(RacetrackCoil(kp, y, r, g["current"] / n))
+    perimeter = coils[1].get_length()
+    current_2 = g2["current"]
+    A_cu = abs(current_2) / J_tar
+    M_coil = A_cu * perimeter * conductor_material_data["density(g/m3)"]
+    Q = abs(current_2 * current_2) * perimeter * conductor_material_data["resistivity(Ohm.m)"] / A_cu
+
+    iron_tags = [TAG_NC, M.TAG_IRON]
+    solver = RedMVPSolver(msh, coils, iron_tags, [M.TAG_AIR], [reluctance_iron] * 2, quad_order=quad_order,
+                          max_newton_iterations=50)
+    solver.verbose = False
+    x = solver.solve()
+    field_density = int(max(0.5 * g1["field_density"], 0.5 * g2["field_density"]))
+    points, B_i = solver.curl_curl_factory.compute_B(x, quad_order=field_density)
+    B_coil = 0.0 * B_i
+    for coil in coils:
+        B_coil += coil.compute_B(points)
+    if result_directory != "none":
+        np.save(os.path.join(result_directory, "x" + result_spec + ".npy"), x)
+    ret_vals = [points, B_i + B_coil, M_iron, M_coil, Q, J_tar]
+    eval_pos = np.asarray(eval_pos, dtype=np.float64).reshape(-1, 3)
+    if eval_pos.shape[0] > 0:
+        B_tot = evaluate_fem_solution_node_interpolation(msh, eval_pos, solver, coils, x, iron_tags + [M.TAG_AIR])
+        name = "B" + result_spec + ".csv"
+        out = os.path.join(result_directory, name) if result_directory != "none" else name
+        np.savetxt(out, np.append(eval_pos, B_tot, axis=1), delimiter=",", header="x(m),y(m),z(m),Bx(T),By(T),Bz(T)",
+                   comments="")
+    return ret_vals
+

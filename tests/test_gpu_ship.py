@@ -9,7 +9,7 @@ import pytest
 from snoopy_b200 import materials as MAT
 from snoopy_b200 import mesh as M
 from snoopy_b200 import ship
-from test_ship_template import template_4_parameters, template_parameters
+from test_ship_template import ncsc_parameters, template_4_parameters, template_parameters
 
 pytestmark = pytest.mark.gpu
 
@@ -94,3 +94,18 @@ def test_template_4(materials_dir, tmp_path):
         assert abs(Be[1]) > 5 * max(abs(Be[0]), abs(Be[2]))  # core field along y
         out[diluted] = Be
     assert np.abs(out[True] - out[False]).max() > 1e-3 * np.abs(out[False]).max()
+
+
+def test_ncsc(materials_dir, tmp_path):
+    P = ncsc_parameters()
+    probes = np.array([[0.1, 0.08, -1.0], [0.1, 0.08, 2.4]])  # NC core, SC core
+    pts, B, M_iron, M_coil, Q, J = ship.get_vector_field_ncsc(P, lc=0.4, eval_pos=probes, quad_order=2,
+                                                              materials_directory=materials_dir,
+                                                              result_directory=str(tmp_path), result_spec="_ncsc")
+    assert np.isfinite(B).all() and M_iron > 0 and M_coil > 0 and J == 3e6
+    Be = np.loadtxt(tmp_path / "B_ncsc.csv", delimiter=",", skiprows=1)[:, 3:]
+    # both cores carry flux along y (the superconducting core's is weaker and less uniform: an
+    # air gap separates it from its yoke)
+    for b in Be:
+        assert abs(b[1]) > 2 * max(abs(b[0]), abs(b[2])) and abs(b[1]) > 0.02
+

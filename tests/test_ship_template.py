@@ -147,3 +147,71 @@ def test_compute_J_opt():
          "resistivity(Ohm.m)": 1.7e-8}
     J = ship.compute_J_opt(d, 5.0)
     assert abs(J - np.sqrt(100.0 * 8.9e3 / 5.0 / 1.7e-8) * 1e-6) < 1e-12 * J
+
+
+def ncsc_parameters():
+    """An NC magnet (row 0, template-1 yoke) followed by an SC magnet (row 1, template-2 core and yoke)."""
+    P = {k: v * 2 for k, v in template_parameters().items()}
+    P["Z_pos(m)"] = [-3.0, 1.2]
+    P["Z_len(m)"] = [3.5, 2.5]
+    for e, (c, v, y, yc, yv, yy) in ((1, (0.2, 0.26, 0.9, 0.15, 0.2, 0.45)), (2, (0.22, 0.28, 1.0, 0.18, 0.24, 0.5))):
+        P[f"Xmgap{e}(m)"] = [0.0, 0.0]
+        P[f"Xcore{e}(m)"] = [P[f"Xcore{e}(m)"][0], c]
+        P[f"Xvoid{e}(m)"] = [P[f"Xvoid{e}(m)"][0], v]
+        P[f"Xyoke{e}(m)"] = [P[f"Xyoke{e}(m)"][0], y]
+        P[f"Ycore{e}(m)"] = [P[f"Ycore{e}(m)"][0], yc]
+        P[f"Yvoid{e}(m)"] = [P[f"Yvoid{e}(m)"][0], yv]
+        P[f"Yyoke{e}(m)"] = [P[f"Yyoke{e}(m)"][0], yy]
+    return P
+
+
+def test_multi_magnet_mesher():
+    """One magnet: the same grid as the single-magnet mesher.  Two magnets along z: each
+    magnet's iron volume is exact, and the box is filled."""
+    g = ship.mag_1_parameters(template_parameters())
+    m = ship.Magnet(g["Z_pos"], g["Z_pos"] + g["Z_len"], ["gap", "core", "void", "leg", "out"],
+                    [g["X_mgap_1"], g["X_core_1"], g["X_void_1"], g["X_yoke_1"]],
+                    [g["X_mgap_2"], g["X_core_2"], g["X_void_2"], g["X_yoke_2"]], ["low", "top", "out"],
+                    [g["Y_core_1"], g["Y_yoke_1"]], [g["Y_core_2"], g["Y_yoke_2"]],
+                    lambda X, Y: np.where(ship._tag_type_1(X, Y), M.TAG_IRON, 0), 0.1)
+    a = ship.magnets_mesh([m], g["lim_x"], g["lim_y"], g["z_min"], g["z_max"], 0.5)
+    b = ship.mag_1_mesh(g, lc=0.5)
+    assert np.array_equal(a.cells, b.cells) and np.array_equal(a.elem_domain, b.elem_domain)
+    assert np.abs(a.nodes - b.nodes).max() < 1e-14
+    P = ncsc_parameters()
+    g1, g2 = ship.mag_1_parameters(P, 0), ship.mag_1_parameters(P, 1)
+
+    def simpson(area, L):
+        return L * (area(0.0) + 4 * area(0.5) + area(1.0)) / 6.0
+
+    def lerp(g, k, t):
+        return g[k + "_1"] + t * (g[k + "_2"] - g[k + "_1"])
+
+    def area1(t):
+        return ((lerp(g1, "X_yoke", t) - lerp(g1, "X_mgap", t)) * lerp(g1, "Y_yoke", t)
+                - (lerp(g1, "X_void", t) - lerp(g1, "X_core", t)) * lerp(g1, "Y_core", t))
+
+    def area2(t):
+        return (lerp(g2, "X_core", t) * lerp(g2, "Y_core", t)
+                + lerp(g2, "X_yoke", t) * (lerp(g2, "Y_yoke", t) - lerp(g2, "Y_void", t))
+                + (lerp(g2, "X_yoke", t) - lerp(g2, "X_void", t)) * lerp(g2, "Y_void", t))
+
+    e = lambda g, keys: ([g[f"{k}_1"] for k in keys], [g[f"{k}_2"] for k in keys])
+    nc = ship.Magnet(g1["Z_pos"], g1["Z_pos"] + g1["Z_len"], ["gap", "core", "void", "leg", "out"],
+                     *e(g1, ["X_mgap", "X_core", "X_void", "X_yoke"]), ["low", "top", "out"],
+                     *e(g1, ["Y_core", "Y_yoke"]), lambda X, Y: np.where(ship._tag_type_1(X, Y), ship.TAG_NC, 0), 0.2)
+    sc = ship.Magnet(g2["Z_pos"], g2["Z_pos"] + g2["Z_len"], ["core", "void", "leg", "out"],
+                     *e(g2, ["X_core", "X_void", "X_yoke"]), ["low", "mid", "top", "out"],
+                     *e(g2, ["Y_core", "Y_void", "Y_yoke"]),
+                     lambda X, Y: np.where(ship._tag_type_2(X, Y), M.TAG_IRON, 0), 0.2)
+    lim_x, lim_y = max(g1["lim_x"], g2["lim_x"]), max(g1["lim_y"], g2["lim_y"])
+    msh = ship.magnets_mesh([nc, sc], lim_x, lim_y, g1["z_min"], g2["z_max"], 0.5)
+    vol = M.tet_volumes6(msh.nodes, msh.cells) / 6.0
+    assert (vol > 0).all()
+    box = lim_x * lim_y * (g2["z_max"] - g1["z_min"])
+    assert abs(vol.sum() - box) < 1e-9 * box
+    v1 = simpson(area1, g1["Z_len"])
+    v2 = simpson(area2, g2["Z_len"])
+    assert abs(vol[msh.elem_domain == ship.TAG_NC].sum() - v1) < 1e-9 * v1
+    assert abs(vol[msh.elem_domain == M.TAG_IRON].sum() - v2) < 1e-9 * v2
+
