@@ -43,6 +43,72 @@ def compute_J_opt(conductor_material_data, kappa_elec):
     return np.sqrt(kappa_cu * dens * 1e-3 / kappa_elec / rho) * 1e-6
 
 
+def compute_area_polygon(kp, isclosed=True):
+    """Signed shoelace area of a polygon kp [M, 2] (``geometry_tools.py:1121-1145``); a closed
+    polygon repeats its first point last, otherwise ``isclosed=False`` adds the closing edge."""
+    kp = np.asarray(kp, dtype=np.float64)
+    area = float(np.sum(kp[:-1, 0] * kp[1:, 1] - kp[1:, 0] * kp[:-1, 1]))
+    if not isclosed:
+        area += kp[-1, 0] * kp[0, 1] - kp[0, 0] * kp[-1, 1]
+    return 0.5 * area
+
+
+def get_NI(B_goal, parameters_df, df_index, materials_directory="files/materials"):
+    """Ampere-turns for a field B_goal from a magnetic-circuit estimate, and whether the
+    geometry suits the template (``SHiP_functions.py:40-202``).
+
+    The three flux-path areas are side views (x-z and y-z polygons over the magnet length) of
+    the core (A1), the top yoke (A2) and the leg (A3), with the reference's polygons as they
+    are (each starts at the origin); path lengths l1 = l3 = mean of Y_core and Y_yoke, l2 = mean
+    leg-to-gap width.  Mag1 / Mag2: flux B_goal A1 through all three parts, valid when A1 < A3;
+    Mag3: flux B_goal A3, valid when A1 > A3.  NI = sum of nu(B_i) B_i l_i, signed like B_goal.
+    """
+    reluctance = Reluctance(os.path.join(materials_directory, str(np.asarray(parameters_df["material"])[df_index])))
+    v = lambda name: _value(parameters_df, name, df_index)
+    Zl = v("Z_len(m)")
+
+    def side(a1, b1, b2, a2):
+        # (0, 0), (b1, 0), (b2, Z_len), (a2, Z_len), (a1, 0): the reference's five points
+        return compute_area_polygon(np.array([[0.0, 0.0], [b1, 0.0], [b2, Zl], [a2, Zl], [a1, 0.0]]))
+
+    A1 = side(v("Xmgap1(m)"), v("Xcore1(m)"), v("Xcore2(m)"), v("Xmgap2(m)"))
+    A2 = side(v("Yvoid1(m)"), v("Yyoke1(m)"), v("Yyoke2(m)"), v("Yvoid2(m)"))
+    A3 = side(v("Xvoid1(m)"), v("Xyoke1(m)"), v("Xyoke2(m)"), v("Xvoid2(m)"))
+    kind = str(np.asarray(parameters_df["yoke_type"])[df_index])
+    l1 = 0.25 * (v("Ycore1(m)") + v("Ycore2(m)") + v("Yyoke1(m)") + v("Yyoke2(m)"))
+    l2 = (0.5 * (v("Xyoke1(m)") + v("Xyoke2(m)")) + 0.5 * (v("Xvoid1(m)") + v("Xvoid2(m)"))
+          - 0.5 * (v("Xcore1(m)") + v("Xcore2(m)")) - 0.5 * (v("Xmgap1(m)") + v("Xmgap2(m)")))
+    l3 = l1
+    H = lambda B: float(reluctance.evaluate_nu(B)) * B
+    NI, valid = 0.0, True
+    if kind in ("Mag1", "Mag2"):
+        Phi = abs(B_goal) * A1
+        NI = H(B_goal) * l1 + H(Phi / A2) * l2 + H(Phi / A3) * l3
+        valid = A1 < A3
+    elif kind == "Mag3":
+        Phi = abs(B_goal) * A3
+        NI = H(Phi / A1) * l1 + H(Phi / A2) * l2 + H(Phi / A3) * l3
+        valid = A1 > A3
+    if kind in ("Mag1", "Mag2", "Mag3") and B_goal < 0.0:
+        NI *= -1.0
+    return NI, valid
+
+
+def compute_prices(magnet_parameters, df_index, M_iron, M_coil, Q, electricity_costs=5.0 / 72000.0, runtime=72000,
+                   materials_directory="files/materials", price_peanuts=0.5):
+    """Costs of iron, coil and electricity (``SHiP_functions.py:204-257``): masses in g times
+    (material + manufacturing cost per kg), power times electricity cost per Wh times runtime,
+    all scaled by ``price_peanuts``."""
+    with open(os.path.join(materials_directory, str(np.asarray(magnet_parameters["material"])[df_index]))) as f:
+        iron = json.load(f)
+    with open(os.path.join(materials_directory, str(np.asarray(magnet_parameters["coil_material"])[df_index]))) as f:
+        coil = json.load(f)
+    C_iron = 1e-3 * M_iron * (iron["material_cost(CHF/kg)"] + iron["manufacturing_cost(CHF/kg)"]) * price_peanuts
+    C_coil = 1e-3 * M_coil * (coil["material_cost(CHF/kg)"] + coil["manufacturing_cost(CHF/kg)"]) * price_peanuts
+    C_edf = Q * electricity_costs * runtime * price_peanuts
+    return C_iron, C_coil, C_edf
+
+
 def _value(parameters, name, df_index):
     return float(np.asarray(parameters[name])[df_index])
 

@@ -1,9 +1,12 @@
 """SHiP template 1 meshed without gmsh: the quarter model's geometry, materials, boundary and
 coils (CPU), checked against their definitions."""
 
+import json
+
 import numpy as np
 import pytest
 
+from snoopy_b200 import materials as MAT
 from snoopy_b200 import mesh as M
 from snoopy_b200 import ship
 
@@ -214,4 +217,45 @@ def test_multi_magnet_mesher():
     v2 = simpson(area2, g2["Z_len"])
     assert abs(vol[msh.elem_domain == ship.TAG_NC].sum() - v1) < 1e-9 * v1
     assert abs(vol[msh.elem_domain == M.TAG_IRON].sum() - v2) < 1e-9 * v2
+
+
+def test_polygon_area():
+    sq = np.array([[0, 0], [1, 0], [1, 1], [0, 1], [0, 0]], dtype=float)
+    assert ship.compute_area_polygon(sq) == 1.0
+    assert ship.compute_area_polygon(sq[:-1], isclosed=False) == 1.0
+    assert ship.compute_area_polygon(sq[::-1]) == -1.0
+
+
+def test_get_NI_and_prices(tmp_path):
+    B, H = MAT.atan_bh_table(mu_r=2500.0, Js=2.0)
+    (tmp_path / "iron_test.json").write_text(json.dumps({"density(g/m3)": 7.8e6, "material_cost(CHF/kg)": 1.5,
+                                                         "manufacturing_cost(CHF/kg)": 2.5,
+                                                         "BH_data": {"B(T)": list(B), "H(A/m)": list(H)}}))
+    (tmp_path / "cu_test.json").write_text(json.dumps({"material_cost(CHF/kg)": 20.0,
+                                                       "manufacturing_cost(CHF/kg)": 80.0}))
+    P = template_parameters()
+    rel = MAT.Reluctance(str(tmp_path / "iron_test.json"))
+    g = ship.mag_1_parameters(P)
+    Zl = g["Z_len"]
+    # the side-view areas of the reference's polygons (first point at the origin)
+    A1 = ship.compute_area_polygon(np.array([[0, 0], [g["X_core_1"], 0], [g["X_core_2"], Zl], [g["X_mgap_2"], Zl],
+                                             [g["X_mgap_1"], 0]]))
+    A2 = ship.compute_area_polygon(np.array([[0, 0], [g["Y_yoke_1"], 0], [g["Y_yoke_2"], Zl], [g["Y_void_2"], Zl],
+                                             [g["Y_void_1"], 0]]))
+    A3 = ship.compute_area_polygon(np.array([[0, 0], [g["X_yoke_1"], 0], [g["X_yoke_2"], Zl], [g["X_void_2"], Zl],
+                                             [g["X_void_1"], 0]]))
+    l1 = 0.25 * (g["Y_core_1"] + g["Y_core_2"] + g["Y_yoke_1"] + g["Y_yoke_2"])
+    l2 = (0.5 * (g["X_yoke_1"] + g["X_yoke_2"]) + 0.5 * (g["X_void_1"] + g["X_void_2"])
+          - 0.5 * (g["X_core_1"] + g["X_core_2"]) - 0.5 * (g["X_mgap_1"] + g["X_mgap_2"]))
+    for kind, Bg in (("Mag1", 1.2), ("Mag1", -1.2), ("Mag3", 0.8)):
+        P["yoke_type"] = [kind]
+        NI, valid = ship.get_NI(Bg, P, 0, materials_directory=str(tmp_path))
+        Phi = abs(Bg) * (A1 if kind == "Mag1" else A3)
+        Bs = ([Bg] if kind == "Mag1" else [Phi / A1]) + [Phi / A2, Phi / A3]
+        want = sum(float(rel.evaluate_nu(b)) * b * l for b, l in zip(Bs, (l1, l2, l1)))
+        want = -want if Bg < 0 and kind == "Mag1" else want
+        assert abs(NI - want) <= 1e-12 * abs(want) and valid == ((A1 < A3) if kind == "Mag1" else (A1 > A3))
+    C_iron, C_coil, C_edf = ship.compute_prices(P, 0, 2e6, 1e5, 3e4, materials_directory=str(tmp_path))
+    assert abs(C_iron - 1e-3 * 2e6 * 4.0 * 0.5) < 1e-9 and abs(C_coil - 1e-3 * 1e5 * 100.0 * 0.5) < 1e-9
+    assert abs(C_edf - 3e4 * 5.0 / 72000.0 * 72000 * 0.5) < 1e-6
 
