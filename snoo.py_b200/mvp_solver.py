@@ -7,6 +7,7 @@ solves (``snoopy/mvp_solver.py``).  ``solve_nonlin`` keeps the reference's Newto
 import numpy as np
 
 from .curl_curl_assembler import CurlCurlAssembler
+from .device import upload, zeros
 from .laplace_subdomain_solver import LaplaceSubdomainSolver
 from .materials import ConstantReluctance
 from .newton import MODE_REFERENCE, MODE_RESIDUAL, DeviceNewton
@@ -66,6 +67,40 @@ class MVPSolver:
                                         stream=getattr(self, "stream", None))
             self._rhs_key = key
         return self._newton
+
+    def solve_lin(self, phi_list, tolerance=1e-4, xcg_0=np.zeros((0,)), maxiter=-1, apply_gauge=False):
+        """Linear solve K(0) x = rhs with the reluctances at |B| = 0 (``mvp_solver.py:128-220``):
+        Jacobi-PCG on the free DoFs with scipy cg's rules as the reference calls it (relative
+        tolerance 1e-5; ``tolerance`` is the absolute tolerance when a start ``xcg_0`` or
+        ``maxiter`` is given; ``maxiter`` -1: 10 x free DoFs).  The reference's diagnostic plots
+        are not drawn; the CG exit code (0 converged, else the iteration count) is kept in
+        ``last_exit_code``.  Returns float64[num_dofs] (numpy), 0 on the constrained DoFs."""
+        import ctypes
+
+        from . import _lib
+
+        n = self.num_dofs_mvp
+        rhs_d = upload(self.compute_source_rhs(phi_list), np.float64)
+        out = self.curl_curl_factory.assemble_device(np.zeros(n), self.quad_order, K=True, J=False, rhs=False)
+        pat = out["pattern"]
+        mask = self.make_boundary_mask()
+        if apply_gauge:
+            tree_dofs, _ = self.curl_curl_factory.mesh.get_cotree_dofs()
+            mask[tree_dofs] = False
+        x = zeros(n)
+        has_x0 = len(xcg_0) == n
+        if has_x0:
+            x[:n] = upload(np.where(mask, np.asarray(xcg_0, dtype=np.float64), 0.0), np.float64)
+        atol = float(tolerance) if (has_x0 or maxiter >= 0) else 0.0
+        free_d = upload(mask.astype(np.uint8), np.uint8)
+        its, res = ctypes.c_int64(), ctypes.c_double()
+        rc = _lib.load().snp_pcg(n, _lib.ptr(pat.row_ptr), _lib.ptr(pat.col_idx), _lib.ptr(out["K"]),
+                                 _lib.ptr(free_d), _lib.ptr(rhs_d), _lib.ptr(x), 1e-5, atol, int(maxiter),
+                                 ctypes.byref(its), ctypes.byref(res), _lib.stream_ptr())
+        if rc not in (0, 3):  # 3: maxiter reached, which scipy reports through its exit code
+            _lib.check(rc)
+        self.last_exit_code = 0 if rc == 0 else int(its.value)
+        return x[:n].cpu().numpy()
 
     def solve_nonlin(self, phi_list, tolerance=1e-4, x_0=np.zeros((0,)), maxiter=-1, apply_gauge=False,
                      plot_current_density=False):

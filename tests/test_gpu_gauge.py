@@ -58,3 +58,39 @@ def test_total_potential_gauged():
     B = A.compute_B_at_points(x, cen[probe], probe)
     assert rel_max(Bg, B) < 1e-7
     assert rel_max(A.compute_B_at_points(xg, cen[probe], probe), B) < 5e-2
+
+
+def test_total_potential_linear_solve(oracle_mod):
+    """MVPSolver.solve_lin: K(0) x = rhs by device Jacobi-PCG to scipy's default relative
+    tolerance (1e-5), with and without the gauge; residual measured with the oracle's K."""
+    from scipy.sparse import csr_array
+
+    from snoopy_b200 import finite_element as FE
+
+    msh = M.bar_conductor_mesh(12000)
+    t1, t2 = msh.coil_terminals[M.TAG_COIL_1]
+    solver = S.MVPSolver(msh, [M.TAG_COIL_1], [M.TAG_IRON], [M.TAG_AIR], [(t1, t2)], [MAT.atan_reluctance()],
+                         quad_order=2)
+    solver.verbose = False
+    rhs = solver.compute_source_rhs([3e6 * 0.8])
+    w, q = FE.quadrature_rule(2)
+    dphi = FE.evaluate_basis_derivative(q)
+    curls, _ = FE.curl_edge_basis_functions(q)
+    mats = []
+    for tag, rel in ((M.TAG_COIL_1, S.ConstantReluctance(0.25e7 / np.pi)), (M.TAG_IRON, MAT.atan_reluctance()),
+                     (M.TAG_AIR, S.ConstantReluctance(0.25e7 / np.pi))):
+        e = msh.domain_elements(tag)
+        mats.append(dict(cells=msh.cells[e], glob_ids=msh.elem_edges[e], orientations=msh.orientations[e],
+                         reluctance=rel))
+    O = oracle_mod.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, w, q, dphi, curls)
+    K, _, _ = O.compute_stiffness_and_jacobi_matrix_c(np.zeros(msh.num_dofs))
+    K = csr_array(K)
+    for gauge in (False, True):
+        x = solver.solve_lin([3e6 * 0.8], apply_gauge=gauge)
+        mask = solver.make_boundary_mask()
+        if gauge:
+            mask[msh.get_cotree_dofs()[0]] = False
+        Kf = K[mask, :][:, mask]
+        r = Kf @ x[mask] - rhs[mask]
+        assert solver.last_exit_code == 0 and not x[~mask].any()
+        assert np.linalg.norm(r) <= 1.01e-5 * np.linalg.norm(rhs[mask])
