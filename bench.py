@@ -358,14 +358,16 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs=None, seed=0):
+def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs=None, seed=0, galerkin_modes=64):
     """Learned warm start on a morphed-yoke family (fixed topology, 8 shape parameters + coil
     current density).  Untimed: ``n_train`` zero-start mixed-precision solves, POD to
     ``n_modes`` modes, MLP training on the tensor-core kernels.  Timed (CUDA events around each
     solve; moving the solver to a member is not timed): ``n_test`` held-out members solved
     three ways to ||F_free|| <= 1e-8 ||F_free(0)||: plain float64 from zero, mixed precision
     from zero, and mixed precision from the network's prediction (inference and reconstruction
-    inside the timed region)."""
+    inside the timed region), and that prediction moved by one Galerkin Newton step in the span
+    of the first ``galerkin_modes`` POD modes inside the solve (``MorphedSolver.attach_basis``;
+    0 skips it).  The members-at-once row uses the corrected starts when the correction runs."""
     import torch
 
     from snoopy_b200 import morph
@@ -385,8 +387,11 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
     torch.cuda.empty_cache()
     stream = torch.cuda.current_stream()
     rows = {"fp64_zero": [], "mixed_zero": [], "mixed_warm": []}
+    galerkin_modes = min(galerkin_modes, modes)
+    if galerkin_modes > 0:
+        rows["mixed_warm_galerkin"] = []
     surr_err, proj_err, b_err = [], [], []
-    warm_x = []
+    warm_x, galerkin_x = [], []
     probes = fam.geometry.aperture_probes(200, margin=0.03)
     el, _ = fam.mesh.locate(probes)
     for p in P_test:
@@ -395,8 +400,11 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            x0 = ws.predict(p)[0] if name == "mixed_warm" else None
+            x0 = ws.predict(p)[0] if name.startswith("mixed_warm") else None
+            if name == "mixed_warm_galerkin":
+                ms.attach_basis(ws.galerkin_basis(galerkin_modes))
             x, st = ms.solve(x0, rtol=RTOL, precision="fp64" if name == "fp64_zero" else "mixed", res_ref=ref)
+            ms.attach_basis(None)
             e1.record(stream)
             torch.cuda.synchronize()
             rows[name].append((e0.elapsed_time(e1), st["newton_iterations"], st["cg_iterations"], st["rel_res"],
@@ -409,6 +417,10 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
                 nrm = float(torch.linalg.vector_norm(x_ref).item())
                 surr_err.append(float(torch.linalg.vector_norm(x0 - x_ref).item()) / nrm)
                 proj_err.append(float(torch.linalg.vector_norm(ws.project(x_ref) - x_ref).item()) / nrm)
+                Bw = ms.solver.curl_curl_factory.compute_B_at_points(x, probes, el)
+                b_err.append(float(np.linalg.norm(Bw - B_ref, axis=1).max() / np.linalg.norm(B_ref, axis=1).max()))
+            elif name == "mixed_warm_galerkin":
+                galerkin_x.append(x.clone())
                 Bw = ms.solver.curl_curl_factory.compute_B_at_points(x, probes, el)
                 b_err.append(float(np.linalg.norm(Bw - B_ref, axis=1).max() / np.linalg.norm(B_ref, axis=1).max()))
     out = {"workload": f"morphed window-frame yoke family, {fam.mesh.num_elements} tets / {fam.mesh.num_dofs} DoFs, "
@@ -424,13 +436,20 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
                      "newton_mean": float(r[:, 1].mean()), "cg_mean": float(r[:, 2].mean()),
                      "rel_res_max": float(r[:, 3].max()), "starts_dropped": int(r[:, 4].sum())}
     out["speedup_mixed_warm_vs_fp64_zero"] = out["mixed_warm"]["solves_per_s"] / out["fp64_zero"]["solves_per_s"]
+    if galerkin_modes > 0:
+        out["galerkin_modes"] = galerkin_modes
+        out["speedup_mixed_warm_galerkin_vs_fp64_zero"] = (out["mixed_warm_galerkin"]["solves_per_s"]
+                                                           / out["fp64_zero"]["solves_per_s"])
     # the same warm-started mixed solves, `batch` members at a time: one solver per member, each
     # on its own stream and host thread (snp_solver_solve_many); wall clock around each batch's
     # predictions and solves (moving the solvers to their members is not timed, as above).
     # Smaller meshes leave more of the GPU idle per solve, so they run more members at once.
-    batch = min(8 if fam.mesh.num_elements < 600_000 else 4, len(P_test))
+    batch = min(16 if fam.mesh.num_elements < 600_000 else 4, len(P_test))
     if batch > 1:
         extra = [SG.MorphedSolver(fam, stream=torch.cuda.Stream()) for _ in range(batch)]
+        if galerkin_modes > 0:
+            for m in extra:
+                m.attach_basis(ws.galerkin_basis(galerkin_modes))
         wall, stats, same = 0.0, [], True
         for c0 in range(0, len(P_test), batch):
             chunk = list(range(c0, min(c0 + batch, len(P_test))))
@@ -438,14 +457,16 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
             refs = [m.set_member(P_test[i]) for m, i in zip(mss, chunk)]
             torch.cuda.synchronize()
             t1 = time.perf_counter()
-            x0s = [ws.predict(P_test[i])[0] for i in chunk]
+            x0s = [ws.predict(P_test[i], check=False)[0] for i in chunk]  # row by row, as one at a time
+            ws.mlp.check_errors()
             xs, st = SG.solve_members_at_once(mss, x0s, refs, rtol=RTOL, precision="mixed")
             torch.cuda.synchronize()
             wall += time.perf_counter() - t1
             stats += st
-            same = same and all(torch.equal(x, warm_x[i]) for x, i in zip(xs, chunk))
+            one_at_a_time = galerkin_x if galerkin_modes > 0 else warm_x
+            same = same and all(torch.equal(x, one_at_a_time[i]) for x, i in zip(xs, chunk))
         out["mixed_warm_batched"] = {
-            "members_at_once": batch, "solves_per_s": len(P_test) / wall,
+            "members_at_once": batch, "galerkin_modes": galerkin_modes, "solves_per_s": len(P_test) / wall,
             "newton_mean": float(np.mean([s_["newton_iterations"] for s_ in stats])),
             "cg_mean": float(np.mean([s_["cg_iterations"] for s_ in stats])),
             "rel_res_max": float(max(s_["rel_res"] for s_ in stats)),

@@ -300,6 +300,7 @@ typedef struct {
     int64_t kernel_launches;     /* this library's kernels launched by the solve (graph nodes counted per execution) */
     int32_t residual_evals;      /* extra residual-only assemblies of the line search */
     int32_t start_dropped;       /* 1 when the initial guess was replaced by 0 (see res_ref) */
+    int32_t galerkin_steps;      /* Galerkin corrections applied to the start (snp_solver_set_galerkin_basis) */
 } snp_solve_stats;
 
 /* x[n_dofs] (device): in = initial guess, out = solution.  Synchronises. */
@@ -346,6 +347,26 @@ int snp_solver_assemble_tensors(snp_solver *s, const double *x, int precision, d
  * mixed-precision solve, x/y float[n].  SNP_BAD_ARGUMENT when no solve of that precision ran.
  * No counterpart in the reference (Jacobian-vector product of the Newton step). */
 int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void *y, void *stream);
+
+/* Galerkin (reduced) Newton system in the span of a basis V (device float32, row-major
+ * [n_dofs][ldv], the first m <= 128 columns used) with the Jacobian of the last
+ * snp_solver_assemble_tensors of that precision: Jr = V^T J V (device float64 [m][m],
+ * row-major) and, when F is not NULL, g = V^T F (device float64 [m]), both over the free DoFs,
+ * summed in float64 in a fixed order (deterministic).  Needs the SNP_LAYOUT_ELEM layout.  The
+ * correction x + V c with Jr c = -g moves a warm start to the Newton point of the reduced
+ * space.  No counterpart in the reference (it has no warm start). */
+int snp_solver_reduced_system(snp_solver *s, int precision, const float *V, int32_t m, int64_t ldv, const double *F,
+                              double *Jr, double *g, void *stream);
+
+/* Attach a basis (device float32, row-major [n_dofs][ldv], first m <= 128 columns) to the
+ * solver's mode-1 solves: the start first takes up to `steps` Galerkin Newton steps
+ * x += V c, (V^T J V) c = -V^T F (snp_solver_reduced_system; the m x m system by Cholesky on
+ * the host), each undone and ending the corrections when it does not lower ||F_free||; the
+ * res_ref drop rule then judges the corrected start.  Without res_ref the convergence target
+ * stays relative to the uncorrected start's ||F_free|| (stats.res0).  V
+ * must stay valid while attached; V = NULL, m = 0 or steps = 0 detaches.  Needs the
+ * SNP_LAYOUT_ELEM layout.  No counterpart in the reference. */
+int snp_solver_set_galerkin_basis(snp_solver *s, const float *V, int32_t m, int64_t ldv, int32_t steps);
 
 /* Replace the node coordinates (device f64[n_nodes][3]) of a solver's mesh: same topology,
  * moved nodes (a morphed geometry).  The CSR pattern, element topology and materials stay.

@@ -38,7 +38,8 @@ class SolveOpts(ctypes.Structure):
 class SolveStats(ctypes.Structure):
     _fields_ = [("newton_iterations", _c_i32), ("cg_iterations", _c_i64), ("res0", _c_f64), ("res", _c_f64),
                 ("t_assemble_ms", _c_f64), ("t_krylov_ms", _c_f64), ("t_total_ms", _c_f64), ("status", _c_i32),
-                ("kernel_launches", _c_i64), ("residual_evals", _c_i32), ("start_dropped", _c_i32)]
+                ("kernel_launches", _c_i64), ("residual_evals", _c_i32), ("start_dropped", _c_i32),
+                ("galerkin_steps", _c_i32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -82,6 +83,8 @@ _SIGS = {
     "snp_solver_assemble": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snp_solver_pattern": [_vp, _pp],
     "snp_solver_jacobian_apply": [_vp, ctypes.c_int, _vp, _vp, _vp],
+    "snp_solver_reduced_system": [_vp, ctypes.c_int, _vp, ctypes.c_int32, ctypes.c_int64, _vp, _vp, _vp, _vp],
+    "snp_solver_set_galerkin_basis": [_vp, _vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32],
     "snp_solver_jacobian_layout": [_vp, ctypes.POINTER(ctypes.c_int)],
     "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
     "snp_solver_set_nodes": [_vp, _vp, _vp],

@@ -380,6 +380,170 @@ __global__ void __launch_bounds__(kEBlock)
     }
 }
 
+// ---------------------------------------------------------------- reduced (Galerkin) system
+//
+// Jr = V^T J V for a basis V [n][ldv] (float32, m <= 128 columns) on the free DoFs:
+// Jr = sum_e W_e^T S_e W_e with W_e = sum_k s_k chat_k V[dof_k, :] (3 x m, the curls of the
+// basis columns on element e).  A block takes one 64 x 64 block (bi, bj), bi <= bj, of Jr and a
+// share of the 32-element eslot groups; per group it forms W_e (columns of block bi) and
+// S_e W_e (columns of block bj) in shared memory (96 rows each), then every thread adds the
+// 96 rank-1 terms of its 4 x 4 piece in float64 registers.  Block partials are summed in a
+// fixed order by k_rsys_sum, so the result is deterministic.
+
+constexpr int kRsB = 64;         // output block edge
+constexpr int kRsRows = 3 * 32;  // rows of W per eslot group
+constexpr size_t kRsSmem = 2 * sizeof(double) * kRsRows * kRsB;
+
+__device__ __forceinline__ void rsys_job(int job, int nb, int &bi, int &bj) {
+    bi = 0;
+    while (job >= nb - bi) {
+        job -= nb - bi;
+        ++bi;
+    }
+    bj = bi + job;
+}
+
+template <typename TT>
+__global__ void __launch_bounds__(256)
+    k_rsys_jac(int64_t ne, const int32_t *__restrict__ edof, const TT *__restrict__ T, const TT *__restrict__ chat,
+               const uint8_t *__restrict__ free_mask, const float *__restrict__ V, int m, int64_t ldv, int nb,
+               double *__restrict__ part) {
+    extern __shared__ double rs_smem[];
+    double *Wi = rs_smem;                  // [96][64]  W_e, columns of block bi
+    double *Yj = rs_smem + kRsRows * kRsB;  // [96][64]  S_e W_e, columns of block bj
+    __shared__ uint32_t s_d[32][6];
+    __shared__ double s_t[32][6];
+    __shared__ double sc[18];
+    int bi, bj;
+    rsys_job(blockIdx.y, nb, bi, bj);
+    if (threadIdx.x < 18) sc[threadIdx.x] = (double)chat[threadIdx.x];
+    const int ti = threadIdx.x >> 4, tj = threadIdx.x & 15;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    const int64_t n_groups = (ne + 31) >> 5;
+    for (int64_t grp = blockIdx.x; grp < n_groups; grp += gridDim.x) {
+        __syncthreads();  // the previous group's rows are consumed
+        if (threadIdx.x < 192) {
+            const int k = threadIdx.x >> 5, l = threadIdx.x & 31;
+            const bool valid = (grp << 5) + l < ne;
+            const int64_t idx = (grp * 6 + k) * 32 + l;
+            s_d[l][k] = valid ? (uint32_t)edof[idx] : 0u;
+            s_t[l][k] = valid ? (double)T[idx] : 0.0;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < 32 * kRsB; q += blockDim.x) {
+            const int c = q & (kRsB - 1), l = q >> 6;
+            const int ci = bi * kRsB + c, cj = bj * kRsB + c;
+            double wi[3] = {0.0, 0.0, 0.0}, wj[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const uint32_t d = s_d[l][k];
+                const uint32_t g = d & ~kSignBit;
+                if (!is_free(free_mask, g)) continue;
+                double vi = ci < m ? (double)V[(int64_t)g * ldv + ci] : 0.0;
+                double vj = cj < m ? (double)V[(int64_t)g * ldv + cj] : 0.0;
+                if (d & kSignBit) {
+                    vi = -vi;
+                    vj = -vj;
+                }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    wi[a] = fma(vi, sc[3 * k + a], wi[a]);
+                    wj[a] = fma(vj, sc[3 * k + a], wj[a]);
+                }
+            }
+            const double *t = s_t[l];  // xx xy xz yy yz zz (zero for the padding of the last group)
+            Wi[(3 * l + 0) * kRsB + c] = wi[0];
+            Wi[(3 * l + 1) * kRsB + c] = wi[1];
+            Wi[(3 * l + 2) * kRsB + c] = wi[2];
+            Yj[(3 * l + 0) * kRsB + c] = t[0] * wj[0] + t[1] * wj[1] + t[2] * wj[2];
+            Yj[(3 * l + 1) * kRsB + c] = t[1] * wj[0] + t[3] * wj[1] + t[4] * wj[2];
+            Yj[(3 * l + 2) * kRsB + c] = t[2] * wj[0] + t[4] * wj[1] + t[5] * wj[2];
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int r = 0; r < kRsRows; ++r) {
+            const double2 a01 = *reinterpret_cast<const double2 *>(Wi + r * kRsB + 4 * ti);
+            const double2 a23 = *reinterpret_cast<const double2 *>(Wi + r * kRsB + 4 * ti + 2);
+            const double2 b01 = *reinterpret_cast<const double2 *>(Yj + r * kRsB + 4 * tj);
+            const double2 b23 = *reinterpret_cast<const double2 *>(Yj + r * kRsB + 4 * tj + 2);
+            const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+            const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        }
+    }
+    double *out = part + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * (kRsB * kRsB);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out[(4 * ti + a) * kRsB + 4 * tj + b] = acc[a][b];
+}
+
+// Jr from the block partials: one thread per entry of each (bi, bj) block, partials summed in
+// block order; the mirror (bj, bi) is written for off-diagonal blocks.
+__global__ void k_rsys_jac_sum(int n_parts, int n_jobs, int nb, int m, const double *__restrict__ part,
+                               double *__restrict__ Jr) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_jobs * kRsB * kRsB) return;
+    const int job = t / (kRsB * kRsB), ij = t - job * kRsB * kRsB;
+    int bi, bj;
+    rsys_job(job, nb, bi, bj);
+    const int r = bi * kRsB + ij / kRsB, c = bj * kRsB + (ij & (kRsB - 1));
+    if (r >= m || c >= m) return;
+    double s = 0.0;
+    for (int p = 0; p < n_parts; ++p) s += part[((int64_t)job * n_parts + p) * (kRsB * kRsB) + ij];
+    Jr[(int64_t)r * m + c] = s;
+    if (bi != bj) Jr[(int64_t)c * m + r] = s;
+}
+
+// g = V^T F over the free DoFs: 64 columns per block row (grid.y), four DoFs per pass.
+__global__ void __launch_bounds__(256)
+    k_rsys_rhs(int32_t n, const uint8_t *__restrict__ free_mask, const float *__restrict__ V, int m, int64_t ldv,
+               const double *__restrict__ F, double *__restrict__ part) {
+    __shared__ double sh[4][kRsB];
+    const int c = blockIdx.y * kRsB + (threadIdx.x & (kRsB - 1)), lane4 = threadIdx.x >> 6;
+    double acc = 0.0;
+    if (c < m)
+        for (int64_t i = (int64_t)blockIdx.x * 4 + lane4; i < n; i += (int64_t)gridDim.x * 4)
+            if (is_free(free_mask, i)) acc = fma((double)V[i * ldv + c], F[i], acc);
+    sh[lane4][threadIdx.x & (kRsB - 1)] = acc;
+    __syncthreads();
+    if (threadIdx.x < kRsB)
+        part[((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * kRsB + threadIdx.x] =
+            (sh[0][threadIdx.x] + sh[1][threadIdx.x]) + (sh[2][threadIdx.x] + sh[3][threadIdx.x]);
+}
+
+__global__ void k_rsys_rhs_sum(int n_parts, int m, const double *__restrict__ part, double *__restrict__ g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    const int cb = c / kRsB, cl = c & (kRsB - 1);
+    double s = 0.0;
+    for (int p = 0; p < n_parts; ++p) s += part[((int64_t)cb * n_parts + p) * kRsB + cl];
+    g[c] = s;
+}
+
+// x_i += sum_c V[i][c] coef_c on the free DoFs: one warp per DoF, lanes over the columns,
+// then a fixed shuffle tree (deterministic).
+__global__ void k_basis_axpy(int32_t n, const uint8_t *__restrict__ free_mask, const float *__restrict__ V, int m,
+                             int64_t ldv, const double *__restrict__ coef, double *__restrict__ x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        if (!is_free(free_mask, i)) continue;
+        double acc = 0.0;
+        for (int c = lane; c < m; c += 32) acc = fma((double)V[i * ldv + c], coef[c], acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) x[i] += acc;
+    }
+}
+
 template <typename TT>
 const TT *chat_ptr(const ElemTopology &top);
 template <>
@@ -651,6 +815,61 @@ int ElemPcg<TT>::apply(const ElemTopology &top, const TT *T, const uint8_t *free
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }
+
+template <typename TT>
+int elem_reduced_system(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const float *V, int m,
+                        int64_t ldv, const double *F, double *Jr, double *g, DevBuf<double> &scratch,
+                        cudaStream_t s) {
+    SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "reduced system: topology not built");
+    SNP_REQUIRE(V != nullptr && Jr != nullptr, "reduced system: V or Jr is NULL");
+    SNP_REQUIRE(m >= 1 && m <= 2 * kRsB && ldv >= m, "reduced system: need 1 <= m <= %d and ldv >= m", 2 * kRsB);
+    SNP_REQUIRE(F == nullptr || g != nullptr, "reduced system: F given without g");
+    const int nb = (m + kRsB - 1) / kRsB, n_jobs = nb * (nb + 1) / 2;
+    // set once per process (thread-safe static initialisation)
+    static const cudaError_t smem_rc = [] {
+        cudaError_t e = cudaFuncSetAttribute(k_rsys_jac<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRsSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_rsys_jac<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRsSmem);
+        return e;
+    }();
+    SNP_CUDA_TRY(smem_rc);
+    const int64_t n_groups = (top.n_elems + 31) >> 5;
+    int per_sm = resident_blocks(reinterpret_cast<const void *>(k_rsys_jac<TT>), 256, kRsSmem);
+    if (per_sm < 1) per_sm = 1;
+    int64_t gx = ((int64_t)sm_count() * per_sm + n_jobs - 1) / n_jobs;
+    if (gx > n_groups) gx = n_groups;
+    const int gr = 4 * sm_count();
+    const size_t need = (size_t)n_jobs * gx * kRsB * kRsB + (size_t)nb * gr * kRsB;
+    if (scratch.n < need) SNP_TRY(scratch.alloc(need));
+    double *pj = scratch.p, *pr = scratch.p + (size_t)n_jobs * gx * kRsB * kRsB;
+    k_rsys_jac<TT><<<dim3((unsigned)gx, (unsigned)n_jobs), 256, kRsSmem, s>>>(top.n_elems, top.edof.p, T,
+                                                                            chat_ptr<TT>(top), free_mask, V, m, ldv,
+                                                                            nb, pj);
+    SNP_LAUNCH_CHECK();
+    const int tot = n_jobs * kRsB * kRsB;
+    k_rsys_jac_sum<<<(tot + 255) / 256, 256, 0, s>>>((int)gx, n_jobs, nb, m, pj, Jr);
+    SNP_LAUNCH_CHECK();
+    if (F) {
+        k_rsys_rhs<<<dim3((unsigned)gr, (unsigned)nb), 256, 0, s>>>(top.n, free_mask, V, m, ldv, F, pr);
+        SNP_LAUNCH_CHECK();
+        k_rsys_rhs_sum<<<(m + 127) / 128, 128, 0, s>>>(gr, m, pr, g);
+        SNP_LAUNCH_CHECK();
+    }
+    return SNP_OK;
+}
+
+int basis_axpy(int32_t n, const uint8_t *free_mask, const float *V, int m, int64_t ldv, const double *coef,
+               double *x, cudaStream_t s) {
+    SNP_REQUIRE(V != nullptr && coef != nullptr && x != nullptr && m >= 1 && ldv >= m, "basis axpy: bad arguments");
+    k_basis_axpy<<<wave_grid(k_basis_axpy, 32 * (int64_t)n, kEBlock), kEBlock, 0, s>>>(n, free_mask, V, m, ldv, coef, x);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+template int elem_reduced_system<double>(const ElemTopology &, const double *, const uint8_t *, const float *, int,
+                                         int64_t, const double *, double *, double *, DevBuf<double> &, cudaStream_t);
+template int elem_reduced_system<float>(const ElemTopology &, const float *, const uint8_t *, const float *, int,
+                                        int64_t, const double *, double *, double *, DevBuf<double> &, cudaStream_t);
 
 template struct ElemPcg<double>;
 template struct ElemPcg<float>;

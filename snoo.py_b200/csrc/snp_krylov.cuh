@@ -134,6 +134,17 @@ int build_elem_topology(ElemTopology &top, int32_t n, const ElemBlock *blocks, i
 int elem_sum_to_dofs(const ElemTopology &top, const double *Fe, const double *De, const double *rhs_extra,
                      double *F, double *diag, cudaStream_t s);
 
+// Reduced (Galerkin) system of the matrix-free Jacobian T for a float32 basis V [n][ldv]
+// (m <= 128 columns): Jr = V^T J V (m x m, row-major) and, when F is given, g = V^T F, both
+// over the free DoFs and summed in float64 in a fixed order.  scratch grows as needed.
+template <typename TT>
+int elem_reduced_system(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const float *V, int m,
+                        int64_t ldv, const double *F, double *Jr, double *g, DevBuf<double> &scratch, cudaStream_t s);
+
+// x += V coef on the free DoFs (V float32 [n][ldv], m columns; coef float64 [m], device).
+int basis_axpy(int32_t n, const uint8_t *free_mask, const float *V, int m, int64_t ldv, const double *coef,
+               double *x, cudaStream_t s);
+
 template <typename TT>
 struct alignas(2 * sizeof(TT)) DofPair {
     TT a, b;

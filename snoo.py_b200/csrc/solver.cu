@@ -44,6 +44,53 @@ struct Material {
     double dil[4] = {0.0, 0.0, 1.0, 0.0};
 };
 
+// c = -A^-1 g for a symmetric positive semi-definite m x m matrix A (row-major): Cholesky of
+// the Jacobi-scaled matrix; a direction whose pivot falls below 1e-10 of its diagonal (a
+// dependent basis column) is left out of the solve.  False when A has a non-positive or
+// non-finite diagonal entry.
+bool spd_solve(int m, const double *A, const double *g, double *c) {
+    std::vector<double> L((size_t)m * m), d(m), y(m);
+    for (int i = 0; i < m; ++i) {
+        const double a = A[(size_t)i * m + i];
+        if (!(a > 0.0) || !std::isfinite(a)) return false;
+        d[i] = 1.0 / std::sqrt(a);
+    }
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) L[(size_t)i * m + j] = A[(size_t)i * m + j] * d[i] * d[j];
+    std::vector<char> keep(m, 1);
+    for (int j = 0; j < m; ++j) {
+        double p = L[(size_t)j * m + j];
+        for (int k = 0; k < j; ++k) p -= L[(size_t)j * m + k] * L[(size_t)j * m + k];
+        if (!(p > 1e-10)) {
+            keep[j] = 0;
+            for (int i = j; i < m; ++i) L[(size_t)i * m + j] = 0.0;
+            continue;
+        }
+        const double ljj = std::sqrt(p);
+        L[(size_t)j * m + j] = ljj;
+        for (int i = j + 1; i < m; ++i) {
+            double t = L[(size_t)i * m + j];
+            for (int k = 0; k < j; ++k) t -= L[(size_t)i * m + k] * L[(size_t)j * m + k];
+            L[(size_t)i * m + j] = t / ljj;
+        }
+    }
+    for (int i = 0; i < m; ++i) {  // L y = -D g
+        double t = -d[i] * g[i];
+        for (int k = 0; k < i; ++k) t -= L[(size_t)i * m + k] * y[k];
+        y[i] = keep[i] ? t / L[(size_t)i * m + i] : 0.0;
+    }
+    for (int i = m - 1; i >= 0; --i) {  // L^T z = y, c = D z
+        double t = y[i];
+        for (int k = i + 1; k < m; ++k) t -= L[(size_t)k * m + i] * c[k];
+        c[i] = keep[i] ? t / L[(size_t)i * m + i] : 0.0;
+    }
+    for (int i = 0; i < m; ++i) {
+        if (!std::isfinite(c[i])) return false;
+    }
+    for (int i = 0; i < m; ++i) c[i] *= d[i];
+    return true;
+}
+
 // res[0] += sum over free i of v[i]^2 (deterministic last-block reduction)
 // res[1]  = max over all i of |v[i]|; res[2] = max |v - w| and res[3] = max |v| (when w != null)
 __global__ void k_vstats(int32_t n, const uint8_t *__restrict__ fm, const double *__restrict__ v,
@@ -186,7 +233,14 @@ struct snp_solver {
     snp::SellLayout sell;
     bool use_sell = false;
     snp::ElemTopology etop;
-    snp::DevBuf<double> T64, Jdiag, Fe, De;
+    snp::DevBuf<double> T64, Jdiag, Fe, De, rsys_scratch;
+    // Galerkin correction of a warm start (snp_solver_set_galerkin_basis): basis, its system
+    // and coefficients on the device and in pinned memory, and a copy of x to fall back to
+    const float *gal_V = nullptr;
+    int32_t gal_m = 0, gal_steps = 0;
+    int64_t gal_ldv = 0;
+    snp::DevBuf<double> gal_sys, gal_x;
+    snp::HostBuf<double> gal_host;
     snp::DevBuf<float> T32;
     snp::ElemPcg<double> epcg64;
     snp::ElemPcg<float> epcg32;
@@ -300,6 +354,32 @@ struct snp_solver {
     }
 
     // Newton-loop assembly at x in the solver's layout: Jacobian (precision f32 or not) and F.
+    // One Galerkin Newton step from x in the span of the attached basis, with the Jacobian and
+    // F of the last assembly at x: x += V c, (V^T J V) c = -V^T F.  *applied = false (x kept)
+    // when the reduced system is not positive definite.
+    int galerkin_step(double *x, bool f32, bool *applied) {
+        *applied = false;
+        const int m = gal_m;
+        double *Jr = gal_sys.p, *g = gal_sys.p + (size_t)m * m, *c = g + m;
+        if (f32)
+            SNP_TRY(snp::elem_reduced_system(etop, T32.p, free_mask.p, gal_V, m, gal_ldv, F.p, Jr, g, rsys_scratch,
+                                             stream));
+        else
+            SNP_TRY(snp::elem_reduced_system(etop, T64.p, free_mask.p, gal_V, m, gal_ldv, F.p, Jr, g, rsys_scratch,
+                                             stream));
+        launches += 4;
+        SNP_CUDA_TRY(cudaMemcpyAsync(gal_host.p, gal_sys.p, sizeof(double) * ((size_t)m * m + m),
+                                     cudaMemcpyDeviceToHost, stream));
+        SNP_CUDA_TRY(cudaStreamSynchronize(stream));
+        double *ch = gal_host.p + (size_t)m * m + m;
+        if (!snp::spd_solve(m, gal_host.p, gal_host.p + (size_t)m * m, ch)) return SNP_OK;
+        SNP_CUDA_TRY(cudaMemcpyAsync(c, ch, sizeof(double) * m, cudaMemcpyHostToDevice, stream));
+        SNP_TRY(snp::basis_axpy(n, free_mask.p, gal_V, m, gal_ldv, c, x, stream));
+        ++launches;
+        *applied = true;
+        return SNP_OK;
+    }
+
     int assemble_newton(const double *x, bool f32) {
         if (layout == SNP_LAYOUT_ELEM) return assemble_elem(x, f32, F.p);
         return assemble(x, nullptr, f32 ? nullptr : J.p, f32 ? J32.p : nullptr, nullptr, F.p, true);
@@ -439,6 +519,35 @@ struct snp_solver {
             S.t_assemble_ms += elapsed(0, 1);
             double fn = std::sqrt(st3[0]);
             S.res0 = fn;
+            // Galerkin correction of the start in the attached basis; a step that does not lower
+            // ||F_free|| is undone.  The drop rule below judges the corrected start.
+            if (gal_V && gal_m > 0 && layout == SNP_LAYOUT_ELEM && fn > 0.0) {
+                for (int gs = 0; gs < gal_steps; ++gs) {
+                    SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
+                    SNP_CUDA_TRY(cudaMemcpyAsync(gal_x.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+                    bool applied = false;
+                    SNP_TRY(galerkin_step(x, f32, &applied));
+                    if (!applied) break;
+                    SNP_TRY(assemble_newton(x, f32));
+                    SNP_TRY(vstats(F.p, nullptr, true, st3));
+                    const double fg = std::sqrt(st3[0]);
+                    if (!(fg < fn)) {
+                        SNP_CUDA_TRY(cudaMemcpyAsync(x, gal_x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+                        SNP_TRY(assemble_newton(x, f32));
+                        SNP_TRY(vstats(F.p, nullptr, true, st3));
+                        SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                        SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
+                        S.t_assemble_ms += elapsed(0, 1);
+                        fn = std::sqrt(st3[0]);
+                        break;
+                    }
+                    SNP_CUDA_TRY(cudaEventRecord(ev[1], stream));
+                    SNP_CUDA_TRY(cudaEventSynchronize(ev[1]));
+                    S.t_assemble_ms += elapsed(0, 1);
+                    fn = fg;
+                    S.galerkin_steps += 1;
+                }
+            }
             if (o.res_ref > 0.0 && !(fn <= o.res_ref * (1.0 + 1e-9))) {
                 // a start worse than x = 0 (by the zero-start residual, up to rounding of the
                 // two evaluations) is dropped for x = 0
@@ -452,7 +561,7 @@ struct snp_solver {
                 fn = std::sqrt(st3[0]);
                 S.start_dropped = 1;
             }
-            F0 = o.res_ref > 0.0 ? o.res_ref : fn;
+            F0 = o.res_ref > 0.0 ? o.res_ref : S.res0;
             for (int it = 0;; ++it) {
                 if (!(fn == fn)) return snp::fail(SNP_NAN_DETECTED, "Newton step %d: non-finite residual", it);
                 S.res = fn;
@@ -811,6 +920,43 @@ int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void 
     SNP_REQUIRE(s->j_valid[precision], "snp_solver_jacobian_apply: no %s Newton Jacobian (run a solve first)",
                 precision ? "float32" : "float64");
     return s->apply_jacobian(precision, x, y, stream ? snp::as_stream(stream) : s->stream);
+}
+
+int snp_solver_set_galerkin_basis(snp_solver *s, const float *V, int32_t m, int64_t ldv, int32_t steps) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_set_galerkin_basis: solver missing or not finalized");
+    if (V == nullptr || m == 0 || steps == 0) {
+        s->gal_V = nullptr;
+        s->gal_m = s->gal_steps = 0;
+        return SNP_OK;
+    }
+    SNP_REQUIRE(s->layout == SNP_LAYOUT_ELEM, "snp_solver_set_galerkin_basis: the solver's Jacobian layout is not elem");
+    SNP_REQUIRE(m >= 1 && m <= 128 && ldv >= m && steps >= 1, "snp_solver_set_galerkin_basis: need 1 <= m <= 128, "
+                "ldv >= m and steps >= 1");
+    if (s->gal_sys.n < (size_t)m * m + 2 * (size_t)m) {
+        SNP_TRY(s->gal_sys.alloc((size_t)m * m + 2 * (size_t)m));
+        SNP_TRY(s->gal_host.alloc((size_t)m * m + 2 * (size_t)m));
+    }
+    if (s->gal_x.n < (size_t)s->n) SNP_TRY(s->gal_x.alloc(s->n));
+    s->gal_V = V;
+    s->gal_m = m;
+    s->gal_ldv = ldv;
+    s->gal_steps = steps;
+    return SNP_OK;
+}
+
+int snp_solver_reduced_system(snp_solver *s, int precision, const float *V, int m, int64_t ldv, const double *F,
+                              double *Jr, double *g, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_reduced_system: solver missing or not finalized");
+    SNP_REQUIRE(s->layout == SNP_LAYOUT_ELEM, "snp_solver_reduced_system: the solver's Jacobian layout is not elem");
+    SNP_REQUIRE(precision == 0 || precision == 1, "snp_solver_reduced_system: precision must be 0 or 1");
+    SNP_REQUIRE(s->j_valid[precision], "snp_solver_reduced_system: no %s Newton Jacobian (assemble first)",
+                precision ? "float32" : "float64");
+    cudaStream_t st = stream ? snp::as_stream(stream) : s->stream;
+    if (precision == 0)
+        return snp::elem_reduced_system(s->etop, s->T64.p, s->free_mask.p, V, m, ldv, F, Jr, g, s->rsys_scratch, st);
+    return snp::elem_reduced_system(s->etop, s->T32.p, s->free_mask.p, V, m, ldv, F, Jr, g, s->rsys_scratch, st);
 }
 
 int snp_solver_jacobian_layout(const snp_solver *s, int *layout) {

@@ -164,6 +164,35 @@ class DeviceNewton:
         self._leave()
         return y
 
+    def reduced_system(self, V, F=None, precision="fp64"):
+        """Galerkin system in the span of V (CUDA float32 [n, m], row-major, m <= 128) with the
+        Jacobian of the last ``assemble_tensors`` of that precision: (V^T J V [m, m], V^T F [m]
+        or None), float64 on the device, summed in a fixed order."""
+        t = torch()
+        assert V.dtype == t.float32 and V.is_cuda and V.dim() == 2 and V.stride(1) == 1 and V.shape[0] == self.n
+        m = int(V.shape[1])
+        Jr = t.empty((m, m), dtype=t.float64, device="cuda")
+        g = t.empty(m, dtype=t.float64, device="cuda") if F is not None else None
+        self._enter()
+        _lib.call("snp_solver_reduced_system", self.handle, {"fp64": 0, "mixed": 1}[precision], _lib.ptr(V), m,
+                  int(V.stride(0)), _lib.ptr(F), _lib.ptr(Jr), _lib.ptr(g), _lib.stream_ptr(self._stream))
+        self._leave()
+        return Jr, g
+
+    def set_galerkin_basis(self, V=None, steps=1):
+        """Attach a basis (CUDA float32 [n, m], row-major, m <= 128) whose Galerkin Newton step
+        corrects every kept start of the residual-mode solves (up to ``steps`` steps, each kept
+        only when it lowers ||F_free||); None detaches.  The tensor is held while attached."""
+        t = torch()
+        if V is None:
+            _lib.call("snp_solver_set_galerkin_basis", self.handle, None, 0, 0, 0)
+            self._galerkin_V = None
+            return
+        assert V.dtype == t.float32 and V.is_cuda and V.dim() == 2 and V.stride(1) == 1 and V.shape[0] == self.n
+        _lib.call("snp_solver_set_galerkin_basis", self.handle, _lib.ptr(V), int(V.shape[1]), int(V.stride(0)),
+                  int(steps))
+        self._galerkin_V = V
+
     def __del__(self):
         try:
             if getattr(self, "handle", None) is not None and _lib._lib is not None:

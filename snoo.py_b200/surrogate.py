@@ -218,6 +218,11 @@ class MorphedSolver:
         self._nodes, self._Bs = nodes, Bs  # keep the uploads referenced while the stream uses them
         return self.eng.residual_norm(self._zero)
 
+    def attach_basis(self, V=None, steps=1):
+        """Galerkin-correct every kept start in the span of V (``WarmStart.galerkin_basis``)
+        inside the solve (``snp_solver_set_galerkin_basis``); None detaches."""
+        self.eng.set_galerkin_basis(V, steps)
+
     def solve(self, x0=None, rtol=1e-8, precision="mixed", res_ref=0.0):
         prec = {"fp64": 0, "mixed": 1}[precision]
         return self.eng.solve(x0, mode=1, tol=rtol, max_newton=self.max_newton, precision=prec, cg_maxiter=50000,
@@ -314,15 +319,44 @@ class WarmStart:
         self.timings["fit_s"] = time.perf_counter() - t0
         return self
 
-    def predict(self, params):
-        """Starting vectors [P, n] (float64, device) for parameter rows."""
+    def predict(self, params, check=True):
+        """Starting vectors [P, n] (float64, device) for parameter rows.  ``check=False`` skips
+        the synchronising check of the GEMM's error flag (call ``mlp.check_errors()`` later)."""
         t = torch()
         X = self.mlp.input_bf16(t.as_tensor(np.atleast_2d(params), dtype=t.float32, device="cuda"))
         Y = self.mlp.forward(X)
-        self.mlp.check_errors()
+        if check:
+            self.mlp.check_errors()
         c = Y.double() * self.c_sd + self.c_mu
         return self.mean + c @ self.U.T
 
     def project(self, x):
         """Best POD approximation of a solution (the surrogate's floor)."""
         return self.mean + ((x.double() - self.mean) @ self.U) @ self.U.T
+
+    def galerkin_basis(self, modes):
+        """The first ``modes`` POD modes as a row-major float32 [n, modes] CUDA tensor (cached)."""
+        modes = int(min(modes, self.U.shape[1]))
+        if getattr(self, "_gb", None) is None or self._gb.shape[1] != modes:
+            self._gb = self.U[:, :modes].float().contiguous()
+        return self._gb
+
+    def correct(self, x0, msolver=None, modes=64, precision="mixed", steps=1):
+        """Galerkin Newton step(s) on a warm start in the span V of the first ``modes`` POD
+        modes: assemble J(x) and F(x) (matrix-free, ``precision``), solve (V^T J V) c = -V^T F
+        (both from ``snp_solver_reduced_system``), x += V c.  The member must already be set on
+        ``msolver`` (default: the training solver).  Returns a new float64 vector; the Newton
+        solve that follows still judges it by its residual.  A singular reduced system leaves
+        x unchanged."""
+        t = torch()
+        ms = msolver or self.ms
+        V = self.galerkin_basis(modes)
+        x = x0.double().clone()
+        F = zeros(ms.n)[: ms.n]
+        for _ in range(steps):
+            ms.eng.assemble_tensors(x, precision, F)
+            Jr, g = ms.eng.reduced_system(V, F, precision)
+            c, info = t.linalg.solve_ex(Jr, -g)
+            c = t.where(info == 0, c, t.zeros_like(c))
+            x += (V @ c.float()).double()
+        return x

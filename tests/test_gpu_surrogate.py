@@ -130,3 +130,86 @@ def test_members_solved_at_once_match_one_at_a_time(family_setup):
         assert s["rel_res"] <= 1e-8 and s["status"] == 0
         assert s["newton_iterations"] == s1["newton_iterations"] and s["cg_iterations"] == s1["cg_iterations"]
         assert torch.equal(x, x1)
+
+
+def test_reduced_system_matches_products(family_setup):
+    """V^T J V and V^T F from the fused kernel against column-by-column Jacobian products,
+    for 80 columns (a full and a partial 64-column block) in float64 and float32."""
+    fam, ms, P_train, P_test = family_setup
+    ref = ms.set_member(P_test[1])
+    x, _ = ms.solve(None, rtol=1e-4, precision="fp64", res_ref=ref)
+    eng = ms.eng
+    fm = eng.free_mask.bool()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    V = torch.randn((ms.n, 80), generator=g, device="cuda", dtype=torch.float32)
+    F = torch.zeros(ms.n, dtype=torch.float64, device="cuda")
+    for prec, dt, tol in (("fp64", torch.float64, 1e-12), ("mixed", torch.float32, 1e-5)):
+        eng.assemble_tensors(x, prec, F)
+        Jr, gr = eng.reduced_system(V, F, prec)
+        JV = torch.empty((ms.n, 80), dtype=torch.float64, device="cuda")
+        for j in range(80):
+            y = torch.zeros(ms.n, dtype=dt, device="cuda")
+            eng.jacobian_apply(V[:, j].to(dt).contiguous(), y, prec)
+            JV[:, j] = y.double()
+        Vf = torch.where(fm[:, None], V.double(), torch.zeros_like(JV))
+        A = Vf.T @ JV
+        assert torch.allclose(Jr, Jr.T, rtol=0, atol=1e-12 * float(Jr.abs().max()))
+        assert float((Jr - A).abs().max()) <= tol * float(A.abs().max()), prec
+        b = Vf.T @ torch.where(fm, F, torch.zeros_like(F))
+        assert float((gr - b).abs().max()) <= 1e-12 * float(b.abs().max()), prec
+    # a basis view with a leading dimension larger than its width
+    eng.assemble_tensors(x, "fp64", F)
+    Jr_all, _ = eng.reduced_system(V, None, "fp64")
+    Jr_view, _ = eng.reduced_system(V[:, :20], None, "fp64")
+    assert float((Jr_view - Jr_all[:20, :20]).abs().max()) <= 1e-12 * float(Jr_all.abs().max())
+
+
+def test_galerkin_correction_cuts_the_residual(family_setup):
+    """One Galerkin Newton step in a POD basis moves a start (the POD mean) closer to the
+    member's solution, and Newton from it reaches the same field."""
+    fam, ms, P_train, P_test = family_setup
+    ws = SG.WarmStart(ms, n_modes=16, hidden=32, seed=0)
+    snaps, _ = ws.generate(P_train[:24], precision="fp64")
+    ws.mean, ws.U, _, _ = SG.pod(snaps, 16)
+    eng = ms.eng
+    for p in P_test[:3]:
+        ref = ms.set_member(p)
+        x0 = ws.mean.clone()
+        x1 = ws.correct(x0, modes=16, precision="mixed")
+        r0, r1 = eng.residual_norm(x0), eng.residual_norm(x1)
+        assert r1 < 0.5 * r0, (r0, r1)
+        xz, sz = ms.solve(None, rtol=1e-8, precision="fp64", res_ref=ref)
+        xg, sg = ms.solve(x1, rtol=1e-8, precision="fp64", res_ref=ref)
+        assert sg["start_dropped"] == 0 and sg["rel_res"] <= 1e-8
+        assert sg["cg_iterations"] < sz["cg_iterations"]
+
+
+def test_galerkin_correction_inside_the_solve(family_setup):
+    """The same step taken inside snp_solver_solve (attached basis): applied to the start,
+    fewer CG iterations to the same target, and members solved at once give bitwise the
+    one-at-a-time answers.  No res_ref, so both starts are kept and held to ||F_free(mean)||."""
+    fam, ms, P_train, P_test = family_setup
+    ws = SG.WarmStart(ms, n_modes=16, hidden=32, seed=0)
+    snaps, _ = ws.generate(P_train[:24], precision="fp64")
+    ws.mean, ws.U, _, _ = SG.pod(snaps, 16)
+    V = ws.galerkin_basis(16)
+    corrected = []
+    for p in P_test[:3]:
+        ms.set_member(p)
+        x0, s0 = ms.solve(ws.mean, rtol=1e-8, precision="mixed")
+        ms.attach_basis(V)
+        x1, s1 = ms.solve(ws.mean, rtol=1e-8, precision="mixed")
+        ms.attach_basis(None)
+        assert s0["galerkin_steps"] == 0 and s1["galerkin_steps"] == 1
+        assert s1["res0"] == s0["res0"] and s1["res"] <= 1e-8 * s1["res0"]
+        assert s1["cg_iterations"] < s0["cg_iterations"], (s0["cg_iterations"], s1["cg_iterations"])
+        corrected.append((x1, s1))
+    mss = [SG.MorphedSolver(fam, stream=torch.cuda.Stream()) for _ in range(3)]
+    for m in mss:
+        m.attach_basis(V)
+    for m, p in zip(mss, P_test[:3]):
+        m.set_member(p)
+    xs, st = SG.solve_members_at_once(mss, [ws.mean] * 3, [0.0] * 3, rtol=1e-8, precision="mixed")
+    for x, s, (x1, s1) in zip(xs, st, corrected):
+        assert s["galerkin_steps"] == 1 and s["cg_iterations"] == s1["cg_iterations"]
+        assert torch.equal(x, x1)
