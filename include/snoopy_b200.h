@@ -358,6 +358,33 @@ int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void 
 int snp_solver_reduced_system(snp_solver *s, int precision, const float *V, int32_t m, int64_t ldv, const double *F,
                               double *Jr, double *g, void *stream);
 
+/* Block-Jacobi preconditioner for the residual-mode (mode 1) Krylov solves of the
+ * SNP_LAYOUT_ELEM layout, in place of point Jacobi.  meta (HOST uint16[n_dofs]) partitions the
+ * DoFs into blocks of 1..8 consecutive DoFs that never cross a multiple of 256:
+ * meta[i] = (offset of DoF i in its block) | (block size << 8); a constrained DoF must be a
+ * block of its own.  Before every Krylov solve the block-diagonal entries of the Newton
+ * Jacobian are summed from the element tensors (per DoF row, fixed order), each block is
+ * inverted by Cholesky in float64 (point Jacobi for a block with a pivot below 1e-12 of its
+ * diagonal) and stored in float32; the DoF pass forms z = M r per block.  Deterministic.  For
+ * edge DoFs numbered by their lower node, blocks of the edges that share that node halve the CG
+ * iterations of the window-frame yoke.  meta = NULL goes back to point Jacobi.  The
+ * reference-semantics mode keeps point Jacobi (red_mvp_solver.py:199 builds
+ * M = diags(1 / diag(J))).  Synchronises (meta is checked and uploaded). */
+int snp_solver_set_block_jacobi(snp_solver *s, const uint16_t *meta);
+
+/* z = M r (device float64 [n_dofs]) with the block Jacobi built from the element tensors of
+ * the last snp_solver_assemble_tensors of that precision; *fallback_blocks (host, may be NULL)
+ * receives the number of blocks inverted as point Jacobi.  Synchronises when fallback_blocks
+ * is given.  No counterpart in the reference. */
+int snp_solver_precond_apply(snp_solver *s, int precision, const double *r, double *z, int32_t *fallback_blocks,
+                             void *stream);
+
+/* The block-Jacobi rows built from the element tensors of the last snp_solver_assemble_tensors
+ * of that precision: bmat (device f64 [n_dofs][8], row i = J_(i, b0 + c) over DoF i's block
+ * starting at b0) and binv (device f32 [n_dofs][8], the rows of the block inverses); either
+ * may be NULL.  Inspection and test entry. */
+int snp_solver_block_jacobi_export(snp_solver *s, int precision, double *bmat, float *binv, void *stream);
+
 /* Attach a basis (device float32, row-major [n_dofs][ldv], first m <= 128 columns) to the
  * solver's mode-1 solves: the start first takes up to `steps` Galerkin Newton steps
  * x += V c, (V^T J V) c = -V^T F (snp_solver_reduced_system; the m x m system by Cholesky on

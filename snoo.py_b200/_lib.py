@@ -85,6 +85,9 @@ _SIGS = {
     "snp_solver_jacobian_apply": [_vp, ctypes.c_int, _vp, _vp, _vp],
     "snp_solver_reduced_system": [_vp, ctypes.c_int, _vp, ctypes.c_int32, ctypes.c_int64, _vp, _vp, _vp, _vp],
     "snp_solver_set_galerkin_basis": [_vp, _vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32],
+    "snp_solver_set_block_jacobi": [_vp, _vp],
+    "snp_solver_block_jacobi_export": [_vp, ctypes.c_int, _vp, _vp, _vp],
+    "snp_solver_precond_apply": [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(ctypes.c_int32), _vp],
     "snp_solver_jacobian_layout": [_vp, ctypes.POINTER(ctypes.c_int)],
     "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
     "snp_solver_set_nodes": [_vp, _vp, _vp],

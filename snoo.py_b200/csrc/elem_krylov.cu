@@ -528,6 +528,307 @@ __global__ void k_rsys_rhs_sum(int n_parts, int m, const double *__restrict__ pa
     g[c] = s;
 }
 
+// ---------------------------------------------------------------- block Jacobi
+//
+// The DoFs are cut into blocks of at most kBjMax consecutive free DoFs (for edge DoFs numbered
+// by their lower node: the edges that share that node) that never cross a multiple of kBjTile;
+// meta[i] = offset of DoF i in its block | block size << 8, constrained DoFs are blocks of their
+// own.  Per Newton step the block-diagonal entries of J are summed per DoF row over the DoF's
+// incidence list (fixed order), each block is inverted by Cholesky (point Jacobi for a block
+// whose pivot falls below 1e-12 of its diagonal) and stored as float32 rows of kBjMax, and the
+// PCG's DoF pass stages r of a kBjTile-DoF tile in shared memory so that each DoF forms
+// z_i = sum_j M_ij r_j over its block.
+
+constexpr int kBjMax = 8;
+constexpr int kBjTile = kEBlock;
+
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_bj_entries(int32_t n, const uint8_t *__restrict__ free_mask, const int32_t *__restrict__ inc_ptr,
+                 const int32_t *__restrict__ inc, const int32_t *__restrict__ edof, const TT *__restrict__ T,
+                 const TT *__restrict__ chat, const uint16_t *__restrict__ meta, double *__restrict__ bmat) {
+    __shared__ double sc[18];
+    if (threadIdx.x < 18) sc[threadIdx.x] = (double)chat[threadIdx.x];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double row[kBjMax];
+#pragma unroll
+        for (int c = 0; c < kBjMax; ++c) row[c] = 0.0;
+        if (is_free(free_mask, i)) {
+            const unsigned mt = meta[i];
+            const int64_t b0 = i - (int64_t)(mt & 0xffu);
+            const int size = (int)(mt >> 8);
+            for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
+                const uint32_t u = (uint32_t)inc[t];
+                const uint32_t ek = u & ~kSignBit;
+                const int k = (int)(ek & 7u);
+                const int64_t eb = eslot((int64_t)(ek >> 3), 0);
+                double tt[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) tt[c] = (double)T[eb + 32 * c];
+                const double c0 = sc[3 * k], c1 = sc[3 * k + 1], c2 = sc[3 * k + 2];
+                const double v0 = tt[0] * c0 + tt[1] * c1 + tt[2] * c2;
+                const double v1 = tt[1] * c0 + tt[3] * c1 + tt[4] * c2;
+                const double v2 = tt[2] * c0 + tt[4] * c1 + tt[5] * c2;
+#pragma unroll
+                for (int k2 = 0; k2 < 6; ++k2) {
+                    const uint32_t d2 = (uint32_t)edof[eb + 32 * k2];
+                    const int64_t r = (int64_t)(d2 & ~kSignBit) - b0;
+                    if (r < 0 || r >= size) continue;
+                    double val = sc[3 * k2] * v0 + sc[3 * k2 + 1] * v1 + sc[3 * k2 + 2] * v2;
+                    if ((u ^ d2) & kSignBit) val = -val;
+#pragma unroll
+                    for (int c = 0; c < kBjMax; ++c)
+                        if (c == r) row[c] += val;
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kBjMax; ++c) bmat[i * kBjMax + c] = row[c];
+    }
+}
+
+// one thread per block: Cholesky of the block (upper triangle of its rows), padded to 8 x 8 with
+// the identity so that every loop unrolls with fixed indices (registers, no local arrays); the
+// lower triangle of the inverse is written to both sides (symmetric by construction), rounded
+// to float32.  Point Jacobi for a block whose pivot is not positive enough.
+__global__ void __launch_bounds__(128)
+    k_bj_invert(int32_t n, const uint8_t *__restrict__ free_mask, const uint16_t *__restrict__ meta,
+                const double *__restrict__ bmat, float *__restrict__ binv, int *n_fallback) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned mt = meta[i];
+        if (mt & 0xffu) continue;
+        const int size = (int)(mt >> 8);
+        const bool fr = is_free(free_mask, i);
+        double L[kBjMax][kBjMax], d0[kBjMax];
+#pragma unroll
+        for (int r = 0; r < kBjMax; ++r) {
+#pragma unroll
+            for (int c = 0; c < kBjMax; ++c) {
+                double v = r == c ? 1.0 : 0.0;
+                if (r < size && c < size) v = c >= r ? bmat[(i + r) * kBjMax + c] : bmat[(i + c) * kBjMax + r];
+                L[r][c] = v;
+            }
+            d0[r] = L[r][r];
+        }
+        bool ok = fr;
+#pragma unroll
+        for (int j = 0; j < kBjMax; ++j) {
+            double p = L[j][j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) p -= L[j][k] * L[j][k];
+            if (!(p > 1e-12 * d0[j]) || !isfinite(p)) {
+                ok = false;
+                p = 1.0;
+            }
+            const double ljj = sqrt(p);
+            L[j][j] = ljj;
+#pragma unroll
+            for (int r = j + 1; r < kBjMax; ++r) {
+                double t = L[r][j];
+#pragma unroll
+                for (int k = 0; k < j; ++k) t -= L[r][k] * L[j][k];
+                L[r][j] = t / ljj;
+            }
+        }
+        if (ok) {
+#pragma unroll
+            for (int c = 0; c < kBjMax; ++c) {
+                double y[kBjMax], x[kBjMax];
+#pragma unroll
+                for (int r = 0; r < kBjMax; ++r) {
+                    double t = r == c ? 1.0 : 0.0;
+#pragma unroll
+                    for (int k = 0; k < r; ++k) t -= L[r][k] * y[k];
+                    y[r] = t / L[r][r];
+                }
+#pragma unroll
+                for (int r = kBjMax - 1; r >= 0; --r) {
+                    double t = y[r];
+#pragma unroll
+                    for (int k = r + 1; k < kBjMax; ++k) t -= L[k][r] * x[k];
+                    x[r] = t / L[r][r];
+                }
+#pragma unroll
+                for (int r = 0; r < kBjMax; ++r) {
+                    if (r >= c && r < size && c < size) {
+                        const float v = (float)x[r];
+                        binv[(i + r) * kBjMax + c] = v;
+                        binv[(i + c) * kBjMax + r] = v;
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kBjMax; ++r)
+#pragma unroll
+                for (int c = 0; c < kBjMax; ++c)
+                    if (r < size && c >= size) binv[(i + r) * kBjMax + c] = 0.0f;
+        } else {
+            if (fr) atomicAdd(n_fallback, 1);
+#pragma unroll
+            for (int r = 0; r < kBjMax; ++r) {
+                if (r >= size) continue;
+                const bool f = is_free(free_mask, i + r);
+#pragma unroll
+                for (int c = 0; c < kBjMax; ++c)
+                    binv[(i + r) * kBjMax + c] = (c == r && f && d0[r] > 0.0) ? (float)(1.0 / d0[r]) : 0.0f;
+            }
+        }
+    }
+}
+
+// z_i = sum over DoF i's block of M_ij r_j, r of the tile in shared memory (t = DoF - tile base)
+template <typename TT>
+__device__ __forceinline__ TT bj_row(unsigned mt, const float *__restrict__ row, const TT *s_r, int t) {
+    const float4 a = reinterpret_cast<const float4 *>(row)[0];
+    const float4 b = reinterpret_cast<const float4 *>(row)[1];
+    const float m[kBjMax] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    const int size = (int)(mt >> 8);
+    const TT *rb = s_r + (t - (int)(mt & 0xffu));
+    TT z = TT(0);
+#pragma unroll
+    for (int c = 0; c < kBjMax; ++c)
+        if (c < size) z = fma((TT)m[c], rb[c], z);
+    return z;
+}
+
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_einit_bj(int32_t n, const uint8_t *__restrict__ free_mask, const double *__restrict__ b, double b_scale,
+               const double *__restrict__ diag, const uint16_t *__restrict__ meta, const float *__restrict__ binv,
+               DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R, PcgState *st, double *part, double rtol,
+               double atol, long long maxit, int *bad) {
+    __shared__ double sh[32];
+    __shared__ TT s_r[kBjTile];
+    double rz = 0.0, rr = 0.0;
+    for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += (int64_t)gridDim.x * kBjTile) {
+        const int64_t i = base + threadIdx.x;
+        const bool fr = i < n && is_free(free_mask, i);
+        TT r = TT(0);
+        if (fr) {
+            const double dg = diag[i];
+            if (dg == 0.0 || !isfinite(dg)) atomicExch(bad, 1);
+            r = (TT)(b_scale * b[i]);
+        }
+        s_r[threadIdx.x] = r;
+        __syncthreads();
+        if (i < n) {
+            const TT z = fr ? bj_row(meta[i], binv + i * kBjMax, s_r, threadIdx.x) : TT(0);
+            G[i] = DofPair<TT>{z, TT(0)};
+            R[i] = DofPair<TT>{r, TT(0)};
+            rz += (double)r * (double)z;
+            rr += (double)r * (double)r;
+        }
+        __syncthreads();
+    }
+    const double a0 = block_sum(rz, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x] = a0;
+    const double a1 = block_sum(rr, sh);
+    if (threadIdx.x == 0) part[3 * blockIdx.x + 1] = a1;
+    if (threadIdx.x == 0) part[3 * blockIdx.x + 2] = a1;
+    if (last_block(&st->counter)) {
+        const double s_rz = reduce_parts(part, gridDim.x, 3, 0, sh);
+        const double s_rr = reduce_parts(part, gridDim.x, 3, 1, sh);
+        if (threadIdx.x == 0) {
+            st->rz = s_rz;
+            st->rr = s_rr;
+            st->bnorm = sqrt(s_rr);
+            st->atol_eff = fmax(atol, rtol * st->bnorm);
+            st->iter = 0;
+            st->maxit = maxit;
+            st->alpha = 0.0;
+            st->beta = 0.0;
+            int done = 0;
+            if (s_rr == 0.0) done = 4;
+            else if (!(s_rr == s_rr) || isinf(s_rr)) done = 3;
+            else if (sqrt(s_rr) < st->atol_eff) done = 1;
+            else if (maxit <= 0) done = 2;
+            st->done = done;
+        }
+    }
+}
+
+template <typename TT>
+__global__ void __launch_bounds__(kEBlock)
+    k_epass2_bj(int32_t n, const uint8_t *__restrict__ free_mask, const int32_t *__restrict__ inc_ptr,
+                const TT *__restrict__ Y, const uint16_t *__restrict__ meta, const float *__restrict__ binv,
+                DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R, PcgState *st, double *part, int use_cond,
+                cudaGraphConditionalHandle cond) {
+    __shared__ double sh2[2][32];
+    __shared__ TT s_r[kBjTile];
+    if (st->done) {
+        if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
+        return;
+    }
+    const TT alpha = (TT)st->alpha, beta = (TT)st->beta;
+    double rz = 0.0, rr = 0.0;
+    for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += (int64_t)gridDim.x * kBjTile) {
+        const int64_t i = base + threadIdx.x;
+        const bool fr = i < n && is_free(free_mask, i);
+        DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
+        TT r = TT(0);
+        if (fr) {
+            g = G[i];
+            rx = R[i];
+            const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
+            double q = 0.0;
+            for (int t = b0; t < b1; ++t) q += (double)Y[t];
+            r = rx.a - alpha * (TT)q;
+        }
+        s_r[threadIdx.x] = r;
+        __syncthreads();
+        if (fr) {
+            const TT z = bj_row(meta[i], binv + i * kBjMax, s_r, threadIdx.x);
+            const TT p = pnext(beta, g.b, g.a);
+            G[i] = DofPair<TT>{z, p};
+            R[i] = DofPair<TT>{r, rx.b + alpha * p};
+            rz += (double)r * (double)z;
+            rr += (double)r * (double)r;
+        }
+        __syncthreads();
+    }
+    block_sum2(rz, rr, sh2);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = rz;
+        part[2 * blockIdx.x + 1] = rr;
+    }
+    if (last_block(&st->counter)) {
+        double a = 0.0, b = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+            a += __ldcg(part + 2 * i);
+            b += __ldcg(part + 2 * i + 1);
+        }
+        __syncthreads();
+        block_sum2(a, b, sh2);
+        if (threadIdx.x == 0) {
+            const double rz_new = a, rr_new = b;
+            st->beta = rz_new / st->rz;
+            st->rz = rz_new;
+            st->rr = rr_new;
+            st->iter += 1;
+            int done = 0;
+            if (!(rr_new == rr_new) || isinf(rr_new)) done = 3;
+            else if (sqrt(rr_new) < st->atol_eff) done = 1;
+            else if (st->iter >= st->maxit) done = 2;
+            st->done = done;
+            if (use_cond && done) cudaGraphSetConditional(cond, 0);
+        }
+    }
+}
+
+__global__ void k_bj_apply(int32_t n, const uint8_t *__restrict__ free_mask, const uint16_t *__restrict__ meta,
+                           const float *__restrict__ binv, const double *__restrict__ r_in, double *__restrict__ z_out) {
+    __shared__ double s_r[kBjTile];
+    for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += (int64_t)gridDim.x * kBjTile) {
+        const int64_t i = base + threadIdx.x;
+        const bool fr = i < n && is_free(free_mask, i);
+        s_r[threadIdx.x] = fr ? r_in[i] : 0.0;
+        __syncthreads();
+        if (i < n) z_out[i] = fr ? bj_row(meta[i], binv + i * kBjMax, s_r, threadIdx.x) : 0.0;
+        __syncthreads();
+    }
+}
+
 // x_i += sum_c V[i][c] coef_c on the free DoFs: one warp per DoF, lanes over the columns,
 // then a fixed shuffle tree (deterministic).
 __global__ void k_basis_axpy(int32_t n, const uint8_t *__restrict__ free_mask, const float *__restrict__ V, int m,
@@ -688,20 +989,26 @@ int ElemPcg<TT>::reserve(int32_t n_, int64_t ne_) {
 }
 
 template <typename TT>
-int ElemPcg<TT>::launch_iteration(const ElemTopology &top, const TT *T, const uint8_t *free_mask, cudaStream_t s,
-                                  int use_cond, cudaGraphConditionalHandle cond) {
+int ElemPcg<TT>::launch_iteration(const ElemTopology &top, const TT *T, const uint8_t *free_mask,
+                                  const uint16_t *bj_meta, const float *bj_inv, cudaStream_t s, int use_cond,
+                                  cudaGraphConditionalHandle cond) {
     const TT *chat = chat_ptr<TT>(top);
     k_epass1<TT><<<wave_grid(k_epass1<TT>, 2 * ne, kEBlock), kEBlock, 0, s>>>(ne, top.edof.p, top.pos.p, T, chat, G.p,
                                                                          Y.p, st.p, part.p);
     SNP_LAUNCH_CHECK();
-    k_epass2<TT><<<wave_grid(k_epass2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, Y.p, G.p, R.p,
-                                                                        D.p, st.p, part.p, use_cond, cond);
+    if (bj_meta)
+        k_epass2_bj<TT><<<wave_grid(k_epass2_bj<TT>, n, kEBlock), kEBlock, 0, s>>>(
+            n, free_mask, top.inc_ptr.p, Y.p, bj_meta, bj_inv, G.p, R.p, st.p, part.p, use_cond, cond);
+    else
+        k_epass2<TT><<<wave_grid(k_epass2<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, top.inc_ptr.p, Y.p, G.p,
+                                                                            R.p, D.p, st.p, part.p, use_cond, cond);
     SNP_LAUNCH_CHECK();
     return SNP_OK;
 }
 
 template <typename TT>
-int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask) {
+int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
+                             const float *bj_inv) {
     drop_graph();
     const char *env = getenv("SNP_PCG_GRAPH");
     if (env && env[0] == '0') return SNP_OK;
@@ -727,7 +1034,7 @@ int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
-            int rc = launch_iteration(top, T, free_mask, cs, 1, h);
+            int rc = launch_iteration(top, T, free_mask, bj_meta, bj_inv, cs, 1, h);
             cudaGraph_t out = nullptr;
             cudaError_t e = cudaStreamEndCapture(cs, &out);
             ok = (rc == SNP_OK) && e == cudaSuccess;
@@ -747,20 +1054,28 @@ int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t
     key_top = &top;
     key_T = T;
     key_fm = free_mask;
+    key_bm = bj_meta;
+    key_bi = bj_inv;
     return SNP_OK;
 }
 
 template <typename TT>
 int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag, const uint8_t *free_mask,
                        const double *b, double b_scale, double *h, double rtol, double atol, int64_t maxit,
-                       cudaStream_t s, int64_t *its, double *res, int *status) {
+                       cudaStream_t s, int64_t *its, double *res, int *status, const uint16_t *bj_meta,
+                       const float *bj_inv) {
+    SNP_REQUIRE((bj_meta == nullptr) == (bj_inv == nullptr), "element PCG: block Jacobi needs both meta and inverse");
     SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "element PCG: topology not built");
     SNP_TRY(reserve(top.n, top.n_elems));
     if (maxit < 0) maxit = 10 * (int64_t)n;
     SNP_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
-    k_einit<TT><<<wave_grid(k_einit<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, b, b_scale, diag, G.p, R.p,
-                                                                      D.p, st.p, part.p, rtol, atol, (long long)maxit,
-                                                                      bad.p);
+    if (bj_meta)
+        k_einit_bj<TT><<<wave_grid(k_einit_bj<TT>, n, kEBlock), kEBlock, 0, s>>>(
+            n, free_mask, b, b_scale, diag, bj_meta, bj_inv, G.p, R.p, st.p, part.p, rtol, atol, (long long)maxit, bad.p);
+    else
+        k_einit<TT><<<wave_grid(k_einit<TT>, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, b, b_scale, diag, G.p, R.p,
+                                                                          D.p, st.p, part.p, rtol, atol,
+                                                                          (long long)maxit, bad.p);
     SNP_LAUNCH_CHECK();
     launches += 1;
     int hbad = 0;
@@ -771,15 +1086,16 @@ int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag,
         return fail(SNP_ZERO_PIVOT, "element PCG: zero or non-finite Jacobian diagonal on a free DoF");
     }
     int64_t chunk_launches = -1;
-    const bool same = exec && key_top == &top && key_T == T && key_fm == free_mask;
-    if (!same) SNP_TRY(build_graph(top, T, free_mask));
+    const bool same = exec && key_top == &top && key_T == T && key_fm == free_mask && key_bm == bj_meta &&
+                      key_bi == bj_inv;
+    if (!same) SNP_TRY(build_graph(top, T, free_mask, bj_meta, bj_inv));
     if (exec) {
         SNP_CUDA_TRY(cudaGraphLaunch(exec, s));
     } else {
         const int chunk = 32;
         int64_t launched = 0;
         while (true) {
-            for (int k = 0; k < chunk; ++k) SNP_TRY(launch_iteration(top, T, free_mask, s, 0, 0));
+            for (int k = 0; k < chunk; ++k) SNP_TRY(launch_iteration(top, T, free_mask, bj_meta, bj_inv, s, 0, 0));
             launched += chunk;
             SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
             SNP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -855,6 +1171,32 @@ int elem_reduced_system(const ElemTopology &top, const TT *T, const uint8_t *fre
         k_rsys_rhs_sum<<<(m + 127) / 128, 128, 0, s>>>(gr, m, pr, g);
         SNP_LAUNCH_CHECK();
     }
+    return SNP_OK;
+}
+
+template <typename TT>
+int block_jacobi_build(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *meta,
+                       double *bmat, float *binv, int *fallback_count, cudaStream_t s) {
+    SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "block Jacobi: topology not built");
+    SNP_REQUIRE(meta && bmat && binv && fallback_count, "block Jacobi: NULL buffer");
+    k_bj_entries<TT><<<wave_grid(k_bj_entries<TT>, top.n, kEBlock), kEBlock, 0, s>>>(
+        top.n, free_mask, top.inc_ptr.p, top.inc.p, top.edof.p, T, chat_ptr<TT>(top), meta, bmat);
+    SNP_LAUNCH_CHECK();
+    k_bj_invert<<<stride_grid(top.n, 128, 8), 128, 0, s>>>(top.n, free_mask, meta, bmat, binv, fallback_count);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+template int block_jacobi_build<double>(const ElemTopology &, const double *, const uint8_t *, const uint16_t *,
+                                        double *, float *, int *, cudaStream_t);
+template int block_jacobi_build<float>(const ElemTopology &, const float *, const uint8_t *, const uint16_t *,
+                                       double *, float *, int *, cudaStream_t);
+
+int block_jacobi_apply(int32_t n, const uint8_t *free_mask, const uint16_t *meta, const float *binv, const double *r,
+                       double *z, cudaStream_t s) {
+    SNP_REQUIRE(meta && binv && r && z && n > 0, "block Jacobi apply: bad arguments");
+    k_bj_apply<<<wave_grid(k_bj_apply, n, kEBlock), kEBlock, 0, s>>>(n, free_mask, meta, binv, r, z);
+    SNP_LAUNCH_CHECK();
     return SNP_OK;
 }
 

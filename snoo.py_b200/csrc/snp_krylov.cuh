@@ -141,6 +141,18 @@ template <typename TT>
 int elem_reduced_system(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const float *V, int m,
                         int64_t ldv, const double *F, double *Jr, double *g, DevBuf<double> &scratch, cudaStream_t s);
 
+// Block Jacobi of the matrix-free Jacobian T: meta[n] = offset in block | size << 8 (blocks of
+// at most 8 consecutive DoFs, never across a multiple of 256; constrained DoFs alone); bmat
+// [n][8] float64 work, binv [n][8] float32 rows of the block inverses; *fallback_count (device
+// int, accumulated) counts blocks inverted as point Jacobi.
+constexpr int kBlockJacobiMax = 8;
+template <typename TT>
+int block_jacobi_build(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *meta,
+                       double *bmat, float *binv, int *fallback_count, cudaStream_t s);
+// z = M r on the free DoFs (0 elsewhere), float64 vectors.
+int block_jacobi_apply(int32_t n, const uint8_t *free_mask, const uint16_t *meta, const float *binv, const double *r,
+                       double *z, cudaStream_t s);
+
 // x += V coef on the free DoFs (V float32 [n][ldv], m columns; coef float64 [m], device).
 int basis_axpy(int32_t n, const uint8_t *free_mask, const float *V, int m, int64_t ldv, const double *coef,
                double *x, cudaStream_t s);
@@ -170,6 +182,8 @@ struct ElemPcg {
     const void *key_top = nullptr;
     const TT *key_T = nullptr;
     const uint8_t *key_fm = nullptr;
+    const uint16_t *key_bm = nullptr;
+    const float *key_bi = nullptr;
     int64_t launches = 0;
 
     ElemPcg() = default;
@@ -178,19 +192,21 @@ struct ElemPcg {
     ~ElemPcg();
     int reserve(int32_t n, int64_t ne);
     void drop_graph();
-    // Solve J h = b_scale * b on the free DoFs from h = 0 with Jacobi from diag; h (float64)
-    // gets the iterate, 0 on constrained DoFs.  SNP_ZERO_PIVOT for a zero/non-finite
-    // diagonal entry on a free DoF.
+    // Solve J h = b_scale * b on the free DoFs from h = 0 with Jacobi from diag, or block
+    // Jacobi when bj_meta / bj_inv are given (block_jacobi_build); h (float64) gets the
+    // iterate, 0 on constrained DoFs.  SNP_ZERO_PIVOT for a zero/non-finite diagonal entry on
+    // a free DoF.
     int solve(const ElemTopology &top, const TT *T, const double *diag, const uint8_t *free_mask, const double *b,
               double b_scale, double *h, double rtol, double atol, int64_t maxit, cudaStream_t s, int64_t *its,
-              double *res, int *status);
+              double *res, int *status, const uint16_t *bj_meta = nullptr, const float *bj_inv = nullptr);
     // y = J x on the free rows and columns (0 on constrained rows).
     int apply(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const TT *x, TT *y, cudaStream_t s);
 
    private:
-    int launch_iteration(const ElemTopology &top, const TT *T, const uint8_t *free_mask, cudaStream_t s, int use_cond,
-                         cudaGraphConditionalHandle cond);
-    int build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask);
+    int launch_iteration(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
+                         const float *bj_inv, cudaStream_t s, int use_cond, cudaGraphConditionalHandle cond);
+    int build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
+                    const float *bj_inv);
 };
 
 }  // namespace snp

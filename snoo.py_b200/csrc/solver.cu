@@ -241,6 +241,37 @@ struct snp_solver {
     int64_t gal_ldv = 0;
     snp::DevBuf<double> gal_sys, gal_x;
     snp::HostBuf<double> gal_host;
+    // block Jacobi of the residual-mode Krylov solves (snp_solver_set_block_jacobi)
+    bool bj_on = false;
+    snp::DevBuf<uint16_t> bj_meta;
+    snp::DevBuf<double> bj_mat;
+    snp::DevBuf<float> bj_inv;
+    snp::DevBuf<int> bj_fallback;
+
+    // z = M r with the block Jacobi of the current element tensors (test and inspection entry)
+    int precond_apply(bool f32, const double *r, double *z, int32_t *fallback_blocks) {
+        SNP_CUDA_TRY(cudaMemsetAsync(bj_fallback.p, 0, sizeof(int), stream));
+        SNP_TRY(build_block_jacobi(f32));
+        SNP_TRY(snp::block_jacobi_apply(n, free_mask.p, bj_meta.p, bj_inv.p, r, z, stream));
+        if (fallback_blocks) {
+            int fb = 0;
+            SNP_CUDA_TRY(cudaMemcpyAsync(&fb, bj_fallback.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            SNP_CUDA_TRY(cudaStreamSynchronize(stream));
+            *fallback_blocks = fb;
+        }
+        return SNP_OK;
+    }
+
+    int build_block_jacobi(bool f32) {
+        if (f32)
+            SNP_TRY(snp::block_jacobi_build(etop, T32.p, free_mask.p, bj_meta.p, bj_mat.p, bj_inv.p, bj_fallback.p,
+                                            stream));
+        else
+            SNP_TRY(snp::block_jacobi_build(etop, T64.p, free_mask.p, bj_meta.p, bj_mat.p, bj_inv.p, bj_fallback.p,
+                                            stream));
+        launches += 2;
+        return SNP_OK;
+    }
     snp::DevBuf<float> T32;
     snp::ElemPcg<double> epcg64;
     snp::ElemPcg<float> epcg32;
@@ -592,10 +623,13 @@ struct snp_solver {
                 bool zp = false;
                 SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));
                 if (layout == SNP_LAYOUT_ELEM) {
+                    if (bj_on) SNP_TRY(build_block_jacobi(f32));
+                    const uint16_t *bm = bj_on ? bj_meta.p : nullptr;
+                    const float *bi = bj_on ? bj_inv.p : nullptr;
                     const int rc = f32 ? epcg32.solve(etop, T32.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0,
-                                                      cg_maxit, stream, &its, &rn, &st)
+                                                      cg_maxit, stream, &its, &rn, &st, bm, bi)
                                        : epcg64.solve(etop, T64.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0,
-                                                      cg_maxit, stream, &its, &rn, &st);
+                                                      cg_maxit, stream, &its, &rn, &st, bm, bi);
                     if (rc == SNP_ZERO_PIVOT)
                         return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
                     SNP_TRY(rc);
@@ -920,6 +954,74 @@ int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void 
     SNP_REQUIRE(s->j_valid[precision], "snp_solver_jacobian_apply: no %s Newton Jacobian (run a solve first)",
                 precision ? "float32" : "float64");
     return s->apply_jacobian(precision, x, y, stream ? snp::as_stream(stream) : s->stream);
+}
+
+int snp_solver_set_block_jacobi(snp_solver *s, const uint16_t *meta) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_set_block_jacobi: solver missing or not finalized");
+    if (meta == nullptr) {
+        s->bj_on = false;
+        return SNP_OK;
+    }
+    SNP_REQUIRE(s->layout == SNP_LAYOUT_ELEM, "snp_solver_set_block_jacobi: the solver's Jacobian layout is not elem");
+    const int32_t n = s->n;
+    std::vector<uint8_t> fm((size_t)n);
+    SNP_CUDA_TRY(cudaMemcpy(fm.data(), s->free_mask.p, (size_t)n, cudaMemcpyDeviceToHost));
+    // every block: 1..8 consecutive DoFs inside one 256-DoF tile, offsets 0..size-1 in order,
+    // free DoFs only unless it is a constrained DoF alone
+    for (int32_t i = 0; i < n;) {
+        const int off = meta[i] & 0xff, size = meta[i] >> 8;
+        SNP_REQUIRE(off == 0 && size >= 1 && size <= snp::kBlockJacobiMax && i + size <= n &&
+                        (i / 256) == ((i + size - 1) / 256),
+                    "snp_solver_set_block_jacobi: bad block at DoF %d (offset %d, size %d)", i, off, size);
+        for (int k = 0; k < size; ++k) {
+            SNP_REQUIRE((meta[i + k] & 0xff) == k && (meta[i + k] >> 8) == size,
+                        "snp_solver_set_block_jacobi: inconsistent block at DoF %d", i + k);
+            SNP_REQUIRE(size == 1 || fm[i + k], "snp_solver_set_block_jacobi: constrained DoF %d inside a block", i + k);
+        }
+        i += size;
+    }
+    SNP_TRY(s->bj_meta.alloc(n));
+    SNP_TRY(s->bj_mat.alloc((size_t)n * snp::kBlockJacobiMax));
+    SNP_TRY(s->bj_inv.alloc((size_t)n * snp::kBlockJacobiMax));
+    SNP_TRY(s->bj_fallback.alloc(1));
+    SNP_CUDA_TRY(cudaMemcpy(s->bj_meta.p, meta, sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    SNP_CUDA_TRY(cudaMemset(s->bj_fallback.p, 0, sizeof(int)));
+    s->bj_on = true;
+    return SNP_OK;
+}
+
+int snp_solver_precond_apply(snp_solver *s, int precision, const double *r, double *z, int32_t *fallback_blocks,
+                             void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_precond_apply: solver missing or not finalized");
+    SNP_REQUIRE(s->layout == SNP_LAYOUT_ELEM && s->bj_on, "snp_solver_precond_apply: no block Jacobi on this solver");
+    SNP_REQUIRE(precision == 0 || precision == 1, "snp_solver_precond_apply: precision must be 0 or 1");
+    SNP_REQUIRE(s->j_valid[precision], "snp_solver_precond_apply: no %s Newton Jacobian (assemble first)",
+                precision ? "float32" : "float64");
+    SNP_REQUIRE(r != nullptr && z != nullptr, "snp_solver_precond_apply: r or z is NULL");
+    cudaStream_t keep = s->stream;
+    if (stream) s->stream = snp::as_stream(stream);
+    const int rc = s->precond_apply(precision == 1, r, z, fallback_blocks);
+    s->stream = keep;
+    return rc;
+}
+
+int snp_solver_block_jacobi_export(snp_solver *s, int precision, double *bmat, float *binv, void *stream) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized && s->bj_on, "snp_solver_block_jacobi_export: no block Jacobi");
+    SNP_REQUIRE(precision == 0 || precision == 1, "snp_solver_block_jacobi_export: precision must be 0 or 1");
+    SNP_REQUIRE(s->j_valid[precision], "snp_solver_block_jacobi_export: assemble first");
+    cudaStream_t st = stream ? snp::as_stream(stream) : s->stream;
+    cudaStream_t keep = s->stream;
+    s->stream = st;
+    int rc = s->build_block_jacobi(precision == 1);
+    s->stream = keep;
+    SNP_TRY(rc);
+    const size_t m = (size_t)s->n * snp::kBlockJacobiMax;
+    if (bmat) SNP_CUDA_TRY(cudaMemcpyAsync(bmat, s->bj_mat.p, sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
+    if (binv) SNP_CUDA_TRY(cudaMemcpyAsync(binv, s->bj_inv.p, sizeof(float) * m, cudaMemcpyDeviceToDevice, st));
+    return SNP_OK;
 }
 
 int snp_solver_set_galerkin_basis(snp_solver *s, const float *V, int32_t m, int64_t ldv, int32_t steps) {

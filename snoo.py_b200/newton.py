@@ -1,6 +1,7 @@
 """Device Newton solver: Python owner of the native ``snp_solver`` handle."""
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -9,6 +10,30 @@ from .device import torch, upload, zeros
 
 MODE_REFERENCE = 0  # increment test + scipy-style CG (red_mvp_solver.py:121-224)
 MODE_RESIDUAL = 1   # ||F_free|| <= tol * ||F_free(x0)||
+
+BLOCK_MAX = 8    # DoFs per block-Jacobi block
+BLOCK_TILE = 256  # blocks never cross a multiple of this (the DoF pass's shared-memory tile)
+
+
+def dof_blocks(keys, free, max_block=BLOCK_MAX, tile=BLOCK_TILE):
+    """Block-Jacobi partition: maximal runs of consecutive free DoFs with equal ``keys`` (for
+    edge DoFs numbered by their lower node, the edges that share that node), cut into pieces of
+    at most ``max_block`` DoFs and at multiples of ``tile``; a constrained DoF is a block of its
+    own.  Returns uint16 [n]: offset of the DoF in its block | block size << 8."""
+    keys = np.asarray(keys)
+    free = np.asarray(free).astype(bool)
+    n = len(keys)
+    idx = np.arange(n)
+    start = np.ones(n, dtype=bool)
+    if n > 1:
+        start[1:] = (keys[1:] != keys[:-1]) | ~free[1:] | ~free[:-1]
+    start[::tile] = True
+    run_start = idx[start][np.cumsum(start) - 1]
+    start |= (idx - run_start) % max_block == 0
+    block = np.cumsum(start) - 1
+    starts = idx[start]
+    sizes = np.diff(np.r_[starts, n])
+    return ((idx - starts[block]) | (sizes[block] << 8)).astype(np.uint16)
 
 
 class DeviceNewton:
@@ -50,6 +75,15 @@ class DeviceNewton:
             r = rhs_extra if hasattr(rhs_extra, "data_ptr") else upload(rhs_extra, np.float64)
             _lib.call("snp_solver_set_rhs", self.handle, _lib.ptr(r))
         _lib.call("snp_solver_finalize", self.handle)
+        # block Jacobi over the edges that share their lower node (DoF i = mesh edge i), unless
+        # SNP_PRECOND=jacobi or the layout is not matrix-free
+        self.block_jacobi = False
+        mesh = getattr(assembler, "mesh", None)
+        edges = getattr(mesh, "edges", None)
+        if (os.environ.get("SNP_PRECOND", "block").lower() != "jacobi" and edges is not None
+                and len(edges) == self.n and self.jacobian_layout == "elem"):
+            fm = self.free_mask.cpu().numpy().astype(bool)
+            self._set_blocks(dof_blocks(edges[:, 0], fm))
         p = ctypes.c_void_p()
         _lib.call("snp_solver_pattern", self.handle, ctypes.byref(p))
         from .device import Pattern
@@ -178,6 +212,40 @@ class DeviceNewton:
                   int(V.stride(0)), _lib.ptr(F), _lib.ptr(Jr), _lib.ptr(g), _lib.stream_ptr(self._stream))
         self._leave()
         return Jr, g
+
+    def _set_blocks(self, meta):
+        if meta is None:
+            _lib.call("snp_solver_set_block_jacobi", self.handle, None)
+            self.block_jacobi = False
+            return
+        meta = np.ascontiguousarray(meta, dtype=np.uint16)
+        assert meta.shape == (self.n,)
+        _lib.call("snp_solver_set_block_jacobi", self.handle, meta.ctypes.data_as(ctypes.c_void_p))
+        self.block_jacobi = True
+
+    def set_preconditioner(self, kind="block", meta=None):
+        """Residual-mode Krylov preconditioner: "block" (block Jacobi; ``meta`` from
+        ``dof_blocks``, default the edges sharing their lower node) or "jacobi" (point Jacobi,
+        as the reference)."""
+        if kind == "jacobi":
+            self._set_blocks(None)
+        else:
+            if meta is None:
+                fm = self.free_mask.cpu().numpy().astype(bool)
+                meta = dof_blocks(self.assembler.mesh.edges[:, 0], fm)
+            self._set_blocks(meta)
+
+    def precond_apply(self, r, precision="fp64"):
+        """z = M r (CUDA float64 [n]) with the block Jacobi of the last ``assemble_tensors`` of
+        that precision; returns (z, number of blocks that fell back to point Jacobi)."""
+        t = torch()
+        z = t.empty_like(r)
+        fb = ctypes.c_int32(0)
+        self._enter()
+        _lib.call("snp_solver_precond_apply", self.handle, {"fp64": 0, "mixed": 1}[precision], _lib.ptr(r),
+                  _lib.ptr(z), ctypes.byref(fb), _lib.stream_ptr(self._stream))
+        self._leave()
+        return z, int(fb.value)
 
     def set_galerkin_basis(self, V=None, steps=1):
         """Attach a basis (CUDA float32 [n, m], row-major, m <= 128) whose Galerkin Newton step

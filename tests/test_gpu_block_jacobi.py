@@ -1,0 +1,113 @@
+"""Block-Jacobi preconditioner of the matrix-free Newton Jacobian: its blocks against the
+oracle's assembled Jacobian, and Newton with it against Newton with point Jacobi."""
+
+import numpy as np
+import pytest
+import torch
+
+import snoopy_b200 as S
+from snoopy_b200 import materials as MAT
+from snoopy_b200 import mesh as M
+from snoopy_b200.device import upload
+
+pytestmark = pytest.mark.gpu
+
+NU0 = 0.25 / np.pi * 1e7
+
+
+def _setup(ntet, seed=7):
+    msh = M.window_frame_mesh(ntet, jitter=0.15, seed=seed)
+    coils = msh.geometry.coils()
+    rel = MAT.atan_reluctance()
+    solver = S.RedMVPSolver(msh, coils, [M.TAG_IRON], [M.TAG_AIR], [rel], max_newton_iterations=50, quad_order=2)
+    solver.verbose = False
+    return msh, coils, rel, solver
+
+
+def _oracle(oracle_mod, msh, coils, rel, solver):
+    tb = solver.curl_curl_factory.tables(solver.quad_order)
+    iron = msh.domain_elements(M.TAG_IRON)
+    air = msh.domain_elements(M.TAG_AIR)
+    P = np.einsum("qi,eid->eqd", tb.phi.reshape(tb.nq, 4), msh.nodes[msh.cells[iron]]).reshape(-1, 3)
+    Bs = sum(oracle_mod.compute_B_line_segs_cpp(c.get_segments(), P, c.current, c.rad) for c in coils)
+    mats = [dict(cells=msh.cells[iron], glob_ids=msh.elem_edges[iron], orientations=msh.orientations[iron],
+                 reluctance=rel),
+            dict(cells=msh.cells[air], glob_ids=msh.elem_edges[air], orientations=msh.orientations[air],
+                 reluctance=S.ConstantReluctance(NU0))]
+    O = oracle_mod.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, tb.w, tb.q, tb.d_phi, tb.curls)
+    return O, [Bs, np.zeros((0, 3))]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_block_inverse_matches_oracle_blocks(oracle_mod, precision):
+    """z = M r from the device blocks against the inverses of the same diagonal blocks of the
+    oracle's assembled Jacobian (float32 storage of the inverse: 1e-5 of max |z|)."""
+    msh, coils, rel, solver = _setup(6000)
+    eng = solver.newton_engine()
+    assert eng.block_jacobi
+    x, st = solver.solve_to_residual(1e-6, return_device=True)  # a state with saturated iron
+    O, sf = _oracle(oracle_mod, msh, coils, rel, solver)
+    _, J, _ = O.compute_stiffness_and_jacobi_matrix_c(x.cpu().numpy(), sf)
+    J = J.tocsr()
+    mask = solver.make_boundary_mask()
+    from snoopy_b200.newton import dof_blocks
+
+    meta = dof_blocks(msh.edges[:, 0], mask)
+    r = np.random.default_rng(2).standard_normal(msh.num_dofs)
+    want = np.zeros_like(r)
+    i, n = 0, msh.num_dofs
+    sizes = []
+    while i < n:
+        s = int(meta[i] >> 8)
+        if mask[i]:
+            idx = np.arange(i, i + s)
+            want[idx] = np.linalg.solve(J[idx][:, idx].toarray(), r[idx])
+        sizes.append(s)
+        i += s
+    assert np.mean(sizes) > 2  # edges sharing their lower node (many boundary DoFs at this size)
+    eng.assemble_tensors(x, precision)
+    z, fallbacks = eng.precond_apply(upload(r, np.float64), precision)
+    z = z.cpu().numpy()
+    assert fallbacks == 0
+    assert np.all(z[~mask] == 0.0)
+    err = np.abs(z - want).max() / np.abs(want).max()
+    assert err < (1e-5 if precision == "fp64" else 1e-4), err
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_block_jacobi_newton_matches_point_jacobi(precision):
+    """Newton to 1e-10 with block Jacobi and with point Jacobi: the same field, fewer CG
+    iterations with the blocks, and bitwise repeatable."""
+    msh, coils, rel, solver = _setup(20000)
+    eng = solver.newton_engine()
+    probes = msh.geometry.aperture_probes(300)
+    el, _ = msh.locate(probes)
+    tol = 1e-10 if precision == "fp64" else 1e-8
+    xb, sb = solver.solve_to_residual(tol, precision=precision, return_device=True)
+    xb2, sb2 = solver.solve_to_residual(tol, precision=precision, return_device=True)
+    eng.set_preconditioner("jacobi")
+    try:
+        xj, sj = solver.solve_to_residual(tol, precision=precision, return_device=True)
+    finally:
+        eng.set_preconditioner("block")
+    assert sb["rel_res"] <= tol and sj["rel_res"] <= tol
+    assert sb["cg_iterations"] < 0.75 * sj["cg_iterations"], (sb["cg_iterations"], sj["cg_iterations"])
+    assert sb2["cg_iterations"] == sb["cg_iterations"] and torch.equal(xb, xb2)
+    A = solver.curl_curl_factory
+    Bb = A.compute_B_at_points(xb, probes, el)
+    Bj = A.compute_B_at_points(xj, probes, el)
+    err = np.linalg.norm(Bb - Bj, axis=1).max() / np.linalg.norm(Bj, axis=1).max()
+    assert err < (1e-8 if precision == "fp64" else 1e-6), err
+
+
+def test_block_partition_is_checked():
+    msh, coils, rel, solver = _setup(2000)
+    eng = solver.newton_engine()
+    meta = np.full(msh.num_dofs, 1 << 8, dtype=np.uint16)
+    meta[0] = (2 << 8)  # claims a block of two that the next entry does not continue
+    from snoopy_b200._lib import SnpError
+
+    with pytest.raises(SnpError):
+        eng._set_blocks(meta)
+    eng.set_preconditioner("block")
+    assert eng.block_jacobi

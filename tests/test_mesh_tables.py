@@ -142,3 +142,31 @@ def test_cotree_split_is_a_spanning_tree(msh):
     bnd = msh.boundary_edge_ids()
     n_bnodes = len(np.unique(msh.edges[bnd].ravel()))
     assert np.isin(tree, bnd).sum() == n_bnodes - 1
+
+
+def test_block_jacobi_partition():
+    """dof_blocks: runs of equal keys among free DoFs, at most 8 long, never across a multiple of
+    256, constrained DoFs alone; offsets and sizes encoded per DoF."""
+    from snoopy_b200.newton import dof_blocks
+
+    rng = np.random.default_rng(4)
+    for n in (1, 7, 255, 256, 257, 3001):
+        keys = np.sort(rng.integers(0, max(1, n // 5), n))
+        free = rng.random(n) > 0.1
+        meta = dof_blocks(keys, free)
+        off, size = meta & 0xFF, meta >> 8
+        i = 0
+        while i < n:
+            s = int(size[i])
+            assert off[i] == 0 and 1 <= s <= 8 and i + s <= n
+            assert i // 256 == (i + s - 1) // 256
+            assert np.array_equal(off[i:i + s], np.arange(s)) and np.all(size[i:i + s] == s)
+            if s > 1:
+                assert np.all(free[i:i + s]) and np.all(keys[i:i + s] == keys[i])
+            if not free[i]:
+                assert s == 1
+            # maximal: the next DoF would have fit (same key, free, same tile, room) only if cut by the cap
+            j = i + s
+            if j < n and s < 8 and j % 256 != 0 and free[i] and free[j] and keys[j] == keys[i]:
+                raise AssertionError(f"block at {i} not maximal")
+            i = j
