@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(128)
         if (mt & 0xffu) continue;
         const int size = (int)(mt >> 8);
         const bool fr = is_free(free_mask, i);
-        double L[kBjMax][kBjMax], d0[kBjMax];
+        double L[kBjMax][kBjMax], d0[kBjMax], rl[kBjMax];
 #pragma unroll
         for (int r = 0; r < kBjMax; ++r) {
 #pragma unroll
@@ -623,12 +623,13 @@ __global__ void __launch_bounds__(128)
             }
             const double ljj = sqrt(p);
             L[j][j] = ljj;
+            rl[j] = 1.0 / ljj;
 #pragma unroll
             for (int r = j + 1; r < kBjMax; ++r) {
                 double t = L[r][j];
 #pragma unroll
                 for (int k = 0; k < j; ++k) t -= L[r][k] * L[j][k];
-                L[r][j] = t / ljj;
+                L[r][j] = t * rl[j];
             }
         }
         if (ok) {
@@ -640,14 +641,14 @@ __global__ void __launch_bounds__(128)
                     double t = r == c ? 1.0 : 0.0;
 #pragma unroll
                     for (int k = 0; k < r; ++k) t -= L[r][k] * y[k];
-                    y[r] = t / L[r][r];
+                    y[r] = t * rl[r];
                 }
 #pragma unroll
                 for (int r = kBjMax - 1; r >= 0; --r) {
                     double t = y[r];
 #pragma unroll
                     for (int k = r + 1; k < kBjMax; ++k) t -= L[k][r] * x[k];
-                    x[r] = t / L[r][r];
+                    x[r] = t * rl[r];
                 }
 #pragma unroll
                 for (int r = 0; r < kBjMax; ++r) {
@@ -677,11 +678,10 @@ __global__ void __launch_bounds__(128)
     }
 }
 
-// z_i = sum over DoF i's block of M_ij r_j, r of the tile in shared memory (t = DoF - tile base)
+// z_i = sum over DoF i's block of M_ij r_j, r of the tile in shared memory (t = DoF - tile base);
+// a, b: DoF i's row of the block inverse, loaded before the tile's barrier
 template <typename TT>
-__device__ __forceinline__ TT bj_row(unsigned mt, const float *__restrict__ row, const TT *s_r, int t) {
-    const float4 a = reinterpret_cast<const float4 *>(row)[0];
-    const float4 b = reinterpret_cast<const float4 *>(row)[1];
+__device__ __forceinline__ TT bj_row(unsigned mt, float4 a, float4 b, const TT *s_r, int t) {
     const float m[kBjMax] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
     const int size = (int)(mt >> 8);
     const TT *rb = s_r + (t - (int)(mt & 0xffu));
@@ -690,6 +690,12 @@ __device__ __forceinline__ TT bj_row(unsigned mt, const float *__restrict__ row,
     for (int c = 0; c < kBjMax; ++c)
         if (c < size) z = fma((TT)m[c], rb[c], z);
     return z;
+}
+
+__device__ __forceinline__ void bj_load(const float *__restrict__ binv, int64_t i, float4 &a, float4 &b) {
+    const float4 *p = reinterpret_cast<const float4 *>(binv + i * kBjMax);
+    a = __ldg(p);
+    b = __ldg(p + 1);
 }
 
 template <typename TT>
@@ -705,15 +711,19 @@ __global__ void __launch_bounds__(kEBlock)
         const int64_t i = base + threadIdx.x;
         const bool fr = i < n && is_free(free_mask, i);
         TT r = TT(0);
+        unsigned mt = 0;
+        float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
         if (fr) {
             const double dg = diag[i];
             if (dg == 0.0 || !isfinite(dg)) atomicExch(bad, 1);
             r = (TT)(b_scale * b[i]);
+            mt = meta[i];
+            bj_load(binv, i, ma, mb);
         }
         s_r[threadIdx.x] = r;
         __syncthreads();
         if (i < n) {
-            const TT z = fr ? bj_row(meta[i], binv + i * kBjMax, s_r, threadIdx.x) : TT(0);
+            const TT z = fr ? bj_row(mt, ma, mb, s_r, threadIdx.x) : TT(0);
             G[i] = DofPair<TT>{z, TT(0)};
             R[i] = DofPair<TT>{r, TT(0)};
             rz += (double)r * (double)z;
@@ -778,7 +788,9 @@ __global__ void __launch_bounds__(kEBlock)
         s_r[threadIdx.x] = r;
         __syncthreads();
         if (fr) {
-            const TT z = bj_row(meta[i], binv + i * kBjMax, s_r, threadIdx.x);
+            float4 ma, mb;
+            bj_load(binv, i, ma, mb);
+            const TT z = bj_row((unsigned)meta[i], ma, mb, s_r, threadIdx.x);
             const TT p = pnext(beta, g.b, g.a);
             G[i] = DofPair<TT>{z, p};
             R[i] = DofPair<TT>{r, rx.b + alpha * p};
@@ -822,9 +834,15 @@ __global__ void k_bj_apply(int32_t n, const uint8_t *__restrict__ free_mask, con
     for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += (int64_t)gridDim.x * kBjTile) {
         const int64_t i = base + threadIdx.x;
         const bool fr = i < n && is_free(free_mask, i);
+        unsigned mt = 0;
+        float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
+        if (fr) {
+            mt = meta[i];
+            bj_load(binv, i, ma, mb);
+        }
         s_r[threadIdx.x] = fr ? r_in[i] : 0.0;
         __syncthreads();
-        if (i < n) z_out[i] = fr ? bj_row(meta[i], binv + i * kBjMax, s_r, threadIdx.x) : 0.0;
+        if (i < n) z_out[i] = fr ? bj_row(mt, ma, mb, s_r, threadIdx.x) : 0.0;
         __syncthreads();
     }
 }
