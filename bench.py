@@ -143,25 +143,32 @@ def bytes_elem_apply(ne, n, tb=8):
     return ne * (24 + 6 * tb + 24) + (n + 1) * 4 + 2 * n * tb
 
 
-def bytes_elem_pcg_iteration(ne, n, tb=8):
+def bytes_elem_pcg_iteration(ne, n, tb=8, block_jacobi=False):
     """One matrix-free PCG iteration (element pass + DoF pass): the operator data as in
     bytes_elem_apply; per DoF {z, p}, {r, x} and 1/diag read once, {z, p} and {r, x} written
-    once (9 words)."""
+    once (9 words).  With block Jacobi the DoF pass reads the DoF's row of its block inverse
+    (8 float32) and its block word (2 B) in place of 1/diag."""
+    if block_jacobi:
+        return ne * (24 + 6 * tb + 24) + (n + 1) * 4 + 8 * n * tb + 34 * n
     return ne * (24 + 6 * tb + 24) + (n + 1) * 4 + 9 * n * tb
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one matrix-free PCG iteration,
-# k_epass1 + k_epass2, from ncu captures of the 1,164,240-tet workload (cold cache: ncu
-# flushes L2 before every replay pass, so slot values and DoF states that stay in L2 between
-# the two passes of a live run are counted as DRAM traffic here).  Summaries and commands:
-# profiles/elem_pcg_passes_window_frame_1p2M.md.  Scaled by the element count for other sizes.
-MEASURED_TRAFFIC = {"ne": 1_164_240, "fp64": (143.15e6 + 129.10e6), "mixed": (100.94e6 + 62.43e6)}
+# k_epass1 + k_epass2 (point Jacobi) or k_epass1 + k_epass2_bj (block Jacobi), from ncu
+# captures of the 1,164,240-tet workload (cold cache: ncu flushes L2 before every replay pass,
+# so slot values and DoF states that stay in L2 between the two passes of a live run are
+# counted as DRAM traffic here).  Summaries and commands: profiles/elem_pcg_passes_window_frame_1p2M.md
+# and profiles/elem_pcg_block_jacobi_window_frame_1p2M.md.  Scaled by the element count.
+MEASURED_TRAFFIC = {"ne": 1_164_240, "fp64": (143.15e6 + 129.10e6), "mixed": (100.94e6 + 62.43e6),
+                    "fp64_bj": (135.04e6 + 7.03e6 + 152.77e6 + 16.10e6),
+                    "mixed_bj": (95.13e6 + 4.47e6 + 103.08e6 + 2.18e6)}
 
 
-def measured_traffic(layout, precision, ne):
-    if layout != "elem" or precision not in MEASURED_TRAFFIC:
+def measured_traffic(layout, precision, ne, block_jacobi=False):
+    key = precision + ("_bj" if block_jacobi else "")
+    if layout != "elem" or key not in MEASURED_TRAFFIC:
         return None
-    return MEASURED_TRAFFIC[precision] * ne / MEASURED_TRAFFIC["ne"]
+    return MEASURED_TRAFFIC[key] * ne / MEASURED_TRAFFIC["ne"]
 
 
 # ---------------------------------------------------------------------------- ranks
@@ -261,10 +268,13 @@ def run_ours(args):
     vb, xb = (8, 8) if args.precision == "fp64" else (4, 4)
     layout = eng.jacobian_layout
     ne = msh.num_elements
+    bj = bool(getattr(eng, "block_jacobi", False))
     if layout == "elem":
-        b_it = bytes_elem_pcg_iteration(ne, n, vb)
+        b_it = bytes_elem_pcg_iteration(ne, n, vb, block_jacobi=bj)
         b_apply = bytes_elem_apply(ne, n, vb)
-        kern_name = "pcg_iteration (k_epass1 element pass + k_epass2 DoF pass)"
+        kern_name = ("pcg_iteration (k_epass1 element pass + k_epass2_bj block-Jacobi DoF pass; the block build of "
+                     "each Newton step, k_bj_entries + k_bj_invert, inside the timed Krylov region)" if bj else
+                     "pcg_iteration (k_epass1 element pass + k_epass2 DoF pass)")
     else:
         b_it = bytes_pcg_iteration(nnz, n, vb, xb)
         b_apply = bytes_spmv(nnz, n, vb, xb)
@@ -310,7 +320,8 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(msh, coils, rel, assemblies / args.steps, cg_its / args.steps)
+        # the reference's own work per solve (point-Jacobi CG), not this solver's counts
+        cpu = cpu_baseline_sample(msh, coils, rel, REFERENCE_COUNTS["assemblies"], REFERENCE_COUNTS["cg"])
 
     launches = int(sum(s.get("kernel_launches", 0) for s in stats)) or None
     line = {
@@ -330,7 +341,7 @@ def run_ours(args):
         "roofline": {"kernel": kern_name, "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "bytes_per_launch": b_it, "launch_ms": it_ms,
-                     "traffic": measured_traffic(layout, args.precision, ne),
+                     "traffic": measured_traffic(layout, args.precision, ne, layout == "elem" and bj),
                      "spmv_alone": {"achieved": spmv_gbs, "frac": spmv_gbs / peak, "ms": spmv_ms,
                                     "bytes": b_apply, "layout": layout},
                      "spmv_csr_f64": {"achieved": csr_gbs, "frac": csr_gbs / peak, "ms": csr_ms,
@@ -651,8 +662,9 @@ def cpu_baseline_sample(msh, coils, rel, assemblies_per_solve, cg_per_solve):
 # reference's kernels and scipy's cg (oracle.newton_residual with forcing="ew" and
 # line_search="energy", the device solver's algorithm) on the 1.16M-tet mesh: 13 Newton steps,
 # 2868 CG iterations and 22 assemblies, 278 s on one core.  The device solver needs 13 steps and
-# 2652 CG iterations; the reference arm projects its measured per-iteration times with the
-# oracle's counts.
+# 2652 CG iterations with the same point Jacobi, 13-14 steps and about 1313 with its block
+# Jacobi; the reference arm and the cpu_baseline object project the measured per-iteration
+# times with the oracle's counts.
 REFERENCE_COUNTS = {"newton": 13.0, "assemblies": 22.0, "cg": 2868.0}
 
 
