@@ -692,6 +692,11 @@ __device__ __forceinline__ TT bj_row(unsigned mt, float4 a, float4 b, const TT *
     return z;
 }
 
+// asks L1 for DoF i's block row ahead of the tile barrier, holding no registers
+__device__ __forceinline__ void bj_prefetch(const float *__restrict__ binv, int64_t i) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(binv + i * kBjMax));
+}
+
 __device__ __forceinline__ void bj_load(const float *__restrict__ binv, int64_t i, float4 &a, float4 &b) {
     const float4 *p = reinterpret_cast<const float4 *>(binv + i * kBjMax);
     a = __ldg(p);
@@ -778,6 +783,7 @@ __global__ void __launch_bounds__(kEBlock)
         DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
         TT r = TT(0);
         if (fr) {
+            bj_prefetch(binv, i);
             g = G[i];
             rx = R[i];
             const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
