@@ -111,3 +111,44 @@ def test_block_partition_is_checked():
         eng._set_blocks(meta)
     eng.set_preconditioner("block")
     assert eng.block_jacobi
+
+
+def test_exported_blocks_and_inverses(oracle_mod):
+    """The device block rows (snp_solver_block_jacobi_export) equal the oracle's Jacobian on
+    each block, and the stored inverses are the symmetric inverses of those blocks (float32)."""
+    from snoopy_b200 import _lib
+    from snoopy_b200.newton import dof_blocks
+
+    msh, coils, rel, solver = _setup(6000)
+    eng = solver.newton_engine()
+    x, _ = solver.solve_to_residual(1e-4, return_device=True)
+    O, sf = _oracle(oracle_mod, msh, coils, rel, solver)
+    _, J, _ = O.compute_stiffness_and_jacobi_matrix_c(x.cpu().numpy(), sf)
+    J = J.tocsr()
+    mask = solver.make_boundary_mask()
+    meta = dof_blocks(msh.edges[:, 0], mask)
+    n = msh.num_dofs
+    eng.assemble_tensors(x, "fp64")
+    bm = torch.zeros(n * 8, dtype=torch.float64, device="cuda")
+    bi = torch.zeros(n * 8, dtype=torch.float32, device="cuda")
+    _lib.call("snp_solver_block_jacobi_export", eng.handle, 0, _lib.ptr(bm), _lib.ptr(bi), _lib.stream_ptr(None))
+    torch.cuda.synchronize()
+    bm = bm.cpu().numpy().reshape(n, 8)
+    bi = bi.cpu().numpy().reshape(n, 8).astype(np.float64)
+    i = 0
+    worst_rows = worst_inv = 0.0
+    while i < n:
+        s = int(meta[i] >> 8)
+        assert not bm[i:i + s, s:].any() and not bi[i:i + s, s:].any()
+        if mask[i]:
+            B = J[i:i + s, i:i + s].toarray()
+            worst_rows = max(worst_rows, np.abs(bm[i:i + s, :s] - B).max() / np.abs(B).max())
+            X = np.linalg.inv(B)
+            assert np.array_equal(bi[i:i + s, :s], bi[i:i + s, :s].T)
+            worst_inv = max(worst_inv, np.abs(bi[i:i + s, :s] - X).max() / np.abs(X).max())
+        else:
+            assert s == 1 and not bi[i].any()
+        i += s
+    assert worst_rows < 1e-12, worst_rows
+    # float32 rounding of entries up to cond(block) ~ 1e4 times 6e-8
+    assert worst_inv < 2e-3, worst_inv
