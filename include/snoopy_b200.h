@@ -385,6 +385,13 @@ int snp_solver_precond_apply(snp_solver *s, int precision, const double *r, doub
  * may be NULL.  Inspection and test entry. */
 int snp_solver_block_jacobi_export(snp_solver *s, int precision, double *bmat, float *binv, void *stream);
 
+/* HOST: c = -A^-1 g for the symmetric positive semi-definite m x m Galerkin system A (host
+ * row-major) and g (host [m]); the solve snp_solver_solve applies to the reduced system of an
+ * attached basis.  Cholesky of the Jacobi-scaled A; a direction whose pivot falls below 1e-10
+ * of its diagonal (a dependent basis column) is left out (c = 0 there).  SNP_BAD_ARG for a
+ * non-positive or non-finite diagonal entry. */
+int snp_spd_solve(int32_t m, const double *A, const double *g, double *c);
+
 /* Attach a basis (device float32, row-major [n_dofs][ldv], first m <= 128 columns) to the
  * solver's mode-1 solves: the start first takes up to `steps` Galerkin Newton steps
  * x += V c, (V^T J V) c = -V^T F (snp_solver_reduced_system; the m x m system by Cholesky on

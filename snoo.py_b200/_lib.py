@@ -86,6 +86,7 @@ _SIGS = {
     "snp_solver_reduced_system": [_vp, ctypes.c_int, _vp, ctypes.c_int32, ctypes.c_int64, _vp, _vp, _vp, _vp],
     "snp_solver_set_galerkin_basis": [_vp, _vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32],
     "snp_solver_set_block_jacobi": [_vp, _vp],
+    "snp_spd_solve": [ctypes.c_int32, _vp, _vp, _vp],
     "snp_solver_block_jacobi_export": [_vp, ctypes.c_int, _vp, _vp, _vp],
     "snp_solver_precond_apply": [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(ctypes.c_int32), _vp],
     "snp_solver_jacobian_layout": [_vp, ctypes.POINTER(ctypes.c_int)],

@@ -1024,6 +1024,13 @@ int snp_solver_block_jacobi_export(snp_solver *s, int precision, double *bmat, f
     return SNP_OK;
 }
 
+int snp_spd_solve(int32_t m, const double *A, const double *g, double *c) {
+    snp::clear_error();
+    SNP_REQUIRE(m >= 1 && A != nullptr && g != nullptr && c != nullptr, "snp_spd_solve: bad arguments");
+    SNP_REQUIRE(snp::spd_solve(m, A, g, c), "snp_spd_solve: non-positive or non-finite diagonal, or non-finite solution");
+    return SNP_OK;
+}
+
 int snp_solver_set_galerkin_basis(snp_solver *s, const float *V, int32_t m, int64_t ldv, int32_t steps) {
     snp::clear_error();
     SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_set_galerkin_basis: solver missing or not finalized");

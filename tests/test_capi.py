@@ -56,3 +56,42 @@ def test_library_is_sm100a_build():
     assert os.path.exists(path)
     blob = open(path, "rb").read()
     assert b"sm_100a" in blob
+
+
+def test_galerkin_spd_solve_on_host():
+    """snp_spd_solve (the host solve of the Galerkin step) against numpy: badly scaled SPD
+    systems, a dependent basis column left out, and a zero diagonal rejected."""
+    import ctypes
+
+    import numpy as np
+
+    from snoopy_b200 import _lib
+
+    L = _lib.load()
+    P = ctypes.POINTER(ctypes.c_double)
+    rng = np.random.default_rng(3)
+    for m in (1, 7, 64, 128):
+        B = rng.normal(size=(m, m))
+        D = np.diag(np.exp(rng.normal(size=m) * 3))
+        A = D @ (B @ B.T + 1e-2 * np.eye(m)) @ D
+        g = rng.normal(size=m)
+        c = np.zeros(m)
+        assert L.snp_spd_solve(m, A.ctypes.data_as(P), g.ctypes.data_as(P), c.ctypes.data_as(P)) == 0
+        want = -np.linalg.solve(A, g)
+        assert np.abs(c - want).max() <= 1e-8 * np.abs(want).max(), m
+    # a repeated column: the dependent direction is dropped and the system is still solved
+    m = 6
+    B = rng.normal(size=(m, m))
+    A = B @ B.T
+    A[:, 5] = A[:, 4]
+    A[5, :] = A[4, :]
+    g = rng.normal(size=m)
+    g[5] = g[4]
+    c = np.zeros(m)
+    assert L.snp_spd_solve(m, A.ctypes.data_as(P), g.ctypes.data_as(P), c.ctypes.data_as(P)) == 0
+    assert c[5] == 0.0 and np.abs(A @ c + g).max() <= 1e-10 * np.abs(g).max()
+    A = np.eye(3)
+    A[1, 1] = 0.0
+    g = np.ones(3)
+    assert L.snp_spd_solve(3, A.ctypes.data_as(P), g.ctypes.data_as(P), c.ctypes.data_as(P)) == 1
+    assert b"diagonal" in L.snp_last_error()
