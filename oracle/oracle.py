@@ -587,8 +587,40 @@ def ew_forcing(it, fn, fprev, eta_prev, F0, tol, eta_max=0.1, fp32=False):
     return min(eta, 0.5)
 
 
+def block_jacobi_inverse(J, meta, mask):
+    """Block-Jacobi preconditioner of the free Jacobian J[mask][:, mask] as a scipy matrix:
+    the inverse of each diagonal block of the partition ``meta`` (uint16 per DoF: offset in
+    the block | block size << 8, constrained DoFs alone; the product's ``newton.dof_blocks``).
+    Restates the product's block build (per-DoF block rows of J, each block inverted) in
+    float64, with its fallback to 1/diag for a block that is not positive definite."""
+    from scipy.sparse import coo_matrix
+
+    J = J.tocsr()
+    n = J.shape[0]
+    rows, cols, vals = [], [], []
+    i = 0
+    while i < n:
+        s = int(meta[i]) >> 8
+        if mask[i]:
+            idx = np.arange(i, i + s)
+            B = J[idx][:, idx].toarray()
+            B = np.triu(B) + np.triu(B, 1).T  # the upper triangle, as the device reads it
+            try:
+                np.linalg.cholesky(B)
+                X = np.linalg.inv(B)
+            except np.linalg.LinAlgError:
+                X = np.diag(1.0 / np.diag(B))
+            ii, jj = np.meshgrid(idx, idx, indexing="ij")
+            rows.append(ii.ravel())
+            cols.append(jj.ravel())
+            vals.append(X.ravel())
+        i += s
+    M = coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n)).tocsr()
+    return M[mask][:, mask]
+
+
 def newton_residual(assembler, mask, source_fields=(), rtol=1e-8, x_0=None, cg_rtol=1e-12, cg_maxiter=None,
-                    max_newton_iterations=50, verbose=False, forcing="fixed", line_search=False):
+                    max_newton_iterations=50, verbose=False, forcing="fixed", line_search=False, blocks=None):
     """Newton on F(x) = K(x) x - rhs(x) until ||F_free|| <= rtol ||F_free(x_0)||.
 
     Each step solves J_free h = -F_free with Jacobi-preconditioned scipy CG to the
@@ -599,6 +631,8 @@ def newton_residual(assembler, mask, source_fields=(), rtol=1e-8, x_0=None, cg_r
     each rejected alpha is replaced by the minimiser of the quadratic model of ||F||^2 along h,
     kept within [0.1, 0.5] alpha, until ||F(x + alpha h)|| <= (1 - 1e-4 alpha) ||F(x)|| (at most
     30 reductions).  ``forcing="ew"`` uses the device solver's inner tolerances (``ew_forcing``).
+    ``blocks`` (a block partition, see ``block_jacobi_inverse``) replaces the point-Jacobi
+    preconditioner by block Jacobi, as the device solver's residual mode does by default.
     Returns x and stats (residual history, CG counts, step lengths).
     """
     n = assembler.num_dofs
@@ -625,7 +659,10 @@ def newton_residual(assembler, mask, source_fields=(), rtol=1e-8, x_0=None, cg_r
         if F0 == 0 or fn <= rtol * F0 or i == max_newton_iterations:
             break
         J_c = J[mask, :][:, mask]
-        M = diags(1.0 / J_c.diagonal(), shape=J_c.shape)
+        if blocks is None:
+            M = diags(1.0 / J_c.diagonal(), shape=J_c.shape)
+        else:
+            M = block_jacobi_inverse(J, blocks, mask)
         its = [0]
 
         def cb(_):

@@ -249,3 +249,42 @@ def test_bf16_rounding_is_nearest_even():
     assert r[2] == 1.0 + 2 ** -7        # above the tie rounds up
     assert r[3] == -2.5
     assert abs(r[4] - 3.140625) < 1e-12
+
+
+def test_block_jacobi_newton_on_the_oracle(oracle_mod):
+    """The oracle's residual Newton with the product's block partition (edges sharing their
+    lower node) reaches the point-Jacobi field in far fewer CG iterations: the preconditioner
+    the device's residual mode runs, restated on scipy's CG."""
+    import snoopy_b200 as S
+    from snoopy_b200 import finite_element as fe
+    from snoopy_b200 import materials as MAT
+    from snoopy_b200 import mesh as M
+    from snoopy_b200.newton import dof_blocks
+
+    msh = M.window_frame_mesh(6000, jitter=0.15, seed=7)
+    n = msh.num_dofs
+    rel = MAT.atan_reluctance()
+    w, q = fe.quadrature_rule(2)
+    dphi = fe.evaluate_basis_derivative(q)
+    curls, n_orient = fe.curl_edge_basis_functions(q)
+    phi = fe.evaluate_basis(q)
+    iron = msh.domain_elements(M.TAG_IRON)
+    air = msh.domain_elements(M.TAG_AIR)
+    P = np.einsum("qi,eid->eqd", phi.reshape(len(w), 4), msh.nodes[msh.cells[iron]]).reshape(-1, 3)
+    Bs = sum(oracle_mod.compute_B_line_segs_cpp(c.get_segments(), P, c.current, c.rad) for c in msh.geometry.coils())
+    mats = [dict(cells=msh.cells[iron], glob_ids=msh.elem_edges[iron], orientations=msh.orientations[iron],
+                 reluctance=rel),
+            dict(cells=msh.cells[air], glob_ids=msh.elem_edges[air], orientations=msh.orientations[air],
+                 reluctance=S.ConstantReluctance(0.25 / np.pi * 1e7))]
+    O = oracle_mod.OracleCurlCurlAssembler(msh.nodes, mats, n, w, q, dphi, curls)
+    mask = np.ones(n, dtype=bool)
+    mask[np.asarray(msh.get_edge_boundary_dofs()) - 1] = False
+    sf = [Bs, np.zeros((0, 3))]
+    kw = dict(rtol=1e-8, cg_rtol=0.1, forcing="ew", line_search="energy", max_newton_iterations=40)
+    xj, sj = oracle_mod.newton_residual(O, mask, sf, **kw)
+    xb, sb = oracle_mod.newton_residual(O, mask, sf, blocks=dof_blocks(msh.edges[:, 0], mask), **kw)
+    assert sj["rel_res"] <= 1e-8 and sb["rel_res"] <= 1e-8
+    assert sum(sb["cg"]) < 0.75 * sum(sj["cg"]), (sum(sb["cg"]), sum(sj["cg"]))
+    Bj = oracle_mod.element_B(msh.nodes, msh.cells, msh.elem_edges, msh.orientations, curls, n_orient, dphi, xj)
+    Bb = oracle_mod.element_B(msh.nodes, msh.cells, msh.elem_edges, msh.orientations, curls, n_orient, dphi, xb)
+    assert np.abs(Bb - Bj).max() <= 1e-6 * np.abs(Bj).max()
