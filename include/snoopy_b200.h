@@ -396,7 +396,7 @@ int snp_spd_solve(int32_t m, const double *A, const double *g, double *c);
  * solver's mode-1 solves: the start first takes up to `steps` Galerkin Newton steps
  * x += V c, (V^T J V) c = -V^T F (snp_solver_reduced_system; the m x m system by Cholesky on
  * the host), each undone and ending the corrections when it does not lower ||F_free||; the
- * res_ref drop rule then judges the corrected start.  Without res_ref the convergence target
+ * res_ref drop rule then applies to the corrected start.  Without res_ref the convergence target
  * stays relative to the uncorrected start's ||F_free|| (stats.res0).  V
  * must stay valid while attached; V = NULL, m = 0 or steps = 0 detaches.  Needs the
  * SNP_LAYOUT_ELEM layout.  No counterpart in the reference. */

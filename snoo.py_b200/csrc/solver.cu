@@ -551,7 +551,7 @@ struct snp_solver {
             double fn = std::sqrt(st3[0]);
             S.res0 = fn;
             // Galerkin correction of the start in the attached basis; a step that does not lower
-            // ||F_free|| is undone.  The drop rule below judges the corrected start.
+            // ||F_free|| is undone.  The drop rule below applies to the corrected start.
             if (gal_V && gal_m > 0 && layout == SNP_LAYOUT_ELEM && fn > 0.0) {
                 for (int gs = 0; gs < gal_steps; ++gs) {
                     SNP_CUDA_TRY(cudaEventRecord(ev[0], stream));

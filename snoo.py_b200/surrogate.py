@@ -346,7 +346,7 @@ class WarmStart:
         modes: assemble J(x) and F(x) (matrix-free, ``precision``), solve (V^T J V) c = -V^T F
         (both from ``snp_solver_reduced_system``), x += V c.  The member must already be set on
         ``msolver`` (default: the training solver).  Returns a new float64 vector; the Newton
-        solve that follows still judges it by its residual.  A singular reduced system leaves
+        solve that follows still checks it by its residual.  A singular reduced system leaves
         x unchanged."""
         t = torch()
         ms = msolver or self.ms
