@@ -333,6 +333,7 @@ def run_ours(args):
                                f"{msh.num_elements} tets / {n} edge DoFs, Q=4, {args.precision}",
                    "tets": msh.num_elements, "dofs": n, "nnz": nnz, "precision": args.precision,
                    "jacobian": layout,
+                   "preconditioner": "block Jacobi (edges sharing a node)" if bj else "point Jacobi",
                    "newton_per_solve": newton / args.steps, "cg_per_solve": cg_its / args.steps,
                    "assemblies_per_solve": assemblies / args.steps,
                    "assembly_ms_per_solve": t_asm / args.steps, "krylov_ms_per_solve": t_kry / args.steps,
@@ -437,6 +438,7 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
     out = {"workload": f"morphed window-frame yoke family, {fam.mesh.num_elements} tets / {fam.mesh.num_dofs} DoFs, "
                        f"8 shape parameters + J, {n_train} training / {n_test} held-out members",
            "setup_s": setup_s, "generate_s": ws.timings["generate_s"], "fit_s": ws.timings["fit_s"],
+           "preconditioner": "block Jacobi" if getattr(ms.eng, "block_jacobi", False) else "point Jacobi",
            "pod_modes": modes, "pod_energy": ws.pod_energy, "train_loss_first_last": [ws.history[0][1], ws.history[-1][1]],
            "train_newton_mean": float(np.mean([s["newton_iterations"] for s in st_train])),
            "surrogate_rel_err_mean": float(np.mean(surr_err)), "pod_floor_rel_err_mean": float(np.mean(proj_err)),
