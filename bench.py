@@ -63,6 +63,36 @@ def workload(tets):
     return msh, msh.geometry.coils(), MAT.atan_reluctance()
 
 
+def oracle_problem(tets):
+    """The workload set up for the CPU oracle with the reference's C kernels (``oracle/_ref``):
+    mesh, coils, reluctance, quadrature tables, the per-material assembler, the free-DoF mask,
+    the iron quadrature points and the source fields there."""
+    import oracle as O
+
+    import snoopy_b200 as S
+    from snoopy_b200 import finite_element as FE
+    from snoopy_b200 import mesh as M
+
+    msh, coils, rel = workload(tets)
+    w, q = FE.quadrature_rule(2)
+    dphi = FE.evaluate_basis_derivative(q)
+    phi = FE.evaluate_basis(q)
+    curls, _ = FE.curl_edge_basis_functions(q)
+    iron = msh.domain_elements(M.TAG_IRON)
+    air = msh.domain_elements(M.TAG_AIR)
+    mats = [dict(cells=msh.cells[iron], glob_ids=msh.elem_edges[iron], orientations=msh.orientations[iron],
+                 reluctance=rel),
+            dict(cells=msh.cells[air], glob_ids=msh.elem_edges[air], orientations=msh.orientations[air],
+                 reluctance=S.ConstantReluctance(0.25 / np.pi * 1e7))]
+    pts = np.einsum("qi,eid->eqd", phi, msh.nodes[msh.cells[iron]]).reshape(-1, 3)
+    Bs = sum(O.compute_B_line_segs_cpp(c.get_segments(), pts, c.current, c.rad, backend="ref") for c in coils)
+    A = O.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, w, q, dphi, curls, backend="ref")
+    mask = np.ones(msh.num_dofs, bool)
+    mask[msh.get_edge_boundary_dofs() - 1] = False
+    return dict(msh=msh, coils=coils, rel=rel, w=w, q=q, dphi=dphi, phi=phi, curls=curls, A=A, mask=mask,
+                iron_points=pts, sf=[Bs, np.zeros((0, 3))])
+
+
 # ---------------------------------------------------------------------------- clocks
 
 class ClockSampler:
@@ -233,6 +263,9 @@ def run_ours(args):
     x = zeros(n)[:n]
 
     def one_solve():
+        # the coils' source field is evaluated on every solve, as the reference's solve does
+        # (red_mvp_solver.py:149-166), then the Newton solve from A = 0
+        solver.compute_source_fields(refresh=True)
         return eng.solve(None, mode=1, tol=RTOL, max_newton=60, precision=prec, x_out=x, cg_maxiter=50000)[1]
 
     for _ in range(args.warmup):
@@ -495,8 +528,10 @@ def mixed_precision_accuracy(tets=4_000_000, n_probes=1000):
     """The same window-frame yoke at ~4M tets solved to the 1e-8 Newton residual twice: in
     float64, and with float32 element tensors and float32 CG inside the float64 Newton loop
     (the Newton residual and update stay float64, so each Newton step refines the float32
-    inner solve).  Reported: B error at 1000 seeded aperture probes of the mixed solve against
-    the float64 solve, and Newton / CG counts and times of both."""
+    inner solve).  Reported: B error at 1000 seeded aperture probes of both solves against the
+    CPU oracle's float64 solve (reference C kernels and scipy cg, converged to 1e-10; stored in
+    tests/golden/config_c3.npz by tests/golden/make_config_golden.py), of the mixed solve against
+    the float64 device solve, and Newton / CG counts and times of both."""
     import torch
 
     import snoopy_b200 as S
@@ -525,6 +560,16 @@ def mixed_precision_accuracy(tets=4_000_000, n_probes=1000):
     d = np.linalg.norm(B["mixed"] - B["fp64"], axis=1)
     out["b_err_max_rel"] = float(d.max() / np.linalg.norm(B["fp64"], axis=1).max())
     out["b_err_rms_rel"] = float(np.sqrt(np.mean(d ** 2)) / np.sqrt(np.mean(np.sum(B["fp64"] ** 2, axis=1))))
+    fx_path = os.path.join(ROOT, "tests", "golden", "config_c3.npz")
+    if os.path.exists(fx_path):
+        fx = np.load(fx_path)
+        if int(fx["tets"]) == msh.num_elements and np.array_equal(fx["elements"], el):
+            Bo = fx["B"]
+            scale = np.linalg.norm(Bo, axis=1).max()
+            out["vs_fp64_oracle"] = {
+                "oracle": f"CPU float64 Newton to rel. residual {float(fx['rel_res']):.1e} (reference C kernels, "
+                          f"scipy Jacobi cg; {int(fx['newton'])} Newton steps, {int(fx['cg'])} CG iterations)",
+                **{f"b_err_max_rel_{p}": float(np.linalg.norm(B[p] - Bo, axis=1).max() / scale) for p in B}}
     del solver
     return out
 
@@ -670,27 +715,149 @@ def cpu_baseline_sample(msh, coils, rel, assemblies_per_solve, cg_per_solve):
 REFERENCE_COUNTS = {"newton": 13.0, "assemblies": 22.0, "cg": 2868.0}
 
 
+def host_info():
+    """Host CPU of the machine the reference arm runs on: model, logical CPUs this process may
+    use, and the numerical libraries of the CPU path."""
+    import platform
+
+    import scipy
+
+    model = platform.processor() or ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    mem_gb = None
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable"):
+                mem_gb = int(line.split()[1]) / 2**20
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "logical_cpus": os.cpu_count(), "usable_cpus": usable, "mem_available_gb": mem_gb,
+            "numpy": np.__version__, "scipy": scipy.__version__}
+
+
+# Host memory one worker of the reference arm holds at the ~1.2M-tet workload (reference
+# triplets, scipy's COO->CSR copies of K, dK and J, the masked Jacobian), measured peak ~4 GB.
+REFERENCE_WORKER_GB = 6.0
+
+
+def _reference_worker(tets, solve_ids, warmup, barrier, out_q):
+    """One host process of the reference arm: build the workload and the oracle problem (the
+    reference's C kernels), run ``warmup`` bounded samples, wait for the others, then run each
+    listed solve completely and report its time."""
+    from threadpoolctl import threadpool_limits
+
+    threadpool_limits(1)
+    import oracle as O
+    from scipy.sparse import diags
+    from scipy.sparse.linalg import cg
+
+    P = oracle_problem(tets)
+    msh, A, mask = P["msh"], P["A"], P["mask"]
+    sample = None
+    for k in range(warmup):
+        # bounded warm-up: one assembly and 10 Jacobi-CG iterations at a seeded state
+        x = np.random.default_rng(k).normal(0.0, 1e-3, msh.num_dofs)
+        x[~mask] = 0.0
+        t0 = time.perf_counter()
+        K, J, rhs = A.compute_stiffness_and_jacobi_matrix_c(x, P["sf"])
+        F = K @ x - rhs
+        J_c = J[mask, :][:, mask]
+        M_ = diags(1.0 / J_c.diagonal(), shape=J_c.shape)
+        t1 = time.perf_counter()
+        cg(J_c, -F[mask], rtol=1e-30, atol=0.0, M=M_, maxiter=10)
+        t2 = time.perf_counter()
+        sample = {"t_assembly_s": t1 - t0, "t_cg_iteration_s": (t2 - t1) / 10}
+        del K, J, rhs, F, J_c, M_
+    barrier.wait()
+    for sid in solve_ids:
+        t0 = time.perf_counter()
+        # the source field at the iron quadrature points, evaluated per solve as
+        # red_mvp_solver.py:149-166 does (reference Biot-Savart kernel)
+        Bs = sum(O.compute_B_line_segs_cpp(c.get_segments(), P["iron_points"], c.current, c.rad, backend="ref")
+                 for c in P["coils"])
+        t_src = time.perf_counter() - t0
+        x, st = O.newton_residual(A, mask, [Bs, np.zeros((0, 3))], rtol=RTOL, forcing="ew", line_search="energy",
+                                  cg_rtol=0.1, max_newton_iterations=60)
+        t1 = time.perf_counter()
+        out_q.put({"solve": sid, "s": t1 - t0, "t_source_s": t_src, "newton": st["newton"], "cg": int(sum(st["cg"])),
+                   "assemblies": st["assemblies"], "rel_res": st["rel_res"], "sample": sample})
+
+
 def run_reference(args):
+    """The reference arm: complete CPU Newton solves of the workload with the reference's own C
+    kernels (``oracle/_ref``: compute_K_dK_Hcurl[_red] and compute_B_line_segs through the Cython
+    layer's marshalling), scipy's COO->CSR and sparse adds, and scipy's Jacobi-preconditioned
+    ``cg`` (``red_mvp_solver.py:178-222``), driven by the same inexact Newton as the device solver
+    (Eisenstat-Walker inner tolerances, energy line search) from A = 0 to the 1e-8 relative
+    residual.  Each step is one complete solve; the steps run in parallel host processes, one
+    single-threaded solve per core, so the value is the host's whole-machine throughput."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    os.environ.setdefault("OMP_NUM_THREADS", "1")
-    msh, coils, rel = workload(args.tets)
-    vals = []
-    sample = None
-    for _ in range(args.warmup + args.steps):
-        sample = reference_sample(msh, coils, rel, REFERENCE_COUNTS["assemblies"], REFERENCE_COUNTS["cg"])
-        vals.append(sample["value"])
-    timed = vals[args.warmup:]
-    value = float(np.median(timed))
+    import multiprocessing as mp
+
+    import oracle as O
+
+    info = host_info()
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's C kernels) is not built"}),
+              flush=True)
+        return
+    mem_cap = int((info["mem_available_gb"] or 64.0) // REFERENCE_WORKER_GB) or 1
+    procs = max(1, min(args.steps, info["usable_cpus"], mem_cap))
+    shares = [list(range(p, args.steps, procs)) for p in range(procs)]
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs + 1)
+    q = ctx.Queue()
+    t_setup = time.perf_counter()
+    workers = [ctx.Process(target=_reference_worker, args=(args.tets, shares[p], args.warmup, barrier, q))
+               for p in range(procs)]
+    for w in workers:
+        w.start()
+    barrier.wait()
+    t_setup = time.perf_counter() - t_setup
+    t0 = time.perf_counter()
+    res = [q.get() for _ in range(args.steps)]
+    t1 = time.perf_counter()
+    for w in workers:
+        w.join()
+    wall = t1 - t0
+    value = args.steps / wall
+    per = np.array([r["s"] for r in res])
+    smp = next((r["sample"] for r in res if r["sample"]), None)
+    counts = {k: float(np.mean([r[k] for r in res])) for k in ("newton", "cg", "assemblies")}
+    projected = None
+    if smp:
+        projected = (float(np.mean([r["t_source_s"] for r in res])) + counts["assemblies"] * smp["t_assembly_s"]
+                     + counts["cg"] * smp["t_cg_iteration_s"])
+    tets_msg = f"{args.tets}"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"reduced-MVP Newton solve to rel. residual 1e-8, window-frame yoke, "
-                                   f"{msh.num_elements} tets / {msh.num_dofs} edge DoFs, Q=4, fp64",
-                       "counts_per_solve": REFERENCE_COUNTS},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": sample["cores"], "kind": sample["kind"],
-                             "sample": sample["sample"]},
+                                   f"~{tets_msg} target tets, Q=4, fp64",
+                       "solves": args.steps, "processes": procs, "counts_per_solve": counts,
+                       "max_rel_res": float(max(r["rel_res"] for r in res)), "setup_s": t_setup},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                             "sample": (f"{args.steps} complete solves (reference C kernels, scipy CSR and Jacobi cg, "
+                                        f"source field per solve) on {procs} single-threaded processes; one solve "
+                                        f"{per.mean():.1f} s mean ({per.min():.1f}-{per.max():.1f} s); warm-up: "
+                                        f"{args.warmup} bounded samples per process (one assembly + 10 CG "
+                                        f"iterations)"),
+                             "solve_s_mean": float(per.mean()), "solve_s_min": float(per.min()),
+                             "solve_s_max": float(per.max()), "single_core_solves_per_s": float(1.0 / per.mean()),
+                             "projected_solve_s": projected, "host": info},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

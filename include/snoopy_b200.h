@@ -240,10 +240,10 @@ int snp_pcg(int32_t n_rows, const int32_t *row_ptr, const int32_t *col_idx, cons
  * Same arguments, results and statuses as snp_pcg, but the work vectors live in one static
  * device array of SNP_PCG_NOALLOC_MAX_ROWS rows (about 11 MB, held by every GPU that loads
  * this library until the process exits); larger systems are rejected with SNP_BAD_ARG.
- * Nothing is allocated: no cudaMalloc, cudaFree or allocating library call.  The array's
- * device address is looked up on the first call on each device (make that call before any
- * stream capture).  All calls share the array: calls whose work overlaps on the GPU race and
- * must be serialised by the caller. */
+ * Nothing is allocated: no cudaMalloc, cudaFree or allocating library call.  Every call looks
+ * the array's device address up for the calling thread's current device and context, and
+ * synchronises `stream`.  All calls share the array, which keeps the last call's contents:
+ * calls whose work overlaps on the GPU race and must be serialised by the caller. */
 #define SNP_PCG_NOALLOC_MAX_ROWS 262144
 int snp_pcg_noalloc(int32_t n_rows, const int32_t *row_ptr, const int32_t *col_idx, const double *vals,
                     const uint8_t *free_mask, const double *b, double *x, double rtol, double atol,

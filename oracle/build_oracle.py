@@ -6,8 +6,10 @@
   minus ``-fopenmp`` (libgomp's spec file is missing in this image; every OpenMP pragma on
   the hot path is commented out in the reference, so the result is behaviour-identical).
 
-Run ``python oracle/build_oracle.py`` (or call ``build()``).  The reference checkout is only
-needed for ``_ref``; where it is absent the prebuilt ``_ref`` library is used as is.
+Run ``python oracle/build_oracle.py [--reference DIR]`` (or call ``build()``).  The reference
+checkout is found from ``--reference``, else the environment variable ``SNOOPY_REFERENCE``, else
+its location in the build container; it is only needed for ``_ref``, and where it is absent the
+prebuilt ``_ref`` library is used as is.
 """
 
 import os
@@ -15,7 +17,17 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_FEM_C = "/root/reference/fem_c"
+
+
+def reference_root(argv=None):
+    """The reference checkout: ``--reference DIR`` in argv, else $SNOOPY_REFERENCE, else the
+    build container's checkout."""
+    argv = sys.argv if argv is None else argv
+    if "--reference" in argv:
+        return argv[argv.index("--reference") + 1]
+    return os.environ.get("SNOOPY_REFERENCE", "/root/reference")
+
+
 LIB_ORACLE = os.path.join(HERE, "_build", "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libctools_ref.so")
 
@@ -27,7 +39,8 @@ def _newer(target, *sources):
     return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
 
 
-def build(force=False, verbose=False):
+def build(force=False, verbose=False, reference=None):
+    fem_c = os.path.join(reference or reference_root([]), "fem_c")
     os.makedirs(os.path.dirname(LIB_ORACLE), exist_ok=True)
     src = os.path.join(HERE, "restated.c")
     if force or _newer(LIB_ORACLE, src):
@@ -35,11 +48,11 @@ def build(force=False, verbose=False):
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)
-    ref_src = os.path.join(REFERENCE_FEM_C, "ctools.c")
+    ref_src = os.path.join(fem_c, "ctools.c")
     if os.path.exists(ref_src):
         os.makedirs(os.path.dirname(LIB_REF), exist_ok=True)
         if force or _newer(LIB_REF, ref_src):
-            cmd = ["gcc", "-O3", "-fPIC", "-shared", "-w", "-I", REFERENCE_FEM_C, "-o", LIB_REF, ref_src, "-lm"]
+            cmd = ["gcc", "-O3", "-fPIC", "-shared", "-w", "-I", fem_c, "-o", LIB_REF, ref_src, "-lm"]
             if verbose:
                 print(" ".join(cmd))
             subprocess.check_call(cmd)
@@ -47,4 +60,4 @@ def build(force=False, verbose=False):
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, reference=reference_root()))

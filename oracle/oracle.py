@@ -28,6 +28,7 @@ The glue around them restates the reference's Python/Cython layers:
 * ``laplace_subdomain_solve``                        ``snoopy/laplace_subdomain_solver.py:117-158``
 * ``locate_points``, ``element_B``, ``nodal_fields``, ``interpolate_nodal``: field-map output
   (``snoopy/evaluators.py:155-410``, ``snoopy/curl_curl_assembler.py:2089-2196``)
+* ``probe_B``: the total field at probe points (``RedMVPSolver``'s output, curl A + B_s)
 """
 
 import ctypes
@@ -877,3 +878,24 @@ def interpolate_nodal(cells, elem, bary, nodal_sets, point_set):
         v = nodal_sets[s].reshape(-1, nc)
         out[p] = bary[p] @ v[cells[e]]
     return out
+
+
+def probe_B(nodes, cells, glob_ids, orientations, curls, phi, d_phi, q, w, num_dofs, x, points, coils=(),
+            backend="ref"):
+    """Total field B = curl A + B_s at points, all arithmetic on the CPU: points located by
+    ``locate_points``, curl A from ``compute_B_Hcurl`` (``interface_c.pyx:555-696``, through the
+    chosen backend) on the located elements (first order: constant per element, so its first
+    quadrature point serves), the source field of ``coils`` (objects with ``get_segments()``,
+    ``current`` and ``rad``) from ``compute_B_line_segs_cpp`` (``interface_c.pyx:928-991``), as
+    ``RedMVPSolver``'s field output adds it.  Returns (B [P, 3], element index [P])."""
+    el, _ = locate_points(nodes, cells, points)
+    if (el < 0).any():
+        raise ValueError(f"{int((el < 0).sum())} points lie outside the mesh")
+    cells = np.asarray(cells).reshape(-1, 4)
+    gids = np.asarray(glob_ids).reshape(-1, 6)
+    ori = np.asarray(orientations).reshape(-1)
+    _, B = compute_B_Hcurl(nodes, cells[el], gids[el], curls, phi, d_phi, ori[el], x, q, w, num_dofs, 6, backend)
+    B = B.reshape(len(el), -1, 3)[:, 0].copy()
+    for c in coils:
+        B += compute_B_line_segs_cpp(c.get_segments(), points, c.current, c.rad, backend=backend)
+    return B, el

@@ -605,8 +605,11 @@ int pcg_on_buffers(const CsrView<double> &A, const uint8_t *free_mask, const dou
     const int64_t nt = (A.n + kVecIlp - 1) / kVecIlp;
     const int gu = wave_grid(k_update<double>, nt, kVecBlock);
     const int gp = wave_grid(k_pupdate<double>, nt, kVecBlock);
-    SNP_REQUIRE(gv <= B.max_blocks && gu <= B.max_blocks, "pcg: %d blocks exceed the %d partial-sum slots",
-                gv > gu ? gv : gu, B.max_blocks);
+    // every grid below (k_dinv, k_init, the SpMV with its dot product, k_update, k_pupdate) is
+    // sized by stride_grid(..., 8) or wave_grid, so at most 8 blocks per SM index the partials
+    SNP_REQUIRE((int64_t)sm_count() * 8 <= B.max_blocks && gv <= B.max_blocks && gu <= B.max_blocks &&
+                    gp <= B.max_blocks,
+                "pcg: %d SMs x 8 blocks exceed the %d partial-sum slots", sm_count(), B.max_blocks);
     k_dinv<double, double><<<gv, kVecBlock, 0, s>>>(A.n, B.diag, A.v, free_mask, B.dinv, B.bad);
     SNP_LAUNCH_CHECK();
     int hbad = 0;

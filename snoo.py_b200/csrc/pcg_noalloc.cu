@@ -9,12 +9,13 @@
 // every GPU that loads this library holds it until the process exits.
 //
 // Host code cannot use the array's name as a device address (it names a host-side shadow), so
-// the address is looked up once per device with cudaGetSymbolAddress, with that device current,
-// on the first call made on the device; make that first call before any stream capture.
+// every call looks the address up with cudaGetSymbolAddress, with the calling thread's current
+// device current, and checks the result.  The lookup allocates nothing; doing it per call (not
+// once per device) keeps the address right after cudaDeviceReset or when another context of
+// the device becomes current, either of which reloads the module at a new address.
+// The call synchronises `stream` (it reads the row count and the CG state back).
 // All calls share the array: calls whose work overlaps on the GPU (different streams, threads
 // or processes sharing a context) race on it and must be serialised by the caller.
-#include <mutex>
-
 #include "snp_common.cuh"
 #include "snp_internal.cuh"
 #include "snp_krylov.cuh"
@@ -41,24 +42,16 @@ constexpr size_t kScratchBytes = kOffBad + 256;
 
 static __device__ __align__(256) unsigned char g_pcg_scratch[kScratchBytes];
 
-std::mutex g_mu;
-void *g_addr[64] = {nullptr};
-
-// Device address of g_pcg_scratch on the current device (looked up on first use).
+// Device address of g_pcg_scratch in the current device's current context.
 int scratch_address(unsigned char **out) {
-    int dev = -1;
-    SNP_CUDA_TRY(cudaGetDevice(&dev));
-    SNP_REQUIRE(dev >= 0 && dev < 64, "snp_pcg_noalloc: device index %d out of range", dev);
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return fail(SNP_CUDA_ERROR, "snp_pcg_noalloc: cudaGetSymbolAddress of the scratch array failed: %s",
-                        cudaGetErrorString(e));
-        g_addr[dev] = p;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+        cudaGetLastError();
+        return fail(SNP_CUDA_ERROR, "snp_pcg_noalloc: cudaGetSymbolAddress of the scratch array failed: %s",
+                    cudaGetErrorString(e));
     }
-    *out = static_cast<unsigned char *>(g_addr[dev]);
+    *out = static_cast<unsigned char *>(p);
     return SNP_OK;
 }
 

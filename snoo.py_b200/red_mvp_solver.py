@@ -56,10 +56,11 @@ class RedMVPSolver:
         mask[np.asarray(self.dirichlet_dofs, dtype=np.int64) - 1] = False
         return mask
 
-    def compute_source_fields(self):
+    def compute_source_fields(self, refresh=False):
         """B_s at the iron quadrature points, summed over coils (``red_mvp_solver.py:149-166``),
-        as device tensors; empty entries for the air domains."""
-        if self._source_fields is None:
+        as device tensors; empty entries for the air domains.  Computed once and kept, or again
+        with ``refresh`` (then also handed to the Newton engines built so far)."""
+        if self._source_fields is None or refresh:
             fields = []
             for i in range(len(self.iron_tags)):
                 pts = self.curl_curl_factory.get_quadrature_points_device(self.quad_order, i)
@@ -71,6 +72,10 @@ class RedMVPSolver:
             for _ in self.air_tags:
                 fields.append(np.zeros((0, 3)))
             self._source_fields = fields
+            for eng in (self._newton, getattr(self, "_newton_gauged", None)):
+                if eng is not None:
+                    for i in range(len(self.iron_tags)):
+                        eng.set_source(i, fields[i])
         return self._source_fields
 
     def gauge_mask(self):
@@ -93,12 +98,23 @@ class RedMVPSolver:
                                         self.quad_order, stream=getattr(self, "stream", None))
         return self._newton
 
+    def _engine_for_solve(self, apply_gauge=False):
+        """The Newton engine with the coils' source field evaluated now: every solve evaluates it,
+        as the reference's does (``red_mvp_solver.py:149-166``), so coil changes between solves
+        are seen."""
+        built = (getattr(self, "_newton_gauged", None) if apply_gauge else self._newton) is not None
+        eng = self.newton_engine(apply_gauge)
+        if built:
+            self.compute_source_fields(refresh=True)
+        return eng
+
     def solve(self, tolerance=1e-4, x_0=np.zeros((0,)), maxiter=-1, apply_gauge=False):
-        """Newton with the reference's increment test (``red_mvp_solver.py:121-224``).
+        """Newton with the reference's increment test (``red_mvp_solver.py:121-224``).  The coils'
+        source field is evaluated on every call, as the reference does (``:149-166``).
 
         :return: the solution vector, float64[num_dofs] (numpy).
         """
-        eng = self.newton_engine(apply_gauge)
+        eng = self._engine_for_solve(apply_gauge)
         x0 = None if len(x_0) == 0 else np.asarray(x_0, dtype=np.float64)
         if self.verbose:
             print("***********************")
@@ -115,9 +131,10 @@ class RedMVPSolver:
         :param precision: "fp64", or "mixed" for float32 Jacobian values and CG inside the
             float64 Newton residual and update.
         :param cg_maxiter: cap on CG iterations per Newton step (-1: 10 x free DoFs, as scipy).
-        :return: (x, stats); x is numpy unless ``return_device``.
+        :return: (x, stats); x is numpy unless ``return_device``.  The source field is evaluated
+        on every call, as in ``solve``.
         """
-        eng = self.newton_engine()
+        eng = self._engine_for_solve()
         prec = {"fp64": 0, "mixed": 1}[precision]
         x, stats = eng.solve(x_0, mode=MODE_RESIDUAL, tol=rtol, cg_maxiter=cg_maxiter,
                              max_newton=max_newton or self.max_newton_iterations, precision=prec, verbose=verbose)

@@ -61,7 +61,8 @@ def reference_dilution_coefficients():
 
     for name in ("matplotlib", "matplotlib.pyplot"):
         sys.modules.setdefault(name, types.ModuleType(name))
-    spec = importlib.util.spec_from_file_location("_ref_materials", "/root/reference/snoopy/materials.py")
+    ref = os.environ.get("SNOOPY_REFERENCE", "/root/reference")
+    spec = importlib.util.spec_from_file_location("_ref_materials", os.path.join(ref, "snoopy", "materials.py"))
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     out = []
