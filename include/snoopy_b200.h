@@ -334,6 +334,55 @@ int snp_solver_jacobian_layout(const snp_solver *s, int *layout);
 int snp_solver_solve_many(snp_solver *const *solvers, int32_t count, double *const *x, const snp_solve_opts *opts,
                           snp_solve_stats *stats, int32_t n_threads, int32_t *status);
 
+/* ------------------------------------------------------------------ batched Newton solver
+ * Many problems of uneven size solved by one set of launches: the problems' elements and
+ * DoFs are concatenated (each problem at its own element and DoF offset, padded to the
+ * reduction units), every pass of the residual-mode Newton loop (element-tensor assembly,
+ * block-Jacobi build, the PCG's element and DoF passes, the line search's trial points and
+ * the Newton update) is one launch over all problems, each problem keeps its own Newton, CG
+ * and line-search state on the device, and the whole Newton loop of all problems is one CUDA
+ * graph (conditional WHILE nodes for the Newton, CG and line-search loops) launched once per
+ * solve.  Every sum runs in a fixed order that depends only on the problem itself, so a
+ * problem's answer is bitwise the same whatever else is in the batch.  The reference solves
+ * one design per call (red_mvp_solver.py:121-224) and a design study loops over designs
+ * (examples/plot_example_baseline.py:61-91); this is the batched form of that loop. */
+typedef struct snp_batch snp_batch;
+
+/* Build a batch over `count` finalized solvers with the matrix-free Jacobian layout
+ * (SNP_LAYOUT_ELEM) and block Jacobi set (snp_solver_set_block_jacobi), all with the same
+ * quadrature and orientation tables.  The batch reads each solver's mesh coordinates, source
+ * fields, materials and extra rhs when it solves (later snp_solver_set_nodes / _set_source
+ * calls are seen); the solvers must outlive the batch.  Allocates the concatenated arrays and
+ * a CUDA stream of its own; synchronises. */
+int snp_batch_create(snp_solver *const *solvers, int32_t count, snp_batch **out);
+
+/* Residual-mode Newton (opts[i].mode must be 1; precision the same for all) of every problem at
+ * once: x[i] (device, [n_dofs of problem i]) in = initial guess, out = solution; per-problem
+ * stats and status (SNP_OK, SNP_NOT_CONVERGED, SNP_NAN_DETECTED, SNP_ZERO_PIVOT) as
+ * snp_solver_solve reports them; Galerkin warm-start bases are not used.  Returns the first
+ * failing problem's status.  Synchronises the device before it starts and its stream at the end. */
+int snp_batch_solve(snp_batch *b, double *const *x, const snp_solve_opts *opts, snp_solve_stats *stats,
+                    int32_t *status);
+
+/* Autotuner: times the candidate launch shapes of the element pass (block size 128, 256 or
+ * 512 threads) and of the batched assembly (grid of one or two waves of resident blocks) on
+ * this batch and keeps the fastest for later solves.  The shapes change no arithmetic (every
+ * reduction order is fixed by the data), only the time.  Synchronises. */
+int snp_batch_tune(snp_batch *b, int32_t precision);
+
+typedef struct {
+    int32_t problems;
+    int64_t dofs, elements;        /* concatenated, padding included */
+    int32_t pass1_block;           /* element-pass block size in use */
+    int32_t asm_waves;             /* assembly grid: waves of resident blocks */
+    int32_t graph;                 /* 1 when the Newton loop runs as one CUDA graph */
+    double tuned_pass1_us[3];      /* autotuner's timings of the element pass at 128/256/512 (0: not tuned) */
+    double tuned_asm_us[2];        /* ... and of the assembly at one/two waves */
+} snp_batch_info;
+int snp_batch_get_info(const snp_batch *b, snp_batch_info *info);
+
+int snp_batch_destroy(snp_batch *b);
+
 /* Matrix-free Newton assembly at x (device, [n_dofs]): the element tensors of the Jacobian
  * (float64 for precision 0, float32 for 1; afterwards snp_solver_jacobian_apply with that
  * precision applies J(x)) and, when F is not NULL, the residual F = K(x) x - rhs(x) - rhs_extra

@@ -45,6 +45,17 @@ class SolveStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("problems", _c_i32), ("dofs", _c_i64), ("elements", _c_i64), ("pass1_block", _c_i32),
+                ("asm_waves", _c_i32), ("graph", _c_i32), ("tuned_pass1_us", _c_f64 * 3), ("tuned_asm_us", _c_f64 * 2)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["tuned_pass1_us"] = list(self.tuned_pass1_us)
+        d["tuned_asm_us"] = list(self.tuned_asm_us)
+        return d
+
+
 # name -> argtypes (every function returns int32 status unless listed in _RESTYPES)
 _SIGS = {
     "snp_last_error": [],
@@ -93,6 +104,11 @@ _SIGS = {
     "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
     "snp_solver_set_nodes": [_vp, _vp, _vp],
     "snp_solver_solve_many": [_vp, _c_i32, _vp, _vp, _vp, _c_i32, _vp],
+    "snp_batch_create": [_vp, _c_i32, _pp],
+    "snp_batch_solve": [_vp, _vp, _vp, _vp, _vp],
+    "snp_batch_tune": [_vp, _c_i32],
+    "snp_batch_get_info": [_vp, _vp],
+    "snp_batch_destroy": [_vp],
     "snp_solver_set_source": [_vp, _c_i32, _vp, _vp],
     "snp_solver_set_dilution": [_vp, _c_i32, _vp, _vp],
     "snp_mesh_index_create": [_vp, _c_i64, _vp, _c_i64, _vp, _vp],

@@ -1,10 +1,15 @@
 """Many magnet variants solved together.
 
 Each variant is its own device solver (its own mesh, materials, source and CSR/element
-topology) created on its own CUDA stream; ``solve_many`` hands all of them to
-``snp_solver_solve_many``, which runs every Newton solve on a host thread of its own so the
-GPU overlaps the variants' kernels (small meshes leave most SMs idle when solved alone).
-Every instance's solve is deterministic, so batched and one-at-a-time answers are identical.
+topology) created on its own CUDA stream.  Two ways to solve them together:
+
+* ``BatchSolver``: one batched solver over all variants (``snp_batch_*``): concatenated element
+  and DoF arrays with per-variant offsets, one launch per pass over all variants, per-variant
+  Newton / CG / line-search state on the device, the whole Newton loop one CUDA graph, launch
+  shapes from its autotuner.  A variant's answer does not depend on what else is batched.
+* ``solve_many``: ``snp_solver_solve_many`` runs every variant's own Newton solve on a host
+  thread of its own so the GPU overlaps the variants' kernels.  Every instance's solve is
+  deterministic, so these answers are identical to one-at-a-time solves.
 
 Variant family (seeded): window-frame yokes with outer width U[0.4, 0.9] m, aperture width
 U[0.1, 0.4] m (capped so each leg keeps 5 cm), length U[0.3, 2.0] m, coil current density
@@ -110,6 +115,75 @@ def solve_many(instances, rtol=1e-8, precision="fp64", n_threads=0):
     if rc != 0:
         _lib.check(rc)
     return out
+
+
+class BatchSolver:
+    """All instances in one batched device solver (``snp_batch_*``): the instances' element and
+    DoF arrays concatenated, one launch per pass over all of them, each instance's Newton / CG /
+    line-search state on the device and the whole Newton loop as one CUDA graph.  The
+    instances' own solvers stay the source of their meshes, materials and source fields, so
+    they must outlive this object.  Every instance's answer is bitwise the one it gets in a
+    batch of its own."""
+
+    def __init__(self, instances):
+        t = torch()
+        t.cuda.synchronize()
+        self.instances = list(instances)
+        k = len(self.instances)
+        handles = (ctypes.c_void_p * k)(*[ins.eng.handle.value for ins in self.instances])
+        h = ctypes.c_void_p()
+        _lib.call("snp_batch_create", handles, k, ctypes.byref(h))
+        self.handle = h
+
+    def tune(self, precision="fp64"):
+        """Run the autotuner (element-pass block size, assembly grid) on this batch."""
+        _lib.call("snp_batch_tune", self.handle, {"fp64": 0, "mixed": 1}[precision])
+        return self.info()
+
+    def info(self):
+        inf = _lib.BatchInfo()
+        _lib.call("snp_batch_get_info", self.handle, ctypes.byref(inf))
+        return inf.as_dict()
+
+    def solve(self, rtol=1e-8, precision="fp64", x0s=None, res_refs=None, raise_on_failure=True):
+        """Zero-start (or ``x0s``) residual-mode Newton of every instance at once; answers in each
+        instance's ``x``; returns per-instance stats dicts."""
+        t = torch()
+        k = len(self.instances)
+        for i, ins in enumerate(self.instances):
+            if x0s is not None and x0s[i] is not None:
+                ins.x.copy_(x0s[i])
+            else:
+                ins.x.zero_()
+        t.cuda.synchronize()
+        xs = (ctypes.c_void_p * k)(*[ins.x.data_ptr() for ins in self.instances])
+        opts = (_lib.SolveOpts * k)()
+        for i, ins in enumerate(self.instances):
+            o = ins.opts(rtol, precision)
+            if res_refs is not None:
+                o.res_ref = float(res_refs[i])
+            opts[i] = o
+        stats = (_lib.SolveStats * k)()
+        status = (ctypes.c_int32 * k)()
+        rc = _lib.load().snp_batch_solve(self.handle, xs, opts, stats, status)
+        out = []
+        for i in range(k):
+            d = stats[i].as_dict()
+            ref = res_refs[i] if (res_refs is not None and res_refs[i] > 0) else d["res0"]
+            d["rel_res"] = d["res"] / ref if ref > 0 else 0.0
+            d["status"] = int(status[i])
+            out.append(d)
+        if rc != 0 and raise_on_failure:
+            _lib.check(rc)
+        return out
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) is not None and _lib._lib is not None:
+                _lib.load().snp_batch_destroy(self.handle)
+        except Exception:
+            pass
+        self.handle = None
 
 
 def solve_one_by_one(instances, rtol=1e-8, precision="fp64"):

@@ -359,6 +359,134 @@ __global__ void k_check_affine(const double *curls, int n_orient, const double *
 //   (K x)_j = chat_j . (kfac Jm^T Jm bh),   rhs_j = chat_j . (Jm^T sum_q rq B_s,q).
 // One pass over the quadrature points; S_e and the six element terms of F and of diag(J)
 // are written once per element (no atomics; the DoF sums follow in a fixed order).
+// Element tensors of one element e of a material (the loop body of k_curlcurl_tensor): S_e into
+// T and the six F and diag(J) terms into a.Fe / a.De, all at eslot(a.t_offset + e, .).  The
+// tables sit in shared memory (s_*), wsum = sum of the weights.
+template <bool HAS_BS, int NQ, typename TT, bool DIL>
+__device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, const double *s_ctab,
+                                               const double *s_dphi, const double *s_w, const double *s_phi,
+                                               const double *s_relc, const double *s_relx, double wsum,
+                                               TT *__restrict__ T) {
+    const int nq = NQ > 0 ? NQ : a.nq;
+    const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
+    const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
+    double Jm[9], Zn[4];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) Jm[r] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const double X0 = __ldg(a.nodes + 3 * (int64_t)cidx[i]);
+        const double X1 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 1);
+        const double X2 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 2);
+        Zn[i] = X2;
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            const double d = s_dphi[3 * i + l];
+            Jm[0 + l] += X0 * d;
+            Jm[3 + l] += X1 * d;
+            Jm[6 + l] += X2 * d;
+        }
+    }
+    const double det = Jm[0] * (Jm[4] * Jm[8] - Jm[7] * Jm[5]) - Jm[1] * (Jm[3] * Jm[8] - Jm[5] * Jm[6]) +
+                       Jm[2] * (Jm[3] * Jm[7] - Jm[4] * Jm[6]);
+    const double idet = 1.0 / det;
+    const double *ct = s_ctab + __ldg(a.orient + e) * 18;
+    int g[6];
+    {
+        const int2 *gp = reinterpret_cast<const int2 *>(a.gids + 6 * e);
+        int2 g01 = __ldg(gp), g23 = __ldg(gp + 1), g45 = __ldg(gp + 2);
+        g[0] = g01.x; g[1] = g01.y; g[2] = g23.x; g[3] = g23.y; g[4] = g45.x; g[5] = g45.y;
+    }
+    // reference-frame curl of the discrete field and the element's own B
+    double bh[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const double xj = __ldg(a.x + g[j]);
+        bh[0] += ct[3 * j] * xj;
+        bh[1] += ct[3 * j + 1] * xj;
+        bh[2] += ct[3 * j + 2] * xj;
+    }
+    double cb[3];  // Jm bh = det * B_element
+#pragma unroll
+    for (int r = 0; r < 3; ++r) cb[r] = Jm[3 * r] * bh[0] + Jm[3 * r + 1] * bh[1] + Jm[3 * r + 2] * bh[2];
+    const double Bc[3] = {cb[0] * idet, cb[1] * idet, cb[2] * idet};
+
+    double kfac, M[6], Rs[3] = {0.0, 0.0, 0.0};
+    if constexpr (!HAS_BS) {
+        const double bm = sqrt(Bc[0] * Bc[0] + Bc[1] * Bc[1] + Bc[2] * Bc[2]);
+        double dnu;
+        const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, bm, dnu);
+        kfac = nu * wsum * idet;
+        const double af = (bm >= 1e-14) ? dnu * wsum * idet / bm : 0.0;
+        M[0] = af * Bc[0] * Bc[0];
+        M[1] = af * Bc[0] * Bc[1];
+        M[2] = af * Bc[0] * Bc[2];
+        M[3] = af * Bc[1] * Bc[1];
+        M[4] = af * Bc[1] * Bc[2];
+        M[5] = af * Bc[2] * Bc[2];
+    } else {
+        kfac = 0.0;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) M[t] = 0.0;
+        const double *bs = a.Bs + (int64_t)e * nq * 3;
+#pragma unroll(NQ > 0 ? NQ : 1)
+        for (int q = 0; q < nq; ++q) {
+            const double s0 = __ldg(bs + 3 * q), s1 = __ldg(bs + 3 * q + 1), s2 = __ldg(bs + 3 * q + 2);
+            const double B0 = s0 + Bc[0], B1 = s1 + Bc[1], B2 = s2 + Bc[2];
+            const double bm = sqrt(B0 * B0 + B1 * B1 + B2 * B2);
+            double dnu;
+            const double nu = nu_at<DIL>(a, s_relc, s_relx, s_phi + 4 * q, Zn, bm, dnu);
+            const double wq = s_w[q];
+            kfac += nu * wq;
+            const double aq = (bm >= 1e-14) ? dnu * wq * idet / bm : 0.0;
+            const double rq = (kNu0 - nu) * wq;
+            M[0] += aq * B0 * B0;
+            M[1] += aq * B0 * B1;
+            M[2] += aq * B0 * B2;
+            M[3] += aq * B1 * B1;
+            M[4] += aq * B1 * B2;
+            M[5] += aq * B2 * B2;
+            Rs[0] += rq * s0;
+            Rs[1] += rq * s1;
+            Rs[2] += rq * s2;
+        }
+        kfac *= idet;
+    }
+    // A = kfac I + M;  P = A Jm;  S = Jm^T P
+    const double A[9] = {kfac + M[0], M[1], M[2], M[1], kfac + M[3], M[4], M[2], M[4], kfac + M[5]};
+    double P[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) P[3 * r + c] = A[3 * r] * Jm[c] + A[3 * r + 1] * Jm[3 + c] + A[3 * r + 2] * Jm[6 + c];
+    double S[6];
+    {
+        int t = 0;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = r; c < 3; ++c) S[t++] = Jm[r] * P[c] + Jm[3 + r] * P[3 + c] + Jm[6 + r] * P[6 + c];
+    }
+    const int64_t eb = eslot(a.t_offset + e, 0);
+#pragma unroll
+    for (int t = 0; t < 6; ++t) T[eb + 32 * t] = (TT)S[t];
+    // G = kfac Jm^T (Jm bh) - Jm^T Rs;  F_j = chat_j . G
+    double G[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        G[c] = kfac * (Jm[c] * cb[0] + Jm[3 + c] * cb[1] + Jm[6 + c] * cb[2]) -
+               (Jm[c] * Rs[0] + Jm[3 + c] * Rs[1] + Jm[6 + c] * Rs[2]);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const double h0 = ct[3 * j], h1 = ct[3 * j + 1], h2 = ct[3 * j + 2];
+        const double sh0 = S[0] * h0 + S[1] * h1 + S[2] * h2;
+        const double sh1 = S[1] * h0 + S[3] * h1 + S[4] * h2;
+        const double sh2 = S[2] * h0 + S[4] * h1 + S[5] * h2;
+        a.Fe[eb + 32 * j] = h0 * G[0] + h1 * G[1] + h2 * G[2];
+        a.De[eb + 32 * j] = h0 * sh0 + h1 * sh1 + h2 * sh2;
+    }
+}
+
 template <bool HAS_BS, int NQ, typename TT, bool DIL>
 __global__ void __launch_bounds__(kBlock)
     k_curlcurl_tensor(CurlArgs a, int quad_stride_ctab, TT *__restrict__ T) {
@@ -388,123 +516,65 @@ __global__ void __launch_bounds__(kBlock)
     double wsum = 0.0;
     for (int q = 0; q < nq; ++q) wsum += s_w[q];
 
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x) {
-        const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
-        const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
-        double Jm[9], Zn[4];
-#pragma unroll
-        for (int r = 0; r < 9; ++r) Jm[r] = 0.0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const double X0 = __ldg(a.nodes + 3 * (int64_t)cidx[i]);
-            const double X1 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 1);
-            const double X2 = __ldg(a.nodes + 3 * (int64_t)cidx[i] + 2);
-            Zn[i] = X2;
-#pragma unroll
-            for (int l = 0; l < 3; ++l) {
-                const double d = s_dphi[3 * i + l];
-                Jm[0 + l] += X0 * d;
-                Jm[3 + l] += X1 * d;
-                Jm[6 + l] += X2 * d;
-            }
-        }
-        const double det = Jm[0] * (Jm[4] * Jm[8] - Jm[7] * Jm[5]) - Jm[1] * (Jm[3] * Jm[8] - Jm[5] * Jm[6]) +
-                           Jm[2] * (Jm[3] * Jm[7] - Jm[4] * Jm[6]);
-        const double idet = 1.0 / det;
-        const double *ct = s_ctab + __ldg(a.orient + e) * 18;
-        int g[6];
-        {
-            const int2 *gp = reinterpret_cast<const int2 *>(a.gids + 6 * e);
-            int2 g01 = __ldg(gp), g23 = __ldg(gp + 1), g45 = __ldg(gp + 2);
-            g[0] = g01.x; g[1] = g01.y; g[2] = g23.x; g[3] = g23.y; g[4] = g45.x; g[5] = g45.y;
-        }
-        // reference-frame curl of the discrete field and the element's own B
-        double bh[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            const double xj = __ldg(a.x + g[j]);
-            bh[0] += ct[3 * j] * xj;
-            bh[1] += ct[3 * j + 1] * xj;
-            bh[2] += ct[3 * j + 2] * xj;
-        }
-        double cb[3];  // Jm bh = det * B_element
-#pragma unroll
-        for (int r = 0; r < 3; ++r) cb[r] = Jm[3 * r] * bh[0] + Jm[3 * r + 1] * bh[1] + Jm[3 * r + 2] * bh[2];
-        const double Bc[3] = {cb[0] * idet, cb[1] * idet, cb[2] * idet};
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x)
+        tensor_element<HAS_BS, NQ, TT, DIL>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, T);
+}
 
-        double kfac, M[6], Rs[3] = {0.0, 0.0, 0.0};
-        if constexpr (!HAS_BS) {
-            const double bm = sqrt(Bc[0] * Bc[0] + Bc[1] * Bc[1] + Bc[2] * Bc[2]);
-            double dnu;
-            const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, bm, dnu);
-            kfac = nu * wsum * idet;
-            const double af = (bm >= 1e-14) ? dnu * wsum * idet / bm : 0.0;
-            M[0] = af * Bc[0] * Bc[0];
-            M[1] = af * Bc[0] * Bc[1];
-            M[2] = af * Bc[0] * Bc[2];
-            M[3] = af * Bc[1] * Bc[1];
-            M[4] = af * Bc[1] * Bc[2];
-            M[5] = af * Bc[2] * Bc[2];
-        } else {
-            kfac = 0.0;
-#pragma unroll
-            for (int t = 0; t < 6; ++t) M[t] = 0.0;
-            const double *bs = a.Bs + (int64_t)e * nq * 3;
-#pragma unroll(NQ > 0 ? NQ : 1)
-            for (int q = 0; q < nq; ++q) {
-                const double s0 = __ldg(bs + 3 * q), s1 = __ldg(bs + 3 * q + 1), s2 = __ldg(bs + 3 * q + 2);
-                const double B0 = s0 + Bc[0], B1 = s1 + Bc[1], B2 = s2 + Bc[2];
-                const double bm = sqrt(B0 * B0 + B1 * B1 + B2 * B2);
-                double dnu;
-                const double nu = nu_at<DIL>(a, s_relc, s_relx, s_phi + 4 * q, Zn, bm, dnu);
-                const double wq = s_w[q];
-                kfac += nu * wq;
-                const double aq = (bm >= 1e-14) ? dnu * wq * idet / bm : 0.0;
-                const double rq = (kNu0 - nu) * wq;
-                M[0] += aq * B0 * B0;
-                M[1] += aq * B0 * B1;
-                M[2] += aq * B0 * B2;
-                M[3] += aq * B1 * B1;
-                M[4] += aq * B1 * B2;
-                M[5] += aq * B2 * B2;
-                Rs[0] += rq * s0;
-                Rs[1] += rq * s1;
-                Rs[2] += rq * s2;
-            }
-            kfac *= idet;
+// Batched element tensors: a grid of resident blocks walks the work items (runs of one
+// segment's elements) of all problems; a block stages a segment's reluctance tables (and its
+// nodal basis, diluted steel) in shared memory when its item changes segment.  Element e of an
+// item is computed exactly as k_curlcurl_tensor computes it for the segment alone.
+template <int NQ, typename TT>
+__global__ void __launch_bounds__(kBlock)
+    k_curlcurl_tensor_batch(const BatchSeg *__restrict__ segs, const BatchAsmItem *__restrict__ items, int n_items,
+                            int max_n_int, const double *__restrict__ ctab, int n_orient, int quad_stride_ctab,
+                            const double *__restrict__ dphi0, const double *__restrict__ w, int nq_rt,
+                            const double *__restrict__ x, const int32_t *__restrict__ run, int run_stride,
+                            TT *__restrict__ T, double *__restrict__ Fe, double *__restrict__ De) {
+    extern __shared__ double sm[];
+    const SmemLayout L = smem_layout(n_orient, nq_rt, max_n_int);
+    double *s_ctab = sm + L.off_ctab;
+    double *s_dphi = sm + L.off_dphi;
+    double *s_w = sm + L.off_w;
+    double *s_phi = sm + L.off_phi;
+    double *s_relc = sm + L.off_relc;
+    double *s_relx = sm + L.off_relx;
+    for (int t = threadIdx.x; t < n_orient * 18; t += blockDim.x) {
+        int o = t / 18, r = t - o * 18;
+        s_ctab[t] = ctab[(int64_t)o * quad_stride_ctab + r];
+    }
+    for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = dphi0[t];
+    for (int t = threadIdx.x; t < nq_rt; t += blockDim.x) s_w[t] = w[t];
+    __syncthreads();
+    const int nq = NQ > 0 ? NQ : nq_rt;
+    double wsum = 0.0;
+    for (int q = 0; q < nq; ++q) wsum += s_w[q];
+    int cur = -1;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const BatchAsmItem item = items[it];
+        if (!run[(int64_t)item.inst * run_stride]) continue;  // uniform across the block
+        CurlArgs a = segs[item.seg].a;
+        if (item.seg != cur) {
+            __syncthreads();
+            const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
+            const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
+            for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
+            for (int t = threadIdx.x; t < nx; t += blockDim.x) s_relx[t] = (a.n_int < 0) ? 0.0 : a.rel_x[t];
+            if (a.phi)
+                for (int t = threadIdx.x; t < 4 * nq; t += blockDim.x) s_phi[t] = a.phi[t];
+            __syncthreads();
+            cur = item.seg;
         }
-        // A = kfac I + M;  P = A Jm;  S = Jm^T P
-        const double A[9] = {kfac + M[0], M[1], M[2], M[1], kfac + M[3], M[4], M[2], M[4], kfac + M[5]};
-        double P[9];
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) P[3 * r + c] = A[3 * r] * Jm[c] + A[3 * r + 1] * Jm[3 + c] + A[3 * r + 2] * Jm[6 + c];
-        double S[6];
-        {
-            int t = 0;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = r; c < 3; ++c) S[t++] = Jm[r] * P[c] + Jm[3 + r] * P[3 + c] + Jm[6 + r] * P[6 + c];
-        }
-        const int64_t eb = eslot(a.t_offset + e, 0);
-#pragma unroll
-        for (int t = 0; t < 6; ++t) T[eb + 32 * t] = (TT)S[t];
-        // G = kfac Jm^T (Jm bh) - Jm^T Rs;  F_j = chat_j . G
-        double G[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-            G[c] = kfac * (Jm[c] * cb[0] + Jm[3 + c] * cb[1] + Jm[6 + c] * cb[2]) -
-                   (Jm[c] * Rs[0] + Jm[3 + c] * Rs[1] + Jm[6 + c] * Rs[2]);
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            const double h0 = ct[3 * j], h1 = ct[3 * j + 1], h2 = ct[3 * j + 2];
-            const double sh0 = S[0] * h0 + S[1] * h1 + S[2] * h2;
-            const double sh1 = S[1] * h0 + S[3] * h1 + S[4] * h2;
-            const double sh2 = S[2] * h0 + S[4] * h1 + S[5] * h2;
-            a.Fe[eb + 32 * j] = h0 * G[0] + h1 * G[1] + h2 * G[2];
-            a.De[eb + 32 * j] = h0 * sh0 + h1 * sh1 + h2 * sh2;
+        a.x = x + segs[item.seg].dof_off;
+        a.Fe = Fe;
+        a.De = De;
+        for (int64_t e = item.e0 + threadIdx.x; e < item.e1; e += blockDim.x) {
+            if (a.Bs == nullptr)
+                tensor_element<false, NQ, TT, false>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, T);
+            else if (a.phi)
+                tensor_element<true, NQ, TT, true>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, T);
+            else
+                tensor_element<true, NQ, TT, false>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, T);
         }
     }
 }
@@ -592,6 +662,43 @@ int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st) {
     const int qstride = a.nq * 18;
     if (a.T64) return launch_tensor<double>(a, a.T64, st, smem, qstride);
     return launch_tensor<float>(a, a.T32, st, smem, qstride);
+}
+
+template <int NQ, typename TT>
+static int launch_batch_t(const BatchSeg *segs, const BatchAsmItem *items, int n_items, int max_n_int,
+                          const double *ctab, int n_orient, int qstride, const double *dphi0, const double *w, int nq,
+                          const double *x, const int32_t *run, int run_stride, TT *T, double *Fe, double *De, int grid,
+                          size_t smem, cudaStream_t st) {
+    auto kern = k_curlcurl_tensor_batch<NQ, TT>;
+    if (smem > 48 * 1024) SNP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (grid <= 0) grid = wave_grid(kern, (int64_t)n_items * kBlock, kBlock, smem);
+    kern<<<grid, kBlock, smem, st>>>(segs, items, n_items, max_n_int, ctab, n_orient, qstride, dphi0, w, nq, x, run,
+                                     run_stride, T, Fe, De);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int launch_curlcurl_tensor_batch(const BatchSeg *segs, const BatchAsmItem *items, int n_items, int max_n_int,
+                                 const double *ctab, int n_orient, int quad_stride_ctab, const double *dphi0,
+                                 const double *w, int nq, const double *x, const int32_t *run, int run_stride, void *T,
+                                 bool f32, double *Fe, double *De, int grid, cudaStream_t st) {
+    static_assert(kBatchAsmBlock == kBlock, "batched assembly block size");
+    if (n_items == 0) return SNP_OK;
+    const SmemLayout L = smem_layout(n_orient, nq, max_n_int);
+    const size_t smem = sizeof(double) * (size_t)L.total;
+    SNP_REQUIRE(smem <= 200 * 1024, "batched assembly: tables need %zu bytes of shared memory", smem);
+    if (f32) {
+        if (nq == 4)
+            return launch_batch_t<4, float>(segs, items, n_items, max_n_int, ctab, n_orient, quad_stride_ctab, dphi0,
+                                            w, nq, x, run, run_stride, static_cast<float *>(T), Fe, De, grid, smem, st);
+        return launch_batch_t<0, float>(segs, items, n_items, max_n_int, ctab, n_orient, quad_stride_ctab, dphi0, w,
+                                        nq, x, run, run_stride, static_cast<float *>(T), Fe, De, grid, smem, st);
+    }
+    if (nq == 4)
+        return launch_batch_t<4, double>(segs, items, n_items, max_n_int, ctab, n_orient, quad_stride_ctab, dphi0, w,
+                                         nq, x, run, run_stride, static_cast<double *>(T), Fe, De, grid, smem, st);
+    return launch_batch_t<0, double>(segs, items, n_items, max_n_int, ctab, n_orient, quad_stride_ctab, dphi0, w, nq,
+                                     x, run, run_stride, static_cast<double *>(T), Fe, De, grid, smem, st);
 }
 
 static int fill_args(CurlArgs &a, const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,

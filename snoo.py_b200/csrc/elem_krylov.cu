@@ -24,6 +24,7 @@
 #include <cub/cub.cuh>
 
 #include "snp_common.cuh"
+#include "snp_elem.cuh"
 #include "snp_internal.cuh"
 #include "snp_krylov.cuh"
 #include "snp_reduce.cuh"
@@ -33,15 +34,10 @@ namespace snp {
 namespace {
 
 constexpr int kEBlock = 256;
-constexpr uint32_t kSignBit = 0x80000000u;
 #ifndef SNP_PASS1_MIN_BLOCKS
 #define SNP_PASS1_MIN_BLOCKS 4
 #endif
 constexpr int kPass1MinBlocks = SNP_PASS1_MIN_BLOCKS;  // resident blocks per SM the element pass asks for
-
-// p = z + beta p_old, rounded the same way wherever it is formed
-__device__ __forceinline__ double pnext(double beta, double p_old, double z) { return __fma_rn(beta, p_old, z); }
-__device__ __forceinline__ float pnext(float beta, float p_old, float z) { return __fmaf_rn(beta, p_old, z); }
 
 // ---------------------------------------------------------------- topology build
 
@@ -105,17 +101,6 @@ __global__ void k_inc_pos(int64_t m, int64_t ne, const int32_t *__restrict__ inc
         const uint32_t u = (uint32_t)inc[t] & ~kSignBit;
         pos[eslot(u >> 3, (int)(u & 7u))] = (int32_t)t;
     }
-}
-
-// Edge term s chat_k . v of one element edge, rounded the same way wherever it is formed.
-template <typename TT>
-__device__ __forceinline__ TT edge_term(const TT *sc, int k, bool neg, TT v0, TT v1, TT v2) {
-    TT c;
-    if constexpr (sizeof(TT) == 8)
-        c = __fma_rn(sc[3 * k + 2], v2, __fma_rn(sc[3 * k + 1], v1, __dmul_rn(sc[3 * k], v0)));
-    else
-        c = __fmaf_rn(sc[3 * k + 2], v2, __fmaf_rn(sc[3 * k + 1], v1, __fmul_rn(sc[3 * k], v0)));
-    return neg ? -c : c;
 }
 
 // ---------------------------------------------------------------- PCG kernels
@@ -539,8 +524,7 @@ __global__ void k_rsys_rhs_sum(int n_parts, int m, const double *__restrict__ pa
 // PCG's DoF pass stages r of a kBjTile-DoF tile in shared memory so that each DoF forms
 // z_i = sum_j M_ij r_j over its block.
 
-constexpr int kBjMax = 8;
-constexpr int kBjTile = kEBlock;
+static_assert(kBjTile == kEBlock, "the DoF pass stages one block-Jacobi tile per block");
 
 template <typename TT>
 __global__ void __launch_bounds__(kEBlock)
@@ -554,153 +538,21 @@ __global__ void __launch_bounds__(kEBlock)
         double row[kBjMax];
 #pragma unroll
         for (int c = 0; c < kBjMax; ++c) row[c] = 0.0;
-        if (is_free(free_mask, i)) {
-            const unsigned mt = meta[i];
-            const int64_t b0 = i - (int64_t)(mt & 0xffu);
-            const int size = (int)(mt >> 8);
-            for (int t = inc_ptr[i]; t < inc_ptr[i + 1]; ++t) {
-                const uint32_t u = (uint32_t)inc[t];
-                const uint32_t ek = u & ~kSignBit;
-                const int k = (int)(ek & 7u);
-                const int64_t eb = eslot((int64_t)(ek >> 3), 0);
-                double tt[6];
-#pragma unroll
-                for (int c = 0; c < 6; ++c) tt[c] = (double)T[eb + 32 * c];
-                const double c0 = sc[3 * k], c1 = sc[3 * k + 1], c2 = sc[3 * k + 2];
-                const double v0 = tt[0] * c0 + tt[1] * c1 + tt[2] * c2;
-                const double v1 = tt[1] * c0 + tt[3] * c1 + tt[4] * c2;
-                const double v2 = tt[2] * c0 + tt[4] * c1 + tt[5] * c2;
-#pragma unroll
-                for (int k2 = 0; k2 < 6; ++k2) {
-                    const uint32_t d2 = (uint32_t)edof[eb + 32 * k2];
-                    const int64_t r = (int64_t)(d2 & ~kSignBit) - b0;
-                    if (r < 0 || r >= size) continue;
-                    double val = sc[3 * k2] * v0 + sc[3 * k2 + 1] * v1 + sc[3 * k2 + 2] * v2;
-                    if ((u ^ d2) & kSignBit) val = -val;
-#pragma unroll
-                    for (int c = 0; c < kBjMax; ++c)
-                        if (c == r) row[c] += val;
-                }
-            }
-        }
+        if (is_free(free_mask, i)) bj_entries_row(i, inc_ptr, inc, edof, T, sc, (unsigned)meta[i], row);
 #pragma unroll
         for (int c = 0; c < kBjMax; ++c) bmat[i * kBjMax + c] = row[c];
     }
 }
 
-// one thread per block: Cholesky of the block (upper triangle of its rows), padded to 8 x 8 with
-// the identity so that every loop unrolls with fixed indices (registers, no local arrays); the
-// lower triangle of the inverse is written to both sides (symmetric by construction), rounded
-// to float32.  Point Jacobi for a block whose pivot is not positive enough.
+// one thread per block: the block's inverse (bj_invert_block)
 __global__ void __launch_bounds__(128)
     k_bj_invert(int32_t n, const uint8_t *__restrict__ free_mask, const uint16_t *__restrict__ meta,
                 const double *__restrict__ bmat, float *__restrict__ binv, int *n_fallback) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const unsigned mt = meta[i];
         if (mt & 0xffu) continue;
-        const int size = (int)(mt >> 8);
-        const bool fr = is_free(free_mask, i);
-        double L[kBjMax][kBjMax], d0[kBjMax], rl[kBjMax];
-#pragma unroll
-        for (int r = 0; r < kBjMax; ++r) {
-#pragma unroll
-            for (int c = 0; c < kBjMax; ++c) {
-                double v = r == c ? 1.0 : 0.0;
-                if (r < size && c < size) v = c >= r ? bmat[(i + r) * kBjMax + c] : bmat[(i + c) * kBjMax + r];
-                L[r][c] = v;
-            }
-            d0[r] = L[r][r];
-        }
-        bool ok = fr;
-#pragma unroll
-        for (int j = 0; j < kBjMax; ++j) {
-            double p = L[j][j];
-#pragma unroll
-            for (int k = 0; k < j; ++k) p -= L[j][k] * L[j][k];
-            if (!(p > 1e-12 * d0[j]) || !isfinite(p)) {
-                ok = false;
-                p = 1.0;
-            }
-            const double ljj = sqrt(p);
-            L[j][j] = ljj;
-            rl[j] = 1.0 / ljj;
-#pragma unroll
-            for (int r = j + 1; r < kBjMax; ++r) {
-                double t = L[r][j];
-#pragma unroll
-                for (int k = 0; k < j; ++k) t -= L[r][k] * L[j][k];
-                L[r][j] = t * rl[j];
-            }
-        }
-        if (ok) {
-#pragma unroll
-            for (int c = 0; c < kBjMax; ++c) {
-                double y[kBjMax], x[kBjMax];
-#pragma unroll
-                for (int r = 0; r < kBjMax; ++r) {
-                    double t = r == c ? 1.0 : 0.0;
-#pragma unroll
-                    for (int k = 0; k < r; ++k) t -= L[r][k] * y[k];
-                    y[r] = t * rl[r];
-                }
-#pragma unroll
-                for (int r = kBjMax - 1; r >= 0; --r) {
-                    double t = y[r];
-#pragma unroll
-                    for (int k = r + 1; k < kBjMax; ++k) t -= L[k][r] * x[k];
-                    x[r] = t * rl[r];
-                }
-#pragma unroll
-                for (int r = 0; r < kBjMax; ++r) {
-                    if (r >= c && r < size && c < size) {
-                        const float v = (float)x[r];
-                        binv[(i + r) * kBjMax + c] = v;
-                        binv[(i + c) * kBjMax + r] = v;
-                    }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < kBjMax; ++r)
-#pragma unroll
-                for (int c = 0; c < kBjMax; ++c)
-                    if (r < size && c >= size) binv[(i + r) * kBjMax + c] = 0.0f;
-        } else {
-            if (fr) atomicAdd(n_fallback, 1);
-#pragma unroll
-            for (int r = 0; r < kBjMax; ++r) {
-                if (r >= size) continue;
-                const bool f = is_free(free_mask, i + r);
-#pragma unroll
-                for (int c = 0; c < kBjMax; ++c)
-                    binv[(i + r) * kBjMax + c] = (c == r && f && d0[r] > 0.0) ? (float)(1.0 / d0[r]) : 0.0f;
-            }
-        }
+        bj_invert_block(i, (int)(mt >> 8), is_free(free_mask, i), free_mask, bmat, binv, n_fallback);
     }
-}
-
-// z_i = sum over DoF i's block of M_ij r_j, r of the tile in shared memory (t = DoF - tile base);
-// a, b: DoF i's row of the block inverse, loaded before the tile's barrier
-template <typename TT>
-__device__ __forceinline__ TT bj_row(unsigned mt, float4 a, float4 b, const TT *s_r, int t) {
-    const float m[kBjMax] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-    const int size = (int)(mt >> 8);
-    const TT *rb = s_r + (t - (int)(mt & 0xffu));
-    TT z = TT(0);
-#pragma unroll
-    for (int c = 0; c < kBjMax; ++c)
-        if (c < size) z = fma((TT)m[c], rb[c], z);
-    return z;
-}
-
-// asks L1 for DoF i's block row ahead of the tile barrier, holding no registers
-__device__ __forceinline__ void bj_prefetch(const float *__restrict__ binv, int64_t i) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(binv + i * kBjMax));
-}
-
-__device__ __forceinline__ void bj_load(const float *__restrict__ binv, int64_t i, float4 &a, float4 &b) {
-    const float4 *p = reinterpret_cast<const float4 *>(binv + i * kBjMax);
-    a = __ldg(p);
-    b = __ldg(p + 1);
 }
 
 template <typename TT>

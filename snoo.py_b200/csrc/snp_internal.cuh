@@ -123,6 +123,30 @@ struct CurlArgs {
 // Launch the fused assembly for one material.  Tables must be affine (checked by the caller).
 int launch_curlcurl(const CurlArgs &a, cudaStream_t st);
 
+// Batched element-tensor assembly (several problems in one launch).  A segment is one
+// material of one problem: its CurlArgs (mesh arrays, source field, reluctance tables,
+// dilution; t_offset = the segment's first element in the concatenated element numbering;
+// x, T, Fe and De are given per launch), the problem's index and its first DoF in the
+// concatenated vectors.  Work items are runs of at most kBatchAsmItem elements of one segment.
+struct BatchSeg {
+    CurlArgs a;
+    int32_t inst;
+    int32_t dof_off;
+};
+struct BatchAsmItem {
+    int32_t seg, inst;
+    int64_t e0, e1;  // elements [e0, e1) of the segment
+};
+constexpr int64_t kBatchAsmItem = 2048;
+constexpr int kBatchAsmBlock = 128;
+// Tables (ctab [n_orient][nq][6][3] read at q = 0, dphi at q = 0, w) are the same for every
+// segment.  Items whose problem has run[inst * run_stride] == 0 are skipped.  x: concatenated
+// DoF vector; T: float64 (f32 false) or float32 element tensors of the concatenated elements.
+int launch_curlcurl_tensor_batch(const BatchSeg *segs, const BatchAsmItem *items, int n_items, int max_n_int,
+                                 const double *ctab, int n_orient, int quad_stride_ctab, const double *dphi0,
+                                 const double *w, int nq, const double *x, const int32_t *run, int run_stride, void *T,
+                                 bool f32, double *Fe, double *De, int grid, cudaStream_t st);
+
 // Element tensors of the Newton Jacobian for one material: S_e = Jm^T (kfac I + M) Jm with
 // J_e,jk = chat_j . S_e chat_k (chat_j: reference curls of the element's orientation), plus
 // the element terms of diag(J) and of F = K(x) x - rhs(x).  Tables must be affine.

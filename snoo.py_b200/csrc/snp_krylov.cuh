@@ -157,6 +157,28 @@ int block_jacobi_apply(int32_t n, const uint8_t *free_mask, const uint16_t *meta
 int basis_axpy(int32_t n, const uint8_t *free_mask, const float *V, int m, int64_t ldv, const double *coef,
                double *x, cudaStream_t s);
 
+// Read-only view of a finalized Newton solver's device data, for the batched solver.
+struct SolverMaterialView {
+    int64_t offset, count;
+    const int32_t *cells, *gids, *orient;
+    const double *Bs;  // [count][nq][3] or NULL
+    int32_t n_int;
+    const double *relc, *relx;
+    const double *phi;  // nodal basis at the quadrature points when diluted, else NULL
+    double dil[4];
+};
+struct SolverView {
+    int32_t n;
+    int64_t n_free, n_nodes, n_elems;
+    int32_t nq, n_orient;
+    const double *nodes, *curls, *dphi, *w, *rhs_extra;
+    const uint8_t *free_mask;
+    const ElemTopology *etop;  // NULL unless the Newton Jacobian is matrix-free
+    const uint16_t *bj_meta;   // NULL unless block Jacobi is set
+    int n_mats;
+    const SolverMaterialView *mats;
+};
+
 template <typename TT>
 struct alignas(2 * sizeof(TT)) DofPair {
     TT a, b;
@@ -208,5 +230,9 @@ struct ElemPcg {
     int build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
                     const float *bj_inv);
 };
+
+// The view of a finalized solver (SNP_BAD_ARG when it is not finalized).  Valid while the
+// solver lives and no material is added.
+int solver_view(const snp_solver *s, SolverView *v);
 
 }  // namespace snp

@@ -285,6 +285,7 @@ struct snp_solver {
     snp::Pcg<float, float> pcg32;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int64_t launches = 0;  // kernels of this library launched by the current solve
+    mutable std::vector<snp::SolverMaterialView> views;  // solver_view's material list
 
     ~snp_solver() {
         if (pat) snp_pattern_destroy(pat);
@@ -711,6 +712,47 @@ struct snp_solver {
         return status == SNP_OK ? SNP_OK : snp::fail(status, "Newton did not reach the tolerance in %d steps", o.max_newton);
     }
 };
+
+namespace snp {
+
+int solver_view(const snp_solver *s, SolverView *v) {
+    SNP_REQUIRE(s != nullptr && s->finalized, "solver missing or not finalized");
+    v->n = s->n;
+    v->n_free = s->n_free;
+    v->n_nodes = s->n_nodes;
+    v->n_elems = s->n_elems_total();
+    v->nq = s->nq;
+    v->n_orient = s->n_orient;
+    v->nodes = s->nodes.p;
+    v->curls = s->curls.p;
+    v->dphi = s->dphi.p;
+    v->w = s->w.p;
+    v->rhs_extra = s->has_extra ? s->rhs_extra.p : nullptr;
+    v->free_mask = s->free_mask.p;
+    v->etop = s->layout == SNP_LAYOUT_ELEM ? &s->etop : nullptr;
+    v->bj_meta = s->bj_on ? s->bj_meta.p : nullptr;
+    s->views.clear();
+    for (auto &m : s->mats) {
+        SolverMaterialView mv{};
+        mv.offset = m->offset;
+        mv.count = m->count;
+        mv.cells = m->cells.p;
+        mv.gids = m->gids.p;
+        mv.orient = m->orient.p;
+        mv.Bs = m->has_bs ? m->Bs.p : nullptr;
+        mv.n_int = m->n_int;
+        mv.relc = m->relc.p;
+        mv.relx = m->relx.p;
+        mv.phi = (m->diluted && m->has_bs) ? m->phi.p : nullptr;
+        for (int k = 0; k < 4; ++k) mv.dil[k] = m->dil[k];
+        s->views.push_back(mv);
+    }
+    v->n_mats = (int)s->views.size();
+    v->mats = s->views.data();
+    return SNP_OK;
+}
+
+}  // namespace snp
 
 extern "C" {
 
