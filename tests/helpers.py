@@ -108,3 +108,70 @@ def rel_max(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+NU0 = 0.25 / np.pi * 1e7
+
+
+def oracle_total_rhs(oracle_mod, msh, Phi, tag=None):
+    """rhs of the total-potential formulation from the coil's electric potential: the oracle's
+    Laplace solve (``laplace_subdomain_solver.py:117-158``) and a numpy statement of
+    ``compute_rhs_electric_potential`` (``curl_curl_assembler.py:1154-1284``)."""
+    from snoopy_b200 import finite_element as FE
+    from snoopy_b200 import mesh as M
+
+    tag = M.TAG_COIL_1 if tag is None else tag
+    w, q = FE.quadrature_rule(2)
+    dphi = FE.evaluate_basis_derivative(q)
+    t1, t2 = msh.coil_terminals[tag]
+    el = msh.domain_elements(tag)
+    phi = oracle_mod.laplace_subdomain_solve(msh.nodes, msh.cells[el], np.concatenate([t1, t2]),
+                                             msh.domain_nodes_mask(tag), Phi, t1, t2, w, q, dphi)
+    X = msh.nodes[msh.cells[el]]
+    Jm = np.einsum("eid,il->edl", X, dphi[0])
+    Ji = np.linalg.inv(Jm)
+    det = np.linalg.det(Jm)
+    G = np.einsum("eld,el->ed", Ji, np.einsum("il,ei->el", dphi[0], phi[msh.cells[el]]))
+    s = FE.orientation_signs(msh.orientations[el])
+    wq = np.einsum("eld,qjl->eqjd", Ji, FE.edge_basis_functions(q)) * s[:, None, :, None]
+    rhs = np.zeros(msh.num_dofs)
+    np.add.at(rhs, msh.elem_edges[el].reshape(-1), np.einsum("eqjd,ed,q,e->ej", wq, G, w, det).reshape(-1))
+    return rhs
+
+
+def oracle_relative_residual(oracle_mod, ins, x):
+    """||F_free(x)|| / ||F_free(0)|| of a batched-family instance (``snoopy_b200.batch.Instance``)
+    by the oracle on the reference's C kernels: its Biot-Savart source (reduced variants) or its
+    electric-potential rhs (total-potential variants), its materials, its Dirichlet mask."""
+    import snoopy_b200 as S
+    from snoopy_b200 import mesh as M
+
+    msh = ins.mesh
+    tb = ins.solver.curl_curl_factory.tables(2)
+    mats_list = ins.solver.curl_curl_factory.material_list
+    if ins.v["kind"] == "reduced":
+        iron = msh.domain_elements(M.TAG_IRON)
+        air = msh.domain_elements(M.TAG_AIR)
+        P = np.einsum("qi,eid->eqd", tb.phi.reshape(tb.nq, 4), msh.nodes[msh.cells[iron]]).reshape(-1, 3)
+        Bs = sum(oracle_mod.compute_B_line_segs_cpp(c.get_segments(), P, c.current, c.rad, backend="ref")
+                 for c in ins.solver.coil_list)
+        mats = [dict(cells=msh.cells[iron], glob_ids=msh.elem_edges[iron], orientations=msh.orientations[iron],
+                     reluctance=mats_list[0]),
+                dict(cells=msh.cells[air], glob_ids=msh.elem_edges[air], orientations=msh.orientations[air],
+                     reluctance=S.ConstantReluctance(NU0))]
+        sf, extra = [Bs, np.zeros((0, 3))], 0.0
+    else:
+        mats = []
+        for tag in (M.TAG_COIL_1, M.TAG_IRON, M.TAG_AIR):
+            e = msh.domain_elements(tag)
+            mats.append(dict(cells=msh.cells[e], glob_ids=msh.elem_edges[e], orientations=msh.orientations[e],
+                             reluctance=mats_list[1] if tag == M.TAG_IRON else S.ConstantReluctance(NU0)))
+        sf, extra = (), oracle_total_rhs(oracle_mod, msh, ins.phi)
+    O = oracle_mod.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, tb.w, tb.q, tb.d_phi, tb.curls,
+                                           backend="ref")
+    mask = ins.solver.make_boundary_mask()
+    _, _, r0 = O.compute_stiffness_and_jacobi_matrix_c(np.zeros(msh.num_dofs), sf)
+    K, _, r = O.compute_stiffness_and_jacobi_matrix_c(x, sf)
+    F0 = -(r0 + extra)
+    F = K @ x - (r + extra)
+    return float(np.linalg.norm(F[mask]) / np.linalg.norm(F0[mask]))

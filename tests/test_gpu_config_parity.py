@@ -20,8 +20,7 @@ import numpy as np
 import pytest
 
 import snoopy_b200 as S
-from helpers import assert_csr_close, rel_max
-from snoopy_b200 import finite_element as FE
+from helpers import assert_csr_close, oracle_relative_residual, rel_max
 from snoopy_b200 import mesh as M
 
 pytestmark = pytest.mark.gpu
@@ -99,28 +98,6 @@ def test_c2_assembly_matches_reference_kernels(oracle_mod):
     assert Kr.nnz > 2e7  # the ~1.2M-tet system (about 22.5M stored entries)
 
 
-def _oracle_total_rhs(oracle_mod, msh, Phi, tag=M.TAG_COIL_1):
-    """rhs of the total-potential formulation from the coil's electric potential: the oracle's
-    Laplace solve (``laplace_subdomain_solver.py:117-158``) and a numpy statement of
-    ``compute_rhs_electric_potential`` (``curl_curl_assembler.py:1154-1284``)."""
-    w, q = FE.quadrature_rule(2)
-    dphi = FE.evaluate_basis_derivative(q)
-    t1, t2 = msh.coil_terminals[tag]
-    el = msh.domain_elements(tag)
-    phi = oracle_mod.laplace_subdomain_solve(msh.nodes, msh.cells[el], np.concatenate([t1, t2]),
-                                             msh.domain_nodes_mask(tag), Phi, t1, t2, w, q, dphi)
-    X = msh.nodes[msh.cells[el]]
-    Jm = np.einsum("eid,il->edl", X, dphi[0])
-    Ji = np.linalg.inv(Jm)
-    det = np.linalg.det(Jm)
-    G = np.einsum("eld,el->ed", Ji, np.einsum("il,ei->el", dphi[0], phi[msh.cells[el]]))
-    s = FE.orientation_signs(msh.orientations[el])
-    wq = np.einsum("eld,qjl->eqjd", Ji, FE.edge_basis_functions(q)) * s[:, None, :, None]
-    rhs = np.zeros(msh.num_dofs)
-    np.add.at(rhs, msh.elem_edges[el].reshape(-1), np.einsum("eqjd,ed,q,e->ej", wq, G, w, det).reshape(-1))
-    return rhs
-
-
 def test_batched_instances_match_oracle_residual(oracle_mod):
     """A reduced-potential and a total-potential variant solved together by snp_solver_solve_many:
     the oracle (reference kernels) finds each device solution at the 1e-8 relative residual."""
@@ -134,37 +111,4 @@ def test_batched_instances_match_oracle_residual(oracle_mod):
     assert {i.v["kind"] for i in inst} == {"reduced", "total"}
     for ins, s in zip(inst, st):
         assert s["status"] == 0 and s["rel_res"] <= 1e-8, s
-        msh = ins.mesh
-        tb = ins.solver.curl_curl_factory.tables(2)
-        rel = ins.solver.curl_curl_factory.material_list[0] if ins.v["kind"] == "reduced" else None
-        x = ins.x.cpu().numpy()
-        if ins.v["kind"] == "reduced":
-            iron = msh.domain_elements(M.TAG_IRON)
-            air = msh.domain_elements(M.TAG_AIR)
-            P = np.einsum("qi,eid->eqd", tb.phi.reshape(tb.nq, 4), msh.nodes[msh.cells[iron]]).reshape(-1, 3)
-            Bs = sum(oracle_mod.compute_B_line_segs_cpp(c.get_segments(), P, c.current, c.rad, backend="ref")
-                     for c in ins.solver.coil_list)
-            mats = [dict(cells=msh.cells[iron], glob_ids=msh.elem_edges[iron], orientations=msh.orientations[iron],
-                         reluctance=rel),
-                    dict(cells=msh.cells[air], glob_ids=msh.elem_edges[air], orientations=msh.orientations[air],
-                         reluctance=S.ConstantReluctance(NU0))]
-            O = oracle_mod.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, tb.w, tb.q, tb.d_phi, tb.curls,
-                                                   backend="ref")
-            sf, extra = [Bs, np.zeros((0, 3))], 0.0
-        else:
-            rel = ins.solver.curl_curl_factory.material_list[1]
-            mats = []
-            for tag in (M.TAG_COIL_1, M.TAG_IRON, M.TAG_AIR):
-                e = msh.domain_elements(tag)
-                mats.append(dict(cells=msh.cells[e], glob_ids=msh.elem_edges[e], orientations=msh.orientations[e],
-                                 reluctance=rel if tag == M.TAG_IRON else S.ConstantReluctance(NU0)))
-            O = oracle_mod.OracleCurlCurlAssembler(msh.nodes, mats, msh.num_dofs, tb.w, tb.q, tb.d_phi, tb.curls,
-                                                   backend="ref")
-            sf, extra = (), _oracle_total_rhs(oracle_mod, msh, ins.phi)
-        mask = ins.solver.make_boundary_mask()
-        K0, _, r0 = O.compute_stiffness_and_jacobi_matrix_c(np.zeros(msh.num_dofs), sf)
-        K, _, r = O.compute_stiffness_and_jacobi_matrix_c(x, sf)
-        F0 = -(r0 + extra)
-        F = K @ x - (r + extra)
-        rel_res = np.linalg.norm(F[mask]) / np.linalg.norm(F0[mask])
-        assert rel_res <= 1.5e-8, (ins.v["kind"], rel_res)
+        assert oracle_relative_residual(oracle_mod, ins, ins.x.cpu().numpy()) <= 1.5e-8
