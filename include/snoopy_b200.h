@@ -476,6 +476,14 @@ int snp_solver_destroy(snp_solver *s);
  * coefficients of the converged edge-DoF vector.  None has a counterpart in the reference
  * (snoo.py has no surrogate); BF16 arrays are passed as raw 16-bit words. */
 
+/* POD reconstruction of the warm start (the surrogate's x = mean + U c, SURVEY N8's projection
+ * GEMMs; the reference has no surrogate): out[p][i] = mean[i] + sum_c V[i][c] coef[p][c] for
+ * p < P (<= 32) vectors, V float32 [n][ldv] with m <= 128 columns, coef float64 [P][m] (device),
+ * mean float64 [n] or NULL, out float64 [P][ldo].  float64 products and sums in a fixed order.
+ * Asynchronous on the stream. */
+int snp_basis_combine(int32_t n, const float *V, int32_t m, int64_t ldv, const double *coef, int32_t P,
+                      const double *mean, double *out, int64_t ldo, void *stream);
+
 /* C[M,N] = A[M,K] . B[N,K]^T (+ bias[N]) on the tcgen05 tensor cores: A, B row-major BF16
  * with K contiguous (K and lda, ldb multiples of 8, A and B 16-byte aligned), FP32
  * accumulation.  Outputs (either may be NULL): C FP32 [M, ldc]; H BF16 [M, ldh] = act(C)

@@ -104,6 +104,7 @@ _SIGS = {
     "snp_solver_assemble_tensors": [_vp, _vp, ctypes.c_int, _vp, _vp],
     "snp_solver_set_nodes": [_vp, _vp, _vp],
     "snp_solver_solve_many": [_vp, _c_i32, _vp, _vp, _vp, _c_i32, _vp],
+    "snp_basis_combine": [_c_i32, _vp, _c_i32, _c_i64, _vp, _c_i32, _vp, _vp, _c_i64, _vp],
     "snp_batch_create": [_vp, _c_i32, _pp],
     "snp_batch_solve": [_vp, _vp, _vp, _vp, _vp],
     "snp_batch_tune": [_vp, _c_i32],

@@ -882,6 +882,51 @@ int ElemPcg<TT>::launch_iteration(const ElemTopology &top, const TT *T, const ui
     return SNP_OK;
 }
 
+// L2 residency of the slot values between the element pass (which writes them) and the DoF
+// pass (which reads them): with SNP_L2_PERSIST=1 the iteration's kernel nodes get an access
+// policy window over Y with persisting hits, and the context's persisting L2 set-aside is
+// raised to cover it (up to the device's maximum).  A per-process setting of this context.
+static void l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes) {
+    const char *env = getenv("SNP_L2_PERSIST");
+    if (!(env && env[0] == '1')) return;
+    int dev = 0, max_persist = 0, max_win = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
+        max_persist <= 0 || max_win <= 0) {
+        cudaGetLastError();
+        return;
+    }
+    const size_t win = bytes < (size_t)max_win ? bytes : (size_t)max_win;
+    const size_t keep = win < (size_t)max_persist ? win : (size_t)max_persist;
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, keep) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaKernelNodeAttrValue v = {};
+    v.accessPolicyWindow.base_ptr = const_cast<void *>(base);
+    v.accessPolicyWindow.num_bytes = win;
+    v.accessPolicyWindow.hitRatio = (float)((double)keep / (double)win);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    size_t n = 0;
+    if (cudaGraphGetNodes(body, nullptr, &n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return;
+    }
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(body, nodes.data(), &n) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+            cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &v);
+    }
+    cudaGetLastError();
+}
+
 template <typename TT>
 int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
                              const float *bj_inv) {
@@ -914,6 +959,7 @@ int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t
             cudaGraph_t out = nullptr;
             cudaError_t e = cudaStreamEndCapture(cs, &out);
             ok = (rc == SNP_OK) && e == cudaSuccess;
+            if (ok) l2_window_on_kernels(body, Y.p, sizeof(TT) * 6 * (size_t)ne);
         }
     }
     if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;

@@ -263,7 +263,61 @@ __global__ void k_f32_to_bf16(int64_t count, const float *__restrict__ a, __nv_b
 
 }  // namespace snp
 
+// out[p][i] = mean[i] + sum_c V[i][c] coef[p][c]: one warp per row i of V (lanes over the m
+// columns, the row read once for all P vectors), float64 products and a fixed shuffle tree;
+// the coefficients of all P vectors staged in shared memory.
+namespace snp {
+namespace {
+constexpr int kCombineMaxM = 128;
+constexpr int kCombineMaxP = 32;
+__global__ void __launch_bounds__(256)
+    k_basis_combine(int32_t n, const float *__restrict__ V, int m, int64_t ldv, const double *__restrict__ coef,
+                    int P, const double *__restrict__ mean, double *__restrict__ out, int64_t ldo) {
+    __shared__ double sc[kCombineMaxP * kCombineMaxM];
+    for (int t = threadIdx.x; t < P * m; t += blockDim.x) sc[t] = coef[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        double v[kCombineMaxM / 32];
+#pragma unroll
+        for (int k = 0; k < kCombineMaxM / 32; ++k) {
+            const int c = lane + 32 * k;
+            v[k] = c < m ? (double)__ldcs(V + i * ldv + c) : 0.0;
+        }
+        const double base = mean ? mean[i] : 0.0;
+        for (int p = 0; p < P; ++p) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < kCombineMaxM / 32; ++k) {
+                const int c = lane + 32 * k;
+                if (c < m) acc = fma(v[k], sc[p * m + c], acc);
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) out[(int64_t)p * ldo + i] = base + acc;
+        }
+    }
+}
+}  // namespace
+}  // namespace snp
+
 extern "C" {
+
+// Reconstruction of P vectors from coefficients in a basis (the POD reconstruction of the
+// warm start): out[p][i] = mean[i] + sum_c V[i][c] coef[p][c].
+int snp_basis_combine(int32_t n, const float *V, int32_t m, int64_t ldv, const double *coef, int32_t P,
+                      const double *mean, double *out, int64_t ldo, void *stream) {
+    using namespace snp;
+    clear_error();
+    SNP_REQUIRE(n >= 0 && m >= 1 && m <= kCombineMaxM && P >= 1 && P <= kCombineMaxP && ldv >= m && ldo >= n,
+                "snp_basis_combine: need 1 <= m <= %d, 1 <= P <= %d, ldv >= m, ldo >= n", kCombineMaxM, kCombineMaxP);
+    SNP_REQUIRE(V && coef && out, "snp_basis_combine: NULL argument");
+    if (n == 0) return SNP_OK;
+    cudaStream_t st = as_stream(stream);
+    k_basis_combine<<<stride_grid(32 * (int64_t)n, 256, 8), 256, 0, st>>>(n, V, m, ldv, coef, P, mean, out, ldo);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
 
 int snp_gemm_bf16(int32_t M, int32_t N, int32_t K, const void *A, int32_t lda, const void *B, int32_t ldb,
                   const float *bias, int32_t act, float *C, int32_t ldc, void *H, int32_t ldh, int32_t *err,

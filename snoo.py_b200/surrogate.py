@@ -264,6 +264,22 @@ def solve_members_at_once(msolvers, x0s, res_refs, rtol=1e-8, precision="mixed",
     return xs, out
 
 
+def basis_combine(V, coef, mean=None):
+    """mean + coef @ V^T on this library's kernel (``snp_basis_combine``): V CUDA float32 [n, m]
+    row-major, coef CUDA float64 [P, m]; returns CUDA float64 [P, n]."""
+    t = torch()
+    assert V.dtype == t.float32 and V.is_cuda and V.stride(1) == 1 and coef.dtype == t.float64
+    n, m = int(V.shape[0]), int(V.shape[1])
+    coef = coef.reshape(-1, m).contiguous()
+    P = int(coef.shape[0])
+    out = t.empty((P, n), dtype=t.float64, device="cuda")
+    for p0 in range(0, P, 32):
+        p1 = min(P, p0 + 32)
+        _lib.call("snp_basis_combine", n, _lib.ptr(V), m, int(V.stride(0)), _lib.ptr(coef[p0:p1]), p1 - p0,
+                  _lib.ptr(mean), _lib.ptr(out[p0:p1]), n, _lib.stream_ptr())
+    return out
+
+
 class WarmStart:
     """Snapshots -> POD -> MLP; predicts starting vectors for new family members."""
 
@@ -327,8 +343,15 @@ class WarmStart:
         Y = self.mlp.forward(X)
         if check:
             self.mlp.check_errors()
-        c = Y.double() * self.c_sd + self.c_mu
-        return self.mean + c @ self.U.T
+        c = (Y.double() * self.c_sd + self.c_mu).contiguous()
+        return basis_combine(self.basis_f32(), c, self.mean)
+
+    def basis_f32(self):
+        """All POD modes as a row-major float32 [n, modes] CUDA tensor (cached): the operand of
+        the reconstruction kernel."""
+        if getattr(self, "_U32", None) is None or self._U32.shape != self.U.shape:
+            self._U32 = self.U.float().contiguous()
+        return self._U32
 
     def project(self, x):
         """Best POD approximation of a solution (the surrogate's floor)."""
