@@ -16,9 +16,12 @@
 // tensor memory and returns.  The kernel asks for more
 // than half of an SM's shared memory, so one CTA (holding 256 TMEM columns) runs per SM and
 // the allocation never waits on another CTA.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <cstdlib>
 
 #include "snp_common.cuh"
 #include "snp_internal.cuh"
@@ -183,6 +186,168 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
+// The same GEMM with its operands brought in by the Tensor Memory Accelerator and two
+// shared-memory stages: thread 0 issues, per 64-wide K chunk, eight 2-D TMA tile loads for A
+// (box 8 x 128: one 16-byte K group of 128 rows, which lands exactly as one K group of the
+// no-swizzle K-major layout) and eight for B (box 8 x nt), all completing on the stage's
+// mbarrier (expect-tx bytes); the MMAs of chunk c run while chunk c + 1 is in flight, and the
+// stage is refilled with chunk c + 2 once the commit of chunk c's MMAs has arrived.  Rows or K
+// columns beyond the matrix are zero-filled by the TMA unit.  Every wait is bounded; after a
+// timeout the CTA records the error, waits (bounded) for the copies and MMAs it issued, frees
+// its tensor memory and returns.  The tensor maps cover this GPU's own memory only and no load
+// uses multicast.
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    k_gemm_bf16_tma(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, int M, int N,
+                    int K, const float *__restrict__ bias, int act, float *__restrict__ C, int ldc,
+                    __nv_bfloat16 *__restrict__ H, int ldh, int nt, int *err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[2], mma_done[2];
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ int failed;
+    const int stage_a = kTileM * kChunkK * 2;  // 16 KiB
+    const int stage_b = kMaxNT * kChunkK * 2;  // 32 KiB (nt rows used)
+    // stage s: A at s * (stage_a + stage_b), B right after it
+    const uint32_t s_base = smem_u32(smem);
+    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * nt;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t tx_bytes = (uint32_t)(kTileM + nt) * kChunkK * 2;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mma_done[s])), "r"(1));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
+        failed = 0;
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base_slot;
+    const uint32_t idesc = instr_desc_bf16(kTileM, nt);
+    const int n_chunks = (K + kChunkK - 1) / kChunkK;
+
+    // chunk c -> stage c % 2: eight K groups of A and of B
+    auto issue = [&](int c) {
+        const int s = c & 1;
+        const uint32_t bar = smem_u32(&full[s]);
+        mbar_expect_tx(bar, tx_bytes);
+#pragma unroll
+        for (int kc = 0; kc < kChunkK / 8; ++kc) {
+            const int x = c * kChunkK + 8 * kc;  // a multiple of 8 BF16 elements (16 bytes)
+            const uint32_t a_s = s_base + (uint32_t)(s * (stage_a + stage_b));
+            tma_load_2d(a_s + kc * kTileM * 16, &map_a, x, m0, bar);
+            tma_load_2d(a_s + stage_a + kc * nt * 16, &map_b, x, n0, bar);
+        }
+    };
+    int issued = 0, mma_issued = 0;  // (thread 0's counts)
+    if (threadIdx.x == 0) {
+        for (; issued < 2 && issued < n_chunks; ++issued) issue(issued);
+    }
+    for (int c = 0; c < n_chunks; ++c) {
+        const int s = c & 1;
+        const uint32_t ph = (uint32_t)((c >> 1) & 1);
+        if (threadIdx.x == 0) {
+            bool ok = mbar_wait(smem_u32(&full[s]), ph);
+            if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t a0 = s_base + (uint32_t)(s * (stage_a + stage_b)), b0 = a0 + stage_a;
+#pragma unroll
+                for (int st = 0; st < kChunkK / 16; ++st) {
+                    const uint64_t da = smem_desc(a0 + 2 * st * (kTileM / 8) * 128, (kTileM / 8) * 128, 128);
+                    const uint64_t db = smem_desc(b0 + 2 * st * (nt / 8) * 128, (nt / 8) * 128, 128);
+                    const uint32_t accumulate = (c > 0 || st > 0) ? 1u : 0u;
+                    const uint32_t no_mask = 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(no_mask));
+                }
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                        smem_u32(&mma_done[s]))
+                    : "memory");
+                mma_issued = c + 1;
+                // refill this stage with chunk c + 2 once these MMAs have read it
+                if (c + 2 < n_chunks) {
+                    ok = mbar_wait(smem_u32(&mma_done[s]), ph);
+                    if (ok) {
+                        issue(c + 2);
+                        issued = c + 3;
+                    }
+                }
+            }
+            if (!ok) failed = 1;
+        }
+        __syncthreads();
+        if (failed) break;
+    }
+    // the last chunk's MMAs (commits arrive in order, so the last one covers all)
+    if (!failed && threadIdx.x == 0) {
+        const int c = n_chunks - 1;
+        if (!mbar_wait(smem_u32(&mma_done[c & 1]), (uint32_t)((c >> 1) & 1))) failed = 1;
+    }
+    __syncthreads();
+    if (failed && threadIdx.x == 0) {
+        // bounded drain of what this CTA still has in flight before the memory goes away
+        for (int c = 0; c < issued; ++c)
+            if (c >= mma_issued) mbar_wait(smem_u32(&full[c & 1]), (uint32_t)((c >> 1) & 1));
+        if (mma_issued > 0) {
+            const int c = mma_issued - 1;
+            mbar_wait(smem_u32(&mma_done[c & 1]), (uint32_t)((c >> 1) & 1));
+        }
+        atomicExch(err, 1);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!failed) {
+        const int row = m0 + 32 * warp + lane;
+        for (int c8 = 0; c8 < nt / 8; ++c8) {
+            uint32_t v[8];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(8 * c8);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int col = n0 + 8 * c8 + j;
+                    if (col < N) {
+                        float z = __uint_as_float(v[j]);
+                        if (bias) z += bias[col];
+                        if (C) C[(int64_t)row * ldc + col] = z;
+                        if (H) H[(int64_t)row * ldh + col] = __float2bfloat16_rn(act == 1 ? gelu(z) : z);
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
 // dZ = dH * GELU'(Z) (FP32 in, BF16 out for the next GEMMs, FP32 copy optional)
 __global__ void k_gelu_backward(int64_t count, const float *__restrict__ dH, const float *__restrict__ Z,
                                 __nv_bfloat16 *__restrict__ dZb, float *__restrict__ dZf) {
@@ -267,6 +432,34 @@ __global__ void k_f32_to_bf16(int64_t count, const float *__restrict__ a, __nv_b
 // columns, the row read once for all P vectors), float64 products and a fixed shuffle tree;
 // the coefficients of all P vectors staged in shared memory.
 namespace snp {
+
+// Tensor map of a row-major BF16 matrix [rows][ld] with K contiguous, read in boxes of one
+// 16-byte K group (8 elements) by box_rows rows: the K-major no-swizzle group layout of the
+// tcgen05 operands.  Out-of-range boxes are zero-filled.  cuTensorMapEncodeTiled comes from
+// the driver through the runtime's entry-point query (no link to libcuda).
+int encode_kmajor_map(CUtensorMap *map, const void *base, int K, int rows, int ld, int box_rows) {
+    using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeFn encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SNP_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        SNP_REQUIRE(q == cudaDriverEntryPointSuccess && fn, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<EncodeFn>(fn);
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    SNP_REQUIRE(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SNP_OK;
+}
+
 namespace {
 constexpr int kCombineMaxM = 128;
 constexpr int kCombineMaxP = 32;
@@ -337,9 +530,21 @@ int snp_gemm_bf16(int32_t M, int32_t N, int32_t K, const void *A, int32_t lda, c
     // N tile: the whole N when it fits, else 256-wide tiles (both multiples of 16)
     const int nt = N <= snp::kMaxNT ? ((N + 15) / 16) * 16 : snp::kMaxNT;
     cudaStream_t s = snp::as_stream(stream);
+    dim3 grid((M + snp::kTileM - 1) / snp::kTileM, (N + nt - 1) / nt);
+    const char *env = getenv("SNP_GEMM_TMA");
+    if (!(env && env[0] == '0')) {
+        CUtensorMap ma, mb;
+        SNP_TRY(snp::encode_kmajor_map(&ma, A, K, M, lda, snp::kTileM));
+        SNP_TRY(snp::encode_kmajor_map(&mb, B, K, N, ldb, nt));
+        SNP_CUDA_TRY(cudaFuncSetAttribute(snp::k_gemm_bf16_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)snp::kGemmSmem));
+        snp::k_gemm_bf16_tma<<<grid, snp::kGemmThreads, snp::kGemmSmem, s>>>(
+            ma, mb, M, N, K, bias, act, C, ldc, static_cast<__nv_bfloat16 *>(H), ldh, nt, err);
+        SNP_LAUNCH_CHECK();
+        return SNP_OK;
+    }
     SNP_CUDA_TRY(cudaFuncSetAttribute(snp::k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)snp::kGemmSmem));
-    dim3 grid((M + snp::kTileM - 1) / snp::kTileM, (N + nt - 1) / nt);
     snp::k_gemm_bf16<<<grid, snp::kGemmThreads, snp::kGemmSmem, s>>>(
         M, N, K, static_cast<const __nv_bfloat16 *>(A), lda, static_cast<const __nv_bfloat16 *>(B), ldb, bias, act, C,
         ldc, static_cast<__nv_bfloat16 *>(H), ldh, nt, err);
