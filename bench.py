@@ -396,6 +396,10 @@ def run_ours(args):
         torch.cuda.empty_cache()
         line["batched_variants_32"] = batched_study(32)
         torch.cuda.empty_cache()
+        # the learned-warm-start configuration at its stated size: the morphed 300k-tet family,
+        # 4000 training solves (generated 32 members at a time by the batched solver), 500 held out
+        line["warm_start_family_300k"] = warm_start_study(300_000, n_train=4000, n_test=500, generate_at_once=32)
+        torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -403,7 +407,8 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs=None, seed=0, galerkin_modes=64):
+def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs=None, seed=0, galerkin_modes=64,
+                     generate_at_once=1):
     """Learned warm start on a morphed-yoke family (fixed topology, 8 shape parameters + coil
     current density).  Untimed: ``n_train`` zero-start mixed-precision solves, POD to
     ``n_modes`` modes, MLP training on the tensor-core kernels.  Timed (CUDA events around each
@@ -426,7 +431,7 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
     setup_s = time.perf_counter() - t0
     modes = min(n_modes, n_train - 1)
     ws = SG.WarmStart(ms, n_modes=modes, hidden=hidden, seed=seed)
-    snaps, st_train = ws.generate(P_train, precision="mixed")
+    snaps, st_train = ws.generate(P_train, precision="mixed", members_at_once=generate_at_once)
     ws.fit(P_train, snaps, epochs=epochs, batch=min(256, (n_train // 8) * 8), lr=2e-3, seed=seed)
     del snaps
     torch.cuda.empty_cache()
@@ -436,7 +441,7 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
     if galerkin_modes > 0:
         rows["mixed_warm_galerkin"] = []
     surr_err, proj_err, b_err = [], [], []
-    warm_x, galerkin_x = [], []
+    warm_x, galerkin_x, b_refs = [], [], []
     probes = fam.geometry.aperture_probes(200, margin=0.03)
     el, _ = fam.mesh.locate(probes)
     for p in P_test:
@@ -457,6 +462,7 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
             if name == "fp64_zero":
                 x_ref = x.clone()
                 B_ref = ms.solver.curl_curl_factory.compute_B_at_points(x, probes, el)
+                b_refs.append(B_ref)
             elif name == "mixed_warm":
                 warm_x.append(x.clone())
                 nrm = float(torch.linalg.vector_norm(x_ref).item())
@@ -520,6 +526,51 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
         out["speedup_mixed_warm_batched_vs_fp64_zero"] = (out["mixed_warm_batched"]["solves_per_s"]
                                                           / out["fp64_zero"]["solves_per_s"])
         del extra
+    # the batched solver (snp_batch_*): every held-out member's warm start (network prediction,
+    # then the Galerkin step on the host path) solved by one batched Newton loop, members in
+    # groups of `eng_batch`; predictions, Galerkin steps and the batched solve are timed
+    from snoopy_b200 import batch as BT
+
+    eng_batch = min(32 if fam.mesh.num_elements < 600_000 else 8, len(P_test))
+    if eng_batch > 1:
+        members = [SG.MorphedSolver(fam) for _ in range(eng_batch)]
+        engine = BT.BatchSolver(members)
+        tuned = engine.tune("mixed")
+        wall, stats, errs = 0.0, [], []
+        for c0 in range(0, len(P_test), eng_batch):
+            chunk = list(range(c0, min(c0 + eng_batch, len(P_test))))
+            if len(chunk) < eng_batch:  # a smaller last group gets a batch of its own size
+                engine = BT.BatchSolver(members[: len(chunk)])
+            mss = members[: len(chunk)]
+            refs = [m.set_member(P_test[i]) for m, i in zip(mss, chunk)]
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            x0s = []
+            for m, i in zip(mss, chunk):
+                x0 = ws.predict(P_test[i], check=False)[0]
+                if galerkin_modes > 0:
+                    x0 = ws.correct(x0, msolver=m, modes=galerkin_modes, precision="mixed")
+                x0s.append(x0)
+            ws.mlp.check_errors()
+            st = engine.solve(RTOL, precision="mixed", x0s=x0s, res_refs=refs)
+            torch.cuda.synchronize()
+            wall += time.perf_counter() - t1
+            stats += st
+            for m, x, i in zip(mss, engine.xs, chunk):
+                Bw = m.solver.curl_curl_factory.compute_B_at_points(x, probes, el)
+                errs.append(float(np.linalg.norm(Bw - b_refs[i], axis=1).max()
+                                  / np.linalg.norm(b_refs[i], axis=1).max()))
+        out["mixed_warm_batched_engine"] = {
+            "members_per_batch": eng_batch, "galerkin_modes": galerkin_modes, "solves_per_s": len(P_test) / wall,
+            "newton_mean": float(np.mean([s_["newton_iterations"] for s_ in stats])),
+            "cg_mean": float(np.mean([s_["cg_iterations"] for s_ in stats])),
+            "rel_res_max": float(max(s_["rel_res"] for s_ in stats)),
+            "starts_dropped": int(sum(s_["start_dropped"] for s_ in stats)),
+            "B_err_vs_fp64_zero_max": float(max(errs)),
+            "autotuner": {k: tuned[k] for k in ("pass1_block", "asm_waves", "graph")}}
+        out["speedup_mixed_warm_batched_engine_vs_fp64_zero"] = (out["mixed_warm_batched_engine"]["solves_per_s"]
+                                                                 / out["fp64_zero"]["solves_per_s"])
+        del engine, members
     del ws, ms, fam
     return out
 
@@ -983,7 +1034,7 @@ def run_warm_start_family(args):
     import torch
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    res = warm_start_study(300_000, n_train=4000, n_test=500)
+    res = warm_start_study(300_000, n_train=4000, n_test=500, generate_at_once=32)
     line = {"metric": "warm-started vs zero-start nonlinear solves/s, morphed 300k-tet yoke family",
             "value": res["mixed_warm"]["solves_per_s"], "unit": UNIT, "higher_is_better": True, "n_gpus": 1,
             "dtype": "f32+f64 (bf16 MLP)", "data": "synthetic (seeded morphed-yoke family)", "config": res}

@@ -118,19 +118,25 @@ def solve_many(instances, rtol=1e-8, precision="fp64", n_threads=0):
 
 
 class BatchSolver:
-    """All instances in one batched device solver (``snp_batch_*``): the instances' element and
-    DoF arrays concatenated, one launch per pass over all of them, each instance's Newton / CG /
-    line-search state on the device and the whole Newton loop as one CUDA graph.  The
-    instances' own solvers stay the source of their meshes, materials and source fields, so
-    they must outlive this object.  Every instance's answer is bitwise the one it gets in a
-    batch of its own."""
+    """Many problems in one batched device solver (``snp_batch_*``): their element and DoF arrays
+    concatenated, one launch per pass over all of them, each problem's Newton / CG / line-search
+    state on the device and the whole Newton loop as one CUDA graph.
 
-    def __init__(self, instances):
+    ``members``: objects with a Newton engine ``eng`` (``Instance``, ``surrogate.MorphedSolver``)
+    or engines themselves; a member's ``x`` (when it has one) receives its answer, otherwise
+    the batch holds a buffer (``xs``).  The members' own solvers stay the source of their
+    meshes, materials and source fields, so they must outlive this object.  Every member's
+    answer is bitwise the one it gets in a batch of its own."""
+
+    def __init__(self, members, max_newton=60):
         t = torch()
         t.cuda.synchronize()
-        self.instances = list(instances)
-        k = len(self.instances)
-        handles = (ctypes.c_void_p * k)(*[ins.eng.handle.value for ins in self.instances])
+        self.members = list(members)
+        self.engines = [m.eng if hasattr(m, "eng") else m for m in self.members]
+        self.xs = [m.x if hasattr(m, "x") else zeros(e.n)[: e.n] for m, e in zip(self.members, self.engines)]
+        self.max_newton = [int(getattr(m, "max_newton", max_newton)) for m in self.members]
+        k = len(self.engines)
+        handles = (ctypes.c_void_p * k)(*[e.handle.value for e in self.engines])
         h = ctypes.c_void_p()
         _lib.call("snp_batch_create", handles, k, ctypes.byref(h))
         self.handle = h
@@ -146,26 +152,26 @@ class BatchSolver:
         return inf.as_dict()
 
     def solve(self, rtol=1e-8, precision="fp64", x0s=None, res_refs=None, raise_on_failure=True):
-        """Zero-start (or ``x0s``) residual-mode Newton of every instance at once; answers in each
-        instance's ``x``; returns per-instance stats dicts."""
+        """Residual-mode Newton of every member at once, from zero or from ``x0s`` (CUDA float64
+        vectors or None); ``res_refs`` (per member, > 0) replaces ||F_free(x0)|| in the stopping
+        rule and drops starts worse than x = 0.  Answers in ``xs``; returns per-member stats."""
         t = torch()
-        k = len(self.instances)
-        for i, ins in enumerate(self.instances):
+        k = len(self.engines)
+        for i, x in enumerate(self.xs):
             if x0s is not None and x0s[i] is not None:
-                ins.x.copy_(x0s[i])
+                x.copy_(x0s[i])
             else:
-                ins.x.zero_()
+                x.zero_()
         t.cuda.synchronize()
-        xs = (ctypes.c_void_p * k)(*[ins.x.data_ptr() for ins in self.instances])
+        xp = (ctypes.c_void_p * k)(*[x.data_ptr() for x in self.xs])
+        prec = {"fp64": 0, "mixed": 1}[precision]
         opts = (_lib.SolveOpts * k)()
-        for i, ins in enumerate(self.instances):
-            o = ins.opts(rtol, precision)
-            if res_refs is not None:
-                o.res_ref = float(res_refs[i])
-            opts[i] = o
+        for i in range(k):
+            ref = float(res_refs[i]) if res_refs is not None else 0.0
+            opts[i] = _lib.SolveOpts(1, float(rtol), 50000, self.max_newton[i], 0.1, prec, 0, 1, ref)
         stats = (_lib.SolveStats * k)()
         status = (ctypes.c_int32 * k)()
-        rc = _lib.load().snp_batch_solve(self.handle, xs, opts, stats, status)
+        rc = _lib.load().snp_batch_solve(self.handle, xp, opts, stats, status)
         out = []
         for i in range(k):
             d = stats[i].as_dict()

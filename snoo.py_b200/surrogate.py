@@ -289,17 +289,37 @@ class WarmStart:
         self.mlp = MLP((9, hidden, hidden, hidden, n_modes), seed=seed)
         self.timings = {}
 
-    def generate(self, params, precision="mixed", rtol=1e-8):
-        """Solve every member (zero start); returns float32 snapshots [S, n] and per-solve stats."""
+    def generate(self, params, precision="mixed", rtol=1e-8, members_at_once=1):
+        """Solve every member (zero start); returns float32 snapshots [S, n] and per-solve stats.
+        ``members_at_once`` > 1 solves groups of members together in the batched solver
+        (``batch.BatchSolver`` over that many ``MorphedSolver`` copies of the family)."""
         t = torch()
         snaps = t.empty((len(params), self.ms.n), dtype=t.float32, device="cuda")
         stats = []
         t0 = time.perf_counter()
-        for i, p in enumerate(params):
-            ref = self.ms.set_member(p)
-            x, st = self.ms.solve(None, rtol=rtol, precision=precision, res_ref=ref)
-            snaps[i] = x.float()
-            stats.append(st)
+        if members_at_once <= 1:
+            for i, p in enumerate(params):
+                ref = self.ms.set_member(p)
+                x, st = self.ms.solve(None, rtol=rtol, precision=precision, res_ref=ref)
+                snaps[i] = x.float()
+                stats.append(st)
+        else:
+            from .batch import BatchSolver
+
+            k = int(members_at_once)
+            members = [MorphedSolver(self.ms.family, max_newton=self.ms.max_newton) for _ in range(k)]
+            engines = {}
+            for c0 in range(0, len(params), k):
+                chunk = list(range(c0, min(c0 + k, len(params))))
+                m = len(chunk)
+                if m not in engines:
+                    engines[m] = BatchSolver(members[:m])
+                refs = [ms.set_member(params[i]) for ms, i in zip(members[:m], chunk)]
+                st = engines[m].solve(rtol, precision=precision, res_refs=refs)
+                for x, i in zip(engines[m].xs, chunk):
+                    snaps[i] = x.float()
+                stats += st
+            del engines, members
         t.cuda.synchronize()
         self.timings["generate_s"] = time.perf_counter() - t0
         return snaps, stats
