@@ -153,7 +153,7 @@ constexpr int kBsBlock = 128;
 __global__ void __launch_bounds__(kBsBlock)
     k_biot_savart(const double *__restrict__ src, int64_t n_src, const double *__restrict__ tar, int64_t n_tar,
                   double current, double rad, double *__restrict__ B) {
-    __shared__ double s[kBsBlock * 6];
+    __shared__ double s[kBsBlock * 7];  // per segment: start, end, 1 / |end - start|^2
     const double rad2 = rad * rad;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n_tar; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = base + threadIdx.x;
@@ -168,18 +168,23 @@ __global__ void __launch_bounds__(kBsBlock)
         for (int64_t j0 = 0; j0 < n_src; j0 += kBsBlock) {
             const int m = (int)((n_src - j0) < kBsBlock ? (n_src - j0) : kBsBlock);
             __syncthreads();
-            for (int t = threadIdx.x; t < m * 6; t += blockDim.x) s[t] = src[6 * j0 + t];
+            for (int t = threadIdx.x; t < m * 6; t += blockDim.x) s[(t / 6) * 7 + t % 6] = src[6 * j0 + t];
+            __syncthreads();
+            for (int t = threadIdx.x; t < m; t += blockDim.x) {
+                const double *sg = s + 7 * t;
+                const double n0 = sg[3] - sg[0], n1 = sg[4] - sg[1], n2 = sg[5] - sg[2];
+                s[7 * t + 6] = 1.0 / (n0 * n0 + n1 * n1 + n2 * n2);
+            }
             __syncthreads();
             if (active) {
                 for (int jj = 0; jj < m; ++jj) {
-                    const double *sg = s + 6 * jj;
+                    const double *sg = s + 7 * jj;
                     const double n0 = sg[3] - sg[0], n1 = sg[4] - sg[1], n2 = sg[5] - sg[2];
-                    const double nn = n0 * n0 + n1 * n1 + n2 * n2;
                     const double d10 = sg[0] - px, d11 = sg[1] - py, d12 = sg[2] - pz;
                     const double d20 = sg[3] - px, d21 = sg[4] - py, d22 = sg[5] - pz;
                     const double nd1 = sqrt(d10 * d10 + d11 * d11 + d12 * d12);
                     const double nd2 = sqrt(d20 * d20 + d21 * d21 + d22 * d22);
-                    const double tp = -1.0 * (d10 * n0 + d11 * n1 + d12 * n2) / nn;
+                    const double tp = -1.0 * (d10 * n0 + d11 * n1 + d12 * n2) * sg[6];
                     const double p0 = px - (sg[0] + tp * n0), p1 = py - (sg[1] + tp * n1), p2 = pz - (sg[2] + tp * n2);
                     const double dmin2 = p0 * p0 + p1 * p1 + p2 * p2;
                     if ((dmin2 < rad2 && tp <= 1.0 && tp >= 0.0) || nd1 < rad || nd2 < rad) {
@@ -190,8 +195,10 @@ __global__ void __launch_bounds__(kBsBlock)
                         by += b1 * f;
                         bz += b2 * f;
                     } else {
+                        // (|d1| + |d2|) / (|d1| |d2| + d1.d2) / |d1| / |d2|, with one division
                         const double dd = d10 * d20 + d11 * d21 + d12 * d22;
-                        const double f = (nd1 + nd2) / (nd1 * nd2 + dd) / nd1 / nd2;
+                        const double pr = nd1 * nd2;
+                        const double f = (nd1 + nd2) / ((pr + dd) * pr);
                         bx += (d11 * d22 - d12 * d21) * f;
                         by += (d12 * d20 - d10 * d22) * f;
                         bz += (d10 * d21 - d11 * d20) * f;

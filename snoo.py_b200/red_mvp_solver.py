@@ -62,12 +62,15 @@ class RedMVPSolver:
         with ``refresh`` (then also handed to the Newton engines built so far)."""
         if self._source_fields is None or refresh:
             fields = []
+            groups = self._coil_groups()
             for i in range(len(self.iron_tags)):
                 pts = self.curl_curl_factory.get_quadrature_points_device(self.quad_order, i)
-                B = zeros(pts.numel())[: pts.numel()]
-                for coil in self.coil_list:
-                    segs = upload(coil.get_segments(), np.float64)
-                    B += biot_savart_device(segs, pts, coil.current, coil.rad)[: pts.numel()]
+                B = None
+                for segs, current, rad in groups:
+                    Bg = biot_savart_device(segs, pts, current, rad)[: pts.numel()]
+                    B = Bg if B is None else B + Bg
+                if B is None:
+                    B = zeros(pts.numel())[: pts.numel()]
                 fields.append(B)
             for _ in self.air_tags:
                 fields.append(np.zeros((0, 3)))
@@ -77,6 +80,22 @@ class RedMVPSolver:
                     for i in range(len(self.iron_tags)):
                         eng.set_source(i, fields[i])
         return self._source_fields
+
+    def _coil_groups(self):
+        """The coils' filament segments on the device, coils of equal current and core radius
+        concatenated (one Biot-Savart launch per group); re-uploaded only when a coil's
+        segments, current or radius change."""
+        key = [(c.current, c.rad, c.get_segments()) for c in self.coil_list]
+        cached = getattr(self, "_coil_cache", None)
+        if cached is not None and len(cached[0]) == len(key) and all(
+                a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2]) for a, b in zip(cached[0], key)):
+            return cached[1]
+        groups = {}
+        for current, rad, segs in key:
+            groups.setdefault((float(current), float(rad)), []).append(np.asarray(segs, dtype=np.float64))
+        dev = [(upload(np.concatenate(v), np.float64), cur, rad) for (cur, rad), v in groups.items()]
+        self._coil_cache = (key, dev)
+        return dev
 
     def gauge_mask(self):
         """Free-DoF mask of the tree-cotree gauged formulation: the Dirichlet edges and the
