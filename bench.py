@@ -865,8 +865,11 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's C kernels) is not built"}),
               flush=True)
         return
+    # one single-threaded process per solve while memory allows: with more solves than cores the
+    # processes share the cores (the wall time is then that of the whole host doing all of them,
+    # not of two uneven waves)
     mem_cap = int((info["mem_available_gb"] or 64.0) // REFERENCE_WORKER_GB) or 1
-    procs = max(1, min(args.steps, info["usable_cpus"], mem_cap))
+    procs = max(1, min(args.steps, mem_cap))
     shares = [list(range(p, args.steps, procs)) for p in range(procs)]
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(procs + 1)
@@ -900,7 +903,7 @@ def run_reference(args):
                                    f"~{tets_msg} target tets, Q=4, fp64",
                        "solves": args.steps, "processes": procs, "counts_per_solve": counts,
                        "max_rel_res": float(max(r["rel_res"] for r in res)), "setup_s": t_setup},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(procs, info["usable_cpus"]), "kind": "reference",
                              "sample": (f"{args.steps} complete solves (reference C kernels, scipy CSR and Jacobi cg, "
                                         f"source field per solve) on {procs} single-threaded processes; one solve "
                                         f"{per.mean():.1f} s mean ({per.min():.1f}-{per.max():.1f} s); warm-up: "
