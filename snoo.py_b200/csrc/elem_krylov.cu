@@ -686,6 +686,226 @@ __global__ void __launch_bounds__(kEBlock)
     }
 }
 
+// ---------------------------------------------------------------- one-launch PCG (cooperative)
+//
+// The whole Krylov loop of one Newton step in one cooperative launch (every block resident):
+// per iteration the element pass and the DoF pass of k_epass1 / k_epass2_bj (or k_epass2) run
+// back to back, separated by grid barriers instead of kernel boundaries; every block sums the
+// per-block partials itself, in block order, so all blocks take the same alpha, beta and
+// stopping decision without a serial last-block step.  Block 0 mirrors the state into *st for
+// the host.  Each barrier wait is bounded: a block that gives up records the failure in *err
+// and leaves; the others then give up at their next barrier.
+
+struct GridBarrier {
+    unsigned long long count;
+};
+
+constexpr long long kCoopSpin = 1ll << 26;
+
+__device__ __forceinline__ bool grid_sync(GridBarrier *bar, unsigned long long &target, int *err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&bar->count, 1ull);
+        target += gridDim.x;
+        int ok = 0;
+        for (long long k = 0; k < kCoopSpin; ++k) {
+            unsigned long long c;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(c) : "l"(&bar->count) : "memory");
+            if (c >= target) {
+                ok = 1;
+                break;
+            }
+        }
+        if (!ok) atomicExch(err, 1);
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// sum of part[i * 3 + comp] over i < gridDim.x, the same order in every block; all threads
+__device__ __forceinline__ double coop_sum(const double *part, int comp, double *sh) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) v += __ldcg(part + 3 * i + comp);
+    v = block_sum(v, sh);
+    __shared__ double s_v;
+    if (threadIdx.x == 0) s_v = v;
+    __syncthreads();
+    v = s_v;
+    __syncthreads();
+    return v;
+}
+
+template <typename TT, bool BJ>
+__global__ void __launch_bounds__(kEBlock, kPass1MinBlocks)
+    k_pcg_coop(int64_t ne, int32_t n, const int32_t *__restrict__ edof, const int32_t *__restrict__ pos,
+               const TT *__restrict__ T, const TT *__restrict__ chat, const uint8_t *__restrict__ free_mask,
+               const int32_t *__restrict__ inc_ptr, const uint16_t *__restrict__ meta, const float *__restrict__ binv,
+               const TT *__restrict__ D, DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R, TT *__restrict__ Y,
+               PcgState *st, double *part, GridBarrier *bar, int *err) {
+    __shared__ TT sc[18];
+    __shared__ double sh[32];
+    __shared__ double sh2[2][32];
+    __shared__ TT s_r[kBjTile];
+    if (st->done) return;  // uniform: written by the start kernel before this launch
+    if (threadIdx.x < 18) sc[threadIdx.x] = chat[threadIdx.x];
+    __syncthreads();
+    double rz = st->rz;
+    const double atol_eff = st->atol_eff;
+    const long long maxit = st->maxit;
+    long long iter = 0;
+    double beta = 0.0;
+    unsigned long long target = 0;
+    const int lane = threadIdx.x & 31;
+    const int h = lane & 1;
+    const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5) * 16;
+    for (;;) {
+        // ---- element pass (k_epass1)
+        const TT tb = (TT)beta;
+        double dot = 0.0;
+#pragma unroll 1
+        for (int64_t e0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 16; e0 < ne; e0 += wstride) {
+            const int64_t e = e0 + (lane >> 1);
+            const bool valid = e < ne;
+            const int64_t eb = eslot(valid ? e : 0, 0);
+            int32_t d[3], ps[3];
+            TT th[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                d[j] = valid ? __ldcs(edof + eb + 32 * (3 * h + j)) : 0;
+                ps[j] = valid ? __ldcs(pos + eb + 32 * (3 * h + j)) : 0;
+                th[j] = valid ? __ldcs(T + eb + 32 * (3 * h + j)) : TT(0);
+            }
+            DofPair<TT> w[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) w[j] = G[(uint32_t)d[j] & ~kSignBit];
+            TT u0 = TT(0), u1 = TT(0), u2 = TT(0);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                TT pk = pnext(tb, w[j].b, w[j].a);
+                if (d[j] < 0) pk = -pk;
+                const TT *c = sc + 3 * (3 * h + j);
+                u0 += pk * c[0];
+                u1 += pk * c[1];
+                u2 += pk * c[2];
+            }
+            if (!valid) u0 = u1 = u2 = TT(0);
+            const TT o0 = __shfl_xor_sync(0xffffffffu, u0, 1);
+            const TT o1 = __shfl_xor_sync(0xffffffffu, u1, 1);
+            const TT o2 = __shfl_xor_sync(0xffffffffu, u2, 1);
+            if (h) {
+                u0 = o0 + u0;
+                u1 = o1 + u1;
+                u2 = o2 + u2;
+            } else {
+                u0 = u0 + o0;
+                u1 = u1 + o1;
+                u2 = u2 + o2;
+            }
+            TT t[6];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const TT other = __shfl_xor_sync(0xffffffffu, th[j], 1);
+                t[j] = h ? other : th[j];
+                t[3 + j] = h ? th[j] : other;
+            }
+            if (!valid) continue;
+            const TT v0 = t[0] * u0 + t[1] * u1 + t[2] * u2;
+            const TT v1 = t[1] * u0 + t[3] * u1 + t[4] * u2;
+            const TT v2 = t[2] * u0 + t[4] * u1 + t[5] * u2;
+            if (!h) dot += (double)u0 * (double)v0 + (double)u1 * (double)v1 + (double)u2 * (double)v2;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) Y[ps[j]] = edge_term(sc, 3 * h + j, d[j] < 0, v0, v1, v2);
+        }
+        dot = block_sum(dot, sh);
+        if (threadIdx.x == 0) part[3 * blockIdx.x] = dot;
+        if (!grid_sync(bar, target, err)) return;
+        const double pq = coop_sum(part, 0, sh);
+        const double alpha = rz / pq;
+        // ---- DoF pass (k_epass2_bj / k_epass2)
+        const TT ta = (TT)alpha;
+        double rz_n = 0.0, rr_n = 0.0;
+        if constexpr (BJ) {
+            for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += (int64_t)gridDim.x * kBjTile) {
+                const int64_t i = base + threadIdx.x;
+                const bool fr = i < n && is_free(free_mask, i);
+                DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
+                TT r = TT(0);
+                if (fr) {
+                    bj_prefetch(binv, i);
+                    g = G[i];
+                    rx = R[i];
+                    const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
+                    double q = 0.0;
+                    for (int k = b0; k < b1; ++k) q += (double)Y[k];
+                    r = rx.a - ta * (TT)q;
+                }
+                s_r[threadIdx.x] = r;
+                __syncthreads();
+                if (fr) {
+                    float4 ma, mb;
+                    bj_load(binv, i, ma, mb);
+                    const TT z = bj_row((unsigned)meta[i], ma, mb, s_r, threadIdx.x);
+                    const TT p = pnext(tb, g.b, g.a);
+                    G[i] = DofPair<TT>{z, p};
+                    R[i] = DofPair<TT>{r, rx.b + ta * p};
+                    rz_n += (double)r * (double)z;
+                    rr_n += (double)r * (double)r;
+                }
+                __syncthreads();
+            }
+        } else {
+            for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+                 i += (int64_t)gridDim.x * blockDim.x) {
+                if (!is_free(free_mask, i)) continue;
+                const DofPair<TT> g = G[i];
+                const DofPair<TT> rx = R[i];
+                const TT dv = D[i];
+                const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
+                double q = 0.0;
+                for (int k = b0; k < b1; ++k) q += (double)Y[k];
+                const TT p = pnext(tb, g.b, g.a);
+                const TT r = rx.a - ta * (TT)q;
+                const TT z = dv * r;
+                G[i] = DofPair<TT>{z, p};
+                R[i] = DofPair<TT>{r, rx.b + ta * p};
+                rz_n += (double)r * (double)z;
+                rr_n += (double)r * (double)r;
+            }
+        }
+        block_sum2(rz_n, rr_n, sh2);
+        if (threadIdx.x == 0) {
+            part[3 * blockIdx.x + 1] = rz_n;
+            part[3 * blockIdx.x + 2] = rr_n;
+        }
+        if (!grid_sync(bar, target, err)) return;
+        const double rz_new = coop_sum(part, 1, sh);
+        const double rr_new = coop_sum(part, 2, sh);
+        beta = rz_new / rz;
+        rz = rz_new;
+        iter += 1;
+        int done = 0;
+        if (!(rr_new == rr_new) || isinf(rr_new)) done = 3;
+        else if (sqrt(rr_new) < atol_eff) done = 1;
+        else if (iter >= maxit) done = 2;
+        if (done) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                st->pq = pq;
+                st->alpha = alpha;
+                st->beta = beta;
+                st->rz = rz;
+                st->rr = rr_new;
+                st->iter = iter;
+                st->done = done;
+            }
+            return;
+        }
+    }
+}
+
 __global__ void k_bj_apply(int32_t n, const uint8_t *__restrict__ free_mask, const uint16_t *__restrict__ meta,
                            const float *__restrict__ binv, const double *__restrict__ r_in, double *__restrict__ z_out) {
     __shared__ double s_r[kBjTile];
@@ -981,6 +1201,59 @@ int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t
     return SNP_OK;
 }
 
+// The iteration loop as one cooperative launch (k_pcg_coop); false when the device cannot
+// hold the grid (the caller then uses the graph).  *rc: the launch's status and the barrier's.
+template <typename TT>
+bool ElemPcg<TT>::solve_coop(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
+                             const float *bj_inv, cudaStream_t s, int *rc) {
+    *rc = SNP_OK;
+    auto kern = bj_meta ? k_pcg_coop<TT, true> : k_pcg_coop<TT, false>;
+    int dev = 0, coop = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+        !coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEBlock, 0) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    const int grid = sm_count() * per_sm;
+    if ((size_t)grid * 3 > part.n) return false;  // part holds 3 x (8 blocks per SM + 1)
+    if (!coop_bar.p && (coop_bar.alloc(1) != SNP_OK || coop_err.alloc(1) != SNP_OK)) {
+        clear_error();
+        return false;
+    }
+    if (cudaMemsetAsync(coop_bar.p, 0, sizeof(GridBarrier), s) != cudaSuccess ||
+        cudaMemsetAsync(coop_err.p, 0, sizeof(int), s) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    int64_t ne_ = ne;
+    int32_t n_ = n;
+    const int32_t *edof = top.edof.p, *pos = top.pos.p, *ip = top.inc_ptr.p;
+    const TT *chat = chat_ptr<TT>(top);
+    const TT *Dp = D.p;
+    DofPair<TT> *Gp = G.p, *Rp = R.p;
+    TT *Yp = Y.p;
+    PcgState *stp = st.p;
+    double *pp = part.p;
+    GridBarrier *bp = reinterpret_cast<GridBarrier *>(coop_bar.p);
+    int *ep = coop_err.p;
+    void *args[] = {&ne_, &n_, &edof, &pos, &T, &chat, &free_mask, &ip, &bj_meta, &bj_inv, &Dp, &Gp, &Rp, &Yp,
+                    &stp, &pp, &bp, &ep};
+    const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kern), dim3(grid), dim3(kEBlock),
+                                                      args, 0, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    int herr = 0;
+    if (cudaMemcpyAsync(&herr, coop_err.p, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        *rc = fail(SNP_CUDA_ERROR, "element PCG: %s", cudaGetErrorString(cudaGetLastError()));
+        return true;
+    }
+    if (herr) *rc = fail(SNP_CUDA_ERROR, "element PCG: a grid barrier of the one-launch loop timed out");
+    return true;
+}
+
 template <typename TT>
 int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag, const uint8_t *free_mask,
                        const double *b, double b_scale, double *h, double rtol, double atol, int64_t maxit,
@@ -1008,9 +1281,20 @@ int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag,
         return fail(SNP_ZERO_PIVOT, "element PCG: zero or non-finite Jacobian diagonal on a free DoF");
     }
     int64_t chunk_launches = -1;
+    const char *coop_env = getenv("SNP_PCG_COOP");
+    if (coop_env && coop_env[0] == '1') {
+        int coop_rc = SNP_OK;
+        if (solve_coop(top, T, free_mask, bj_meta, bj_inv, s, &coop_rc)) {
+            SNP_TRY(coop_rc);
+            chunk_launches = 1;
+            goto extract;
+        }
+    }
+    {
     const bool same = exec && key_top == &top && key_T == T && key_fm == free_mask && key_bm == bj_meta &&
                       key_bi == bj_inv;
     if (!same) SNP_TRY(build_graph(top, T, free_mask, bj_meta, bj_inv));
+    }
     if (exec) {
         SNP_CUDA_TRY(cudaGraphLaunch(exec, s));
     } else {
@@ -1025,6 +1309,7 @@ int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag,
         }
         chunk_launches = 2 * launched;
     }
+extract:
     k_eextract<TT><<<stride_grid(n, kEBlock, 8), kEBlock, 0, s>>>(n, R.p, h);
     SNP_LAUNCH_CHECK();
     SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));

@@ -229,6 +229,10 @@ struct ElemPcg {
                          const float *bj_inv, cudaStream_t s, int use_cond, cudaGraphConditionalHandle cond);
     int build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
                     const float *bj_inv);
+    bool solve_coop(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
+                    const float *bj_inv, cudaStream_t s, int *rc);
+    DevBuf<unsigned long long> coop_bar;
+    DevBuf<int> coop_err;
 };
 
 // The view of a finalized solver (SNP_BAD_ARG when it is not finalized).  Valid while the

@@ -152,3 +152,31 @@ def test_exported_blocks_and_inverses(oracle_mod):
     assert worst_rows < 1e-12, worst_rows
     # float32 rounding of entries up to cond(block) ~ 1e4 times 6e-8
     assert worst_inv < 2e-3, worst_inv
+
+
+@pytest.mark.parametrize("precond", ["block", "jacobi"])
+def test_one_launch_pcg_reaches_the_graph_loops_answer(precond):
+    """The Krylov loop as one cooperative launch (SNP_PCG_COOP=1: grid barriers between the
+    element and DoF passes, every block summing the partials itself) solves the same Newton
+    problem as the graph-captured loop: both reach 1e-8 and the fields agree to that level."""
+    import os
+
+    msh, coils, rel, solver = _setup(20000, seed=9)
+    eng = solver.newton_engine()
+    eng.set_preconditioner(precond)
+    x_graph, st_g = solver.solve_to_residual(1e-8)
+    os.environ["SNP_PCG_COOP"] = "1"
+    try:
+        x_coop, st_c = solver.solve_to_residual(1e-8)
+        x_coop2, _ = solver.solve_to_residual(1e-8)
+    finally:
+        del os.environ["SNP_PCG_COOP"]
+    eng.set_preconditioner("block")
+    assert st_g["rel_res"] <= 1e-8 and st_c["rel_res"] <= 1e-8
+    assert abs(st_c["newton_iterations"] - st_g["newton_iterations"]) <= 1
+    assert np.array_equal(x_coop, x_coop2)  # deterministic run to run
+    probes = msh.geometry.aperture_probes(300)
+    el, _ = msh.locate(probes)
+    Bg = solver.evaluate_B(x_graph, probes, el)
+    Bc = solver.evaluate_B(x_coop, probes, el)
+    assert float(np.abs(Bc - Bg).max() / np.abs(Bg).max()) < 1e-7
