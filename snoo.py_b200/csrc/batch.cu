@@ -56,6 +56,15 @@ static_assert(kGroups == 64, "the chunk sum adds two group partials per lane");
 // CG outcome per problem (as the single-problem PcgState.done, plus idle and zero pivot)
 enum : int { CG_RUN = 0, CG_CONV = 1, CG_MAXIT = 2, CG_NAN = 3, CG_ZERO_RHS = 4, CG_IDLE = 5, CG_PIVOT = 6 };
 
+// Where each problem stands in its Newton loop.  Every pass of the solver's loop advances each
+// problem by its own next step, so problems do not wait for one another:
+//   HEAD     start of a Newton step: inner tolerance, block-Jacobi build, PCG start
+//   CG       one PCG iteration per pass
+//   EXTRACT  CG finished: the direction, the line search opened
+//   LS       one trial point of the line search per pass
+//   ACCEPT   the accepted trial point becomes x; converged, out of steps, or the next HEAD
+enum : int { PH_DONE = 0, PH_HEAD = 1, PH_CG = 2, PH_EXTRACT = 3, PH_LS = 4, PH_ACCEPT = 5, PH_LIVE = 6 };
+
 struct BInst {
     int32_t dof_off, n;
     int32_t unit0, n_units;
@@ -68,7 +77,7 @@ struct BInst {
 // marks the problems that take part in the next assembly and residual sums.
 struct BState {
     int32_t run;
-    int32_t active, status, it, ls_it, res_evals, dropped, bad, line_search, max_newton, cg_done, pad0;
+    int32_t active, status, it, ls_it, res_evals, dropped, bad, line_search, max_newton, cg_done, ph;
     long long cg_iter, cg_maxit, cg_total;
     double rz, pq, alpha, beta, rr, bnorm, atol_eff;
     double fn, res0, F0, fprev, eta_prev, eta, tol, res_ref, eta_max;
@@ -82,9 +91,10 @@ struct BCtl {
     unsigned long long launches;
     int passes;
     int fallback_blocks;
+    int any_phase[8];  // per phase (PH_LIVE: any problem not done), for the host-driven loop
 };
 
-constexpr int kMaxPasses = 100000;  // Newton passes per solve before every problem is stopped
+constexpr int kMaxPasses = 4000000;  // passes of the solver's loop before every problem is stopped
 
 struct BOpts {
     double tol, res_ref, eta_max;
@@ -239,6 +249,7 @@ __global__ void __launch_bounds__(kBB)
             } else {
                 s.active = (s.F0 == 0.0 || s.fn <= s.tol * s.F0) ? 0 : 1;
             }
+            s.ph = s.active ? PH_HEAD : PH_DONE;
             if (s.active) atomicOr(&s_any, 1);
         } else {  // SUM_LS: one trial point of the line search
             if (!ran) continue;
@@ -268,6 +279,7 @@ __global__ void __launch_bounds__(kBB)
             }
             s.ls_it += 1;
             s.run = accept ? 0 : 1;
+            if (accept) s.ph = PH_ACCEPT;
             if (!accept) atomicOr(&s_any, 1);
         }
     }
@@ -287,13 +299,9 @@ __global__ void __launch_bounds__(kBB)
 __global__ void k_b_step_begin(int n_inst, BState *st, int f32, BCtl *ctl) {
     count_launch(ctl);
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p == 0) ctl->passes += 1;
     if (p >= n_inst) return;
     BState &s = st[p];
-    if (!s.active) {
-        s.cg_done = CG_IDLE;
-        return;
-    }
+    if (s.ph != PH_HEAD) return;
     double eta = s.eta_max;
     if (s.it > 0) {
         const double ratio = s.fn / s.fprev;
@@ -326,7 +334,7 @@ __global__ void __launch_bounds__(kBB)
     if (threadIdx.x < 18) sc[threadIdx.x] = (double)chat[threadIdx.x];
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_tot; i += (int64_t)gridDim.x * blockDim.x) {
-        if (!st[unit_inst[i / kUnit]].active) continue;
+        if (st[unit_inst[i / kUnit]].ph != PH_HEAD) continue;
         double row[kBjMax];
 #pragma unroll
         for (int c = 0; c < kBjMax; ++c) row[c] = 0.0;
@@ -344,7 +352,7 @@ __global__ void __launch_bounds__(128)
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_tot; i += (int64_t)gridDim.x * blockDim.x) {
         const unsigned mt = meta[i];
         if (mt & 0xffu) continue;
-        if (!st[unit_inst[i / kUnit]].active) continue;
+        if (st[unit_inst[i / kUnit]].ph != PH_HEAD) continue;
         bj_invert_block(i, (int)(mt >> 8), free_mask[i] != 0, free_mask, bmat, binv, &ctl->fallback_blocks);
     }
 }
@@ -364,7 +372,7 @@ __global__ void __launch_bounds__(kBB)
     count_launch(ctl);
     for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
         const int p = unit_inst[u];
-        if (!st[p].active) continue;  // uniform across the block
+        if (st[p].ph != PH_HEAD) continue;  // uniform across the block
         double rz = 0.0, rr = 0.0;
         int bad = 0;
         for (int t = 0; t < kUnitTiles; ++t) {
@@ -403,7 +411,7 @@ __global__ void __launch_bounds__(kBB)
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
     for (int p = warp; p < n_inst; p += nw) {
         BState &s = st[p];
-        if (!s.active) continue;
+        if (s.ph != PH_HEAD) continue;
         const double rz = warp_ordered_sum(part, inst[p].unit0, inst[p].n_units, 2, 0);
         const double rr = warp_ordered_sum(part, inst[p].unit0, inst[p].n_units, 2, 1);
         if (lane != 0) continue;
@@ -421,6 +429,7 @@ __global__ void __launch_bounds__(kBB)
         else if (sqrt(rr) < s.atol_eff) done = CG_CONV;
         else if (s.cg_maxit <= 0) done = CG_MAXIT;
         s.cg_done = done;
+        s.ph = done == CG_RUN ? PH_CG : PH_EXTRACT;
         if (done == CG_RUN) atomicOr(&s_any, 1);
     }
     __syncthreads();
@@ -450,7 +459,7 @@ __global__ void __launch_bounds__(BS)
     constexpr int kWarps = BS / 32;
     for (int64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
         const int p = chunk_inst[c];
-        if (st[p].cg_done != CG_RUN) continue;  // uniform across the block
+        if (st[p].ph != PH_CG) continue;  // uniform across the block
         const TT beta = (TT)st[p].beta;
         const int64_t e_end = inst[p].elem_off + inst[p].ne;
         for (int g = warp; g < kGroups; g += kWarps) {
@@ -524,7 +533,7 @@ __global__ void __launch_bounds__(BS)
     const int nw = blockDim.x >> 5;
     for (int p = warp; p < n_inst; p += nw) {
         BState &s = st[p];
-        if (s.cg_done != CG_RUN) continue;
+        if (s.ph != PH_CG) continue;
         const double pq = warp_ordered_sum(part, inst[p].chunk0, inst[p].n_chunks, 1, 0);
         if (lane == 0) {
             s.pq = pq;
@@ -549,7 +558,7 @@ __global__ void __launch_bounds__(kBB)
     count_launch(ctl);
     for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
         const int p = unit_inst[u];
-        if (st[p].cg_done != CG_RUN) continue;  // uniform across the block
+        if (st[p].ph != PH_CG) continue;  // uniform across the block
         const TT alpha = (TT)st[p].alpha, beta = (TT)st[p].beta;
         double rz = 0.0, rr = 0.0;
         for (int t = 0; t < kUnitTiles; ++t) {
@@ -593,7 +602,7 @@ __global__ void __launch_bounds__(kBB)
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
     for (int p = warp; p < n_inst; p += nw) {
         BState &s = st[p];
-        if (s.cg_done != CG_RUN) continue;
+        if (s.ph != PH_CG) continue;
         const double rz_new = warp_ordered_sum(part, inst[p].unit0, inst[p].n_units, 2, 0);
         const double rr_new = warp_ordered_sum(part, inst[p].unit0, inst[p].n_units, 2, 1);
         if (lane != 0) continue;
@@ -606,6 +615,7 @@ __global__ void __launch_bounds__(kBB)
         else if (sqrt(rr_new) < s.atol_eff) done = CG_CONV;
         else if (s.cg_iter >= s.cg_maxit) done = CG_MAXIT;
         s.cg_done = done;
+        if (done != CG_RUN) s.ph = PH_EXTRACT;
         if (done == CG_RUN) atomicOr(&s_any, 1);
     }
     __syncthreads();
@@ -629,7 +639,7 @@ __global__ void __launch_bounds__(kBB)
     count_launch(ctl);
     for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
         const int p = unit_inst[u];
-        if (!st[p].active) continue;  // uniform across the block
+        if (st[p].ph != PH_EXTRACT) continue;  // uniform across the block
         double fh = 0.0;
         for (int t = 0; t < kUnitTiles; ++t) {
             const int64_t i = u * kUnit + t * kBB + threadIdx.x;
@@ -647,19 +657,21 @@ __global__ void __launch_bounds__(kBB)
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
     for (int p = warp; p < n_inst; p += nw) {
         BState &s = st[p];
-        if (!s.active) continue;
+        if (s.ph != PH_EXTRACT) continue;
         const double g0 = warp_ordered_sum(part, inst[p].unit0, inst[p].n_units, 1, 0);
         if (lane != 0) continue;
         s.cg_total += s.cg_iter;
         if (s.cg_done == CG_NAN) {
             s.status = SNP_NAN_DETECTED;
             s.active = 0;
+            s.ph = PH_DONE;
             s.it += 1;
             continue;
         }
         if (s.cg_done == CG_PIVOT) {
             s.status = SNP_ZERO_PIVOT;
             s.active = 0;
+            s.ph = PH_DONE;
             continue;
         }
         s.g0 = s.line_search ? g0 : 0.0;
@@ -670,6 +682,7 @@ __global__ void __launch_bounds__(kBB)
         s.g_hi = 0.0;
         s.ls_it = 0;
         s.run = 1;
+        s.ph = PH_LS;
         atomicOr(&s_any, 1);
     }
     __syncthreads();
@@ -704,7 +717,7 @@ __global__ void __launch_bounds__(kBB)
     count_launch(ctl);
     for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
         const int p = unit_inst[u];
-        if (!st[p].active) continue;
+        if (st[p].ph != PH_ACCEPT) continue;
         for (int t = 0; t < kUnitTiles; ++t) {
             const int64_t i = u * kUnit + t * kBB + threadIdx.x;
             x[i] = xw[i];
@@ -716,7 +729,7 @@ __global__ void __launch_bounds__(kBB)
     const bool stop_all = ctl->passes >= kMaxPasses;
     for (int p = threadIdx.x; p < n_inst; p += blockDim.x) {
         BState &s = st[p];
-        if (!s.active) continue;
+        if (s.ph != PH_ACCEPT) continue;
         s.fn = sqrt(s.f2);
         s.it += 1;
         if (!(s.fn == s.fn)) {
@@ -728,6 +741,7 @@ __global__ void __launch_bounds__(kBB)
             s.status = SNP_NOT_CONVERGED;
             s.active = 0;
         }
+        s.ph = s.active ? PH_HEAD : PH_DONE;
         if (s.active) atomicOr(&s_any, 1);
     }
     __syncthreads();
@@ -735,6 +749,39 @@ __global__ void __launch_bounds__(kBB)
         ctl->any_active = s_any;
         if (use_cond) cudaGraphSetConditional(cond, s_any ? 1u : 0u);
     }
+}
+
+// Whether any problem stands at `phase` (PH_LIVE: any problem not done): the condition of the
+// next IF node (or of the loop's WHILE node), and the host-driven loop's flag.  With PH_LIVE it
+// also counts the loop's passes and, past kMaxPasses, stops every problem.
+__global__ void k_b_flag(int n_inst, BState *st, int phase, BCtl *ctl, int use_cond, cudaGraphConditionalHandle cond) {
+    __shared__ int s_any;
+    count_launch(ctl);
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    const bool stop = phase == PH_LIVE && ctl->passes >= kMaxPasses;
+    for (int p = threadIdx.x; p < n_inst; p += blockDim.x) {
+        BState &s = st[p];
+        if (stop && s.ph != PH_DONE) {
+            s.status = SNP_NOT_CONVERGED;
+            s.active = 0;
+            s.run = 0;
+            s.ph = PH_DONE;
+        }
+        const bool hit = phase == PH_LIVE ? s.ph != PH_DONE : s.ph == phase;
+        if (hit) atomicOr(&s_any, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (phase == PH_LIVE) ctl->passes += 1;
+        ctl->any_phase[phase] = s_any;
+        if (use_cond) cudaGraphSetConditional(cond, s_any ? 1u : 0u);
+    }
+}
+
+// every problem takes part in the next assembly (the autotuner's timing of it)
+__global__ void k_b_set_run(int n_inst, BState *st) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_inst; p += gridDim.x * blockDim.x) st[p].run = 1;
 }
 
 // ---------------------------------------------------------------- batch build
@@ -868,7 +915,13 @@ struct snp_batch {
         snp::k_b_zero_run<<<grid_units(), snp::kBB, 0, s>>>(unit_inst.p, n_units, st.p, x.p, ctl.p);
         SNP_LAUNCH_CHECK();
         SNP_TRY(assemble<TT>(x.p, s));
-        SNP_TRY(sum<snp::SUM_DROP>(s, use_cond, newton));
+        SNP_TRY(sum<snp::SUM_DROP>(s, 0, 0));
+        return flag(s, snp::PH_LIVE, use_cond, newton);
+    }
+
+    int flag(cudaStream_t s, int phase, int use_cond, cudaGraphConditionalHandle c) {
+        snp::k_b_flag<<<1, 256, 0, s>>>(count, st.p, phase, ctl.p, use_cond, c);
+        SNP_LAUNCH_CHECK();
         return SNP_OK;
     }
 
@@ -885,7 +938,7 @@ struct snp_batch {
         SNP_LAUNCH_CHECK();
         snp::k_b_pcg_init<TT><<<grid_units(), snp::kBB, 0, s>>>(count, inst.p, unit_inst.p, n_units, free_mask.p, F.p,
                                                                 diag.p, meta.p, binv.p, Gp<TT>(), Rp<TT>(), st.p,
-                                                                part.p, ctl.p, use_cond, cg);
+                                                                part.p, ctl.p, 0, 0);
         SNP_LAUNCH_CHECK();
         return SNP_OK;
     }
@@ -976,11 +1029,11 @@ struct snp_batch {
         return SNP_OK;
     }
 
-    int add_while(Seq &q, cudaGraphConditionalHandle hnd, Seq *body) {
+    int add_cond(Seq &q, cudaGraphConditionalHandle hnd, cudaGraphConditionalNodeType type, Seq *body) {
         cudaGraphNodeParams cp = {};
         cp.type = cudaGraphNodeTypeConditional;
         cp.conditional.handle = hnd;
-        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.type = type;
         cp.conditional.size = 1;
         cudaGraphNode_t node;
         SNP_CUDA_TRY(cudaGraphAddNode(&node, q.g, q.tail.empty() ? nullptr : q.tail.data(), q.tail.size(), &cp));
@@ -990,27 +1043,44 @@ struct snp_batch {
         return SNP_OK;
     }
 
+    // One pass of the solver's loop as graph nodes in `nb`: for each phase, a flag kernel and an
+    // IF node over that phase's kernels; then the loop's own condition.
+    template <typename TT>
+    int build_pass(Seq &nb, cudaStream_t cs, const cudaGraphConditionalHandle *hp, cudaGraphConditionalHandle hn) {
+        const int phases[5] = {snp::PH_HEAD, snp::PH_CG, snp::PH_EXTRACT, snp::PH_LS, snp::PH_ACCEPT};
+        for (int k = 0; k < 5; ++k) {
+            const int ph = phases[k];
+            SNP_TRY(capture(nb, cs, [&](cudaStream_t s) { return flag(s, ph, 1, hp[k]); }));
+            Seq body;
+            SNP_TRY(add_cond(nb, hp[k], cudaGraphCondTypeIf, &body));
+            SNP_TRY(capture(body, cs, [&](cudaStream_t s) { return phase_body<TT>(ph, s); }));
+        }
+        return capture(nb, cs, [&](cudaStream_t s) { return flag(s, snp::PH_LIVE, 1, hn); });
+    }
+
+    // the kernels of one phase (host loop and graph alike)
+    template <typename TT>
+    int phase_body(int ph, cudaStream_t s) {
+        switch (ph) {
+            case snp::PH_HEAD: return phase_step_head<TT>(s, 0, 0);
+            case snp::PH_CG: return phase_cg_body<TT>(s, 0, 0);
+            case snp::PH_EXTRACT: return phase_extract<TT>(s, 0, 0);
+            case snp::PH_LS: return phase_ls_body<TT>(s, 0, 0);
+            default: return phase_accept(s, 0, 0);
+        }
+    }
+
     template <typename TT>
     int build_graph_t(cudaGraph_t g, cudaStream_t cs) {
-        cudaGraphConditionalHandle hn, hc, hl;
+        cudaGraphConditionalHandle hn, hp[5];
         SNP_CUDA_TRY(cudaGraphConditionalHandleCreate(&hn, g, 0, 0));
-        SNP_CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, g, 0, 0));
-        SNP_CUDA_TRY(cudaGraphConditionalHandleCreate(&hl, g, 0, 0));
+        for (auto &h : hp) SNP_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
         Seq top;
         top.g = g;
         SNP_TRY(capture(top, cs, [&](cudaStream_t s) { return phase_start<TT>(s, 1, hn); }));
         Seq nb;
-        SNP_TRY(add_while(top, hn, &nb));
-        SNP_TRY(capture(nb, cs, [&](cudaStream_t s) { return phase_step_head<TT>(s, 1, hc); }));
-        Seq cb;
-        SNP_TRY(add_while(nb, hc, &cb));
-        SNP_TRY(capture(cb, cs, [&](cudaStream_t s) { return phase_cg_body<TT>(s, 1, hc); }));
-        SNP_TRY(capture(nb, cs, [&](cudaStream_t s) { return phase_extract<TT>(s, 1, hl); }));
-        Seq lb;
-        SNP_TRY(add_while(nb, hl, &lb));
-        SNP_TRY(capture(lb, cs, [&](cudaStream_t s) { return phase_ls_body<TT>(s, 1, hl); }));
-        SNP_TRY(capture(nb, cs, [&](cudaStream_t s) { return phase_accept(s, 1, hn); }));
-        return SNP_OK;
+        SNP_TRY(add_cond(top, hn, cudaGraphCondTypeWhile, &nb));
+        return build_pass<TT>(nb, cs, hp, hn);
     }
 
     template <typename TT>
@@ -1055,20 +1125,14 @@ struct snp_batch {
     int run_host_loop() {
         SNP_TRY(phase_start<TT>(stream, 0, 0));
         SNP_TRY(read_ctl());
-        for (int pass = 0; hctl.p->any_active && pass < snp::kMaxPasses; ++pass) {
-            SNP_TRY(phase_step_head<TT>(stream, 0, 0));
-            SNP_TRY(read_ctl());
-            while (hctl.p->any_cg) {
-                for (int k = 0; k < 16; ++k) SNP_TRY(phase_cg_body<TT>(stream, 0, 0));
+        const int phases[5] = {snp::PH_HEAD, snp::PH_CG, snp::PH_EXTRACT, snp::PH_LS, snp::PH_ACCEPT};
+        while (hctl.p->any_phase[snp::PH_LIVE]) {
+            for (int ph : phases) {
+                SNP_TRY(flag(stream, ph, 0, 0));
                 SNP_TRY(read_ctl());
+                if (hctl.p->any_phase[ph]) SNP_TRY(phase_body<TT>(ph, stream));
             }
-            SNP_TRY(phase_extract<TT>(stream, 0, 0));
-            SNP_TRY(read_ctl());
-            while (hctl.p->any_ls) {
-                SNP_TRY(phase_ls_body<TT>(stream, 0, 0));
-                SNP_TRY(read_ctl());
-            }
-            SNP_TRY(phase_accept(stream, 0, 0));
+            SNP_TRY(flag(stream, snp::PH_LIVE, 0, 0));
             SNP_TRY(read_ctl());
         }
         return SNP_OK;
@@ -1161,6 +1225,8 @@ int tune_t(snp_batch *b) {
             best_b = blocks[k];
         }
     }
+    k_b_set_run<<<(b->count + 127) / 128, 128, 0, s>>>(b->count, b->st.p);
+    SNP_LAUNCH_CHECK();
     double best_a = 1e300;
     int best_w = b->asm_waves;
     for (int wv = 1; wv <= 2; ++wv) {
