@@ -120,6 +120,11 @@ struct CurlArgs {
     double dil[4];
 };
 
+// Give every kernel node of `body` an L2 access policy window over [base, base + bytes) with
+// persisting hits (the slot values the element pass writes and the DoF pass reads), raising the
+// context's persisting set-aside to cover it as far as the device allows; SNP_L2_PERSIST=0 skips.
+void l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes);
+
 // Launch the fused assembly for one material.  Tables must be affine (checked by the caller).
 int launch_curlcurl(const CurlArgs &a, cudaStream_t st);
 
