@@ -635,8 +635,11 @@ def assembly_microbench(reps=5, warmup=3, seed=5, grid=(120, 120, 116)):
     x ~ N(0, 1e-3), seeded 40% iron flags (PCHIP atan B-H) against air, no Dirichlet mask,
     4-point rule, float64.  Two Newton assemblies at x are timed (CUDA events, after warm-up):
 
-    * csr: the drop-in path, J = K + dK scattered into the fixed CSR through the slot map
-      plus the residual F (``snp_solver_assemble``, the value zeroing included);
+    * csr: the drop-in path, J = K + dK into the fixed CSR plus the residual F
+      (``snp_solver_assemble``): element records, then one gather per CSR row writing each value
+      once (deterministic); ``csr_atomic``: the same outputs from the element kernel that adds
+      into the CSR through the slot map with float64 atomics (``SNP_ASSEMBLY=atomic``, the value
+      zeroing included);
     * tensors: the matrix-free path of the Newton loop, S_e per element plus F and diag(J)
       summed per DoF (``snp_solver_assemble_tensors``).
 
@@ -659,6 +662,11 @@ def assembly_microbench(reps=5, warmup=3, seed=5, grid=(120, 120, 116)):
     E, N, n = msh.num_elements, msh.nodes.shape[0], msh.num_dofs
     asm = CurlCurlAssembler(msh, [M.TAG_IRON, M.TAG_AIR], [MAT.atan_reluctance(), S.ConstantReluctance(1e7 / (4 * np.pi))])
     eng = DeviceNewton(asm, np.ones(n, dtype=np.uint8), (), quad_order=2)
+    os.environ["SNP_ASSEMBLY"] = "atomic"
+    try:
+        eng_atomic = DeviceNewton(asm, np.ones(n, dtype=np.uint8), (), quad_order=2)
+    finally:
+        del os.environ["SNP_ASSEMBLY"]
     nnz = eng.pattern.nnz
     x = upload(np.random.default_rng(seed).normal(0.0, 1e-3, n), np.float64)
     J = zeros(nnz)
@@ -680,6 +688,8 @@ def assembly_microbench(reps=5, warmup=3, seed=5, grid=(120, 120, 116)):
 
     ms_csr = timed(lambda: _lib.call("snp_solver_assemble", eng.handle, _lib.ptr(x), None, _lib.ptr(J), None,
                                      _lib.ptr(F), _lib.stream_ptr()))
+    ms_atomic = timed(lambda: _lib.call("snp_solver_assemble", eng_atomic.handle, _lib.ptr(x), None, _lib.ptr(J), None,
+                                        _lib.ptr(F), _lib.stream_ptr()))
     ms_t = timed(lambda: eng.assemble_tensors(x, "fp64", F))
     peak, peak_kind = measured_peaks()
     b_csr = E * (16 + 24 + 4 + 144) + 24 * N + 8 * n + 8 * nnz + 8 * n
@@ -687,11 +697,11 @@ def assembly_microbench(reps=5, warmup=3, seed=5, grid=(120, 120, 116)):
     out = {"workload": f"Kuhn grid {grid[0]}x{grid[1]}x{grid[2]} x 6 = {E} tets, {N} nodes, {n} edge DoFs, nnz {nnz}, "
                        f"40% iron, x ~ N(0, 1e-3), Q=4, f64",
            "setup_s": setup_s, "peak_gbs": peak, "peak_kind": peak_kind}
-    for name, ms, b in (("csr", ms_csr, b_csr), ("tensors", ms_t, b_t)):
+    for name, ms, b in (("csr", ms_csr, b_csr), ("csr_atomic", ms_atomic, b_csr), ("tensors", ms_t, b_t)):
         gbs = b / (ms / 1e3) / 1e9
         out[name] = {"ms": ms, "gelem_per_s": E / (ms / 1e3) / 1e9, "bytes": b, "achieved_gbs": gbs,
                      "frac": gbs / peak}
-    del eng, asm, J, F, x
+    del eng, eng_atomic, asm, J, F, x
     return out
 
 

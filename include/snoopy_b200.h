@@ -131,6 +131,45 @@ int snp_curlcurl_rhs_red(int64_t n_elems, const double *nodes, const int32_t *ce
                          const double *B_s, int32_t n_int, const double *rel_c, const double *rel_x,
                          double *rhs, void *stream);
 
+/* Deterministic two-phase form of snp_curlcurl_assemble[_diluted] over a whole pattern (same
+ * element arithmetic, fem_c/ctools.c:960-1388 and 1565-1759; the reference's sum over
+ * elements happens in scipy's COO->CSR conversion, fem_c/interface_c.pyx:365-368).
+ *
+ * Phase 1, once per material: snp_curlcurl_terms writes one record per element of
+ * [elem_offset, elem_offset + n_elems) into terms (record e at terms + e * stride doubles,
+ * e counted over the pattern's elements; stride from snp_curlcurl_terms_stride).  `parts`
+ * (SNP_TERMS_* bits) selects what the records hold: the reference-frame element tensors of
+ * K, dK or J = K + dK, the element vector of the residual F = K(x) x - rhs(x), the element
+ * vector of the reduced rhs.  phi and dilution as for snp_curlcurl_assemble_diluted (both
+ * NULL: plain steel).
+ *
+ * Phase 2, once: snp_curlcurl_rows forms every CSR row from the records of the elements
+ * incident to it, in element order, with no atomics, and OVERWRITES each requested output
+ * (no zeroing needed): K_vals needs SNP_TERMS_K, dK_vals SNP_TERMS_DK, J_vals SNP_TERMS_J or
+ * both K and DK (then J = K + dK per entry, as the reference's dK + K), J32_vals likewise
+ * (float32), F needs SNP_TERMS_F, rhs SNP_TERMS_RHS (elements without a source field give 0).
+ * Results are bitwise repeatable.  Needs a pattern built with 6 DoFs per element whose longest
+ * row has at most SNP_ROWS_MAX_ENTRIES entries (snp_curlcurl_rows_supported). */
+#define SNP_TERMS_K 1
+#define SNP_TERMS_DK 2
+#define SNP_TERMS_J 4
+#define SNP_TERMS_F 8
+#define SNP_TERMS_RHS 16
+#define SNP_ROWS_MAX_ENTRIES 64
+int snp_curlcurl_terms_stride(int32_t parts, int32_t *stride);
+int snp_curlcurl_rows_supported(const snp_pattern *pat, int32_t *supported);
+int snp_curlcurl_terms(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems,
+                       const double *nodes, const int32_t *cells, const int32_t *glob_ids,
+                       const int32_t *orientations, const double *curls, int32_t n_orient,
+                       const double *phi, const double *d_phi, const double *w, int32_t n_quad,
+                       const double *x, const double *B_s,
+                       int32_t n_int, const double *rel_c, const double *rel_x, const double *dilution,
+                       int32_t parts, double *terms, void *stream);
+int snp_curlcurl_rows(const snp_pattern *pat, const double *terms, int32_t parts,
+                      const double *curls, int32_t n_orient, int32_t n_quad,
+                      double *K_vals, double *dK_vals, double *J_vals, float *J32_vals,
+                      double *rhs, double *F, void *stream);
+
 /* ------------------------------------------------------------------ grad-grad assembly
  * Replaces fem_c.compute_stiffness_and_jacobi_matrix (fem_c/interface_c.pyx:11-160)
  * -> compute_K_dK (fem_c/ctools.c:730-919).  P1 nodal elements [elem_offset, +n_elems)

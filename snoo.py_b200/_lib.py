@@ -25,6 +25,9 @@ class SnpError(RuntimeError):
         self.status = status
 
 
+# parts of the two-phase curl-curl assembly's element records (SNP_TERMS_* in the header)
+TERMS_K, TERMS_DK, TERMS_J, TERMS_F, TERMS_RHS = 1, 2, 4, 8, 16
+
 STATUS = {0: "SNP_OK", 1: "SNP_BAD_ARG", 2: "SNP_CUDA_ERROR", 3: "SNP_NOT_CONVERGED", 4: "SNP_NAN_DETECTED",
           5: "SNP_ZERO_PIVOT", 6: "SNP_NO_MEMORY"}
 
@@ -72,6 +75,11 @@ _SIGS = {
                                       _vp, _vp, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snp_curlcurl_assemble_f32": [_vp, _c_i64, _c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp,
                                   _c_i32, _vp, _vp, _vp, _vp],
+    "snp_curlcurl_terms_stride": [_c_i32, ctypes.POINTER(_c_i32)],
+    "snp_curlcurl_rows_supported": [_vp, ctypes.POINTER(_c_i32)],
+    "snp_curlcurl_terms": [_vp, _c_i64, _c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _vp, _c_i32, _vp, _vp,
+                           _c_i32, _vp, _vp, _vp, _c_i32, _vp, _vp],
+    "snp_curlcurl_rows": [_vp, _vp, _c_i32, _vp, _c_i32, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snp_curlcurl_rhs_red": [_c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp,
                              _vp, _vp],
     "snp_gradgrad_assemble": [_vp, _c_i64, _c_i64, _vp, _vp, _vp, _vp, _c_i32, _vp, _c_i32, _c_i32, _c_i32, _vp, _vp,

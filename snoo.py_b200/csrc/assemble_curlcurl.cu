@@ -359,18 +359,26 @@ __global__ void k_check_affine(const double *curls, int n_orient, const double *
 //   (K x)_j = chat_j . (kfac Jm^T Jm bh),   rhs_j = chat_j . (Jm^T sum_q rq B_s,q).
 // One pass over the quadrature points; S_e and the six element terms of F and of diag(J)
 // are written once per element (no atomics; the DoF sums follow in a fixed order).
-// Element tensors of one element e of a material (the loop body of k_curlcurl_tensor): S_e into
-// T and the six F and diag(J) terms into a.Fe / a.De, all at eslot(a.t_offset + e, .).  The
-// tables sit in shared memory (s_*), wsum = sum of the weights.
-template <bool HAS_BS, int NQ, typename TT, bool DIL>
-__device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, const double *s_ctab,
-                                               const double *s_dphi, const double *s_w, const double *s_phi,
-                                               const double *s_relc, const double *s_relx, double wsum,
-                                               TT *__restrict__ T) {
+// What the element kernels of the Newton system share about one element e of a material:
+// the map Jm, the reference-frame curl of the discrete field bh (Jm bh = det B_element) as
+// cb = Jm bh, kfac = sum_q nu_q w_q / det, M = sum_q a_q B_q B_q^T with
+// a_q = [|B_q| >= 1e-14] nu'_q w_q / (det |B_q|), Rs = sum_q (nu0 - nu_q) w_q B_s,q, and the
+// element's reference curls ct (its orientation's table in shared memory).
+struct ElemCore {
+    double Jm[9], cb[3], kfac, M[6], Rs[3];
+    const double *ct;
+    int orient;
+};
+
+template <bool HAS_BS, int NQ, bool DIL>
+__device__ __forceinline__ void elem_core(const CurlArgs &a, int64_t e, const double *s_ctab, const double *s_dphi,
+                                          const double *s_w, const double *s_phi, const double *s_relc,
+                                          const double *s_relx, double wsum, ElemCore &c) {
     const int nq = NQ > 0 ? NQ : a.nq;
     const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
     const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
-    double Jm[9], Zn[4];
+    double *Jm = c.Jm;
+    double Zn[4];
 #pragma unroll
     for (int r = 0; r < 9; ++r) Jm[r] = 0.0;
 #pragma unroll
@@ -390,7 +398,9 @@ __device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, con
     const double det = Jm[0] * (Jm[4] * Jm[8] - Jm[7] * Jm[5]) - Jm[1] * (Jm[3] * Jm[8] - Jm[5] * Jm[6]) +
                        Jm[2] * (Jm[3] * Jm[7] - Jm[4] * Jm[6]);
     const double idet = 1.0 / det;
-    const double *ct = s_ctab + __ldg(a.orient + e) * 18;
+    c.orient = __ldg(a.orient + e);
+    const double *ct = s_ctab + c.orient * 18;
+    c.ct = ct;
     int g[6];
     {
         const int2 *gp = reinterpret_cast<const int2 *>(a.gids + 6 * e);
@@ -406,17 +416,18 @@ __device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, con
         bh[1] += ct[3 * j + 1] * xj;
         bh[2] += ct[3 * j + 2] * xj;
     }
-    double cb[3];  // Jm bh = det * B_element
+    double *cb = c.cb;  // Jm bh = det * B_element
 #pragma unroll
     for (int r = 0; r < 3; ++r) cb[r] = Jm[3 * r] * bh[0] + Jm[3 * r + 1] * bh[1] + Jm[3 * r + 2] * bh[2];
     const double Bc[3] = {cb[0] * idet, cb[1] * idet, cb[2] * idet};
 
-    double kfac, M[6], Rs[3] = {0.0, 0.0, 0.0};
+    double *M = c.M, *Rs = c.Rs;
+    Rs[0] = Rs[1] = Rs[2] = 0.0;
     if constexpr (!HAS_BS) {
         const double bm = sqrt(Bc[0] * Bc[0] + Bc[1] * Bc[1] + Bc[2] * Bc[2]);
         double dnu;
         const double nu = pchip_eval<double>(a.n_int, s_relc, s_relx, bm, dnu);
-        kfac = nu * wsum * idet;
+        c.kfac = nu * wsum * idet;
         const double af = (bm >= 1e-14) ? dnu * wsum * idet / bm : 0.0;
         M[0] = af * Bc[0] * Bc[0];
         M[1] = af * Bc[0] * Bc[1];
@@ -425,7 +436,7 @@ __device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, con
         M[4] = af * Bc[1] * Bc[2];
         M[5] = af * Bc[2] * Bc[2];
     } else {
-        kfac = 0.0;
+        double kfac = 0.0;
 #pragma unroll
         for (int t = 0; t < 6; ++t) M[t] = 0.0;
         const double *bs = a.Bs + (int64_t)e * nq * 3;
@@ -450,32 +461,49 @@ __device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, con
             Rs[1] += rq * s1;
             Rs[2] += rq * s2;
         }
-        kfac *= idet;
+        c.kfac = kfac * idet;
     }
-    // A = kfac I + M;  P = A Jm;  S = Jm^T P
-    const double A[9] = {kfac + M[0], M[1], M[2], M[1], kfac + M[3], M[4], M[2], M[4], kfac + M[5]};
+}
+
+// Jm^T A Jm of a symmetric A (a: xx xy xz yy yz zz) into S (same order)
+__device__ __forceinline__ void congruence(const double *Jm, const double (&A)[9], double (&S)[6]) {
     double P[9];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int c = 0; c < 3; ++c) P[3 * r + c] = A[3 * r] * Jm[c] + A[3 * r + 1] * Jm[3 + c] + A[3 * r + 2] * Jm[6 + c];
+    int t = 0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = r; c < 3; ++c) S[t++] = Jm[r] * P[c] + Jm[3 + r] * P[3 + c] + Jm[6 + r] * P[6 + c];
+}
+
+// Element tensors of one element e of a material (the loop body of k_curlcurl_tensor): S_e into
+// T and the six F and diag(J) terms into a.Fe / a.De, all at eslot(a.t_offset + e, .).  The
+// tables sit in shared memory (s_*), wsum = sum of the weights.
+template <bool HAS_BS, int NQ, typename TT, bool DIL>
+__device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, const double *s_ctab,
+                                               const double *s_dphi, const double *s_w, const double *s_phi,
+                                               const double *s_relc, const double *s_relx, double wsum,
+                                               TT *__restrict__ T) {
+    ElemCore c;
+    elem_core<HAS_BS, NQ, DIL>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, c);
+    const double *Jm = c.Jm, *M = c.M, *cb = c.cb, *Rs = c.Rs, *ct = c.ct;
+    const double kfac = c.kfac;
+    // A = kfac I + M;  S = Jm^T A Jm
+    const double A[9] = {kfac + M[0], M[1], M[2], M[1], kfac + M[3], M[4], M[2], M[4], kfac + M[5]};
     double S[6];
-    {
-        int t = 0;
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int c = r; c < 3; ++c) S[t++] = Jm[r] * P[c] + Jm[3 + r] * P[3 + c] + Jm[6 + r] * P[6 + c];
-    }
+    congruence(Jm, A, S);
     const int64_t eb = eslot(a.t_offset + e, 0);
 #pragma unroll
     for (int t = 0; t < 6; ++t) T[eb + 32 * t] = (TT)S[t];
     // G = kfac Jm^T (Jm bh) - Jm^T Rs;  F_j = chat_j . G
     double G[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-        G[c] = kfac * (Jm[c] * cb[0] + Jm[3 + c] * cb[1] + Jm[6 + c] * cb[2]) -
-               (Jm[c] * Rs[0] + Jm[3 + c] * Rs[1] + Jm[6 + c] * Rs[2]);
+    for (int cc = 0; cc < 3; ++cc)
+        G[cc] = kfac * (Jm[cc] * cb[0] + Jm[3 + cc] * cb[1] + Jm[6 + cc] * cb[2]) -
+                (Jm[cc] * Rs[0] + Jm[3 + cc] * Rs[1] + Jm[6 + cc] * Rs[2]);
 #pragma unroll
     for (int j = 0; j < 6; ++j) {
         const double h0 = ct[3 * j], h1 = ct[3 * j + 1], h2 = ct[3 * j + 2];
@@ -485,6 +513,83 @@ __device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, con
         a.Fe[eb + 32 * j] = h0 * G[0] + h1 * G[1] + h2 * G[2];
         a.De[eb + 32 * j] = h0 * sh0 + h1 * sh1 + h2 * sh2;
     }
+}
+
+// Record of one element for the two-phase assembly (TermLayout parts), at rec.
+template <bool HAS_BS, int NQ, bool DIL>
+__device__ __forceinline__ void terms_element(const CurlArgs &a, int64_t e, const double *s_ctab,
+                                              const double *s_dphi, const double *s_w, const double *s_phi,
+                                              const double *s_relc, const double *s_relx, double wsum,
+                                              const TermLayout &L, double *__restrict__ rec) {
+    ElemCore c;
+    elem_core<HAS_BS, NQ, DIL>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, c);
+    const double *Jm = c.Jm, *M = c.M, *cb = c.cb, *Rs = c.Rs;
+    const double kfac = c.kfac;
+    if (L.k >= 0) {
+        const double A[9] = {kfac, 0.0, 0.0, 0.0, kfac, 0.0, 0.0, 0.0, kfac};
+        double S[6];
+        congruence(Jm, A, S);
+#pragma unroll
+        for (int t = 0; t < 6; ++t) rec[L.k + t] = S[t];
+    }
+    if (L.d >= 0) {
+        const double A[9] = {M[0], M[1], M[2], M[1], M[3], M[4], M[2], M[4], M[5]};
+        double S[6];
+        congruence(Jm, A, S);
+#pragma unroll
+        for (int t = 0; t < 6; ++t) rec[L.d + t] = S[t];
+    }
+    if (L.j >= 0) {
+        const double A[9] = {kfac + M[0], M[1], M[2], M[1], kfac + M[3], M[4], M[2], M[4], kfac + M[5]};
+        double S[6];
+        congruence(Jm, A, S);
+#pragma unroll
+        for (int t = 0; t < 6; ++t) rec[L.j + t] = S[t];
+    }
+    double R[3];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) R[cc] = Jm[cc] * Rs[0] + Jm[3 + cc] * Rs[1] + Jm[6 + cc] * Rs[2];
+    if (L.f >= 0) {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) rec[L.f + cc] = kfac * (Jm[cc] * cb[0] + Jm[3 + cc] * cb[1] + Jm[6 + cc] * cb[2]) - R[cc];
+    }
+    if (L.r >= 0) {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) rec[L.r + cc] = R[cc];
+    }
+    rec[L.o] = (double)c.orient;
+}
+
+template <bool HAS_BS, int NQ, bool DIL>
+__global__ void __launch_bounds__(kBlock)
+    k_curlcurl_terms(CurlArgs a, int quad_stride_ctab, TermLayout L, double *__restrict__ terms) {
+    extern __shared__ double sm[];
+    const SmemLayout SL = smem_layout(a.n_orient, a.nq, a.n_int);
+    double *s_ctab = sm + SL.off_ctab;
+    double *s_dphi = sm + SL.off_dphi;
+    double *s_w = sm + SL.off_w;
+    double *s_phi = sm + SL.off_phi;
+    double *s_relc = sm + SL.off_relc;
+    double *s_relx = sm + SL.off_relx;
+    for (int t = threadIdx.x; t < a.n_orient * 18; t += blockDim.x) {
+        int o = t / 18, r = t - o * 18;
+        s_ctab[t] = a.ctab[(int64_t)o * quad_stride_ctab + r];
+    }
+    for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = a.dphi0[t];
+    for (int t = threadIdx.x; t < a.nq; t += blockDim.x) s_w[t] = a.w[t];
+    if (a.phi)
+        for (int t = threadIdx.x; t < 4 * a.nq; t += blockDim.x) s_phi[t] = a.phi[t];
+    const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
+    const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
+    for (int t = threadIdx.x; t < nx; t += blockDim.x) s_relx[t] = (a.n_int < 0) ? 0.0 : a.rel_x[t];
+    __syncthreads();
+    const int nq = NQ > 0 ? NQ : a.nq;
+    double wsum = 0.0;
+    for (int q = 0; q < nq; ++q) wsum += s_w[q];
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x)
+        terms_element<HAS_BS, NQ, DIL>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, L,
+                                       terms + e * (int64_t)L.stride);
 }
 
 template <bool HAS_BS, int NQ, typename TT, bool DIL>
@@ -664,6 +769,51 @@ int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st) {
     return launch_tensor<float>(a, a.T32, st, smem, qstride);
 }
 
+TermLayout term_layout(int parts) {
+    TermLayout L;
+    int o = 0;
+    if (parts & SNP_TERMS_K) { L.k = o; o += 6; }
+    if (parts & SNP_TERMS_DK) { L.d = o; o += 6; }
+    if (parts & SNP_TERMS_J) { L.j = o; o += 6; }
+    if (parts & SNP_TERMS_F) { L.f = o; o += 3; }
+    if (parts & SNP_TERMS_RHS) { L.r = o; o += 3; }
+    L.o = o;
+    L.stride = o + 1;
+    return L;
+}
+
+template <bool HAS_BS, int NQ, bool DIL = false>
+static int launch_terms_t(const CurlArgs &a, const TermLayout &L, double *terms, cudaStream_t st, size_t smem,
+                          int qstride) {
+    if (a.n_elems == 0) return SNP_OK;
+    auto kern = k_curlcurl_terms<HAS_BS, NQ, DIL>;
+    if (smem > 48 * 1024) SNP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<wave_grid(kern, a.n_elems, kBlock, smem), kBlock, smem, st>>>(a, qstride, L, terms);
+    SNP_LAUNCH_CHECK();
+    return SNP_OK;
+}
+
+int launch_curlcurl_terms(const CurlArgs &a, const TermLayout &L, double *terms, cudaStream_t st) {
+    SNP_REQUIRE(terms != nullptr || a.n_elems == 0, "element records: terms is NULL");
+    const SmemLayout SL = smem_layout(a.n_orient, a.nq, a.n_int);
+    const size_t smem = sizeof(double) * (size_t)SL.total;
+    SNP_REQUIRE(smem <= 200 * 1024, "curl-curl assembly: tables need %zu bytes of shared memory (max 200 KiB)", smem);
+    const int qs = a.nq * 18;
+    if (a.Bs == nullptr) {
+        if (a.nq == 1) return launch_terms_t<false, 1>(a, L, terms, st, smem, qs);
+        if (a.nq == 4) return launch_terms_t<false, 4>(a, L, terms, st, smem, qs);
+        return launch_terms_t<false, 0>(a, L, terms, st, smem, qs);
+    }
+    if (a.phi) {
+        if (a.nq == 4) return launch_terms_t<true, 4, true>(a, L, terms, st, smem, qs);
+        return launch_terms_t<true, 0, true>(a, L, terms, st, smem, qs);
+    }
+    if (a.nq == 1) return launch_terms_t<true, 1>(a, L, terms, st, smem, qs);
+    if (a.nq == 4) return launch_terms_t<true, 4>(a, L, terms, st, smem, qs);
+    if (a.nq == 5) return launch_terms_t<true, 5>(a, L, terms, st, smem, qs);
+    return launch_terms_t<true, 0>(a, L, terms, st, smem, qs);
+}
+
 template <int NQ, typename TT>
 static int launch_batch_t(const BatchSeg *segs, const BatchAsmItem *items, int n_items, int max_n_int,
                           const double *ctab, int n_orient, int qstride, const double *dphi0, const double *w, int nq,
@@ -701,7 +851,7 @@ int launch_curlcurl_tensor_batch(const BatchSeg *segs, const BatchAsmItem *items
                                      x, run, run_stride, static_cast<double *>(T), Fe, De, grid, smem, st);
 }
 
-static int fill_args(CurlArgs &a, const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,
+int fill_args(CurlArgs &a, const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,
                      const int32_t *cells, const int32_t *glob_ids, const int32_t *orientations, const double *curls,
                      int32_t n_orient, const double *d_phi, const double *w, int32_t n_quad, const double *x,
                      const double *B_s, int32_t n_int, const double *rel_c, const double *rel_x) {

@@ -65,10 +65,79 @@ __global__ void k_fill_i32(int32_t *p, int64_t n, int32_t v) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) p[t] = v;
 }
 
+// (DoF, e * 8 + k) pairs of every element's DoFs, counted per row
+__global__ void k_inc_pairs(const int32_t *__restrict__ dofs, int64_t n_elems, uint32_t *__restrict__ key,
+                            int32_t *__restrict__ val, int32_t *__restrict__ cnt) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_elems * 6; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = t / 6;
+        const int k = (int)(t - e * 6);
+        const int32_t r = dofs[t];
+        key[t] = (uint32_t)r;
+        val[t] = (int32_t)((e << 3) | k);
+        atomicAdd(cnt + r, 1);
+    }
+}
+
+__global__ void k_max_row(int32_t n, const int32_t *__restrict__ rp, int *__restrict__ mx) {
+    int m = 0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int len = rp[r + 1] - rp[r];
+        m = len > m ? len : m;
+    }
+    atomicMax(mx, m);
+}
+
 int bits_for(uint32_t v) {
     int b = 0;
     while (b < 32 && (1ull << b) <= v) ++b;
     return b;
+}
+
+// Row incidence lists (the two-phase assembly's gather order) and the longest row.  Built for
+// 6 DoFs per element and fewer than 2^28 elements (the e * 8 + k word); otherwise left empty.
+int build_incidence(snp_pattern *P, const int32_t *elem_dofs, cudaStream_t st) {
+    const int32_t n = P->n_rows;
+    {
+        DevBuf<int> mx;
+        SNP_TRY(mx.alloc(1));
+        SNP_CUDA_TRY(cudaMemsetAsync(mx.p, 0, sizeof(int), st));
+        k_max_row<<<stride_grid(n, 256, 4), 256, 0, st>>>(n, P->row_ptr.p, mx.p);
+        SNP_LAUNCH_CHECK();
+        int h = 0;
+        SNP_CUDA_TRY(cudaMemcpyAsync(&h, mx.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SNP_CUDA_TRY(cudaStreamSynchronize(st));
+        P->max_row = h;
+    }
+    if (P->dpe != 6 || P->n_elems >= ((int64_t)1 << 28)) return SNP_OK;
+    const int64_t m = P->n_elems * 6;
+    SNP_TRY(P->inc_ptr.alloc((size_t)n + 1));
+    SNP_TRY(P->inc.alloc(m > 0 ? m : 1));
+    SNP_CUDA_TRY(cudaMemsetAsync(P->inc_ptr.p, 0, sizeof(int32_t) * ((size_t)n + 1), st));
+    if (m > 0) {
+        DevBuf<uint32_t> key, key2;
+        DevBuf<int32_t> val2;
+        DevBuf<unsigned char> temp;
+        SNP_TRY(key.alloc(m));
+        SNP_TRY(key2.alloc(m));
+        SNP_TRY(val2.alloc(m));
+        k_inc_pairs<<<stride_grid(m, 256, 16), 256, 0, st>>>(elem_dofs, P->n_elems, key.p, P->inc.p, P->inc_ptr.p);
+        SNP_LAUNCH_CHECK();
+        const int end_bit = bits_for((uint32_t)n);
+        cub::DoubleBuffer<uint32_t> dk(key.p, key2.p);
+        cub::DoubleBuffer<int32_t> dv(P->inc.p, val2.p);
+        size_t tb_sort = 0, tb_scan = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, dk, dv, m, 0, end_bit > 0 ? end_bit : 1, st);
+        cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, P->inc_ptr.p, P->inc_ptr.p, n + 1, st);
+        SNP_TRY(temp.alloc(tb_sort > tb_scan ? tb_sort : tb_scan));
+        // LSD radix sort is stable: within a row the pairs keep their element order
+        SNP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.p, tb_sort, dk, dv, m, 0, end_bit > 0 ? end_bit : 1, st));
+        if (dv.Current() != P->inc.p)
+            SNP_CUDA_TRY(cudaMemcpyAsync(P->inc.p, dv.Current(), sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, st));
+        SNP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp.p, tb_scan, P->inc_ptr.p, P->inc_ptr.p, n + 1, st));
+        SNP_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    P->has_incidence = true;
+    return SNP_OK;
 }
 
 }  // namespace
@@ -152,6 +221,7 @@ int pattern_create(const int32_t *elem_dofs, int64_t n_elems, int32_t dpe, int32
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: %s", cudaGetErrorString(e)));
+    if ((rc = build_incidence(P, elem_dofs, st))) return cleanup_fail(rc);
     *out = P;
     return SNP_OK;
 }

@@ -125,6 +125,13 @@ struct CurlArgs {
 // context's persisting set-aside to cover it as far as the device allows; SNP_L2_PERSIST=0 skips.
 void l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes);
 
+// Validate the inputs of a curl-curl launch over elements [elem_offset, +n_elems) of `pat` (may
+// be NULL) and fill `a` (slots offset to the range; outputs unset).
+int fill_args(CurlArgs &a, const snp_pattern *pat, int64_t elem_offset, int64_t n_elems, const double *nodes,
+              const int32_t *cells, const int32_t *glob_ids, const int32_t *orientations, const double *curls,
+              int32_t n_orient, const double *d_phi, const double *w, int32_t n_quad, const double *x,
+              const double *B_s, int32_t n_int, const double *rel_c, const double *rel_x);
+
 // Launch the fused assembly for one material.  Tables must be affine (checked by the caller).
 int launch_curlcurl(const CurlArgs &a, cudaStream_t st);
 
@@ -157,6 +164,35 @@ int launch_curlcurl_tensor_batch(const BatchSeg *segs, const BatchAsmItem *items
 // the element terms of diag(J) and of F = K(x) x - rhs(x).  Tables must be affine.
 int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st);
 
+// Per-element record of the two-phase (deterministic) assembly into a CSR pattern.  Parts, in
+// this order when present (reference-frame symmetric tensors as xx xy xz yy yz zz; vectors in
+// the reference frame, so that an element edge k with reference curl chat_k of the element's
+// orientation gets K_e,kl = chat_k . SK chat_l, F_e,k = chat_k . G and so on):
+//   SNP_TERMS_K   SK = kfac Jm^T Jm                     (6)
+//   SNP_TERMS_DK  SdK = Jm^T M Jm                        (6)
+//   SNP_TERMS_J   SJ = Jm^T (kfac I + M) Jm              (6)
+//   SNP_TERMS_F   G  = kfac Jm^T Jm bh - Jm^T Rs         (3)
+//   SNP_TERMS_RHS R  = Jm^T Rs                           (3)
+// and last the element's orientation index (stored as a double).
+struct TermLayout {
+    int stride = 1;
+    int k = -1, d = -1, j = -1, f = -1, r = -1, o = 0;
+};
+TermLayout term_layout(int parts);
+
+// Phase 1: the records of one material's elements, record e at terms + e * L.stride.
+int launch_curlcurl_terms(const CurlArgs &a, const TermLayout &L, double *terms, cudaStream_t st);
+
+// Phase 2: every row of `pat` formed from the records of its incident elements, in the rows'
+// incidence order (no atomics; bitwise repeatable); each requested output is overwritten.
+// J = K + dK per entry when the records hold SK and SdK, else from SJ.
+int launch_curlcurl_rows(const snp_pattern *pat, const double *terms, const TermLayout &L, const double *ctab,
+                         int n_orient, int quad_stride_ctab, double *K, double *dK, double *J, float *J32, double *rhs,
+                         double *F, cudaStream_t st);
+
+// Whether launch_curlcurl_rows can serve the pattern (incidence lists built, rows short enough).
+bool rows_supported(const snp_pattern *pat);
+
 // Validate that d_phi and curls do not vary across quadrature points; sets *affine.
 int check_affine_tables(const double *curls, int32_t n_orient, const double *d_phi, int32_t nq, cudaStream_t st,
                         bool *affine);
@@ -182,6 +218,11 @@ struct snp_pattern {
     int64_t n_elems = 0;
     int32_t dpe = 0;
     snp::DevBuf<int32_t> row_ptr, col_idx, slots, diag_pos;
+    // incidence lists of the rows (6 DoFs per element, fewer than 2^28 elements): row r's
+    // (element, local DoF) pairs as e * 8 + k in element order, inc[inc_ptr[r] .. inc_ptr[r + 1])
+    snp::DevBuf<int32_t> inc_ptr, inc;
+    int32_t max_row = 0;  // entries of the longest row
+    bool has_incidence = false;
 };
 
 namespace snp {

@@ -234,6 +234,9 @@ struct snp_solver {
     bool use_sell = false;
     snp::ElemTopology etop;
     snp::DevBuf<double> T64, Jdiag, Fe, De, rsys_scratch;
+    // two-phase CSR assembly (element records, then one gather per row)
+    bool rows_asm = false;
+    snp::DevBuf<double> terms;
     // Galerkin correction of a warm start (snp_solver_set_galerkin_basis): basis, its system
     // and coefficients on the device and in pinned memory, and a copy of x to fall back to
     const float *gal_V = nullptr;
@@ -427,6 +430,7 @@ struct snp_solver {
         const bool newton_j = sell_order && layout != SNP_LAYOUT_ELEM;
         if (Jv == J.p) j_valid[0] = newton_j;
         if (J32v == J32.p) j_valid[1] = newton_j;
+        if (!so && rows_asm) return assemble_rows(x, Kv, Jv, J32v, rhsv, Fv);
         if (Kv) SNP_CUDA_TRY(cudaMemsetAsync(Kv, 0, sizeof(double) * nnz, stream));
         if (Jv) SNP_CUDA_TRY(cudaMemsetAsync(Jv, 0, sizeof(double) * nnz, stream));
         if (J32v) SNP_CUDA_TRY(cudaMemsetAsync(J32v, 0, sizeof(float) * nnz, stream));
@@ -462,6 +466,52 @@ struct snp_solver {
             SNP_TRY(snp::launch_curlcurl(a, stream));
             if (m->count) ++launches;
         }
+        if (Fv && has_extra) {
+            snp::k_sub<<<snp::stride_grid(n, snp::kVB, 4), snp::kVB, 0, stream>>>(n, Fv, rhs_extra.p);
+            SNP_LAUNCH_CHECK();
+            ++launches;
+        }
+        return SNP_OK;
+    }
+
+    // CSR assembly in two phases: each material's element records, then every row gathered
+    // from its elements' records (bitwise repeatable; each output overwritten once)
+    int assemble_rows(const double *x, double *Kv, double *Jv, float *J32v, double *rhsv, double *Fv) {
+        int parts = 0;
+        if (Kv) parts |= SNP_TERMS_K | ((Jv || J32v) ? SNP_TERMS_DK : 0);
+        else if (Jv || J32v) parts |= SNP_TERMS_J;
+        if (Fv) parts |= SNP_TERMS_F;
+        if (rhsv) parts |= SNP_TERMS_RHS;
+        const snp::TermLayout L = snp::term_layout(parts);
+        const size_t need = (size_t)pat->n_elems * (size_t)L.stride;
+        if (terms.n < need) SNP_TRY(terms.alloc(need));
+        for (auto &m : mats) {
+            snp::CurlArgs a{};
+            a.n_elems = m->count;
+            a.nodes = nodes.p;
+            a.cells = m->cells.p;
+            a.gids = m->gids.p;
+            a.orient = m->orient.p;
+            a.ctab = curls.p;
+            a.n_orient = n_orient;
+            a.dphi0 = dphi.p;
+            a.w = w.p;
+            a.nq = nq;
+            a.x = x;
+            a.Bs = m->has_bs ? m->Bs.p : nullptr;
+            a.n_int = m->n_int;
+            a.rel_c = m->relc.p;
+            a.rel_x = m->relx.p;
+            if (m->diluted && m->has_bs) {
+                a.phi = m->phi.p;
+                for (int i = 0; i < 4; ++i) a.dil[i] = m->dil[i];
+            }
+            SNP_TRY(snp::launch_curlcurl_terms(a, L, terms.p + m->offset * (int64_t)L.stride, stream));
+            if (m->count) ++launches;
+        }
+        SNP_TRY(snp::launch_curlcurl_rows(pat, terms.p, L, curls.p, n_orient, nq * 18, Kv, nullptr, Jv, J32v, rhsv, Fv,
+                                          stream));
+        ++launches;
         if (Fv && has_extra) {
             snp::k_sub<<<snp::stride_grid(n, snp::kVB, 4), snp::kVB, 0, stream>>>(n, Fv, rhs_extra.p);
             SNP_LAUNCH_CHECK();
@@ -854,6 +904,11 @@ int snp_solver_finalize(snp_solver *s) {
                                          cudaMemcpyDeviceToDevice, st));
     SNP_TRY(snp::pattern_create(all.p, E, 6, s->n, st, &s->pat));
     int64_t nnz = s->pat->nnz;
+    // CSR assembly: deterministic row gather (default) or element atomics (SNP_ASSEMBLY=atomic)
+    {
+        const char *ea = getenv("SNP_ASSEMBLY");
+        s->rows_asm = snp::rows_supported(s->pat) && !(ea && std::string(ea) == "atomic");
+    }
     // Newton-loop Jacobian layout: SNP_JACOBIAN = elem (default) | csr | sell
     const char *env = getenv("SNP_JACOBIAN");
     const std::string want = env ? env : "elem";

@@ -4,11 +4,17 @@ The reference gathers per-material cells and edge ids from gmsh (``:19-137``), a
 Newton step re-queries element orientations from gmsh, re-creates reference tables, calls
 the C kernel per material, converts triplets to CSR and adds the matrices (``:815-932``).
 Here the mesh arrays, tables and one CSR pattern over all materials are uploaded once and
-cached; each call is one kernel launch per material into that pattern.
+cached.  Each call writes one record per element (one launch per material) and then forms
+every CSR row from the records of its elements in element order (one launch): the values are
+bitwise repeatable and each is written once.  ``SNP_ASSEMBLY=atomic`` (or ``method="atomic"``)
+selects the one-launch-per-material kernels that add element values into the CSR with atomics.
 
 ``mesh`` is a ``snoopy_b200.mesh.TetMesh`` (gmsh is not a dependency); ``volume_tags`` are
 its volume tags, in the order of ``material_list``.
 """
+
+import ctypes
+import os
 
 import numpy as np
 
@@ -109,10 +115,13 @@ class CurlCurlAssembler:
         return out
 
     def assemble_device(self, x, quad_order=2, source_fields=(), K=True, J=True, rhs=True, F=False, dK=False,
-                        stream=None):
+                        stream=None, method=None):
         """Assemble on the device into the cached pattern.
 
         :param x: float64 DoF vector (numpy or CUDA tensor).
+        :param method: ``"rows"`` (element records, then one gather per CSR row: deterministic),
+            ``"atomic"`` (element kernels adding into the CSR), or None: ``$SNP_ASSEMBLY``, else
+            rows where the pattern allows it.
         :return: dict of CUDA tensors ``K``, ``J`` (= K + dK), ``dK`` [nnz], ``rhs``, ``F`` [n]
             (those requested), plus ``pattern``.
         """
@@ -122,18 +131,59 @@ class CurlCurlAssembler:
         x_d = x if hasattr(x, "data_ptr") else upload(x, np.float64)
         bs = self.upload_source_fields(source_fields)
         out = {"pattern": pat}
+        method = method or os.environ.get("SNP_ASSEMBLY", "rows")
+        s = _lib.stream_ptr(stream)
+        if method != "atomic" and pat.rows_supported:
+            t = torch()
+            for key, want, size in (("K", K, pat.nnz), ("J", J, pat.nnz), ("dK", dK, pat.nnz),
+                                    ("rhs", rhs, self.num_dofs), ("F", F, self.num_dofs)):
+                out[key] = t.empty(max(size, 1), dtype=t.float64, device="cuda") if want else None
+            parts = ((_lib.TERMS_K if (K or J) else 0) | (_lib.TERMS_DK if (dK or J) else 0)
+                     | (_lib.TERMS_F if F else 0) | (_lib.TERMS_RHS if rhs else 0))
+            stride = ctypes.c_int32()
+            _lib.call("snp_curlcurl_terms_stride", parts, ctypes.byref(stride))
+            need = pat.n_elems * stride.value
+            if d.get("terms") is None or d["terms"].numel() < need:
+                d["terms"] = t.empty(max(need, 1), dtype=t.float64, device="cuda")
+            for n, m in enumerate(d["mats"]):
+                n_int, rc, rx = d["rel"][n]
+                coef = self._dilution_coef(n)
+                _lib.call("snp_curlcurl_terms", pat.handle, m["offset"], m["count"], _lib.ptr(d["nodes"]),
+                          _lib.ptr(m["cells"]), _lib.ptr(m["gids"]), _lib.ptr(m["orient"]), _lib.ptr(tb.curls_d),
+                          tb.n_orient, _lib.ptr(tb.phi_d) if coef is not None else None, _lib.ptr(tb.d_phi_d),
+                          _lib.ptr(tb.w_d), tb.nq, _lib.ptr(x_d), _lib.ptr(bs[n]), n_int, _lib.ptr(rc), _lib.ptr(rx),
+                          coef, parts, _lib.ptr(d["terms"]), s)
+            _lib.call("snp_curlcurl_rows", pat.handle, _lib.ptr(d["terms"]), parts, _lib.ptr(tb.curls_d), tb.n_orient,
+                      tb.nq, _lib.ptr(out["K"]), _lib.ptr(out["dK"]), _lib.ptr(out["J"]), None, _lib.ptr(out["rhs"]),
+                      _lib.ptr(out["F"]), s)
+            for key, want, size in (("K", K, pat.nnz), ("J", J, pat.nnz), ("dK", dK, pat.nnz),
+                                    ("rhs", rhs, self.num_dofs), ("F", F, self.num_dofs)):
+                if want:
+                    out[key] = out[key][:size]
+            return out
         for key, want, size in (("K", K, pat.nnz), ("J", J, pat.nnz), ("dK", dK, pat.nnz), ("rhs", rhs, self.num_dofs),
                                 ("F", F, self.num_dofs)):
             out[key] = zeros(size) if want else None
-        s = _lib.stream_ptr(stream)
         for n, m in enumerate(d["mats"]):
             n_int, rc, rx = d["rel"][n]
-            _lib.call("snp_curlcurl_assemble", pat.handle, m["offset"], m["count"], _lib.ptr(d["nodes"]),
-                      _lib.ptr(m["cells"]), _lib.ptr(m["gids"]), _lib.ptr(m["orient"]), _lib.ptr(tb.curls_d),
-                      tb.n_orient, _lib.ptr(tb.d_phi_d), _lib.ptr(tb.w_d), tb.nq, _lib.ptr(x_d), _lib.ptr(bs[n]),
-                      n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(out["K"]), _lib.ptr(out["dK"]), _lib.ptr(out["J"]),
-                      _lib.ptr(out["rhs"]), _lib.ptr(out["F"]), s)
+            coef = self._dilution_coef(n)
+            common = (pat.handle, m["offset"], m["count"], _lib.ptr(d["nodes"]), _lib.ptr(m["cells"]),
+                      _lib.ptr(m["gids"]), _lib.ptr(m["orient"]), _lib.ptr(tb.curls_d), tb.n_orient)
+            outs = (_lib.ptr(out["K"]), _lib.ptr(out["dK"]), _lib.ptr(out["J"]), _lib.ptr(out["rhs"]),
+                    _lib.ptr(out["F"]), s)
+            if coef is None:
+                _lib.call("snp_curlcurl_assemble", *common, _lib.ptr(tb.d_phi_d), _lib.ptr(tb.w_d), tb.nq,
+                          _lib.ptr(x_d), _lib.ptr(bs[n]), n_int, _lib.ptr(rc), _lib.ptr(rx), *outs)
+            else:
+                _lib.call("snp_curlcurl_assemble_diluted", *common, _lib.ptr(tb.phi_d), _lib.ptr(tb.d_phi_d),
+                          _lib.ptr(tb.w_d), tb.nq, _lib.ptr(x_d), _lib.ptr(bs[n]), n_int, _lib.ptr(rc), _lib.ptr(rx),
+                          coef, *outs)
         return out
+
+    def _dilution_coef(self, n):
+        """Dilution coefficients {c_num, m_num, c_den, m_den} of material ``n`` as a ctypes array,
+        or None for plain steel and air (the diluted assembler overrides this)."""
+        return None
 
     # ---------------------------------------------------------------- reference API
     def compute_stiffness_and_jacobi_matrix_c(self, x, quad_order=2, source_fields=[], device=False):

@@ -69,6 +69,9 @@ class Pattern:
         self.row_ptr = t.as_tensor(_CudaArray(rp.value, self.n_rows + 1, "<i4", self), device=dev)
         self.col_idx = t.as_tensor(_CudaArray(ci.value, max(self.nnz, 1), "<i4", self), device=dev)[: self.nnz]
         self.diag_pos = t.as_tensor(_CudaArray(dg.value, self.n_rows, "<i4", self), device=dev)
+        sup = ctypes.c_int32()
+        _lib.call("snp_curlcurl_rows_supported", self.handle, ctypes.byref(sup))
+        self.rows_supported = bool(sup.value)
 
     def to_scipy(self, values, drop_zeros=False):
         """Host scipy ``csr_array`` with this pattern and the given device values."""

@@ -11,6 +11,7 @@ reference's solvers make with ``element_order=1``.
 """
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -71,6 +72,43 @@ def compute_stiffness_and_jacobi_matrix(nodes, cells, d_phi, x, permeability, q,
     return pat.to_scipy(K), pat.to_scipy(dK)
 
 
+def _curlcurl_K_dK_rhs(pat, num_el, num_dofs, nodes_d, cells_d, gids_d, or_d, curls_d, n_orient, phi_d, dphi_d, w_d,
+                       nq, x_d, bs_d, n_int, rc, rx, dil):
+    """K, dK and the reduced rhs of all elements of ``pat`` (device float64).  Element records and
+    one gather per CSR row (deterministic) where the pattern allows it and ``SNP_ASSEMBLY`` is not
+    ``atomic``; otherwise the element kernel adding into the CSR (diluted when ``dil`` is set)."""
+    if pat.rows_supported and os.environ.get("SNP_ASSEMBLY", "rows") != "atomic":
+        t = torch()
+        parts = _lib.TERMS_K | _lib.TERMS_DK | _lib.TERMS_RHS
+        stride = ctypes.c_int32()
+        _lib.call("snp_curlcurl_terms_stride", parts, ctypes.byref(stride))
+        terms = t.empty(max(num_el * stride.value, 1), dtype=t.float64, device="cuda")
+        K = t.empty(max(pat.nnz, 1), dtype=t.float64, device="cuda")
+        dK = t.empty(max(pat.nnz, 1), dtype=t.float64, device="cuda")
+        rhs = t.empty(max(num_dofs, 1), dtype=t.float64, device="cuda")
+        _lib.call("snp_curlcurl_terms", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d), _lib.ptr(gids_d),
+                  _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(phi_d) if dil is not None else None,
+                  _lib.ptr(dphi_d), _lib.ptr(w_d), nq, _lib.ptr(x_d), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx),
+                  dil, parts, _lib.ptr(terms), _lib.stream_ptr())
+        _lib.call("snp_curlcurl_rows", pat.handle, _lib.ptr(terms), parts, _lib.ptr(curls_d), n_orient, nq,
+                  _lib.ptr(K), _lib.ptr(dK), None, None, _lib.ptr(rhs), None, _lib.stream_ptr())
+        return K[: pat.nnz], dK[: pat.nnz], rhs
+    K = zeros(pat.nnz)
+    dK = zeros(pat.nnz)
+    rhs = zeros(num_dofs)
+    if dil is None:
+        _lib.call("snp_curlcurl_assemble", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d),
+                  _lib.ptr(gids_d), _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(dphi_d), _lib.ptr(w_d), nq,
+                  _lib.ptr(x_d), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(K), _lib.ptr(dK), None,
+                  _lib.ptr(rhs), None, _lib.stream_ptr())
+    else:
+        _lib.call("snp_curlcurl_assemble_diluted", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d),
+                  _lib.ptr(gids_d), _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(phi_d), _lib.ptr(dphi_d),
+                  _lib.ptr(w_d), nq, _lib.ptr(x_d), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), dil,
+                  _lib.ptr(K), _lib.ptr(dK), None, _lib.ptr(rhs), None, _lib.stream_ptr())
+    return K, dK, rhs
+
+
 def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls, d_phi, orientations, x, B_s,
                                                   reluctance, q, w, num_dofs, num_el_dofs, device=False):
     """Curl-curl stiffness matrix, Jacobian correction and reduced rhs (``interface_c.pyx:162-374``).
@@ -96,15 +134,10 @@ def compute_stiffness_and_jacobi_matrix_curl_curl(nodes, cells, glob_ids, curls,
     B_s = np.asarray(B_s)
     bs_d = upload(B_s, np.float64) if B_s.size > 0 else None
     n_orient = int(np.asarray(curls).size // (nq * 18))
-    K = zeros(pat.nnz)
-    dK = zeros(pat.nnz)
-    rhs = zeros(int(num_dofs))
     nodes_d, or_d, curls_d = upload(nodes, np.float64), upload(orientations, np.int32), upload(curls, np.float64)
     dphi_d, w_d, x_d = upload(d_phi, np.float64), upload(w, np.float64), upload(x, np.float64)
-    _lib.call("snp_curlcurl_assemble", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d), _lib.ptr(gids_d),
-              _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(dphi_d), _lib.ptr(w_d), nq, _lib.ptr(x_d),
-              _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), _lib.ptr(K), _lib.ptr(dK), None, _lib.ptr(rhs), None,
-              _lib.stream_ptr())
+    K, dK, rhs = _curlcurl_K_dK_rhs(pat, num_el, int(num_dofs), nodes_d, cells_d, gids_d, or_d, curls_d, n_orient,
+                                    None, dphi_d, w_d, nq, x_d, bs_d, n_int, rc, rx, None)
     if device:
         return pat.to_torch(K), pat.to_torch(dK), rhs[: int(num_dofs)]
     return pat.to_scipy(K), pat.to_scipy(dK), rhs[: int(num_dofs)].cpu().numpy()
@@ -140,16 +173,11 @@ def compute_stiffness_and_jacobi_matrix_curl_curl_diluted(nodes, cells, glob_ids
     B_s = np.asarray(B_s)
     bs_d = upload(B_s, np.float64) if B_s.size > 0 else None
     dil = (ctypes.c_double * 4)(dilution.c_num, dilution.m_num, dilution.c_den, dilution.m_den)
-    K = zeros(pat.nnz)
-    dK = zeros(pat.nnz)
-    rhs = zeros(int(num_dofs))
     nodes_d, or_d, curls_d = upload(nodes, np.float64), upload(orientations, np.int32), upload(curls, np.float64)
     phi_d, dphi_d, w_d, x_d = (upload(phi, np.float64), upload(d_phi, np.float64), upload(w, np.float64),
                                upload(x, np.float64))
-    _lib.call("snp_curlcurl_assemble_diluted", pat.handle, 0, num_el, _lib.ptr(nodes_d), _lib.ptr(cells_d),
-              _lib.ptr(gids_d), _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(phi_d), _lib.ptr(dphi_d),
-              _lib.ptr(w_d), nq, _lib.ptr(x_d), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx), dil, _lib.ptr(K),
-              _lib.ptr(dK), None, _lib.ptr(rhs), None, _lib.stream_ptr())
+    K, dK, rhs = _curlcurl_K_dK_rhs(pat, num_el, int(num_dofs), nodes_d, cells_d, gids_d, or_d, curls_d, n_orient,
+                                    phi_d, dphi_d, w_d, nq, x_d, bs_d, n_int, rc, rx, dil)
     if device:
         return pat.to_torch(K), pat.to_torch(dK), rhs[: int(num_dofs)]
     return pat.to_scipy(K), pat.to_scipy(dK), rhs[: int(num_dofs)].cpu().numpy()
