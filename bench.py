@@ -52,6 +52,12 @@ def parse():
     ap.add_argument("--warm-start-family", action="store_true",
                     help="only the learned-warm-start study on the 300k-tet morphed family "
                          "(4000 training / 500 held-out members); prints its own JSON line")
+    ap.add_argument("--assembly-grid", type=int, default=0, metavar="G",
+                    help="only the assembly microbenchmark on a G x G x round(G*116/120) grid x 6 tets "
+                         "(120: the 10M-tet configuration); prints its own JSON line")
+    ap.add_argument("--gemm", type=int, nargs=3, default=None, metavar=("M", "N", "K"),
+                    help="only the surrogate's BF16 tensor-core GEMM C = A B^T at M x N x K; prints its "
+                         "own JSON line")
     return ap.parse_args()
 
 
@@ -1058,9 +1064,62 @@ def run_warm_start_family(args):
     print(json.dumps(line), flush=True)
 
 
+def run_assembly_grid(a):
+    g = a.assembly_grid
+    out = assembly_microbench(reps=max(a.steps, 1), warmup=max(a.warmup, 1), grid=(g, g, max(2, round(g * 116 / 120))))
+    print(json.dumps({"metric": "assembly microbenchmark", **out}), flush=True)
+
+
+def run_gemm(a):
+    """snp_gemm_bf16 (tcgen05 MMA, TMA-fed) on seeded BF16 operands: CUDA-event time per call
+    after warm-up and dense TFLOP/s (2 M N K per call) against the measured BF16 peak."""
+    import torch
+
+    from snoopy_b200 import _lib
+
+    M, N, K = a.gemm
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    C = torch.empty(M, N, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def call():
+        _lib.call("snp_gemm_bf16", M, N, K, _lib.ptr(A), K, _lib.ptr(B), K, None, 0, _lib.ptr(C), N, None, N,
+                  _lib.ptr(err), _lib.stream_ptr())
+
+    for _ in range(max(a.warmup, 1)):
+        call()
+    reps = max(a.steps, 1) * 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ms = e0.elapsed_time(e1) / reps
+    ref = A.float() @ B.float().T
+    rel = float(((C - ref).abs().max() / ref.abs().max()).item())
+    tf = 2.0 * M * N * K / (ms / 1e3) / 1e12
+    peak = None
+    try:
+        pk = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")))
+        peak = pk.get("bf16_tflops")
+    except Exception:
+        pass
+    print(json.dumps({"metric": "bf16 GEMM", "M": M, "N": N, "K": K, "ms": ms, "tflops": tf,
+                      "peak_tflops": peak, "frac": (tf / peak) if peak else None, "max_rel_err_vs_fp32": rel}),
+          flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.warm_start_family:
+    if a.assembly_grid:
+        run_assembly_grid(a)
+    elif a.gemm:
+        run_gemm(a)
+    elif a.warm_start_family:
         run_warm_start_family(a)
     elif a.batched:
         run_batched(a)

@@ -11,8 +11,10 @@
  *   - Every function returns an snp_status; snp_last_error() gives the message of the
  *     calling thread's last failure.  The reference's C returns void and prints
  *     (fem_c/ctools.c:428, fem_c/interface_c.pyx:71,234,952-959).
- *   - Assembly entry points ACCUMULATE (+=) into their outputs, like the reference's
- *     `K += this_K` per material (snoopy/curl_curl_assembler.py:928-930): zero first.
+ *   - The single-launch assembly entry points ACCUMULATE (+=) into their outputs, like the
+ *     reference's `K += this_K` per material (snoopy/curl_curl_assembler.py:928-930): zero
+ *     first.  The two-phase curl-curl assembly (snp_curlcurl_terms + snp_curlcurl_rows)
+ *     overwrites its outputs.
  *
  * Table layouts are the reference C kernels' (fem_c/ctools.c):
  *   nodes[N][3]; cells[E][4]; glob_ids[E][6]; orientations[E];
@@ -138,17 +140,19 @@ int snp_curlcurl_rhs_red(int64_t n_elems, const double *nodes, const int32_t *ce
  * Phase 1, once per material: snp_curlcurl_terms writes one record per element of
  * [elem_offset, elem_offset + n_elems) into terms (record e at terms + e * stride doubles,
  * e counted over the pattern's elements; stride from snp_curlcurl_terms_stride).  `parts`
- * (SNP_TERMS_* bits) selects what the records hold: the reference-frame element tensors of
- * K, dK or J = K + dK, the element vector of the residual F = K(x) x - rhs(x), the element
- * vector of the reduced rhs.  phi and dilution as for snp_curlcurl_assemble_diluted (both
- * NULL: plain steel).
+ * (SNP_TERMS_* bits) selects what the records hold: the element map and nu-weight from which
+ * K's entries are formed with the reference kernels' arithmetic (kfac (c_j . c_k)) and the
+ * tensor of dK (SNP_TERMS_K, SNP_TERMS_DK), the reference-frame tensor of J = K + dK alone
+ * (SNP_TERMS_J, for Jacobian-only assembly), the element vector of the residual
+ * F = K(x) x - rhs(x), the element vector of the reduced rhs.  phi and dilution as for
+ * snp_curlcurl_assemble_diluted (both NULL: plain steel).
  *
  * Phase 2, once: snp_curlcurl_rows forms every CSR row from the records of the elements
  * incident to it, in element order, with no atomics, and OVERWRITES each requested output
- * (no zeroing needed): K_vals needs SNP_TERMS_K, dK_vals SNP_TERMS_DK, J_vals SNP_TERMS_J or
- * both K and DK (then J = K + dK per entry, as the reference's dK + K), J32_vals likewise
- * (float32), F needs SNP_TERMS_F, rhs SNP_TERMS_RHS (elements without a source field give 0).
- * Results are bitwise repeatable.  Needs a pattern built with 6 DoFs per element whose longest
+ * (no zeroing needed): K_vals needs SNP_TERMS_K (or DK), dK_vals SNP_TERMS_DK, J_vals either
+ * SNP_TERMS_DK (J = K + dK per entry, as the reference's dK + K; used whenever K or dK is
+ * requested too) or SNP_TERMS_J, J32_vals likewise (float32), F needs SNP_TERMS_F, rhs
+ * SNP_TERMS_RHS (elements without a source field give 0).  Results are bitwise repeatable.  Needs a pattern built with 6 DoFs per element whose longest
  * row has at most SNP_ROWS_MAX_ENTRIES entries (snp_curlcurl_rows_supported). */
 #define SNP_TERMS_K 1
 #define SNP_TERMS_DK 2
@@ -459,6 +463,15 @@ int snp_solver_reduced_system(snp_solver *s, int precision, const float *V, int3
  * reference-semantics mode keeps point Jacobi (red_mvp_solver.py:199 builds
  * M = diags(1 / diag(J))).  Synchronises (meta is checked and uploaded). */
 int snp_solver_set_block_jacobi(snp_solver *s, const uint16_t *meta);
+
+/* Krylov method of the residual-mode Newton steps (the reference's scipy cg in each Newton step,
+ * red_mvp_solver.py:199-203): SNP_KRYLOV_CG (default) or SNP_KRYLOV_GMRES, restarted GMRES(restart)
+ * with right preconditioning by the same block or point Jacobi, float64 only (a mixed-precision
+ * solve with GMRES returns SNP_BAD_ARG), matrix-free Jacobian layout.  Each Arnoldi step counts as
+ * one iteration in snp_solve_stats.cg_iterations. */
+#define SNP_KRYLOV_CG 0
+#define SNP_KRYLOV_GMRES 1
+int snp_solver_set_krylov(snp_solver *s, int32_t method, int32_t restart);
 
 /* z = M r (device float64 [n_dofs]) with the block Jacobi built from the element tensors of
  * the last snp_solver_assemble_tensors of that precision; *fallback_blocks (host, may be NULL)

@@ -526,18 +526,13 @@ __device__ __forceinline__ void terms_element(const CurlArgs &a, int64_t e, cons
     const double *Jm = c.Jm, *M = c.M, *cb = c.cb, *Rs = c.Rs;
     const double kfac = c.kfac;
     if (L.k >= 0) {
-        const double A[9] = {kfac, 0.0, 0.0, 0.0, kfac, 0.0, 0.0, 0.0, kfac};
-        double S[6];
-        congruence(Jm, A, S);
 #pragma unroll
-        for (int t = 0; t < 6; ++t) rec[L.k + t] = S[t];
+        for (int t = 0; t < 9; ++t) rec[L.k + t] = Jm[t];
+        rec[L.k + 9] = kfac;
     }
     if (L.d >= 0) {
-        const double A[9] = {M[0], M[1], M[2], M[1], M[3], M[4], M[2], M[4], M[5]};
-        double S[6];
-        congruence(Jm, A, S);
 #pragma unroll
-        for (int t = 0; t < 6; ++t) rec[L.d + t] = S[t];
+        for (int t = 0; t < 6; ++t) rec[L.d + t] = M[t];
     }
     if (L.j >= 0) {
         const double A[9] = {kfac + M[0], M[1], M[2], M[1], kfac + M[3], M[4], M[2], M[4], kfac + M[5]};
@@ -772,7 +767,7 @@ int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st) {
 TermLayout term_layout(int parts) {
     TermLayout L;
     int o = 0;
-    if (parts & SNP_TERMS_K) { L.k = o; o += 6; }
+    if (parts & (SNP_TERMS_K | SNP_TERMS_DK)) { L.k = o; o += 10; }
     if (parts & SNP_TERMS_DK) { L.d = o; o += 6; }
     if (parts & SNP_TERMS_J) { L.j = o; o += 6; }
     if (parts & SNP_TERMS_F) { L.f = o; o += 3; }

@@ -78,6 +78,22 @@ __global__ void k_inc_pairs(const int32_t *__restrict__ dofs, int64_t n_elems, u
     }
 }
 
+// inc_loc of every incidence of row r (rows no longer than 255 entries)
+__global__ void k_inc_loc(int32_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ inc_ptr,
+                          const int32_t *__restrict__ inc, const int32_t *__restrict__ slots, uint2 *__restrict__ loc) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t base = rp[r];
+        for (int32_t t = inc_ptr[r]; t < inc_ptr[r + 1]; ++t) {
+            const uint32_t u = (uint32_t)inc[t];
+            const int32_t *sl = slots + (int64_t)(u >> 3) * 36 + (u & 7u) * 6;
+            uint32_t lo = 0, hi = 0;
+            for (int b = 0; b < 4; ++b) lo |= (uint32_t)(sl[b] - base) << (8 * b);
+            for (int b = 4; b < 6; ++b) hi |= (uint32_t)(sl[b] - base) << (8 * (b - 4));
+            loc[t] = make_uint2(lo, hi);
+        }
+    }
+}
+
 __global__ void k_max_row(int32_t n, const int32_t *__restrict__ rp, int *__restrict__ mx) {
     int m = 0;
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
@@ -136,7 +152,16 @@ int build_incidence(snp_pattern *P, const int32_t *elem_dofs, cudaStream_t st) {
         SNP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp.p, tb_scan, P->inc_ptr.p, P->inc_ptr.p, n + 1, st));
         SNP_CUDA_TRY(cudaStreamSynchronize(st));
     }
-    P->has_incidence = true;
+    if (P->max_row <= 255) {
+        SNP_TRY(P->inc_loc.alloc(m > 0 ? m : 1));
+        if (m > 0) {
+            k_inc_loc<<<stride_grid(n, 256, 8), 256, 0, st>>>(n, P->row_ptr.p, P->inc_ptr.p, P->inc.p, P->slots.p,
+                                                              P->inc_loc.p);
+            SNP_LAUNCH_CHECK();
+            SNP_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+        P->has_incidence = true;
+    }
     return SNP_OK;
 }
 

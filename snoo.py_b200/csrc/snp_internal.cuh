@@ -165,14 +165,13 @@ int launch_curlcurl_tensor_batch(const BatchSeg *segs, const BatchAsmItem *items
 int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st);
 
 // Per-element record of the two-phase (deterministic) assembly into a CSR pattern.  Parts, in
-// this order when present (reference-frame symmetric tensors as xx xy xz yy yz zz; vectors in
-// the reference frame, so that an element edge k with reference curl chat_k of the element's
-// orientation gets K_e,kl = chat_k . SK chat_l, F_e,k = chat_k . G and so on):
-//   SNP_TERMS_K   SK = kfac Jm^T Jm                     (6)
-//   SNP_TERMS_DK  SdK = Jm^T M Jm                        (6)
-//   SNP_TERMS_J   SJ = Jm^T (kfac I + M) Jm              (6)
-//   SNP_TERMS_F   G  = kfac Jm^T Jm bh - Jm^T Rs         (3)
-//   SNP_TERMS_RHS R  = Jm^T Rs                           (3)
+// this order when present (symmetric tensors as xx xy xz yy yz zz; an element edge k with
+// reference curl chat_k of the element's orientation has the curl c_k = Jm chat_k):
+//   SNP_TERMS_K or _DK   Jm (9, row-major) and kfac (1): K_e,kl = kfac (c_k . c_l)
+//   SNP_TERMS_DK         M = sum_q a_q B_q B_q^T (6):    dK_e,kl = c_l . (M c_k)
+//   SNP_TERMS_J          SJ = Jm^T (kfac I + M) Jm (6):  J_e,kl = chat_l . (SJ chat_k)
+//   SNP_TERMS_F          G  = kfac Jm^T Jm bh - Jm^T Rs (3): F_e,k = chat_k . G
+//   SNP_TERMS_RHS        R  = Jm^T Rs (3):               rhs_e,k = chat_k . R
 // and last the element's orientation index (stored as a double).
 struct TermLayout {
     int stride = 1;
@@ -185,7 +184,7 @@ int launch_curlcurl_terms(const CurlArgs &a, const TermLayout &L, double *terms,
 
 // Phase 2: every row of `pat` formed from the records of its incident elements, in the rows'
 // incidence order (no atomics; bitwise repeatable); each requested output is overwritten.
-// J = K + dK per entry when the records hold SK and SdK, else from SJ.
+// With K or dK requested, J = K + dK per entry (Jm, kfac and M records); J alone from SJ.
 int launch_curlcurl_rows(const snp_pattern *pat, const double *terms, const TermLayout &L, const double *ctab,
                          int n_orient, int quad_stride_ctab, double *K, double *dK, double *J, float *J32, double *rhs,
                          double *F, cudaStream_t st);
@@ -221,6 +220,9 @@ struct snp_pattern {
     // incidence lists of the rows (6 DoFs per element, fewer than 2^28 elements): row r's
     // (element, local DoF) pairs as e * 8 + k in element order, inc[inc_ptr[r] .. inc_ptr[r + 1])
     snp::DevBuf<int32_t> inc_ptr, inc;
+    // per incidence (row r, element e, local DoF a): the positions in row r of e's six
+    // couplings (a, b), slot[e][a][b] - row_ptr[r], as bytes 0..5 (rows of at most 64 entries)
+    snp::DevBuf<uint2> inc_loc;
     int32_t max_row = 0;  // entries of the longest row
     bool has_incidence = false;
 };

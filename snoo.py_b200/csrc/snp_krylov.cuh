@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
+
 #include "snp_internal.cuh"
 
 namespace snp {
@@ -153,6 +155,10 @@ int block_jacobi_build(const ElemTopology &top, const TT *T, const uint8_t *free
 int block_jacobi_apply(int32_t n, const uint8_t *free_mask, const uint16_t *meta, const float *binv, const double *r,
                        double *z, cudaStream_t s);
 
+// z = r / diag on the free DoFs (0 elsewhere), float64 vectors.
+int point_jacobi_apply(int32_t n, const uint8_t *free_mask, const double *diag, const double *r, double *z,
+                       cudaStream_t s);
+
 // x += V coef on the free DoFs (V float32 [n][ldv], m columns; coef float64 [m], device).
 int basis_axpy(int32_t n, const uint8_t *free_mask, const float *V, int m, int64_t ldv, const double *coef,
                double *x, cudaStream_t s);
@@ -233,6 +239,25 @@ struct ElemPcg {
                     const float *bj_inv, cudaStream_t s, int *rc);
     DevBuf<unsigned long long> coop_bar;
     DevBuf<int> coop_err;
+};
+
+// Restarted GMRES(m), right-preconditioned, float64 (gmres.cu).  apply_J(x, y): y = J x on the
+// free DoFs; apply_M(r, z): z = M r (0 on constrained DoFs).  Solves J h = b_scale b from h = 0
+// to ||b_scale b - J h|| <= max(rtol ||b_scale b||, atol) or maxit Arnoldi steps; *status is
+// SNP_OK, SNP_NOT_CONVERGED or SNP_NAN_DETECTED.
+struct Gmres {
+    using Op = std::function<int(const double *, double *)>;
+    int64_t n = -1;
+    int m = 0;
+    int blocks = 0;
+    int64_t launches = 0;
+    DevBuf<double> V, w, z, part, hdev;
+    DevBuf<unsigned int> counter;
+    HostBuf<double> hhost;
+    int reserve(int64_t n, int m);
+    int solve(const Op &apply_J, const Op &apply_M, const uint8_t *free_mask, const double *b, double b_scale,
+              double *x, double rtol, double atol, int64_t maxit, cudaStream_t s, int64_t *its, double *res,
+              int *status);
 };
 
 // The view of a finalized solver (SNP_BAD_ARG when it is not finalized).  Valid while the

@@ -237,6 +237,9 @@ struct snp_solver {
     // two-phase CSR assembly (element records, then one gather per row)
     bool rows_asm = false;
     snp::DevBuf<double> terms;
+    // Krylov method of the residual-mode Newton steps (snp_solver_set_krylov): 0 CG, 1 GMRES(restart)
+    int krylov = 0, krylov_restart = 30;
+    snp::Gmres gmres;
     // Galerkin correction of a warm start (snp_solver_set_galerkin_basis): basis, its system
     // and coefficients on the device and in pinned memory, and a copy of x to fall back to
     const float *gal_V = nullptr;
@@ -478,7 +481,7 @@ struct snp_solver {
     // from its elements' records (bitwise repeatable; each output overwritten once)
     int assemble_rows(const double *x, double *Kv, double *Jv, float *J32v, double *rhsv, double *Fv) {
         int parts = 0;
-        if (Kv) parts |= SNP_TERMS_K | ((Jv || J32v) ? SNP_TERMS_DK : 0);
+        if (Kv) parts |= (Jv || J32v) ? SNP_TERMS_DK : SNP_TERMS_K;
         else if (Jv || J32v) parts |= SNP_TERMS_J;
         if (Fv) parts |= SNP_TERMS_F;
         if (rhsv) parts |= SNP_TERMS_RHS;
@@ -677,10 +680,29 @@ struct snp_solver {
                     if (bj_on) SNP_TRY(build_block_jacobi(f32));
                     const uint16_t *bm = bj_on ? bj_meta.p : nullptr;
                     const float *bi = bj_on ? bj_inv.p : nullptr;
-                    const int rc = f32 ? epcg32.solve(etop, T32.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0,
-                                                      cg_maxit, stream, &its, &rn, &st, bm, bi)
-                                       : epcg64.solve(etop, T64.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0,
-                                                      cg_maxit, stream, &its, &rn, &st, bm, bi);
+                    int rc;
+                    if (krylov == 1) {
+                        if (f32) return snp::fail(SNP_BAD_ARG, "GMRES runs in float64 (solve with precision 0)");
+                        SNP_TRY(gmres.reserve(n, krylov_restart));
+                        gmres.launches = 0;
+                        const snp::Gmres::Op opJ = [&](const double *xx, double *yy) {
+                            launches += 2;
+                            return epcg64.apply(etop, T64.p, free_mask.p, xx, yy, stream);
+                        };
+                        const snp::Gmres::Op opM = [&](const double *rr, double *zz) {
+                            ++launches;
+                            return bj_on ? snp::block_jacobi_apply(n, free_mask.p, bm, bi, rr, zz, stream)
+                                         : snp::point_jacobi_apply(n, free_mask.p, Jdiag.p, rr, zz, stream);
+                        };
+                        rc = gmres.solve(opJ, opM, free_mask.p, F.p, -1.0, h.p, eta, 0.0, cg_maxit, stream, &its, &rn,
+                                         &st);
+                        launches += gmres.launches;
+                    } else {
+                        rc = f32 ? epcg32.solve(etop, T32.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0, cg_maxit,
+                                                stream, &its, &rn, &st, bm, bi)
+                                 : epcg64.solve(etop, T64.p, Jdiag.p, free_mask.p, F.p, -1.0, h.p, eta, 0.0, cg_maxit,
+                                                stream, &its, &rn, &st, bm, bi);
+                    }
                     if (rc == SNP_ZERO_PIVOT)
                         return snp::fail(SNP_ZERO_PIVOT, "Newton step %d: zero Jacobian diagonal on a free DoF", it);
                     SNP_TRY(rc);
@@ -1051,6 +1073,19 @@ int snp_solver_jacobian_apply(snp_solver *s, int precision, const void *x, void 
     SNP_REQUIRE(s->j_valid[precision], "snp_solver_jacobian_apply: no %s Newton Jacobian (run a solve first)",
                 precision ? "float32" : "float64");
     return s->apply_jacobian(precision, x, y, stream ? snp::as_stream(stream) : s->stream);
+}
+
+int snp_solver_set_krylov(snp_solver *s, int32_t method, int32_t restart) {
+    snp::clear_error();
+    SNP_REQUIRE(s != nullptr && s->finalized, "snp_solver_set_krylov: solver missing or not finalized");
+    SNP_REQUIRE(method == SNP_KRYLOV_CG || method == SNP_KRYLOV_GMRES, "snp_solver_set_krylov: unknown method %d",
+                method);
+    SNP_REQUIRE(method == SNP_KRYLOV_CG || s->layout == SNP_LAYOUT_ELEM,
+                "snp_solver_set_krylov: GMRES needs the matrix-free (elem) Jacobian layout");
+    SNP_REQUIRE(restart >= 1 && restart <= 200, "snp_solver_set_krylov: restart must be in [1, 200] (got %d)", restart);
+    s->krylov = method;
+    s->krylov_restart = restart;
+    return SNP_OK;
 }
 
 int snp_solver_set_block_jacobi(snp_solver *s, const uint16_t *meta) {

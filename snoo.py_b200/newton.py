@@ -235,6 +235,11 @@ class DeviceNewton:
                 meta = dof_blocks(self.assembler.mesh.edges[:, 0], fm)
             self._set_blocks(meta)
 
+    def set_krylov(self, method="cg", restart=30):
+        """Krylov method of the residual-mode Newton steps: "cg" (default) or "gmres"
+        (restarted GMRES(``restart``), right-preconditioned, float64 solves only)."""
+        _lib.call("snp_solver_set_krylov", self.handle, {"cg": 0, "gmres": 1}[method], int(restart))
+
     def precond_apply(self, r, precision="fp64"):
         """z = M r (CUDA float64 [n]) with the block Jacobi of the last ``assemble_tensors`` of
         that precision; returns (z, number of blocks that fell back to point Jacobi)."""

@@ -180,3 +180,34 @@ def test_one_launch_pcg_reaches_the_graph_loops_answer(precond):
     Bg = solver.evaluate_B(x_graph, probes, el)
     Bc = solver.evaluate_B(x_coop, probes, el)
     assert float(np.abs(Bc - Bg).max() / np.abs(Bg).max()) < 1e-7
+
+
+@pytest.mark.parametrize("precond", ["block", "jacobi"])
+def test_gmres_newton_reaches_the_cg_answer(precond):
+    """Newton steps solved by restarted GMRES (snp_solver_set_krylov, right-preconditioned by the
+    same block or point Jacobi) reach the 1e-8 residual and the CG solve's field: B at 300
+    aperture probes within 1e-7 of the CG answer (both stop at 1e-8), bitwise repeatable; a
+    mixed-precision solve with GMRES is refused."""
+    from snoopy_b200._lib import SnpError
+
+    msh, coils, rel, solver = _setup(20000, seed=11)
+    eng = solver.newton_engine()
+    eng.set_preconditioner(precond)
+    x_cg, st_cg = solver.solve_to_residual(1e-8)
+    eng.set_krylov("gmres", restart=40)
+    try:
+        x_gm, st_gm = solver.solve_to_residual(1e-8)
+        x_gm2, _ = solver.solve_to_residual(1e-8)
+        with pytest.raises(SnpError):
+            solver.solve_to_residual(1e-8, precision="mixed")
+    finally:
+        eng.set_krylov("cg")
+        eng.set_preconditioner("block")
+    assert st_gm["rel_res"] <= 1e-8 and st_cg["rel_res"] <= 1e-8
+    assert st_gm["cg_iterations"] > 0
+    assert np.array_equal(x_gm, x_gm2)
+    probes = msh.geometry.aperture_probes(300)
+    el, _ = msh.locate(probes)
+    Bc = solver.evaluate_B(x_cg, probes, el)
+    Bg = solver.evaluate_B(x_gm, probes, el)
+    assert float(np.abs(Bg - Bc).max() / np.abs(Bc).max()) < 1e-7
