@@ -642,10 +642,11 @@ def assembly_microbench(reps=5, warmup=3, seed=5, grid=(120, 120, 116)):
     4-point rule, float64.  Two Newton assemblies at x are timed (CUDA events, after warm-up):
 
     * csr: the drop-in path, J = K + dK into the fixed CSR plus the residual F
-      (``snp_solver_assemble``): element records, then one gather per CSR row writing each value
-      once (deterministic); ``csr_atomic``: the same outputs from the element kernel that adds
-      into the CSR through the slot map with float64 atomics (``SNP_ASSEMBLY=atomic``, the value
-      zeroing included);
+      (``snp_solver_assemble``): the element kernel stores each element's 21 matrix values and six
+      residual terms, then every CSR entry and every F entry is summed from its contributions in
+      element order, each value written once (deterministic); ``csr_atomic``: the same outputs
+      from the element kernel adding into the CSR through the slot map with float64 atomics
+      (``SNP_ASSEMBLY=atomic``, the value zeroing included);
     * tensors: the matrix-free path of the Newton loop, S_e per element plus F and diag(J)
       summed per DoF (``snp_solver_assemble_tensors``).
 

@@ -137,29 +137,26 @@ int snp_curlcurl_rhs_red(int64_t n_elems, const double *nodes, const int32_t *ce
  * element arithmetic, fem_c/ctools.c:960-1388 and 1565-1759; the reference's sum over
  * elements happens in scipy's COO->CSR conversion, fem_c/interface_c.pyx:365-368).
  *
- * Phase 1, once per material: snp_curlcurl_terms writes one record per element of
- * [elem_offset, elem_offset + n_elems) into terms (record e at terms + e * stride doubles,
- * e counted over the pattern's elements; stride from snp_curlcurl_terms_stride).  `parts`
- * (SNP_TERMS_* bits) selects what the records hold: the element map and nu-weight from which
- * K's entries are formed with the reference kernels' arithmetic (kfac (c_j . c_k)) and the
- * tensor of dK (SNP_TERMS_K, SNP_TERMS_DK), the reference-frame tensor of J = K + dK alone
- * (SNP_TERMS_J, for Jacobian-only assembly), the element vector of the residual
- * F = K(x) x - rhs(x), the element vector of the reduced rhs.  phi and dilution as for
- * snp_curlcurl_assemble_diluted (both NULL: plain steel).
+ * Phase 1, once per material: snp_curlcurl_terms stores the element values of elements
+ * [elem_offset, elem_offset + n_elems) in `terms`: stride blocks (snp_curlcurl_terms_stride) of
+ * the pattern's n_elems doubles each, value b of element e at terms[b * n_elems + e].  `parts`
+ * (SNP_TERMS_* bits) selects the blocks: the 21 upper-triangle values of the element's K, dK
+ * or J = K + dK, its six residual terms (F = K(x) x - rhs(x)), its six reduced-rhs terms.  phi
+ * and dilution as for snp_curlcurl_assemble_diluted (both NULL: plain steel).
  *
- * Phase 2, once: snp_curlcurl_rows forms every CSR row from the records of the elements
- * incident to it, in element order, with no atomics, and OVERWRITES each requested output
- * (no zeroing needed): K_vals needs SNP_TERMS_K (or DK), dK_vals SNP_TERMS_DK, J_vals either
- * SNP_TERMS_DK (J = K + dK per entry, as the reference's dK + K; used whenever K or dK is
- * requested too) or SNP_TERMS_J, J32_vals likewise (float32), F needs SNP_TERMS_F, rhs
- * SNP_TERMS_RHS (elements without a source field give 0).  Results are bitwise repeatable.  Needs a pattern built with 6 DoFs per element whose longest
- * row has at most SNP_ROWS_MAX_ENTRIES entries (snp_curlcurl_rows_supported). */
+ * Phase 2, once: snp_curlcurl_rows forms every CSR entry as the sum of its element
+ * contributions in element order (one thread per entry, over the pattern's sorted coupling
+ * list) and every entry of F / rhs over the DoF's incidences, with no atomics, and OVERWRITES
+ * each requested output (no zeroing needed): K_vals needs SNP_TERMS_K, dK_vals SNP_TERMS_DK,
+ * J_vals / J32_vals SNP_TERMS_K | SNP_TERMS_DK (J = K + dK per entry, as the reference's dK + K)
+ * or SNP_TERMS_J, F SNP_TERMS_F, rhs SNP_TERMS_RHS (elements without a source field give 0).
+ * Results are bitwise repeatable.  Needs a pattern built with 6 DoFs per element and fewer than
+ * 2^31 couplings (snp_curlcurl_rows_supported). */
 #define SNP_TERMS_K 1
 #define SNP_TERMS_DK 2
 #define SNP_TERMS_J 4
 #define SNP_TERMS_F 8
 #define SNP_TERMS_RHS 16
-#define SNP_ROWS_MAX_ENTRIES 64
 int snp_curlcurl_terms_stride(int32_t parts, int32_t *stride);
 int snp_curlcurl_rows_supported(const snp_pattern *pat, int32_t *supported);
 int snp_curlcurl_terms(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems,
@@ -170,7 +167,6 @@ int snp_curlcurl_terms(const snp_pattern *pat, int64_t elem_offset, int64_t n_el
                        int32_t n_int, const double *rel_c, const double *rel_x, const double *dilution,
                        int32_t parts, double *terms, void *stream);
 int snp_curlcurl_rows(const snp_pattern *pat, const double *terms, int32_t parts,
-                      const double *curls, int32_t n_orient, int32_t n_quad,
                       double *K_vals, double *dK_vals, double *J_vals, float *J32_vals,
                       double *rhs, double *F, void *stream);
 

@@ -79,7 +79,7 @@ _SIGS = {
     "snp_curlcurl_rows_supported": [_vp, ctypes.POINTER(_c_i32)],
     "snp_curlcurl_terms": [_vp, _c_i64, _c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _vp, _c_i32, _vp, _vp,
                            _c_i32, _vp, _vp, _vp, _c_i32, _vp, _vp],
-    "snp_curlcurl_rows": [_vp, _vp, _c_i32, _vp, _c_i32, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "snp_curlcurl_rows": [_vp, _vp, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "snp_solver_set_krylov": [_vp, _c_i32, _c_i32],
     "snp_curlcurl_rhs_red": [_c_i64, _vp, _vp, _vp, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp, _c_i32, _vp, _vp,
                              _vp, _vp],

@@ -63,6 +63,24 @@ __device__ __forceinline__ void red_add(T *p, T v) {
     atomicAdd(p, v);
 }
 
+// Element values of the two-phase assembly (CurlArgs::ET): the (j, k) pair's K, dK and J, and
+// the residual and reduced-rhs terms, each into its block at element eo.
+__device__ __forceinline__ void store_pair(const CurlArgs &a, int tri, int64_t eo, double kv, double dv) {
+    const int64_t S = a.et_stride;
+    if (a.et_k >= 0) a.ET[(a.et_k + tri) * S + eo] = kv;
+    if (a.et_d >= 0) a.ET[(a.et_d + tri) * S + eo] = dv;
+    if (a.et_j >= 0) a.ET[(a.et_j + tri) * S + eo] = kv + dv;
+}
+
+__device__ __forceinline__ void store_vectors(const CurlArgs &a, int64_t eo, const double *Fj, const double *rj) {
+    const int64_t S = a.et_stride;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        if (a.et_f >= 0) a.ET[(a.et_f + j) * S + eo] = Fj[j];
+        if (a.et_r >= 0) a.ET[(a.et_r + j) * S + eo] = rj ? rj[j] : 0.0;
+    }
+}
+
 // nu and nu' at one quadrature point; DIL: diluted steel with the point's nodal basis ph[4]
 // and the element's node z coordinates Zn[4]
 template <bool DIL>
@@ -115,6 +133,7 @@ __global__ void __launch_bounds__(kBlock)
     for (int q = 0; q < nq; ++q) wsum += s_w[q];
 
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t eo = a.t_offset + e;
         const int4 cv = __ldg(reinterpret_cast<const int4 *>(a.cells) + e);
         const int cidx[4] = {cv.x, cv.y, cv.z, cv.w};
         // Jacobian J[k][l] = sum_i X[i][k] dphi[i][l]
@@ -178,12 +197,14 @@ __global__ void __launch_bounds__(kBlock)
             for (int j = 0; j < 6; ++j) p[j] = c[j][0] * Bc[0] + c[j][1] * Bc[1] + c[j][2] * Bc[2];
 #pragma unroll
             for (int j = 0; j < 6; ++j) Fj[j] = 0.0;
+            int tri = 0;
 #pragma unroll
             for (int j = 0; j < 6; ++j) {
 #pragma unroll
-                for (int k = j; k < 6; ++k) {
+                for (int k = j; k < 6; ++k, ++tri) {
                     const double kv = kfac * (c[j][0] * c[k][0] + c[j][1] * c[k][1] + c[j][2] * c[k][2]);
                     const double dv = af * p[j] * p[k];
+                    if (a.ET) store_pair(a, tri, eo, kv, dv);
                     const int s1 = want_mat ? __ldg(sl + j * 6 + k) : 0;
                     if (a.K) red_add(a.K + s1, kv);
                     if (a.dK) red_add(a.dK + s1, dv);
@@ -204,6 +225,7 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
                 for (int j = 0; j < 6; ++j) red_add(a.F + g[j], Fj[j]);
             }
+            if (a.ET) store_vectors(a, eo, Fj, nullptr);
         } else {
             // one pass over the quadrature points: accumulate sum_q nu w, the reduced rhs
             // and the 21 dK pair sums (any number of points, fixed register footprint)
@@ -251,6 +273,7 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
                 for (int k = j; k < 6; ++k) {
                     const double kv = kfac * (c[j][0] * c[k][0] + c[j][1] * c[k][1] + c[j][2] * c[k][2]);
+                    if (a.ET) store_pair(a, t, eo, kv, dk[t]);
                     const double dv = dk[t++];
                     const int s1 = want_mat ? __ldg(sl + j * 6 + k) : 0;
                     if (a.K) red_add(a.K + s1, kv);
@@ -272,6 +295,7 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
                 for (int j = 0; j < 6; ++j) red_add(a.F + g[j], Fj[j]);
             }
+            if (a.ET) store_vectors(a, eo, Fj, r);
         }
     }
 }
@@ -515,78 +539,6 @@ __device__ __forceinline__ void tensor_element(const CurlArgs &a, int64_t e, con
     }
 }
 
-// Record of one element for the two-phase assembly (TermLayout parts), at rec.
-template <bool HAS_BS, int NQ, bool DIL>
-__device__ __forceinline__ void terms_element(const CurlArgs &a, int64_t e, const double *s_ctab,
-                                              const double *s_dphi, const double *s_w, const double *s_phi,
-                                              const double *s_relc, const double *s_relx, double wsum,
-                                              const TermLayout &L, double *__restrict__ rec) {
-    ElemCore c;
-    elem_core<HAS_BS, NQ, DIL>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, c);
-    const double *Jm = c.Jm, *M = c.M, *cb = c.cb, *Rs = c.Rs;
-    const double kfac = c.kfac;
-    if (L.k >= 0) {
-#pragma unroll
-        for (int t = 0; t < 9; ++t) rec[L.k + t] = Jm[t];
-        rec[L.k + 9] = kfac;
-    }
-    if (L.d >= 0) {
-#pragma unroll
-        for (int t = 0; t < 6; ++t) rec[L.d + t] = M[t];
-    }
-    if (L.j >= 0) {
-        const double A[9] = {kfac + M[0], M[1], M[2], M[1], kfac + M[3], M[4], M[2], M[4], kfac + M[5]};
-        double S[6];
-        congruence(Jm, A, S);
-#pragma unroll
-        for (int t = 0; t < 6; ++t) rec[L.j + t] = S[t];
-    }
-    double R[3];
-#pragma unroll
-    for (int cc = 0; cc < 3; ++cc) R[cc] = Jm[cc] * Rs[0] + Jm[3 + cc] * Rs[1] + Jm[6 + cc] * Rs[2];
-    if (L.f >= 0) {
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) rec[L.f + cc] = kfac * (Jm[cc] * cb[0] + Jm[3 + cc] * cb[1] + Jm[6 + cc] * cb[2]) - R[cc];
-    }
-    if (L.r >= 0) {
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) rec[L.r + cc] = R[cc];
-    }
-    rec[L.o] = (double)c.orient;
-}
-
-template <bool HAS_BS, int NQ, bool DIL>
-__global__ void __launch_bounds__(kBlock)
-    k_curlcurl_terms(CurlArgs a, int quad_stride_ctab, TermLayout L, double *__restrict__ terms) {
-    extern __shared__ double sm[];
-    const SmemLayout SL = smem_layout(a.n_orient, a.nq, a.n_int);
-    double *s_ctab = sm + SL.off_ctab;
-    double *s_dphi = sm + SL.off_dphi;
-    double *s_w = sm + SL.off_w;
-    double *s_phi = sm + SL.off_phi;
-    double *s_relc = sm + SL.off_relc;
-    double *s_relx = sm + SL.off_relx;
-    for (int t = threadIdx.x; t < a.n_orient * 18; t += blockDim.x) {
-        int o = t / 18, r = t - o * 18;
-        s_ctab[t] = a.ctab[(int64_t)o * quad_stride_ctab + r];
-    }
-    for (int t = threadIdx.x; t < 12; t += blockDim.x) s_dphi[t] = a.dphi0[t];
-    for (int t = threadIdx.x; t < a.nq; t += blockDim.x) s_w[t] = a.w[t];
-    if (a.phi)
-        for (int t = threadIdx.x; t < 4 * a.nq; t += blockDim.x) s_phi[t] = a.phi[t];
-    const int nc = a.n_int < 0 ? 1 : 4 * a.n_int;
-    const int nx = a.n_int < 0 ? 1 : a.n_int + 1;
-    for (int t = threadIdx.x; t < nc; t += blockDim.x) s_relc[t] = a.rel_c[t];
-    for (int t = threadIdx.x; t < nx; t += blockDim.x) s_relx[t] = (a.n_int < 0) ? 0.0 : a.rel_x[t];
-    __syncthreads();
-    const int nq = NQ > 0 ? NQ : a.nq;
-    double wsum = 0.0;
-    for (int q = 0; q < nq; ++q) wsum += s_w[q];
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.n_elems; e += (int64_t)gridDim.x * blockDim.x)
-        terms_element<HAS_BS, NQ, DIL>(a, e, s_ctab, s_dphi, s_w, s_phi, s_relc, s_relx, wsum, L,
-                                       terms + e * (int64_t)L.stride);
-}
-
 template <bool HAS_BS, int NQ, typename TT, bool DIL>
 __global__ void __launch_bounds__(kBlock)
     k_curlcurl_tensor(CurlArgs a, int quad_stride_ctab, TT *__restrict__ T) {
@@ -767,46 +719,31 @@ int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st) {
 TermLayout term_layout(int parts) {
     TermLayout L;
     int o = 0;
-    if (parts & (SNP_TERMS_K | SNP_TERMS_DK)) { L.k = o; o += 10; }
-    if (parts & SNP_TERMS_DK) { L.d = o; o += 6; }
-    if (parts & SNP_TERMS_J) { L.j = o; o += 6; }
-    if (parts & SNP_TERMS_F) { L.f = o; o += 3; }
-    if (parts & SNP_TERMS_RHS) { L.r = o; o += 3; }
-    L.o = o;
-    L.stride = o + 1;
+    if (parts & SNP_TERMS_K) { L.k = o; o += 21; }
+    if (parts & SNP_TERMS_DK) { L.d = o; o += 21; }
+    if (parts & SNP_TERMS_J) { L.j = o; o += 21; }
+    if (parts & SNP_TERMS_F) { L.f = o; o += 6; }
+    if (parts & SNP_TERMS_RHS) { L.r = o; o += 6; }
+    L.stride = o;
     return L;
 }
 
-template <bool HAS_BS, int NQ, bool DIL = false>
-static int launch_terms_t(const CurlArgs &a, const TermLayout &L, double *terms, cudaStream_t st, size_t smem,
-                          int qstride) {
-    if (a.n_elems == 0) return SNP_OK;
-    auto kern = k_curlcurl_terms<HAS_BS, NQ, DIL>;
-    if (smem > 48 * 1024) SNP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<wave_grid(kern, a.n_elems, kBlock, smem), kBlock, smem, st>>>(a, qstride, L, terms);
-    SNP_LAUNCH_CHECK();
-    return SNP_OK;
-}
-
-int launch_curlcurl_terms(const CurlArgs &a, const TermLayout &L, double *terms, cudaStream_t st) {
-    SNP_REQUIRE(terms != nullptr || a.n_elems == 0, "element records: terms is NULL");
-    const SmemLayout SL = smem_layout(a.n_orient, a.nq, a.n_int);
-    const size_t smem = sizeof(double) * (size_t)SL.total;
-    SNP_REQUIRE(smem <= 200 * 1024, "curl-curl assembly: tables need %zu bytes of shared memory (max 200 KiB)", smem);
-    const int qs = a.nq * 18;
-    if (a.Bs == nullptr) {
-        if (a.nq == 1) return launch_terms_t<false, 1>(a, L, terms, st, smem, qs);
-        if (a.nq == 4) return launch_terms_t<false, 4>(a, L, terms, st, smem, qs);
-        return launch_terms_t<false, 0>(a, L, terms, st, smem, qs);
-    }
-    if (a.phi) {
-        if (a.nq == 4) return launch_terms_t<true, 4, true>(a, L, terms, st, smem, qs);
-        return launch_terms_t<true, 0, true>(a, L, terms, st, smem, qs);
-    }
-    if (a.nq == 1) return launch_terms_t<true, 1>(a, L, terms, st, smem, qs);
-    if (a.nq == 4) return launch_terms_t<true, 4>(a, L, terms, st, smem, qs);
-    if (a.nq == 5) return launch_terms_t<true, 5>(a, L, terms, st, smem, qs);
-    return launch_terms_t<true, 0>(a, L, terms, st, smem, qs);
+int launch_curlcurl_terms(const CurlArgs &a0, const TermLayout &L, double *terms, int64_t n_elems, cudaStream_t st) {
+    SNP_REQUIRE(terms != nullptr || a0.n_elems == 0 || L.stride == 0, "element matrices: terms is NULL");
+    CurlArgs a = a0;
+    a.K = a.dK = a.J = nullptr;
+    a.J32 = nullptr;
+    a.rhs = a.F = nullptr;
+    a.slots = nullptr;
+    a.ET = terms;
+    a.et_stride = n_elems;
+    a.et_k = L.k;
+    a.et_d = L.d;
+    a.et_j = L.j;
+    a.et_f = L.f;
+    a.et_r = L.r;
+    if (L.stride == 0) return SNP_OK;
+    return launch_curlcurl(a, st);
 }
 
 template <int NQ, typename TT>

@@ -1054,7 +1054,6 @@ struct snp_batch {
             Seq body;
             SNP_TRY(add_cond(nb, hp[k], cudaGraphCondTypeIf, &body));
             SNP_TRY(capture(body, cs, [&](cudaStream_t s) { return phase_body<TT>(ph, s); }));
-            if (ph == snp::PH_CG) snp::l2_window_on_kernels(body.g, Y.p, sizeof(TT) * (size_t)inc_tot);
         }
         return capture(nb, cs, [&](cudaStream_t s) { return flag(s, snp::PH_LIVE, 1, hn); });
     }

@@ -94,6 +94,52 @@ __device__ __forceinline__ void load_chunk(uint8_t *dst, const __nv_bfloat16 *sr
     }
 }
 
+// C (float32) and H (BF16) rows accept whole 16-byte stores: both 16-byte aligned, ldc a multiple
+// of 4 floats, ldh a multiple of 8 BF16 (every row then starts on a 16-byte boundary).
+__device__ __forceinline__ bool vector_stores_ok(const float *C, int ldc, const __nv_bfloat16 *H, int ldh) {
+    return (C == nullptr || ((reinterpret_cast<uintptr_t>(C) & 15) == 0 && (ldc & 3) == 0)) &&
+           (H == nullptr || ((reinterpret_cast<uintptr_t>(H) & 15) == 0 && (ldh & 7) == 0));
+}
+
+// Epilogue of eight accumulator columns col0 .. col0 + 7 of one row: z = acc + bias, C = z,
+// H = BF16(GELU(z)) (act 1) or BF16(z); one thread's eight values as two 16-byte stores into C
+// and one into H when the row allows it (every 32-byte sector written whole), else one by one.
+__device__ __forceinline__ void store_row8(const uint32_t (&v)[8], int row, int col0, int N, const float *bias,
+                                           int act, float *C, int ldc, __nv_bfloat16 *H, int ldh, bool vec_ok) {
+    float z[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        z[j] = __uint_as_float(v[j]);
+        if (bias && col0 + j < N) z[j] += bias[col0 + j];
+    }
+    if (vec_ok && col0 + 8 <= N && (col0 & 7) == 0) {
+        if (C) {
+            float4 *cp = reinterpret_cast<float4 *>(C + (int64_t)row * ldc + col0);
+            cp[0] = make_float4(z[0], z[1], z[2], z[3]);
+            cp[1] = make_float4(z[4], z[5], z[6], z[7]);
+        }
+        if (H) {
+            uint32_t hw[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat16 lo = __float2bfloat16_rn(act == 1 ? gelu(z[2 * j]) : z[2 * j]);
+                const __nv_bfloat16 hi = __float2bfloat16_rn(act == 1 ? gelu(z[2 * j + 1]) : z[2 * j + 1]);
+                hw[j] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+            }
+            *reinterpret_cast<uint4 *>(H + (int64_t)row * ldh + col0) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int col = col0 + j;
+        if (col < N) {
+            if (C) C[(int64_t)row * ldc + col] = z[j];
+            if (H) H[(int64_t)row * ldh + col] = __float2bfloat16_rn(act == 1 ? gelu(z[j]) : z[j]);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_gemm_bf16(int M, int N, int K, const __nv_bfloat16 *__restrict__ A, int lda,
                 const __nv_bfloat16 *__restrict__ B, int ldb, const float *__restrict__ bias, int act,
@@ -157,6 +203,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
     if (!failed) {
         const int row = m0 + 32 * warp + lane;
+        const bool vec_ok = vector_stores_ok(C, ldc, H, ldh);
         for (int c8 = 0; c8 < nt / 8; ++c8) {
             uint32_t v[8];
             const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(8 * c8);
@@ -165,18 +212,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                            "=r"(v[7])
                          : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int col = n0 + 8 * c8 + j;
-                    if (col < N) {
-                        float z = __uint_as_float(v[j]);
-                        if (bias) z += bias[col];
-                        if (C) C[(int64_t)row * ldc + col] = z;
-                        if (H) H[(int64_t)row * ldh + col] = __float2bfloat16_rn(act == 1 ? gelu(z) : z);
-                    }
-                }
-            }
+            if (row < M) store_row8(v, row, n0 + 8 * c8, N, bias, act, C, ldc, H, ldh, vec_ok);
         }
     } else if (threadIdx.x == 0) {
         atomicExch(err, 1);
@@ -321,6 +357,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (!failed) {
         const int row = m0 + 32 * warp + lane;
+        const bool vec_ok = vector_stores_ok(C, ldc, H, ldh);
         for (int c8 = 0; c8 < nt / 8; ++c8) {
             uint32_t v[8];
             const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(8 * c8);
@@ -329,18 +366,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                            "=r"(v[7])
                          : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int col = n0 + 8 * c8 + j;
-                    if (col < N) {
-                        float z = __uint_as_float(v[j]);
-                        if (bias) z += bias[col];
-                        if (C) C[(int64_t)row * ldc + col] = z;
-                        if (H) H[(int64_t)row * ldh + col] = __float2bfloat16_rn(act == 1 ? gelu(z) : z);
-                    }
-                }
-            }
+            if (row < M) store_row8(v, row, n0 + 8 * c8, N, bias, act, C, ldc, H, ldh, vec_ok);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");

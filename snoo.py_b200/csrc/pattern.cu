@@ -78,20 +78,11 @@ __global__ void k_inc_pairs(const int32_t *__restrict__ dofs, int64_t n_elems, u
     }
 }
 
-// inc_loc of every incidence of row r (rows no longer than 255 entries)
-__global__ void k_inc_loc(int32_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ inc_ptr,
-                          const int32_t *__restrict__ inc, const int32_t *__restrict__ slots, uint2 *__restrict__ loc) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t base = rp[r];
-        for (int32_t t = inc_ptr[r]; t < inc_ptr[r + 1]; ++t) {
-            const uint32_t u = (uint32_t)inc[t];
-            const int32_t *sl = slots + (int64_t)(u >> 3) * 36 + (u & 7u) * 6;
-            uint32_t lo = 0, hi = 0;
-            for (int b = 0; b < 4; ++b) lo |= (uint32_t)(sl[b] - base) << (8 * b);
-            for (int b = 4; b < 6; ++b) hi |= (uint32_t)(sl[b] - base) << (8 * (b - 4));
-            loc[t] = make_uint2(lo, hi);
-        }
-    }
+// cptr[p] = first sorted coupling of CSR position p (heads of the sorted keys)
+__global__ void k_cptr(const uint32_t *__restrict__ head, const uint32_t *__restrict__ pos, int64_t n,
+                       int32_t *__restrict__ cptr) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        if (head[t]) cptr[pos[t] - 1] = (int32_t)t;
 }
 
 __global__ void k_max_row(int32_t n, const int32_t *__restrict__ rp, int *__restrict__ mx) {
@@ -152,16 +143,7 @@ int build_incidence(snp_pattern *P, const int32_t *elem_dofs, cudaStream_t st) {
         SNP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(temp.p, tb_scan, P->inc_ptr.p, P->inc_ptr.p, n + 1, st));
         SNP_CUDA_TRY(cudaStreamSynchronize(st));
     }
-    if (P->max_row <= 255) {
-        SNP_TRY(P->inc_loc.alloc(m > 0 ? m : 1));
-        if (m > 0) {
-            k_inc_loc<<<stride_grid(n, 256, 8), 256, 0, st>>>(n, P->row_ptr.p, P->inc_ptr.p, P->inc.p, P->slots.p,
-                                                              P->inc_loc.p);
-            SNP_LAUNCH_CHECK();
-            SNP_CUDA_TRY(cudaStreamSynchronize(st));
-        }
-        P->has_incidence = true;
-    }
+    P->has_incidence = true;
     return SNP_OK;
 }
 
@@ -236,6 +218,20 @@ int pattern_create(const int32_t *elem_dofs, int64_t n_elems, int32_t dpe, int32
                                                            P->col_idx.p, P->row_ptr.p, P->diag_pos.p);
         if (cub::DeviceScan::ExclusiveSum(temp.p, tb, P->row_ptr.p, P->row_ptr.p, n_rows + 1, st) != cudaSuccess)
             return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: row scan failed"));
+        // the sorted couplings (stable radix sort: element order within a position) and the
+        // first of each position: every CSR entry's contributions, for the deterministic gather
+        if (n < ((int64_t)1 << 31)) {
+            if ((rc = P->cid.alloc(n)) || (rc = P->cptr.alloc(P->nnz + 1))) return cleanup_fail(rc);
+            if (cudaMemcpyAsync(P->cid.p, dv.Current(), sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st) !=
+                cudaSuccess)
+                return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: copy of the sorted couplings failed"));
+            k_cptr<<<stride_grid(n, 256, 16), 256, 0, st>>>(head.p, pos.p, n, P->cptr.p);
+            const int32_t nn = (int32_t)n;
+            if (cudaMemcpyAsync(P->cptr.p + P->nnz, &nn, sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return cleanup_fail(fail(SNP_CUDA_ERROR, "snp_pattern_create: contribution pointers failed"));
+            P->has_contrib = true;
+        }
     } else {
         P->nnz = 0;
         if ((rc = P->col_idx.alloc(1))) return cleanup_fail(rc);

@@ -114,6 +114,14 @@ struct CurlArgs {
     int64_t t_offset;
     double *Fe;
     double *De;
+    // element matrices of the two-phase assembly (instead of the atomics into the CSR): block b
+    // of ET holds value b of every element, ET[b * et_stride + t_offset + e]; the blocks are
+    // K (21, upper triangle row by row: (j, k), j <= k), dK (21), J = K + dK (21), the six
+    // residual terms F_e,j and the six reduced-rhs terms, at the block offsets et_k .. et_r
+    // (-1: not written)
+    double *ET;
+    int64_t et_stride;
+    int et_k, et_d, et_j, et_f, et_r;
     // diluted steel (reduced formulation only): phi[Q][4] nodal basis at the quadrature
     // points or null; dil = {c_num, m_num, c_den, m_den}, s(z) = (c_num + z m_num) / (c_den + z m_den)
     const double *phi;
@@ -164,32 +172,29 @@ int launch_curlcurl_tensor_batch(const BatchSeg *segs, const BatchAsmItem *items
 // the element terms of diag(J) and of F = K(x) x - rhs(x).  Tables must be affine.
 int launch_curlcurl_tensor(const CurlArgs &a, cudaStream_t st);
 
-// Per-element record of the two-phase (deterministic) assembly into a CSR pattern.  Parts, in
-// this order when present (symmetric tensors as xx xy xz yy yz zz; an element edge k with
-// reference curl chat_k of the element's orientation has the curl c_k = Jm chat_k):
-//   SNP_TERMS_K or _DK   Jm (9, row-major) and kfac (1): K_e,kl = kfac (c_k . c_l)
-//   SNP_TERMS_DK         M = sum_q a_q B_q B_q^T (6):    dK_e,kl = c_l . (M c_k)
-//   SNP_TERMS_J          SJ = Jm^T (kfac I + M) Jm (6):  J_e,kl = chat_l . (SJ chat_k)
-//   SNP_TERMS_F          G  = kfac Jm^T Jm bh - Jm^T Rs (3): F_e,k = chat_k . G
-//   SNP_TERMS_RHS        R  = Jm^T Rs (3):               rhs_e,k = chat_k . R
-// and last the element's orientation index (stored as a double).
+// Element matrices of the two-phase (deterministic) assembly into a CSR pattern, structure of
+// arrays over the pattern's elements: `stride` blocks of n_elems values each, at these block
+// offsets (-1: absent): K 21 values (upper triangle, row by row), dK 21, J = K + dK 21, residual
+// terms F_e,j 6, reduced-rhs terms 6.  The values are the single-launch kernel's element values
+// (the reference kernels' arithmetic), stored instead of added into the CSR.
 struct TermLayout {
-    int stride = 1;
-    int k = -1, d = -1, j = -1, f = -1, r = -1, o = 0;
+    int stride = 0;
+    int k = -1, d = -1, j = -1, f = -1, r = -1;
 };
 TermLayout term_layout(int parts);
 
-// Phase 1: the records of one material's elements, record e at terms + e * L.stride.
-int launch_curlcurl_terms(const CurlArgs &a, const TermLayout &L, double *terms, cudaStream_t st);
+// Phase 1: the element matrices of one material's elements (a.t_offset = the material's first
+// element in the pattern), into terms with n_elems values per block.
+int launch_curlcurl_terms(const CurlArgs &a, const TermLayout &L, double *terms, int64_t n_elems, cudaStream_t st);
 
-// Phase 2: every row of `pat` formed from the records of its incident elements, in the rows'
-// incidence order (no atomics; bitwise repeatable); each requested output is overwritten.
-// With K or dK requested, J = K + dK per entry (Jm, kfac and M records); J alone from SJ.
-int launch_curlcurl_rows(const snp_pattern *pat, const double *terms, const TermLayout &L, const double *ctab,
-                         int n_orient, int quad_stride_ctab, double *K, double *dK, double *J, float *J32, double *rhs,
-                         double *F, cudaStream_t st);
+// Phase 2: every CSR entry of `pat` summed from its element contributions in element order, and
+// every entry of F / rhs from the DoF's incidences in element order (no atomics; bitwise
+// repeatable); each requested output is overwritten.  J = K + dK per entry when both K and dK
+// blocks are present, else from the J block.
+int launch_curlcurl_rows(const snp_pattern *pat, const double *terms, const TermLayout &L, double *K, double *dK,
+                         double *J, float *J32, double *rhs, double *F, cudaStream_t st);
 
-// Whether launch_curlcurl_rows can serve the pattern (incidence lists built, rows short enough).
+// Whether launch_curlcurl_rows can serve the pattern (contribution and incidence lists built).
 bool rows_supported(const snp_pattern *pat);
 
 // Validate that d_phi and curls do not vary across quadrature points; sets *affine.
@@ -217,12 +222,13 @@ struct snp_pattern {
     int64_t n_elems = 0;
     int32_t dpe = 0;
     snp::DevBuf<int32_t> row_ptr, col_idx, slots, diag_pos;
+    // contributions of every CSR entry p: the coupling ids t = e * dpe^2 + a * dpe + b of the
+    // element pairs that add into it, in element order, cid[cptr[p] .. cptr[p + 1])
+    snp::DevBuf<int32_t> cid, cptr;
+    bool has_contrib = false;
     // incidence lists of the rows (6 DoFs per element, fewer than 2^28 elements): row r's
     // (element, local DoF) pairs as e * 8 + k in element order, inc[inc_ptr[r] .. inc_ptr[r + 1])
     snp::DevBuf<int32_t> inc_ptr, inc;
-    // per incidence (row r, element e, local DoF a): the positions in row r of e's six
-    // couplings (a, b), slot[e][a][b] - row_ptr[r], as bytes 0..5 (rows of at most 64 entries)
-    snp::DevBuf<uint2> inc_loc;
     int32_t max_row = 0;  // entries of the longest row
     bool has_incidence = false;
 };

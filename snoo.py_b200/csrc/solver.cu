@@ -477,11 +477,12 @@ struct snp_solver {
         return SNP_OK;
     }
 
-    // CSR assembly in two phases: each material's element records, then every row gathered
-    // from its elements' records (bitwise repeatable; each output overwritten once)
+    // CSR assembly in two phases: each material's element values, then every CSR entry and
+    // vector entry summed from its element contributions (bitwise repeatable; each output
+    // overwritten once)
     int assemble_rows(const double *x, double *Kv, double *Jv, float *J32v, double *rhsv, double *Fv) {
         int parts = 0;
-        if (Kv) parts |= (Jv || J32v) ? SNP_TERMS_DK : SNP_TERMS_K;
+        if (Kv) parts |= SNP_TERMS_K | ((Jv || J32v) ? SNP_TERMS_DK : 0);
         else if (Jv || J32v) parts |= SNP_TERMS_J;
         if (Fv) parts |= SNP_TERMS_F;
         if (rhsv) parts |= SNP_TERMS_RHS;
@@ -509,11 +510,11 @@ struct snp_solver {
                 a.phi = m->phi.p;
                 for (int i = 0; i < 4; ++i) a.dil[i] = m->dil[i];
             }
-            SNP_TRY(snp::launch_curlcurl_terms(a, L, terms.p + m->offset * (int64_t)L.stride, stream));
+            a.t_offset = m->offset;
+            SNP_TRY(snp::launch_curlcurl_terms(a, L, terms.p, pat->n_elems, stream));
             if (m->count) ++launches;
         }
-        SNP_TRY(snp::launch_curlcurl_rows(pat, terms.p, L, curls.p, n_orient, nq * 18, Kv, nullptr, Jv, J32v, rhsv, Fv,
-                                          stream));
+        SNP_TRY(snp::launch_curlcurl_rows(pat, terms.p, L, Kv, nullptr, Jv, J32v, rhsv, Fv, stream));
         ++launches;
         if (Fv && has_extra) {
             snp::k_sub<<<snp::stride_grid(n, snp::kVB, 4), snp::kVB, 0, stream>>>(n, Fv, rhs_extra.p);

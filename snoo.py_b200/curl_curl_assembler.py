@@ -4,9 +4,9 @@ The reference gathers per-material cells and edge ids from gmsh (``:19-137``), a
 Newton step re-queries element orientations from gmsh, re-creates reference tables, calls
 the C kernel per material, converts triplets to CSR and adds the matrices (``:815-932``).
 Here the mesh arrays, tables and one CSR pattern over all materials are uploaded once and
-cached.  Each call writes one record per element (one launch per material) and then forms
-every CSR row from the records of its elements in element order (one launch): the values are
-bitwise repeatable and each is written once.  ``SNP_ASSEMBLY=atomic`` (or ``method="atomic"``)
+cached.  Each call stores every element's matrix values (one launch per material) and then
+sums every CSR entry from its element contributions in element order (one launch): the values
+are bitwise repeatable and each is written once.  ``SNP_ASSEMBLY=atomic`` (or ``method="atomic"``)
 selects the one-launch-per-material kernels that add element values into the CSR with atomics.
 
 ``mesh`` is a ``snoopy_b200.mesh.TetMesh`` (gmsh is not a dependency); ``volume_tags`` are
@@ -119,7 +119,7 @@ class CurlCurlAssembler:
         """Assemble on the device into the cached pattern.
 
         :param x: float64 DoF vector (numpy or CUDA tensor).
-        :param method: ``"rows"`` (element records, then one gather per CSR row: deterministic),
+        :param method: ``"rows"`` (element values, then one sum per CSR entry: deterministic),
             ``"atomic"`` (element kernels adding into the CSR), or None: ``$SNP_ASSEMBLY``, else
             rows where the pattern allows it.
         :return: dict of CUDA tensors ``K``, ``J`` (= K + dK), ``dK`` [nnz], ``rhs``, ``F`` [n]
@@ -153,9 +153,8 @@ class CurlCurlAssembler:
                           tb.n_orient, _lib.ptr(tb.phi_d) if coef is not None else None, _lib.ptr(tb.d_phi_d),
                           _lib.ptr(tb.w_d), tb.nq, _lib.ptr(x_d), _lib.ptr(bs[n]), n_int, _lib.ptr(rc), _lib.ptr(rx),
                           coef, parts, _lib.ptr(d["terms"]), s)
-            _lib.call("snp_curlcurl_rows", pat.handle, _lib.ptr(d["terms"]), parts, _lib.ptr(tb.curls_d), tb.n_orient,
-                      tb.nq, _lib.ptr(out["K"]), _lib.ptr(out["dK"]), _lib.ptr(out["J"]), None, _lib.ptr(out["rhs"]),
-                      _lib.ptr(out["F"]), s)
+            _lib.call("snp_curlcurl_rows", pat.handle, _lib.ptr(d["terms"]), parts, _lib.ptr(out["K"]),
+                      _lib.ptr(out["dK"]), _lib.ptr(out["J"]), None, _lib.ptr(out["rhs"]), _lib.ptr(out["F"]), s)
             for key, want, size in (("K", K, pat.nnz), ("J", J, pat.nnz), ("dK", dK, pat.nnz),
                                     ("rhs", rhs, self.num_dofs), ("F", F, self.num_dofs)):
                 if want:

@@ -74,8 +74,8 @@ def compute_stiffness_and_jacobi_matrix(nodes, cells, d_phi, x, permeability, q,
 
 def _curlcurl_K_dK_rhs(pat, num_el, num_dofs, nodes_d, cells_d, gids_d, or_d, curls_d, n_orient, phi_d, dphi_d, w_d,
                        nq, x_d, bs_d, n_int, rc, rx, dil):
-    """K, dK and the reduced rhs of all elements of ``pat`` (device float64).  Element records and
-    one gather per CSR row (deterministic) where the pattern allows it and ``SNP_ASSEMBLY`` is not
+    """K, dK and the reduced rhs of all elements of ``pat`` (device float64).  Element values and
+    one sum per CSR entry (deterministic) where the pattern allows it and ``SNP_ASSEMBLY`` is not
     ``atomic``; otherwise the element kernel adding into the CSR (diluted when ``dil`` is set)."""
     if pat.rows_supported and os.environ.get("SNP_ASSEMBLY", "rows") != "atomic":
         t = torch()
@@ -90,8 +90,8 @@ def _curlcurl_K_dK_rhs(pat, num_el, num_dofs, nodes_d, cells_d, gids_d, or_d, cu
                   _lib.ptr(or_d), _lib.ptr(curls_d), n_orient, _lib.ptr(phi_d) if dil is not None else None,
                   _lib.ptr(dphi_d), _lib.ptr(w_d), nq, _lib.ptr(x_d), _lib.ptr(bs_d), n_int, _lib.ptr(rc), _lib.ptr(rx),
                   dil, parts, _lib.ptr(terms), _lib.stream_ptr())
-        _lib.call("snp_curlcurl_rows", pat.handle, _lib.ptr(terms), parts, _lib.ptr(curls_d), n_orient, nq,
-                  _lib.ptr(K), _lib.ptr(dK), None, None, _lib.ptr(rhs), None, _lib.stream_ptr())
+        _lib.call("snp_curlcurl_rows", pat.handle, _lib.ptr(terms), parts, _lib.ptr(K), _lib.ptr(dK), None, None,
+                  _lib.ptr(rhs), None, _lib.stream_ptr())
         return K[: pat.nnz], dK[: pat.nnz], rhs
     K = zeros(pat.nnz)
     dK = zeros(pat.nnz)
