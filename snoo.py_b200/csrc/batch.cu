@@ -48,10 +48,9 @@ namespace {
 constexpr int kBB = kBjTile;             // threads of the DoF-indexed kernels (one block-Jacobi tile)
 constexpr int kUnitTiles = 8;            // tiles per DoF partial-sum unit
 constexpr int kUnit = kBB * kUnitTiles;  // DoFs per unit
-constexpr int kChunk = 1024;             // elements per element-pass partial-sum chunk
+constexpr int kChunk = 256;              // elements per element-pass partial-sum chunk (one warp's work)
 constexpr int kGroup = 16;               // elements per warp step of the element pass (two lanes each)
 constexpr int kGroups = kChunk / kGroup;
-static_assert(kGroups == 64, "the chunk sum adds two group partials per lane");
 
 // CG outcome per problem (as the single-problem PcgState.done, plus idle and zero pivot)
 enum : int { CG_RUN = 0, CG_CONV = 1, CG_MAXIT = 2, CG_NAN = 3, CG_ZERO_RHS = 4, CG_IDLE = 5, CG_PIVOT = 6 };
@@ -440,8 +439,9 @@ __global__ void __launch_bounds__(kBB)
 }
 
 // Element pass of a CG iteration over the chunks of the problems still iterating: as the
-// single-problem k_epass1 (two lanes per element, three edges each), the p.Jp partial of every
-// 16-element group summed by a fixed shuffle tree, the chunk's 64 groups in order.
+// single-problem k_epass1 (two lanes per element, three edges each).  A warp owns a whole chunk
+// (64 steps of 16 elements): each step's p.Jp partial is summed by a fixed shuffle tree and added
+// to the chunk's sum in step order, with no block barrier inside the pass.
 template <typename TT, int BS>
 __global__ void __launch_bounds__(BS)
     k_b_pass1(int n_inst, const BInst *__restrict__ inst, const int32_t *__restrict__ chunk_inst, int64_t n_chunks,
@@ -449,7 +449,6 @@ __global__ void __launch_bounds__(BS)
               const TT *__restrict__ chat, const DofPair<TT> *__restrict__ G, TT *__restrict__ Y, BState *st,
               double *part, BCtl *ctl) {
     __shared__ TT sc[18];
-    __shared__ double s_grp[kGroups];
     count_launch(ctl);
     if (threadIdx.x < 18) sc[threadIdx.x] = chat[threadIdx.x];
     __syncthreads();
@@ -457,12 +456,15 @@ __global__ void __launch_bounds__(BS)
     const int h = lane & 1;  // edges 3h .. 3h+2
     const int warp = threadIdx.x >> 5;
     constexpr int kWarps = BS / 32;
-    for (int64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+    const int64_t wstride = (int64_t)gridDim.x * kWarps;
+    for (int64_t c = (int64_t)blockIdx.x * kWarps + warp; c < n_chunks; c += wstride) {
         const int p = chunk_inst[c];
-        if (st[p].ph != PH_CG) continue;  // uniform across the block
+        if (st[p].ph != PH_CG) continue;  // uniform across the warp
         const TT beta = (TT)st[p].beta;
         const int64_t e_end = inst[p].elem_off + inst[p].ne;
-        for (int g = warp; g < kGroups; g += kWarps) {
+        double acc = 0.0;
+#pragma unroll 1
+        for (int g = 0; g < kGroups; ++g) {
             const int64_t e = c * kChunk + g * kGroup + (lane >> 1);
             const bool valid = e < e_end;
             const int64_t eb = eslot(valid ? e : 0, 0);
@@ -517,17 +519,9 @@ __global__ void __launch_bounds__(BS)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) Y[ps[j]] = edge_term(sc, 3 * h + j, d[j] < 0, v0, v1, v2);
             }
-            dot = warp_sum(dot);
-            if (lane == 0) s_grp[g] = dot;
+            acc += warp_sum(dot);
         }
-        __syncthreads();
-        if (warp == 0) {
-            double v = s_grp[lane];
-            v += s_grp[lane + 32];
-            v = warp_sum(v);
-            if (lane == 0) part[c] = v;
-        }
-        __syncthreads();
+        if (lane == 0) part[c] = acc;
     }
     if (!last_block(&ctl->counter)) return;
     const int nw = blockDim.x >> 5;
@@ -881,7 +875,8 @@ struct snp_batch {
     int grid_units() const { return (int)std::min<int64_t>(n_units, (int64_t)snp::sm_count() * 8); }
     int grid_chunks(int block) const {
         const int per_sm = std::max(1, 2048 / block);
-        return (int)std::min<int64_t>(n_chunks, (int64_t)snp::sm_count() * per_sm);
+        const int64_t need = (n_chunks + block / 32 - 1) / (block / 32);  // a warp per chunk
+        return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)snp::sm_count() * per_sm));
     }
     int run_stride() const { return (int)(sizeof(snp::BState) / sizeof(int32_t)); }
 
