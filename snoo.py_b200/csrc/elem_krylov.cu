@@ -1107,38 +1107,40 @@ int ElemPcg<TT>::launch_iteration(const ElemTopology &top, const TT *T, const ui
 // persisting hits, and this context's persisting L2 set-aside is raised to cover it (up to the
 // device's maximum; it lasts as long as the context).  Measured on the 1.16M-tet benchmark: 92.5
 // -> 84.1 us per float64 PCG iteration.  SNP_L2_PERSIST=0 leaves the nodes' cache policy alone.
-void l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes) {
+bool l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes) {
     const char *env = getenv("SNP_L2_PERSIST");
-    if (env && env[0] == '0') return;
+    if (env && env[0] == '0') return false;
     int dev = 0, max_persist = 0, max_win = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
         max_persist <= 0 || max_win <= 0) {
         cudaGetLastError();
-        return;
+        return false;
     }
-    const size_t win = bytes < (size_t)max_win ? bytes : (size_t)max_win;
-    const size_t keep = win < (size_t)max_persist ? win : (size_t)max_persist;
+    // only a window that covers the whole array: a partial one (hit ratio below 1) marks the
+    // rest streaming, which evicts it early and made a 187 MB slot array three times slower
+    if (bytes > (size_t)max_win || bytes > (size_t)max_persist) return false;
+    const size_t win = bytes, keep = bytes;
     if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, keep) != cudaSuccess) {
         cudaGetLastError();
-        return;
+        return false;
     }
     cudaKernelNodeAttrValue v = {};
     v.accessPolicyWindow.base_ptr = const_cast<void *>(base);
     v.accessPolicyWindow.num_bytes = win;
-    v.accessPolicyWindow.hitRatio = (float)((double)keep / (double)win);
+    v.accessPolicyWindow.hitRatio = 1.0f;
     v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
     v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
     size_t n = 0;
     if (cudaGraphGetNodes(body, nullptr, &n) != cudaSuccess || n == 0) {
         cudaGetLastError();
-        return;
+        return false;
     }
     std::vector<cudaGraphNode_t> nodes(n);
     if (cudaGraphGetNodes(body, nodes.data(), &n) != cudaSuccess) {
         cudaGetLastError();
-        return;
+        return false;
     }
     for (auto nd : nodes) {
         cudaGraphNodeType t;
@@ -1146,12 +1148,14 @@ void l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes) {
             cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &v);
     }
     cudaGetLastError();
+    return true;
 }
 
 template <typename TT>
 int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t *free_mask, const uint16_t *bj_meta,
                              const float *bj_inv) {
     drop_graph();
+    l2_window = false;
     const char *env = getenv("SNP_PCG_GRAPH");
     if (env && env[0] == '0') return SNP_OK;
     cudaGraph_t g = nullptr;
@@ -1180,7 +1184,7 @@ int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t
             cudaGraph_t out = nullptr;
             cudaError_t e = cudaStreamEndCapture(cs, &out);
             ok = (rc == SNP_OK) && e == cudaSuccess;
-            if (ok) l2_window_on_kernels(body, Y.p, sizeof(TT) * 6 * (size_t)ne);
+            if (ok) l2_window = l2_window_on_kernels(body, Y.p, sizeof(TT) * 6 * (size_t)ne);
         }
     }
     if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
@@ -1315,6 +1319,12 @@ extract:
     SNP_LAUNCH_CHECK();
     SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
     SNP_CUDA_TRY(cudaStreamSynchronize(s));
+    // the slot values' persisting lines go back to normal once the solve is over, so that
+    // they do not hold the L2 against whatever the program runs next
+    if (exec && l2_window) {
+        cudaCtxResetPersistingL2Cache();
+        cudaGetLastError();
+    }
     const PcgState &H = *hst.p;
     launches += 1 + (chunk_launches >= 0 ? chunk_launches : 2 * (H.iter > 0 ? H.iter : 1));
     if (its) *its = H.iter;

@@ -130,8 +130,9 @@ struct CurlArgs {
 
 // Give every kernel node of `body` an L2 access policy window over [base, base + bytes) with
 // persisting hits (the slot values the element pass writes and the DoF pass reads), raising the
-// context's persisting set-aside to cover it as far as the device allows; SNP_L2_PERSIST=0 skips.
-void l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes);
+// context's persisting set-aside to cover it; only when the whole range fits the device's
+// persisting maximum (returns whether the window was set).  SNP_L2_PERSIST=0 skips.
+bool l2_window_on_kernels(cudaGraph_t body, const void *base, size_t bytes);
 
 // Validate the inputs of a curl-curl launch over elements [elem_offset, +n_elems) of `pat` (may
 // be NULL) and fill `a` (slots offset to the range; outputs unset).

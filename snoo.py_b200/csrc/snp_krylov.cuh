@@ -212,6 +212,7 @@ struct ElemPcg {
     const uint8_t *key_fm = nullptr;
     const uint16_t *key_bm = nullptr;
     const float *key_bi = nullptr;
+    bool l2_window = false;  // the graph's kernels carry the L2 window over Y
     int64_t launches = 0;
 
     ElemPcg() = default;

@@ -28,6 +28,16 @@ def upload(a, dtype):
     return t.from_numpy(arr).to(device(), non_blocking=False)
 
 
+def to_host(x):
+    """numpy copy of a device vector, read back through page-locked memory (torch's caching host
+    allocator reuses the pinned block once the previous result is freed), so the copy runs at
+    full PCIe rate instead of through a pageable staging buffer."""
+    t = torch()
+    out = t.empty(x.shape, dtype=x.dtype, pin_memory=True)
+    out.copy_(x)
+    return out.numpy()
+
+
 def zeros(n, dtype="f64"):
     t = torch()
     dt = {"f64": t.float64, "f32": t.float32, "i32": t.int32}[dtype]

@@ -7,7 +7,7 @@ solves (``snoopy/mvp_solver.py``).  ``solve_nonlin`` keeps the reference's Newto
 import numpy as np
 
 from .curl_curl_assembler import CurlCurlAssembler
-from .device import upload, zeros
+from .device import to_host, upload, zeros
 from .laplace_subdomain_solver import LaplaceSubdomainSolver
 from .materials import ConstantReluctance
 from .newton import MODE_REFERENCE, MODE_RESIDUAL, DeviceNewton
@@ -100,7 +100,7 @@ class MVPSolver:
         if rc not in (0, 3):  # 3: maxiter reached, which scipy reports through its exit code
             _lib.check(rc)
         self.last_exit_code = 0 if rc == 0 else int(its.value)
-        return x[:n].cpu().numpy()
+        return to_host(x[:n])
 
     def solve_nonlin(self, phi_list, tolerance=1e-4, x_0=np.zeros((0,)), maxiter=-1, apply_gauge=False,
                      plot_current_density=False):
@@ -113,7 +113,7 @@ class MVPSolver:
         x, stats = eng.solve(x0, mode=MODE_REFERENCE, tol=tolerance, cg_maxiter=maxiter,
                              max_newton=self.max_newton_iterations, cg_rtol=1e-5, verbose=self.verbose)
         self.last_stats = stats
-        return x.cpu().numpy()
+        return to_host(x)
 
     def solve_to_residual(self, phi_list, rtol=1e-8, x_0=None, precision="fp64", max_newton=None, cg_maxiter=50000):
         """Newton until ||F_free(x)|| <= rtol ||F_free(x_0)|| (see ``RedMVPSolver.solve_to_residual``)."""
@@ -121,4 +121,4 @@ class MVPSolver:
         x, stats = eng.solve(x_0, mode=MODE_RESIDUAL, tol=rtol, max_newton=max_newton or self.max_newton_iterations,
                              precision={"fp64": 0, "mixed": 1}[precision], cg_maxiter=cg_maxiter)
         self.last_stats = stats
-        return x.cpu().numpy(), stats
+        return to_host(x), stats

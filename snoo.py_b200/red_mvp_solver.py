@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from .curl_curl_assembler import CurlCurlAssembler
-from .device import torch, upload, zeros
+from .device import to_host, torch, upload, zeros
 from .fem_c import biot_savart_device
 from .materials import ConstantReluctance
 from .newton import MODE_REFERENCE, MODE_RESIDUAL, DeviceNewton
@@ -141,7 +141,7 @@ class RedMVPSolver:
         x, stats = eng.solve(x0, mode=MODE_REFERENCE, tol=tolerance, cg_maxiter=maxiter,
                              max_newton=self.max_newton_iterations, cg_rtol=1e-5, verbose=self.verbose)
         self.last_stats = stats
-        return x.cpu().numpy()
+        return to_host(x)
 
     def solve_to_residual(self, rtol=1e-8, x_0=None, precision="fp64", max_newton=None, cg_maxiter=50000,
                           return_device=False, verbose=False):
@@ -158,7 +158,7 @@ class RedMVPSolver:
         x, stats = eng.solve(x_0, mode=MODE_RESIDUAL, tol=rtol, cg_maxiter=cg_maxiter,
                              max_newton=max_newton or self.max_newton_iterations, precision=prec, verbose=verbose)
         self.last_stats = stats
-        return (x if return_device else x.cpu().numpy()), stats
+        return (x if return_device else to_host(x)), stats
 
     def evaluate_B(self, x, points, elements=None):
         """Total field B = B_s + curl A_r at points (reduced formulation)."""
