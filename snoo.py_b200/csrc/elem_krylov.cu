@@ -1184,7 +1184,10 @@ int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t
             cudaGraph_t out = nullptr;
             cudaError_t e = cudaStreamEndCapture(cs, &out);
             ok = (rc == SNP_OK) && e == cudaSuccess;
-            if (ok) l2_window = l2_window_on_kernels(body, Y.p, sizeof(TT) * 6 * (size_t)ne);
+            if (ok) {
+                l2_bytes = sizeof(TT) * 6 * (size_t)ne;
+                l2_window = l2_window_on_kernels(body, Y.p, l2_bytes);
+            }
         }
     }
     if (ok) ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
@@ -1301,6 +1304,8 @@ int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag,
     if (!same) SNP_TRY(build_graph(top, T, free_mask, bj_meta, bj_inv));
     }
     if (exec) {
+        // the L2 set-aside for the slot values' persisting lines, only while this solve runs
+        if (l2_window && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, l2_bytes) != cudaSuccess) cudaGetLastError();
         SNP_CUDA_TRY(cudaGraphLaunch(exec, s));
     } else {
         const int chunk = 32;
@@ -1319,10 +1324,11 @@ extract:
     SNP_LAUNCH_CHECK();
     SNP_CUDA_TRY(cudaMemcpyAsync(hst.p, st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
     SNP_CUDA_TRY(cudaStreamSynchronize(s));
-    // the slot values' persisting lines go back to normal once the solve is over, so that
-    // they do not hold the L2 against whatever the program runs next
+    // the slot values' persisting lines go back to normal and the set-aside is released once
+    // the solve is over, so that they do not hold the L2 against whatever the program runs next
     if (exec && l2_window) {
         cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
         cudaGetLastError();
     }
     const PcgState &H = *hst.p;

@@ -213,6 +213,7 @@ struct ElemPcg {
     const uint16_t *key_bm = nullptr;
     const float *key_bi = nullptr;
     bool l2_window = false;  // the graph's kernels carry the L2 window over Y
+    size_t l2_bytes = 0;     // its size, the set-aside raised while a solve runs
     int64_t launches = 0;
 
     ElemPcg() = default;
