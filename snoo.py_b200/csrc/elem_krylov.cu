@@ -1267,6 +1267,7 @@ int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag,
                        const double *b, double b_scale, double *h, double rtol, double atol, int64_t maxit,
                        cudaStream_t s, int64_t *its, double *res, int *status, const uint16_t *bj_meta,
                        const float *bj_inv) {
+    bool hold = false;  // this solve raised the L2 set-aside
     SNP_REQUIRE((bj_meta == nullptr) == (bj_inv == nullptr), "element PCG: block Jacobi needs both meta and inverse");
     SNP_REQUIRE(top.n > 0 && top.n_elems > 0, "element PCG: topology not built");
     SNP_TRY(reserve(top.n, top.n_elems));
@@ -1303,9 +1304,10 @@ int ElemPcg<TT>::solve(const ElemTopology &top, const TT *T, const double *diag,
                       key_bi == bj_inv;
     if (!same) SNP_TRY(build_graph(top, T, free_mask, bj_meta, bj_inv));
     }
+    hold = exec && l2_window && l2_hold;
     if (exec) {
         // the L2 set-aside for the slot values' persisting lines, only while this solve runs
-        if (l2_window && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, l2_bytes) != cudaSuccess) cudaGetLastError();
+        if (hold && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, l2_bytes) != cudaSuccess) cudaGetLastError();
         SNP_CUDA_TRY(cudaGraphLaunch(exec, s));
     } else {
         const int chunk = 32;
@@ -1326,7 +1328,7 @@ extract:
     SNP_CUDA_TRY(cudaStreamSynchronize(s));
     // the slot values' persisting lines go back to normal and the set-aside is released once
     // the solve is over, so that they do not hold the L2 against whatever the program runs next
-    if (exec && l2_window) {
+    if (hold) {
         cudaCtxResetPersistingL2Cache();
         cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
         cudaGetLastError();

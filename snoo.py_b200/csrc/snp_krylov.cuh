@@ -214,6 +214,9 @@ struct ElemPcg {
     const float *key_bi = nullptr;
     bool l2_window = false;  // the graph's kernels carry the L2 window over Y
     size_t l2_bytes = 0;     // its size, the set-aside raised while a solve runs
+    // raise and release the context's persisting-L2 set-aside around each solve (a device-wide
+    // setting: off while several solvers run at once, snp_solver_solve_many)
+    bool l2_hold = true;
     int64_t launches = 0;
 
     ElemPcg() = default;

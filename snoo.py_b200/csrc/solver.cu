@@ -1029,9 +1029,13 @@ int snp_solver_solve_many(snp_solver *const *solvers, int32_t count, double *con
             if (rc[i] != SNP_OK) msg[i] = snp_last_error();
         }
     };
+    // the persisting-L2 set-aside is one setting of the whole context: solves running at once
+    // leave it alone (a solve alone raises it around each Krylov solve)
+    for (int32_t i = 0; i < count; ++i) solvers[i]->epcg64.l2_hold = solvers[i]->epcg32.l2_hold = false;
     std::vector<std::thread> pool;
     for (int32_t t = 0; t < nt; ++t) pool.emplace_back(worker);
     for (auto &th : pool) th.join();
+    for (int32_t i = 0; i < count; ++i) solvers[i]->epcg64.l2_hold = solvers[i]->epcg32.l2_hold = true;
     int first = -1;
     for (int32_t i = 0; i < count; ++i) {
         if (status) status[i] = rc[i];

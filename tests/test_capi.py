@@ -95,3 +95,20 @@ def test_galerkin_spd_solve_on_host():
     g = np.ones(3)
     assert L.snp_spd_solve(3, A.ctypes.data_as(P), g.ctypes.data_as(P), c.ctypes.data_as(P)) == 1
     assert b"diagonal" in L.snp_last_error()
+
+
+def test_two_phase_assembly_block_counts():
+    """The element-value blocks of the two-phase curl-curl assembly (no GPU needed): 21 per
+    matrix (upper triangle of the 6 x 6 element matrix), 6 per vector; unknown bits refused."""
+    import ctypes
+
+    from snoopy_b200 import _lib
+
+    L = _lib.load()
+    out = ctypes.c_int32()
+    for parts, want in ((_lib.TERMS_K, 21), (_lib.TERMS_K | _lib.TERMS_DK, 42), (_lib.TERMS_J | _lib.TERMS_F, 27),
+                        (_lib.TERMS_K | _lib.TERMS_DK | _lib.TERMS_RHS, 48), (_lib.TERMS_F, 6), (0, 0)):
+        assert L.snp_curlcurl_terms_stride(parts, ctypes.byref(out)) == 0
+        assert out.value == want, (parts, out.value)
+    assert L.snp_curlcurl_terms_stride(64, ctypes.byref(out)) != 0
+    assert b"unknown bits" in L.snp_last_error()

@@ -84,8 +84,10 @@ def test_rows_subsets_of_outputs():
     jf = A.assemble_device(x, 2, sf, method="rows", K=False, J=True, rhs=False, F=True)
     k_only = A.assemble_device(x, 2, sf, method="rows", K=True, J=False, rhs=False)
     f_only = A.assemble_device(x, 2, sf, method="rows", K=False, J=False, rhs=False, F=True)
+    d_only = A.assemble_device(x, 2, sf, method="rows", K=False, J=False, dK=True, rhs=False)
     torch.cuda.synchronize()
     assert torch.equal(k_only["K"], full["K"])
+    assert torch.equal(d_only["dK"], full["dK"])
     assert torch.equal(f_only["F"], full["F"])
     assert torch.equal(jf["F"], full["F"])
     assert torch.equal(jf["J"], full["J"])
