@@ -1039,16 +1039,24 @@ struct snp_batch {
     }
 
     // One pass of the solver's loop as graph nodes in `nb`: for each phase, a flag kernel and an
-    // IF node over that phase's kernels; then the loop's own condition.
+    // IF node over that phase's kernels; then the loop's own condition.  The CG phase's node
+    // holds pcg_body_unroll() CG iterations (a problem whose CG ends inside it leaves the phase,
+    // and the remaining iterations skip its units), so a pass's fixed cost (six flag kernels,
+    // five conditional nodes) is shared by several CG iterations.
     template <typename TT>
     int build_pass(Seq &nb, cudaStream_t cs, const cudaGraphConditionalHandle *hp, cudaGraphConditionalHandle hn) {
         const int phases[5] = {snp::PH_HEAD, snp::PH_CG, snp::PH_EXTRACT, snp::PH_LS, snp::PH_ACCEPT};
+        const int cg_unroll = snp::pcg_body_unroll();
         for (int k = 0; k < 5; ++k) {
             const int ph = phases[k];
             SNP_TRY(capture(nb, cs, [&](cudaStream_t s) { return flag(s, ph, 1, hp[k]); }));
             Seq body;
             SNP_TRY(add_cond(nb, hp[k], cudaGraphCondTypeIf, &body));
-            SNP_TRY(capture(body, cs, [&](cudaStream_t s) { return phase_body<TT>(ph, s); }));
+            const int reps = ph == snp::PH_CG ? cg_unroll : 1;
+            SNP_TRY(capture(body, cs, [&](cudaStream_t s) -> int {
+                for (int r = 0; r < reps; ++r) SNP_TRY(phase_body<TT>(ph, s));
+                return SNP_OK;
+            }));
         }
         return capture(nb, cs, [&](cudaStream_t s) { return flag(s, snp::PH_LIVE, 1, hn); });
     }

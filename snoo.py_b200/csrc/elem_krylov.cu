@@ -1180,7 +1180,10 @@ int ElemPcg<TT>::build_graph(const ElemTopology &top, const TT *T, const uint8_t
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
-            int rc = launch_iteration(top, T, free_mask, bj_meta, bj_inv, cs, 1, h);
+            const int unroll = pcg_body_unroll();
+            int rc = SNP_OK;
+            for (int u = 0; u < unroll && rc == SNP_OK; ++u)
+                rc = launch_iteration(top, T, free_mask, bj_meta, bj_inv, cs, 1, h);
             cudaGraph_t out = nullptr;
             cudaError_t e = cudaStreamEndCapture(cs, &out);
             ok = (rc == SNP_OK) && e == cudaSuccess;

@@ -512,7 +512,9 @@ int Pcg<VT, XT>::build_graph(const CsrView<VT> &A, const uint8_t *free_mask, XT 
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         ok = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
-            int rc = launch_iteration(A, free_mask, x, cs, 1, h);
+            const int unroll = pcg_body_unroll();
+            int rc = SNP_OK;
+            for (int u = 0; u < unroll && rc == SNP_OK; ++u) rc = launch_iteration(A, free_mask, x, cs, 1, h);
             cudaGraph_t out = nullptr;
             cudaError_t e = cudaStreamEndCapture(cs, &out);
             ok = (rc == SNP_OK) && e == cudaSuccess;

@@ -4,11 +4,24 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
 #include <functional>
 
 #include "snp_internal.cuh"
 
 namespace snp {
+
+// CG iterations captured per execution of a Krylov graph's conditional WHILE body:
+// SNP_PCG_UNROLL (1-16), default 4.  Every execution of the body costs a few microseconds
+// beyond its kernels (about 3.5 us per float64 iteration of the 1.16M-tet benchmark with one
+// iteration per body); the passes of a solve that finished inside a body return at once, so
+// the body's remaining iterations cost only their launches.
+inline int pcg_body_unroll() {
+    const char *e = getenv("SNP_PCG_UNROLL");
+    if (!e || !e[0]) return 4;
+    const int u = atoi(e);
+    return u < 1 ? 1 : (u > 16 ? 16 : u);
+}
 
 // A square sparse matrix: CSR (rp, ci, v), or, when sell_off is set, the SELL-C-sigma layout
 // of the same pattern with the values v stored in SELL order (rp/ci still describe the CSR).
