@@ -560,8 +560,13 @@ __global__ void __launch_bounds__(kBB)
             const bool fr = free_mask[i] != 0;
             DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
             TT r = TT(0);
+            unsigned mt = 0;
+            float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
             if (fr) {
-                bj_prefetch(binv, i);
+                // as the single solver's DoF pass: the DoF's words before the slot values
+                mt = meta[i];
+                if constexpr (sizeof(TT) == 4) bj_load(binv, i, ma, mb);
+                else bj_prefetch(binv, i);
                 g = G[i];
                 rx = R[i];
                 const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
@@ -572,9 +577,8 @@ __global__ void __launch_bounds__(kBB)
             s_r[threadIdx.x] = r;
             __syncthreads();
             if (fr) {
-                float4 ma, mb;
-                bj_load(binv, i, ma, mb);
-                const TT z = bj_row((unsigned)meta[i], ma, mb, s_r, threadIdx.x);
+                if constexpr (sizeof(TT) == 8) bj_load(binv, i, ma, mb);
+                const TT z = bj_row(mt, ma, mb, s_r, threadIdx.x);
                 const TT pp = pnext(beta, g.b, g.a);
                 G[i] = DofPair<TT>{z, pp};
                 R[i] = DofPair<TT>{r, rx.b + alpha * pp};

@@ -634,8 +634,14 @@ __global__ void __launch_bounds__(kEBlock)
         const bool fr = i < n && is_free(free_mask, i);
         DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
         TT r = TT(0);
+        unsigned mt = 0;
+        float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
         if (fr) {
-            bj_prefetch(binv, i);
+            // the DoF's words are requested before the slot values and the tile barrier; in
+            // float64 the block row only as an L1 prefetch (its registers would cost a block per SM)
+            mt = meta[i];
+            if constexpr (sizeof(TT) == 4) bj_load(binv, i, ma, mb);
+            else bj_prefetch(binv, i);
             g = G[i];
             rx = R[i];
             const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
@@ -646,9 +652,8 @@ __global__ void __launch_bounds__(kEBlock)
         s_r[threadIdx.x] = r;
         __syncthreads();
         if (fr) {
-            float4 ma, mb;
-            bj_load(binv, i, ma, mb);
-            const TT z = bj_row((unsigned)meta[i], ma, mb, s_r, threadIdx.x);
+            if constexpr (sizeof(TT) == 8) bj_load(binv, i, ma, mb);
+            const TT z = bj_row(mt, ma, mb, s_r, threadIdx.x);
             const TT p = pnext(beta, g.b, g.a);
             G[i] = DofPair<TT>{z, p};
             R[i] = DofPair<TT>{r, rx.b + alpha * p};
@@ -834,8 +839,12 @@ __global__ void __launch_bounds__(kEBlock, kPass1MinBlocks)
                 const bool fr = i < n && is_free(free_mask, i);
                 DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
                 TT r = TT(0);
+                unsigned mt = 0;
+                float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
                 if (fr) {
-                    bj_prefetch(binv, i);
+                    mt = meta[i];
+                    if constexpr (sizeof(TT) == 4) bj_load(binv, i, ma, mb);
+                    else bj_prefetch(binv, i);
                     g = G[i];
                     rx = R[i];
                     const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
@@ -846,9 +855,8 @@ __global__ void __launch_bounds__(kEBlock, kPass1MinBlocks)
                 s_r[threadIdx.x] = r;
                 __syncthreads();
                 if (fr) {
-                    float4 ma, mb;
-                    bj_load(binv, i, ma, mb);
-                    const TT z = bj_row((unsigned)meta[i], ma, mb, s_r, threadIdx.x);
+                    if constexpr (sizeof(TT) == 8) bj_load(binv, i, ma, mb);
+                    const TT z = bj_row(mt, ma, mb, s_r, threadIdx.x);
                     const TT p = pnext(tb, g.b, g.a);
                     G[i] = DofPair<TT>{z, p};
                     R[i] = DofPair<TT>{r, rx.b + ta * p};
