@@ -623,15 +623,31 @@ __global__ void __launch_bounds__(kEBlock)
                 cudaGraphConditionalHandle cond) {
     __shared__ double sh2[2][32];
     __shared__ TT s_r[kBjTile];
+    // each tile's slot range is read one tile ahead (the first one before the CG state), so
+    // that a tile's slot values are requested together with its DoF words
+    const int64_t tstride = (int64_t)gridDim.x * kBjTile;
+    int nb0 = 0, nb1 = 0;
+    {
+        const int64_t i0 = (int64_t)blockIdx.x * kBjTile + threadIdx.x;
+        if (i0 < n) {
+            nb0 = __ldcs(inc_ptr + i0);
+            nb1 = __ldcs(inc_ptr + i0 + 1);
+        }
+    }
     if (st->done) {
         if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
         return;
     }
     const TT alpha = (TT)st->alpha, beta = (TT)st->beta;
     double rz = 0.0, rr = 0.0;
-    for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += (int64_t)gridDim.x * kBjTile) {
+    for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += tstride) {
         const int64_t i = base + threadIdx.x;
         const bool fr = i < n && is_free(free_mask, i);
+        const int b0 = nb0, b1 = nb1;
+        if (i + tstride < n) {
+            nb0 = __ldcs(inc_ptr + i + tstride);
+            nb1 = __ldcs(inc_ptr + i + tstride + 1);
+        }
         DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
         TT r = TT(0);
         unsigned mt = 0;
@@ -644,7 +660,6 @@ __global__ void __launch_bounds__(kEBlock)
             else bj_prefetch(binv, i);
             g = G[i];
             rx = R[i];
-            const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
             double q = 0.0;
             for (int t = b0; t < b1; ++t) q += (double)Y[t];
             r = rx.a - alpha * (TT)q;
