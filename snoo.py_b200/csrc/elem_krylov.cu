@@ -178,29 +178,37 @@ __global__ void __launch_bounds__(kEBlock, kPass1MinBlocks)
              TT *__restrict__ Y, PcgState *st, double *part) {
     __shared__ TT sc[18];
     __shared__ double sh[32];
-    if (st->done) return;
-    load_chat(sc, chat);
-    const TT beta = (TT)st->beta;
     const int lane = threadIdx.x & 31;
     const int h = lane & 1;  // edges 3h .. 3h+2
-    double dot = 0.0;
     // a warp takes 16 consecutive elements per pass; the loop bound is uniform across the warp
     const int64_t wstride = (int64_t)gridDim.x * (blockDim.x >> 5) * 16;
-#pragma unroll 1
-    for (int64_t e0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 16; e0 < ne; e0 += wstride) {
+    const int64_t first = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 16;
+    // every streamed word of a pass is requested before its gathers: the lane's three DoF words,
+    // slots and tensor components (the partner lane holds the other three); the first pass's
+    // words before the CG state is read
+    int32_t d[3], ps[3];
+    TT th[3];
+    auto stream_in = [&](int64_t e0) {
         const int64_t e = e0 + (lane >> 1);
         const bool valid = e < ne;
         const int64_t eb = eslot(valid ? e : 0, 0);
-        // every streamed word of this pass is requested before the gathers: the lane's three
-        // DoF words, slots and tensor components (the partner lane holds the other three)
-        int32_t d[3], ps[3];
-        TT th[3];
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             d[j] = valid ? __ldcs(edof + eb + 32 * (3 * h + j)) : 0;
             ps[j] = valid ? __ldcs(pos + eb + 32 * (3 * h + j)) : 0;
             th[j] = valid ? __ldcs(T + eb + 32 * (3 * h + j)) : TT(0);
         }
+    };
+    if (first < ne) stream_in(first);
+    if (st->done) return;
+    load_chat(sc, chat);
+    const TT beta = (TT)st->beta;
+    double dot = 0.0;
+#pragma unroll 1
+    for (int64_t e0 = first; e0 < ne; e0 += wstride) {
+        const int64_t e = e0 + (lane >> 1);
+        const bool valid = e < ne;
+        if (e0 != first) stream_in(e0);
         DofPair<TT> w[3];
 #pragma unroll
         for (int j = 0; j < 3; ++j) w[j] = G[(uint32_t)d[j] & ~kSignBit];
@@ -625,13 +633,21 @@ __global__ void __launch_bounds__(kEBlock)
     __shared__ TT s_r[kBjTile];
     // each tile's slot range is read one tile ahead (the first one before the CG state), so
     // that a tile's slot values are requested together with its DoF words
+    // In float32 the tile's DoF states {z, p}, {r, x} are read one tile ahead as well (in float64
+    // their registers would cost a resident block per SM).
+    constexpr bool kStateAhead = sizeof(TT) == 4;
     const int64_t tstride = (int64_t)gridDim.x * kBjTile;
     int nb0 = 0, nb1 = 0;
+    DofPair<TT> ng{TT(0), TT(0)}, nrx{TT(0), TT(0)};
     {
         const int64_t i0 = (int64_t)blockIdx.x * kBjTile + threadIdx.x;
         if (i0 < n) {
             nb0 = __ldcs(inc_ptr + i0);
             nb1 = __ldcs(inc_ptr + i0 + 1);
+            if constexpr (kStateAhead) {
+                ng = G[i0];
+                nrx = R[i0];
+            }
         }
     }
     if (st->done) {
@@ -644,11 +660,21 @@ __global__ void __launch_bounds__(kEBlock)
         const int64_t i = base + threadIdx.x;
         const bool fr = i < n && is_free(free_mask, i);
         const int b0 = nb0, b1 = nb1;
+        DofPair<TT> g = ng, rx = nrx;
         if (i + tstride < n) {
             nb0 = __ldcs(inc_ptr + i + tstride);
             nb1 = __ldcs(inc_ptr + i + tstride + 1);
+            if constexpr (kStateAhead) {
+                ng = G[i + tstride];
+                nrx = R[i + tstride];
+            }
         }
-        DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
+        if constexpr (!kStateAhead) {
+            if (fr) {
+                g = G[i];
+                rx = R[i];
+            }
+        }
         TT r = TT(0);
         unsigned mt = 0;
         float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
@@ -658,8 +684,6 @@ __global__ void __launch_bounds__(kEBlock)
             mt = meta[i];
             if constexpr (sizeof(TT) == 4) bj_load(binv, i, ma, mb);
             else bj_prefetch(binv, i);
-            g = G[i];
-            rx = R[i];
             double q = 0.0;
             for (int t = b0; t < b1; ++t) q += (double)Y[t];
             r = rx.a - alpha * (TT)q;
