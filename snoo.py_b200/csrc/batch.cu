@@ -457,7 +457,24 @@ __global__ void __launch_bounds__(BS)
     const int warp = threadIdx.x >> 5;
     constexpr int kWarps = BS / 32;
     const int64_t wstride = (int64_t)gridDim.x * kWarps;
+    // as the single solver's element pass: a group's streamed words are requested before its
+    // gathers, the chunk's first group's before its problem's state is read (every padded chunk
+    // position is allocated, so the words are read unconditionally and used only for elements of
+    // the problem), and in float32 each group's words one group ahead
+    constexpr bool kAhead = sizeof(TT) == 4;
+    int32_t d[3], ps[3], nd[3], nps[3];
+    TT th[3], nth[3];
+    auto stream_in = [&](int64_t c, int g, int32_t(&od)[3], int32_t(&ops)[3], TT(&oth)[3]) {
+        const int64_t eb = eslot(c * kChunk + g * kGroup + (lane >> 1), 0);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            od[j] = __ldcs(edof + eb + 32 * (3 * h + j));
+            ops[j] = __ldcs(pos + eb + 32 * (3 * h + j));
+            oth[j] = __ldcs(T + eb + 32 * (3 * h + j));
+        }
+    };
     for (int64_t c = (int64_t)blockIdx.x * kWarps + warp; c < n_chunks; c += wstride) {
+        stream_in(c, 0, d, ps, th);
         const int p = chunk_inst[c];
         if (st[p].ph != PH_CG) continue;  // uniform across the warp
         const TT beta = (TT)st[p].beta;
@@ -467,14 +484,18 @@ __global__ void __launch_bounds__(BS)
         for (int g = 0; g < kGroups; ++g) {
             const int64_t e = c * kChunk + g * kGroup + (lane >> 1);
             const bool valid = e < e_end;
-            const int64_t eb = eslot(valid ? e : 0, 0);
-            int32_t d[3], ps[3];
-            TT th[3];
+            if constexpr (kAhead) {
+                if (g > 0) {
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                d[j] = valid ? __ldcs(edof + eb + 32 * (3 * h + j)) : 0;
-                ps[j] = valid ? __ldcs(pos + eb + 32 * (3 * h + j)) : 0;
-                th[j] = valid ? __ldcs(T + eb + 32 * (3 * h + j)) : TT(0);
+                    for (int j = 0; j < 3; ++j) {
+                        d[j] = nd[j];
+                        ps[j] = nps[j];
+                        th[j] = nth[j];
+                    }
+                }
+                if (g + 1 < kGroups) stream_in(c, g + 1, nd, nps, nth);
+            } else {
+                if (g > 0) stream_in(c, g, d, ps, th);
             }
             DofPair<TT> w[3];
 #pragma unroll
@@ -551,6 +572,21 @@ __global__ void __launch_bounds__(kBB)
     __shared__ int s_any;
     count_launch(ctl);
     for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
+        // as the single solver's DoF pass: each tile's slot range one tile ahead (the unit's first
+        // before its problem's state is read), in float32 the DoF states too, the DoF's other
+        // words before the slot values
+        constexpr bool kStateAhead = sizeof(TT) == 4;
+        int nb0, nb1;
+        DofPair<TT> ng{TT(0), TT(0)}, nrx{TT(0), TT(0)};
+        {
+            const int64_t i0 = u * kUnit + threadIdx.x;
+            nb0 = __ldcs(inc_ptr + i0);
+            nb1 = __ldcs(inc_ptr + i0 + 1);
+            if constexpr (kStateAhead) {
+                ng = G[i0];
+                nrx = R[i0];
+            }
+        }
         const int p = unit_inst[u];
         if (st[p].ph != PH_CG) continue;  // uniform across the block
         const TT alpha = (TT)st[p].alpha, beta = (TT)st[p].beta;
@@ -558,18 +594,29 @@ __global__ void __launch_bounds__(kBB)
         for (int t = 0; t < kUnitTiles; ++t) {
             const int64_t i = u * kUnit + t * kBB + threadIdx.x;
             const bool fr = free_mask[i] != 0;
-            DofPair<TT> g{TT(0), TT(0)}, rx{TT(0), TT(0)};
+            const int b0 = nb0, b1 = nb1;
+            DofPair<TT> g = ng, rx = nrx;
+            if (t + 1 < kUnitTiles) {
+                nb0 = __ldcs(inc_ptr + i + kBB);
+                nb1 = __ldcs(inc_ptr + i + kBB + 1);
+                if constexpr (kStateAhead) {
+                    ng = G[i + kBB];
+                    nrx = R[i + kBB];
+                }
+            }
+            if constexpr (!kStateAhead) {
+                if (fr) {
+                    g = G[i];
+                    rx = R[i];
+                }
+            }
             TT r = TT(0);
             unsigned mt = 0;
             float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
             if (fr) {
-                // as the single solver's DoF pass: the DoF's words before the slot values
                 mt = meta[i];
                 if constexpr (sizeof(TT) == 4) bj_load(binv, i, ma, mb);
                 else bj_prefetch(binv, i);
-                g = G[i];
-                rx = R[i];
-                const int b0 = __ldcs(inc_ptr + i), b1 = __ldcs(inc_ptr + i + 1);
                 double q = 0.0;
                 for (int k = b0; k < b1; ++k) q += (double)Y[k];
                 r = rx.a - alpha * (TT)q;
