@@ -211,3 +211,26 @@ def test_gmres_newton_reaches_the_cg_answer(precond):
     Bc = solver.evaluate_B(x_cg, probes, el)
     Bg = solver.evaluate_B(x_gm, probes, el)
     assert float(np.abs(Bg - Bc).max() / np.abs(Bc).max()) < 1e-7
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_iterations_per_graph_body_do_not_change_the_answer(precision):
+    """The Krylov graph's loop body holds SNP_PCG_UNROLL CG iterations (read when the graph is
+    built); the passes of a finished solve return at once, so one and four iterations per body
+    give bitwise the same Newton solve, CG count and residual."""
+    import os
+
+    out = {}
+    for unroll in ("1", "4"):
+        os.environ["SNP_PCG_UNROLL"] = unroll
+        try:
+            msh, coils, rel, solver = _setup(15000, seed=11)
+            x, st = solver.solve_to_residual(1e-8, precision=precision)
+        finally:
+            del os.environ["SNP_PCG_UNROLL"]
+        out[unroll] = (x, st)
+    (x1, s1), (x4, s4) = out["1"], out["4"]
+    assert s1["rel_res"] <= 1e-8
+    assert np.array_equal(x1, x4)
+    assert (s1["newton_iterations"], s1["cg_iterations"], s1["res"]) == (s4["newton_iterations"], s4["cg_iterations"],
+                                                                         s4["res"])
