@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(kBB)
 // (64 steps of 16 elements): each step's p.Jp partial is summed by a fixed shuffle tree and added
 // to the chunk's sum in step order, with no block barrier inside the pass.
 template <typename TT, int BS>
-__global__ void __launch_bounds__(BS)
+__global__ void __launch_bounds__(BS, 1)
     k_b_pass1(int n_inst, const BInst *__restrict__ inst, const int32_t *__restrict__ chunk_inst, int64_t n_chunks,
               const int32_t *__restrict__ edof, const int32_t *__restrict__ pos, const TT *__restrict__ T,
               const TT *__restrict__ chat, const DofPair<TT> *__restrict__ G, TT *__restrict__ Y, BState *st,
