@@ -501,8 +501,9 @@ def warm_start_study(base_tets, n_train, n_test, n_modes=128, hidden=256, epochs
     # the same warm-started mixed solves, `batch` members at a time: one solver per member, each
     # on its own stream and host thread (snp_solver_solve_many); wall clock around each batch's
     # predictions and solves (moving the solvers to their members is not timed, as above).
-    # Smaller meshes leave more of the GPU idle per solve, so they run more members at once.
-    batch = min(16 if fam.mesh.num_elements < 600_000 else 4, len(P_test))
+    # Smaller meshes leave more of the GPU idle per solve, so they run more members at once (at
+    # 287k tets a sweep gave 145 / 157 / 162 / 161 solves/s for 8 / 16 / 24 / 32 at once).
+    batch = min(24 if fam.mesh.num_elements < 600_000 else 4, len(P_test))
     if batch > 1:
         extra = [SG.MorphedSolver(fam, stream=torch.cuda.Stream()) for _ in range(batch)]
         if galerkin_modes > 0:
