@@ -438,13 +438,50 @@ __global__ void __launch_bounds__(kBB)
     }
 }
 
+// The problems in their CG phase, compacted for the CG passes (k_b_cg_list, once per CG phase
+// node): act[0] = m, act[1 + j] = the j-th such problem (problem order), act[1 + n_inst + j] and
+// act[2 + 2 n_inst + j] the prefix sums of their units and chunks (m + 1 entries each).  The
+// passes walk only those units and chunks, so a pass with one problem left costs that problem's
+// work and not a sweep over every problem's.  A problem that leaves CG during the unrolled CG
+// iterations of the node stays listed and is skipped by its phase test.
+inline int act_size(int n_inst) { return 3 + 3 * n_inst; }
+
+__global__ void k_b_cg_list(int n_inst, const BInst *__restrict__ inst, const BState *__restrict__ st,
+                            int32_t *__restrict__ act, BCtl *ctl) {
+    count_launch(ctl);
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int32_t *ids = act + 1, *up = act + 1 + n_inst, *cp = act + 2 + 2 * n_inst;
+    int m = 0;
+    up[0] = 0;
+    cp[0] = 0;
+    for (int p = 0; p < n_inst; ++p) {
+        if (st[p].ph != PH_CG) continue;
+        ids[m] = p;
+        up[m + 1] = up[m] + inst[p].n_units;
+        cp[m + 1] = cp[m] + inst[p].n_chunks;
+        ++m;
+    }
+    act[0] = m;
+}
+
+// the listed problem j (< m) whose prefix range [pre[j], pre[j + 1]) holds k
+__device__ __forceinline__ int act_find(const int32_t *__restrict__ pre, int m, int64_t k) {
+    int lo = 0, hi = m;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pre[mid] <= k) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // Element pass of a CG iteration over the chunks of the problems still iterating: as the
 // single-problem k_epass1 (two lanes per element, three edges each).  A warp owns a whole chunk
 // (64 steps of 16 elements): each step's p.Jp partial is summed by a fixed shuffle tree and added
 // to the chunk's sum in step order, with no block barrier inside the pass.
 template <typename TT, int BS>
 __global__ void __launch_bounds__(BS, 1)
-    k_b_pass1(int n_inst, const BInst *__restrict__ inst, const int32_t *__restrict__ chunk_inst, int64_t n_chunks,
+    k_b_pass1(int n_inst, const BInst *__restrict__ inst, const int32_t *__restrict__ act,
               const int32_t *__restrict__ edof, const int32_t *__restrict__ pos, const TT *__restrict__ T,
               const TT *__restrict__ chat, const DofPair<TT> *__restrict__ G, TT *__restrict__ Y, BState *st,
               double *part, BCtl *ctl) {
@@ -473,9 +510,14 @@ __global__ void __launch_bounds__(BS, 1)
             oth[j] = __ldcs(T + eb + 32 * (3 * h + j));
         }
     };
-    for (int64_t c = (int64_t)blockIdx.x * kWarps + warp; c < n_chunks; c += wstride) {
+    const int m = act[0];
+    const int32_t *cpre = act + 2 + 2 * n_inst;
+    const int64_t total = cpre[m];
+    for (int64_t k = (int64_t)blockIdx.x * kWarps + warp; k < total; k += wstride) {
+        const int j = act_find(cpre, m, k);
+        const int p = act[1 + j];
+        const int64_t c = inst[p].chunk0 + (k - cpre[j]);
         stream_in(c, 0, d, ps, th);
-        const int p = chunk_inst[c];
         if (st[p].ph != PH_CG) continue;  // uniform across the warp
         const TT beta = (TT)st[p].beta;
         const int64_t e_end = inst[p].elem_off + inst[p].ne;
@@ -562,7 +604,7 @@ __global__ void __launch_bounds__(BS, 1)
 // p = z + beta p, x += alpha p; the last block moves each problem's CG state on.
 template <typename TT>
 __global__ void __launch_bounds__(kBB)
-    k_b_pass2(int n_inst, const BInst *__restrict__ inst, const int32_t *__restrict__ unit_inst, int64_t n_units,
+    k_b_pass2(int n_inst, const BInst *__restrict__ inst, const int32_t *__restrict__ act,
               const uint8_t *__restrict__ free_mask, const int32_t *__restrict__ inc_ptr, const TT *__restrict__ Y,
               const uint16_t *__restrict__ meta, const float *__restrict__ binv, DofPair<TT> *__restrict__ G,
               DofPair<TT> *__restrict__ R, BState *st, double *part, BCtl *ctl, int use_cond,
@@ -571,7 +613,13 @@ __global__ void __launch_bounds__(kBB)
     __shared__ TT s_r[kBB];
     __shared__ int s_any;
     count_launch(ctl);
-    for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int m = act[0];
+    const int32_t *upre = act + 1 + n_inst;
+    const int64_t total = upre[m];
+    for (int64_t k = blockIdx.x; k < total; k += gridDim.x) {
+        const int j = act_find(upre, m, k);
+        const int p = act[1 + j];
+        const int64_t u = inst[p].unit0 + (k - upre[j]);
         // as the single solver's DoF pass: each tile's slot range one tile ahead (the unit's first
         // before its problem's state is read), in float32 the DoF states too, the DoF's other
         // words before the slot values
@@ -587,7 +635,6 @@ __global__ void __launch_bounds__(kBB)
                 nrx = R[i0];
             }
         }
-        const int p = unit_inst[u];
         if (st[p].ph != PH_CG) continue;  // uniform across the block
         const TT alpha = (TT)st[p].alpha, beta = (TT)st[p].beta;
         double rz = 0.0, rr = 0.0;
@@ -875,6 +922,7 @@ struct snp_batch {
     snp::DevBuf<snp::BCtl> ctl;
     snp::HostBuf<snp::BCtl> hctl;
     snp::DevBuf<int32_t> unit_inst, chunk_inst, edof, pos, inc, inc_ptr;
+    snp::DevBuf<int32_t> act;  // the problems in CG, compacted (k_b_cg_list)
     snp::DevBuf<uint8_t> free_mask;
     snp::DevBuf<uint16_t> meta;
     snp::DevBuf<double> x, xw, h, F, diag, Fe, De, bmat, part;
@@ -993,17 +1041,17 @@ struct snp_batch {
     int pass1(cudaStream_t s, int block) {
         switch (block) {
             case 128:
-                snp::k_b_pass1<TT, 128><<<grid_chunks(128), 128, 0, s>>>(count, inst.p, chunk_inst.p, n_chunks, edof.p,
+                snp::k_b_pass1<TT, 128><<<grid_chunks(128), 128, 0, s>>>(count, inst.p, act.p, edof.p,
                                                                          pos.p, Tp<TT>(), chat<TT>(), Gp<TT>(),
                                                                          Yp<TT>(), st.p, part.p, ctl.p);
                 break;
             case 512:
-                snp::k_b_pass1<TT, 512><<<grid_chunks(512), 512, 0, s>>>(count, inst.p, chunk_inst.p, n_chunks, edof.p,
+                snp::k_b_pass1<TT, 512><<<grid_chunks(512), 512, 0, s>>>(count, inst.p, act.p, edof.p,
                                                                          pos.p, Tp<TT>(), chat<TT>(), Gp<TT>(),
                                                                          Yp<TT>(), st.p, part.p, ctl.p);
                 break;
             default:
-                snp::k_b_pass1<TT, 256><<<grid_chunks(256), 256, 0, s>>>(count, inst.p, chunk_inst.p, n_chunks, edof.p,
+                snp::k_b_pass1<TT, 256><<<grid_chunks(256), 256, 0, s>>>(count, inst.p, act.p, edof.p,
                                                                          pos.p, Tp<TT>(), chat<TT>(), Gp<TT>(),
                                                                          Yp<TT>(), st.p, part.p, ctl.p);
                 break;
@@ -1012,10 +1060,25 @@ struct snp_batch {
         return SNP_OK;
     }
 
+    // the compacted list of the problems in CG, for the passes of the CG iterations that follow
+    int cg_list(cudaStream_t s) {
+        snp::k_b_cg_list<<<1, 32, 0, s>>>(count, inst.p, st.p, act.p, ctl.p);
+        SNP_LAUNCH_CHECK();
+        return SNP_OK;
+    }
+
+    // the CG phase: the list, then `reps` CG iterations
+    template <typename TT>
+    int phase_cg(cudaStream_t s, int reps) {
+        SNP_TRY(cg_list(s));
+        for (int r = 0; r < reps; ++r) SNP_TRY(phase_cg_body<TT>(s, 0, 0));
+        return SNP_OK;
+    }
+
     template <typename TT>
     int phase_cg_body(cudaStream_t s, int use_cond, cudaGraphConditionalHandle cg) {
         SNP_TRY(pass1<TT>(s, pass1_block));
-        snp::k_b_pass2<TT><<<grid_units(), snp::kBB, 0, s>>>(count, inst.p, unit_inst.p, n_units, free_mask.p,
+        snp::k_b_pass2<TT><<<grid_units(), snp::kBB, 0, s>>>(count, inst.p, act.p, free_mask.p,
                                                              inc_ptr.p, Yp<TT>(), meta.p, binv.p, Gp<TT>(), Rp<TT>(),
                                                              st.p, part.p, ctl.p, use_cond, cg);
         SNP_LAUNCH_CHECK();
@@ -1103,10 +1166,8 @@ struct snp_batch {
             SNP_TRY(capture(nb, cs, [&](cudaStream_t s) { return flag(s, ph, 1, hp[k]); }));
             Seq body;
             SNP_TRY(add_cond(nb, hp[k], cudaGraphCondTypeIf, &body));
-            const int reps = ph == snp::PH_CG ? cg_unroll : 1;
             SNP_TRY(capture(body, cs, [&](cudaStream_t s) -> int {
-                for (int r = 0; r < reps; ++r) SNP_TRY(phase_body<TT>(ph, s));
-                return SNP_OK;
+                return ph == snp::PH_CG ? phase_cg<TT>(s, cg_unroll) : phase_body<TT>(ph, s);
             }));
         }
         return capture(nb, cs, [&](cudaStream_t s) { return flag(s, snp::PH_LIVE, 1, hn); });
@@ -1117,7 +1178,7 @@ struct snp_batch {
     int phase_body(int ph, cudaStream_t s) {
         switch (ph) {
             case snp::PH_HEAD: return phase_step_head<TT>(s, 0, 0);
-            case snp::PH_CG: return phase_cg_body<TT>(s, 0, 0);
+            case snp::PH_CG: return phase_cg<TT>(s, 1);
             case snp::PH_EXTRACT: return phase_extract<TT>(s, 0, 0);
             case snp::PH_LS: return phase_ls_body<TT>(s, 0, 0);
             default: return phase_accept(s, 0, 0);
@@ -1267,6 +1328,7 @@ int tune_t(snp_batch *b) {
     SNP_CUDA_TRY(cudaMemsetAsync(b->x.p, 0, sizeof(double) * b->n_tot, s));
     SNP_TRY(b->phase_start<TT>(s, 0, 0));
     SNP_TRY(b->phase_step_head<TT>(s, 0, 0));
+    SNP_TRY(b->cg_list(s));
     const int blocks[3] = {128, 256, 512};
     double best = 1e300;
     int best_b = b->pass1_block;
@@ -1393,6 +1455,7 @@ int snp_batch_create(snp_solver *const *solvers, int32_t count, snp_batch **out)
     SNP_TRY(B->hctl.alloc(1));
     SNP_TRY(B->unit_inst.alloc(B->n_units));
     SNP_TRY(B->chunk_inst.alloc(B->n_chunks));
+    SNP_TRY(B->act.alloc(snp::act_size(count)));
     SNP_TRY(B->edof.alloc(es));
     SNP_TRY(B->pos.alloc(es));
     SNP_TRY(B->inc.alloc(std::max<int64_t>(incn, 1)));
