@@ -476,11 +476,15 @@ __device__ __forceinline__ int act_find(const int32_t *__restrict__ pre, int m, 
 }
 
 // Element pass of a CG iteration over the chunks of the problems still iterating: as the
-// single-problem k_epass1 (two lanes per element, three edges each).  A warp owns a whole chunk
-// (64 steps of 16 elements): each step's p.Jp partial is summed by a fixed shuffle tree and added
-// to the chunk's sum in step order, with no block barrier inside the pass.
+// single-problem k_epass1 (two lanes per element, three edges each).  Four warps of a block
+// share a chunk, four steps of 16 elements each (so that one problem left alone still has a
+// warp per 64 elements); each step's p.Jp partial is summed by a fixed shuffle tree and added to
+// the warp's sum in step order, and the chunk's sum is the four warps' sums added in warp order
+// (shared memory, one block barrier per chunk step): fixed whatever the batch and launch shape.
+constexpr int kSplit = 4;                     // warps per chunk
+constexpr int kWarpGroups = kGroups / kSplit;  // steps per warp
 template <typename TT, int BS>
-__global__ void __launch_bounds__(BS, 1)
+__global__ void __launch_bounds__(BS, 1024 / BS)
     k_b_pass1(int n_inst, const BInst *__restrict__ inst, const int32_t *__restrict__ act,
               const int32_t *__restrict__ edof, const int32_t *__restrict__ pos, const TT *__restrict__ T,
               const TT *__restrict__ chat, const DofPair<TT> *__restrict__ G, TT *__restrict__ Y, BState *st,
@@ -493,7 +497,6 @@ __global__ void __launch_bounds__(BS, 1)
     const int h = lane & 1;  // edges 3h .. 3h+2
     const int warp = threadIdx.x >> 5;
     constexpr int kWarps = BS / 32;
-    const int64_t wstride = (int64_t)gridDim.x * kWarps;
     // as the single solver's element pass: a group's streamed words are requested before its
     // gathers, the chunk's first group's before its problem's state is read (every padded chunk
     // position is allocated, so the words are read unconditionally and used only for elements of
@@ -510,81 +513,97 @@ __global__ void __launch_bounds__(BS, 1)
             oth[j] = __ldcs(T + eb + 32 * (3 * h + j));
         }
     };
+    __shared__ double s_acc[kWarps];
     const int m = act[0];
     const int32_t *cpre = act + 2 + 2 * n_inst;
     const int64_t total = cpre[m];
-    for (int64_t k = (int64_t)blockIdx.x * kWarps + warp; k < total; k += wstride) {
-        const int j = act_find(cpre, m, k);
-        const int p = act[1 + j];
-        const int64_t c = inst[p].chunk0 + (k - cpre[j]);
-        stream_in(c, 0, d, ps, th);
-        if (st[p].ph != PH_CG) continue;  // uniform across the warp
-        const TT beta = (TT)st[p].beta;
-        const int64_t e_end = inst[p].elem_off + inst[p].ne;
-        double acc = 0.0;
-#pragma unroll 1
-        for (int g = 0; g < kGroups; ++g) {
-            const int64_t e = c * kChunk + g * kGroup + (lane >> 1);
-            const bool valid = e < e_end;
-            if constexpr (kAhead) {
-                if (g > 0) {
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        d[j] = nd[j];
-                        ps[j] = nps[j];
-                        th[j] = nth[j];
-                    }
-                }
-                if (g + 1 < kGroups) stream_in(c, g + 1, nd, nps, nth);
-            } else {
-                if (g > 0) stream_in(c, g, d, ps, th);
-            }
-            DofPair<TT> w[3];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) w[j] = valid ? G[(uint32_t)d[j] & ~kSignBit] : DofPair<TT>{TT(0), TT(0)};
-            TT u0 = TT(0), u1 = TT(0), u2 = TT(0);
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                TT pk = pnext(beta, w[j].b, w[j].a);
-                if (d[j] < 0) pk = -pk;
-                const TT *cc = sc + 3 * (3 * h + j);
-                u0 += pk * cc[0];
-                u1 += pk * cc[1];
-                u2 += pk * cc[2];
-            }
-            if (!valid) u0 = u1 = u2 = TT(0);
-            // u_e = (edges 0-2) + (edges 3-5), added in that order on both lanes
-            const TT o0 = __shfl_xor_sync(0xffffffffu, u0, 1);
-            const TT o1 = __shfl_xor_sync(0xffffffffu, u1, 1);
-            const TT o2 = __shfl_xor_sync(0xffffffffu, u2, 1);
-            if (h) {
-                u0 = o0 + u0;
-                u1 = o1 + u1;
-                u2 = o2 + u2;
-            } else {
-                u0 = u0 + o0;
-                u1 = u1 + o1;
-                u2 = u2 + o2;
-            }
-            TT t[6];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const TT other = __shfl_xor_sync(0xffffffffu, th[j], 1);
-                t[j] = h ? other : th[j];
-                t[3 + j] = h ? th[j] : other;
-            }
-            const TT v0 = t[0] * u0 + t[1] * u1 + t[2] * u2;
-            const TT v1 = t[1] * u0 + t[3] * u1 + t[4] * u2;
-            const TT v2 = t[2] * u0 + t[4] * u1 + t[5] * u2;
-            double dot = 0.0;
-            if (valid && !h) dot = (double)u0 * (double)v0 + (double)u1 * (double)v1 + (double)u2 * (double)v2;
-            if (valid) {
-#pragma unroll
-                for (int j = 0; j < 3; ++j) Y[ps[j]] = edge_term(sc, 3 * h + j, d[j] < 0, v0, v1, v2);
-            }
-            acc += warp_sum(dot);
+    constexpr int kPerStep = kWarps / kSplit;  // chunks per block step
+    const int q = warp % kSplit;               // this warp's quarter of its chunk
+    for (int64_t kb = (int64_t)blockIdx.x * kPerStep; kb < total; kb += (int64_t)gridDim.x * kPerStep) {
+        const int64_t k = kb + warp / kSplit;
+        bool active = k < total;
+        int p = 0;
+        int64_t c = 0;
+        if (active) {
+            const int j = act_find(cpre, m, k);
+            p = act[1 + j];
+            c = inst[p].chunk0 + (k - cpre[j]);
+            stream_in(c, q * kWarpGroups, d, ps, th);
+            active = st[p].ph == PH_CG;  // uniform across the warp
         }
-        if (lane == 0) part[c] = acc;
+        double acc = 0.0;
+        if (active) {
+            const TT beta = (TT)st[p].beta;
+            const int64_t e_end = inst[p].elem_off + inst[p].ne;
+#pragma unroll 1
+            for (int g = q * kWarpGroups; g < (q + 1) * kWarpGroups; ++g) {
+                const int64_t e = c * kChunk + g * kGroup + (lane >> 1);
+                const bool valid = e < e_end;
+                if constexpr (kAhead) {
+                    if (g > q * kWarpGroups) {
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            d[j] = nd[j];
+                            ps[j] = nps[j];
+                            th[j] = nth[j];
+                        }
+                    }
+                    if (g + 1 < (q + 1) * kWarpGroups) stream_in(c, g + 1, nd, nps, nth);
+                } else {
+                    if (g > q * kWarpGroups) stream_in(c, g, d, ps, th);
+                }
+                DofPair<TT> w[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    w[j] = valid ? G[(uint32_t)d[j] & ~kSignBit] : DofPair<TT>{TT(0), TT(0)};
+                TT u0 = TT(0), u1 = TT(0), u2 = TT(0);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    TT pk = pnext(beta, w[j].b, w[j].a);
+                    if (d[j] < 0) pk = -pk;
+                    const TT *cc = sc + 3 * (3 * h + j);
+                    u0 += pk * cc[0];
+                    u1 += pk * cc[1];
+                    u2 += pk * cc[2];
+                }
+                if (!valid) u0 = u1 = u2 = TT(0);
+                // u_e = (edges 0-2) + (edges 3-5), added in that order on both lanes
+                const TT o0 = __shfl_xor_sync(0xffffffffu, u0, 1);
+                const TT o1 = __shfl_xor_sync(0xffffffffu, u1, 1);
+                const TT o2 = __shfl_xor_sync(0xffffffffu, u2, 1);
+                if (h) {
+                    u0 = o0 + u0;
+                    u1 = o1 + u1;
+                    u2 = o2 + u2;
+                } else {
+                    u0 = u0 + o0;
+                    u1 = u1 + o1;
+                    u2 = u2 + o2;
+                }
+                TT t[6];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const TT other = __shfl_xor_sync(0xffffffffu, th[j], 1);
+                    t[j] = h ? other : th[j];
+                    t[3 + j] = h ? th[j] : other;
+                }
+                const TT v0 = t[0] * u0 + t[1] * u1 + t[2] * u2;
+                const TT v1 = t[1] * u0 + t[3] * u1 + t[4] * u2;
+                const TT v2 = t[2] * u0 + t[4] * u1 + t[5] * u2;
+                double dot = 0.0;
+                if (valid && !h) dot = (double)u0 * (double)v0 + (double)u1 * (double)v1 + (double)u2 * (double)v2;
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) Y[ps[j]] = edge_term(sc, 3 * h + j, d[j] < 0, v0, v1, v2);
+                }
+                acc += warp_sum(dot);
+            }
+        }
+        if (lane == 0) s_acc[warp] = acc;
+        __syncthreads();
+        if (active && q == 0 && lane == 0)
+            part[c] = ((s_acc[warp] + s_acc[warp + 1]) + s_acc[warp + 2]) + s_acc[warp + 3];
+        __syncthreads();
     }
     if (!last_block(&ctl->counter)) return;
     const int nw = blockDim.x >> 5;
@@ -974,7 +993,7 @@ struct snp_batch {
     int grid_units() const { return (int)std::min<int64_t>(n_units, (int64_t)snp::sm_count() * 8); }
     int grid_chunks(int block) const {
         const int per_sm = std::max(1, 2048 / block);
-        const int64_t need = (n_chunks + block / 32 - 1) / (block / 32);  // a warp per chunk
+        const int64_t need = (n_chunks * snp::kSplit + block / 32 - 1) / (block / 32);  // kSplit warps per chunk
         return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)snp::sm_count() * per_sm));
     }
     int run_stride() const { return (int)(sizeof(snp::BState) / sizeof(int32_t)); }
