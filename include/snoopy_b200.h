@@ -174,7 +174,11 @@ int snp_curlcurl_rows(const snp_pattern *pat, const double *terms, int32_t parts
  * Replaces fem_c.compute_stiffness_and_jacobi_matrix (fem_c/interface_c.pyx:11-160)
  * -> compute_K_dK (fem_c/ctools.c:730-919).  P1 nodal elements [elem_offset, +n_elems)
  * of a pattern built with dofs_per_elem = 4 over `cells`.  Outputs may be NULL, accumulated:
- * K_vals, dK_vals, J_vals = K + dK (all [nnz]). */
+ * K_vals, dK_vals, J_vals = K + dK (all [nnz]).  Each CSR entry gets one addition per call, the
+ * sum of its contributions from these elements in element order, so repeated calls give bitwise
+ * the same values (SNP_ASSEMBLY=atomic: float64 atomics per contribution instead).  The call
+ * keeps its element values in a work array of the pattern: calls on one pattern must not
+ * overlap on the GPU. */
 int snp_gradgrad_assemble(const snp_pattern *pat, int64_t elem_offset, int64_t n_elems,
                           const double *nodes, const int32_t *cells, const double *d_phi,
                           const double *w, int32_t n_quad, const double *x,

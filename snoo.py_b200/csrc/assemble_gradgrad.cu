@@ -8,6 +8,16 @@
 //   dK_ab = sum_q [|H| >= 1e-14] mu' det w_q (g_a . H)(g_b . H) / |H|
 // For linear tetrahedra the gradients are constant per element, so mu is evaluated once
 // and the sums over q factor through sum_q w_q.
+//
+// By default the values are added deterministically: the element kernel stores each element's
+// 10 upper-triangle values of K and of dK, then one thread per CSR entry adds the sum of the
+// entry's couplings from this call's elements, taken in element order from the pattern's sorted
+// coupling list, to K, dK and J (one add per entry and call, so the result does not depend on
+// the launch).  SNP_ASSEMBLY=atomic, or a pattern without coupling lists, adds each element's
+// contributions with float64 atomics instead.
+#include <cstdlib>
+#include <cstring>
+
 #include "snp_common.cuh"
 #include "snp_internal.cuh"
 
@@ -30,7 +40,15 @@ struct GradArgs {
     double H_min, mu_H_min;
     const int32_t *slots;
     double *K, *dK, *J;
+    double *ET;        // store mode: element values, K block [10][et_stride] then dK block
+    int64_t et_stride;
 };
+
+// upper-triangle index of the element pair (a, b), 4 nodes: row min, column max, row by row
+__host__ __device__ __forceinline__ int tri4(int a, int b) {
+    const int j = a < b ? a : b, k = a < b ? b : a;
+    return j * 4 - (j * (j - 1)) / 2 + (k - j);
+}
 
 __global__ void __launch_bounds__(kBlock) k_gradgrad(GradArgs a) {
     extern __shared__ double sm[];
@@ -108,6 +126,11 @@ __global__ void __launch_bounds__(kBlock) k_gradgrad(GradArgs a) {
             for (int k = i; k < 4; ++k) {
                 const double kv = kf * (gphi[i][0] * gphi[k][0] + gphi[i][1] * gphi[k][1] + gphi[i][2] * gphi[k][2]);
                 const double dv = df * p[i] * p[k];
+                if (a.ET) {
+                    a.ET[(int64_t)tri4(i, k) * a.et_stride + e] = kv;
+                    a.ET[(int64_t)(10 + tri4(i, k)) * a.et_stride + e] = dv;
+                    continue;
+                }
                 const int s1 = __ldg(sl + 4 * i + k);
                 if (a.K) atomicAdd(a.K + s1, kv);
                 if (a.dK) atomicAdd(a.dK + s1, dv);
@@ -120,6 +143,33 @@ __global__ void __launch_bounds__(kBlock) k_gradgrad(GradArgs a) {
                 }
             }
         }
+    }
+}
+
+// K_p += sum, over the couplings t = e * 16 + a * 4 + b of CSR entry p whose element lies in
+// [e_lo, e_lo + n), in element order, of the stored K value of (e, a, b); dK likewise; J gets the
+// two sums added.  Entries without such a coupling are left alone.
+__global__ void __launch_bounds__(256)
+    k_gg_entries(int64_t nnz, const int32_t *__restrict__ cptr, const int32_t *__restrict__ cid,
+                 const double *__restrict__ ET, int64_t stride, int64_t e_lo, int64_t n, double *K, double *dK,
+                 double *J) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x) {
+        double s0 = 0.0, s1 = 0.0;
+        int cnt = 0;
+        for (int c = __ldg(cptr + p); c < __ldg(cptr + p + 1); ++c) {
+            const uint32_t t = (uint32_t)__ldg(cid + c);
+            const int64_t e = (int64_t)(t >> 4) - e_lo;
+            if (e < 0 || e >= n) continue;
+            const int ab = (int)(t & 15u);
+            const int q = tri4(ab >> 2, ab & 3);
+            s0 += __ldg(ET + (int64_t)q * stride + e);
+            s1 += __ldg(ET + (int64_t)(10 + q) * stride + e);
+            ++cnt;
+        }
+        if (cnt == 0) continue;
+        if (K) K[p] += s0;
+        if (dK) dK[p] += s1;
+        if (J) J[p] += s0 + s1;
     }
 }
 
@@ -169,7 +219,20 @@ extern "C" int snp_gradgrad_assemble(const snp_pattern *pat, int64_t elem_offset
     if (smem > 48 * 1024)
         SNP_CUDA_TRY(cudaFuncSetAttribute(snp::k_gradgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaStream_t st = snp::as_stream(stream);
+    const char *env = getenv("SNP_ASSEMBLY");
+    const bool atomic = (env && std::strcmp(env, "atomic") == 0) || !pat->has_contrib;
+    if (!atomic) {
+        const size_t need = (size_t)20 * (size_t)n_elems;
+        if (pat->gg_terms.n < need) SNP_TRY(pat->gg_terms.alloc(need));
+        a.ET = pat->gg_terms.p;
+        a.et_stride = n_elems;
+    }
     snp::k_gradgrad<<<snp::stride_grid(n_elems, snp::kBlock, 16), snp::kBlock, smem, st>>>(a);
     SNP_LAUNCH_CHECK();
+    if (!atomic) {
+        snp::k_gg_entries<<<snp::stride_grid(pat->nnz, 256, 8), 256, 0, st>>>(
+            pat->nnz, pat->cptr.p, pat->cid.p, pat->gg_terms.p, n_elems, elem_offset, n_elems, K_vals, dK_vals, J_vals);
+        SNP_LAUNCH_CHECK();
+    }
     return SNP_OK;
 }

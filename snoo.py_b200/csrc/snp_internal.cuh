@@ -232,6 +232,9 @@ struct snp_pattern {
     snp::DevBuf<int32_t> inc_ptr, inc;
     int32_t max_row = 0;  // entries of the longest row
     bool has_incidence = false;
+    // work space of the deterministic grad-grad assembly (element values of one call); calls on
+    // one pattern are serialised by its users (one stream)
+    mutable snp::DevBuf<double> gg_terms;
 };
 
 namespace snp {

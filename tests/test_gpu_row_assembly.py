@@ -137,3 +137,32 @@ def test_solver_assembly_rows_vs_atomic():
     x2 = atomic.solve(1e-8)
     d = float(np.abs(x1 - x2).max() / np.abs(x2).max())
     assert d < 1e-6, d
+
+
+def test_gradgrad_assembly_is_repeatable_and_matches_atomic():
+    """Grad-grad (P1) assembly: each CSR entry gets the sum of the call's contributions in
+    element order, so two assemblies agree bit for bit; SNP_ASSEMBLY=atomic (float64 atomics per
+    contribution) agrees to rounding (1e-12 of the row's largest entry)."""
+    msh = M.window_frame_mesh(8000, jitter=0.1, seed=2, coils=True)
+    perm = MAT.atan_permeability()
+    tags = [M.TAG_COIL_1, M.TAG_IRON]
+    x = np.random.default_rng(3).normal(0, 30.0, msh.num_nodes)
+    mus = [S.ConstantPermeability(1.0), perm]
+
+    def run():
+        G = S.GradGradAssembler(msh, tags)
+        K, J = G.compute_stiffness_and_jacobi_matrix_c(x, mus, quad_order=2, device=True)
+        torch.cuda.synchronize()
+        return K.values().clone(), J.values().clone(), K.crow_indices()
+
+    K1, J1, rp = run()
+    K2, J2, _ = run()
+    assert torch.equal(K1, K2) and torch.equal(J1, J2)
+    os.environ["SNP_ASSEMBLY"] = "atomic"
+    try:
+        Ka, Ja, _ = run()
+    finally:
+        del os.environ["SNP_ASSEMBLY"]
+    assert _row_close(K1, Ka, rp) < 1e-12
+    assert _row_close(J1, Ja, rp) < 1e-12
+    assert K1.abs().max() > 0
