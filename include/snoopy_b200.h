@@ -528,8 +528,8 @@ int snp_solver_destroy(snp_solver *s);
  * coefficients of the converged edge-DoF vector.  None has a counterpart in the reference
  * (snoo.py has no surrogate); BF16 arrays are passed as raw 16-bit words. */
 
-/* POD reconstruction of the warm start (the surrogate's x = mean + U c, SURVEY N8's projection
- * GEMMs; the reference has no surrogate): out[p][i] = mean[i] + sum_c V[i][c] coef[p][c] for
+/* POD reconstruction of the warm start (the surrogate's x = mean + U c, the projection GEMM of
+ * the learned warm start; the reference has no surrogate): out[p][i] = mean[i] + sum_c V[i][c] coef[p][c] for
  * p < P (<= 32) vectors, V float32 [n][ldv] with m <= 128 columns, coef float64 [P][m] (device),
  * mean float64 [n] or NULL, out float64 [P][ldo].  float64 products and sums in a fixed order.
  * Asynchronous on the stream. */
