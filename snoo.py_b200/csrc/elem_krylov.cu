@@ -646,7 +646,12 @@ __global__ void __launch_bounds__(kEBlock)
                 DofPair<TT> *__restrict__ G, DofPair<TT> *__restrict__ R, PcgState *st, double *part, int use_cond,
                 cudaGraphConditionalHandle cond) {
     __shared__ double sh2[2][32];
-    __shared__ TT s_r[kBjTile];
+    // float64: r of the tile in two alternating buffers, so a tile needs one barrier: it writes
+    // the buffer its predecessor's predecessor read, which every thread has finished with once
+    // past the barrier in between (77.8 -> 77.0 us per iteration at 1.16M tets; in float32 the
+    // second barrier per tile measured slightly faster, 56.3 against 56.8 us, and stays)
+    constexpr bool kTwoBuffers = sizeof(TT) == 8;
+    __shared__ TT s_r2[2][kBjTile];
     // each tile's slot range is read one tile ahead (the first one before the CG state), so
     // that a tile's slot values are requested together with its DoF words
     // In float32 the tile's DoF states {z, p}, {r, x} are read one tile ahead as well (in float64
@@ -672,7 +677,9 @@ __global__ void __launch_bounds__(kEBlock)
     }
     const TT alpha = (TT)st->alpha, beta = (TT)st->beta;
     double rz = 0.0, rr = 0.0;
-    for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += tstride) {
+    int par = 0;
+    for (int64_t base = (int64_t)blockIdx.x * kBjTile; base < n; base += tstride, par ^= (kTwoBuffers ? 1 : 0)) {
+        TT *s_r = s_r2[par];
         const int64_t i = base + threadIdx.x;
         const bool fr = i < n && is_free(free_mask, i);
         const int b0 = nb0, b1 = nb1;
@@ -715,7 +722,7 @@ __global__ void __launch_bounds__(kEBlock)
             rz += (double)r * (double)z;
             rr += (double)r * (double)r;
         }
-        __syncthreads();
+        if constexpr (!kTwoBuffers) __syncthreads();
     }
     block_sum2(rz, rr, sh2);
     if (threadIdx.x == 0) {
